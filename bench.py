@@ -1,0 +1,312 @@
+#!/usr/bin/env python
+"""Benchmark of the hosono-2DMHD time-step path on B200.
+
+Metric: FP64 zone-updates/s -- interior cells x full RK3 time steps (every
+MOOD pass and the CFL reduction included) per second.  A step is one
+cfl_computedt + timeStep_advanceSolution on the resident state.
+
+Default workload: Orszag-Tang vortex 2048x2048, GP radius 2 (cascade 2->1->0),
+ell/Delta = 12, HLLC, SSP-RK3, CFL 0.8, FLICD on, periodic, FP64, synthetic
+initial state generated on the host.  The state (270 MB of U alone) is
+larger than the 126 MB L2, so no L2 flush is needed between steps.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Multi-GPU: the path is not partitioned (no domain decomposition exists in
+the reference); N ranks run N independent replicas of the workload
+("replicas only", weak scaling), value = all ranks' zone-updates / max time.
+
+--impl reference times the reference algorithm on the host cores: the CPU
+oracle restatement (the Fortran reference cannot be compiled here), with all
+host threads, same metric and workload; rank 0 only.
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "tests"))
+
+MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM_GBS = 6650.0
+
+WORKLOADS = {
+    "ot2048_r2": dict(n=2048, radius=2, ell=12.0, desc="Orszag-Tang 2048x2048, GP-MOOD R=2 (5th->3rd->1st), ell/dx=12"),
+    "ot1024_r2": dict(n=1024, radius=2, ell=12.0, desc="Orszag-Tang 1024x1024, GP-MOOD R=2 (5th->3rd->1st), ell/dx=12"),
+    "ot128_r1": dict(n=128, radius=1, ell=6.0, desc="Orszag-Tang 128x128, GP-MOOD R=1 (3rd->1st), ell/dx=6"),
+}
+
+
+def load_pkg():
+    import pkg
+    return pkg.load()
+
+
+def par_for(workload, d):
+    import parfiles
+    w = WORKLOADS[workload]
+    kv = parfiles.orszag_tang(w["n"], w["radius"], ell=w["ell"], tmax=0.5, cfl=0.8)
+    return parfiles.make(d, workload, kv)
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower() in ("active", "1", "yes"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def peaks():
+    try:
+        with open(MEASURED_PEAKS) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def pass1_bytes(n, radius):
+    """Algorithmic HBM bytes of one MOOD pass-1 kernel launch (n x n interior):
+    read U once over the interior plus NGC guard rings (8 doubles/cell), write
+    fluxRaw x/y (16 doubles) and the two corrected-B copies (2 doubles) on the
+    (n+3)^2 flux faces, and the per-face admissibility bytes (2 per cell)."""
+    ngc = radius + 2
+    cells_u = (n + 2 * ngc) ** 2
+    faces = (n + 3) ** 2
+    return cells_u * 8 * 8 + faces * 18 * 8 + (n + 5) ** 2 * 2
+
+
+def run_cpu_baseline(workload, steps, threads, fast=True):
+    """Time the oracle restatement on the host cores: returns (zone-updates/s, sample text)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    oracle.set_threads(threads, fast=fast)
+    w = WORKLOADS[workload]
+    with tempfile.TemporaryDirectory() as d:
+        par = par_for(workload, d)
+        o = oracle.Oracle(par, fast=fast)
+        dt = o.cfl()
+        o.advance(dt)  # warm-up step (page faults, thread pool)
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            dt = o.cfl()
+            o.advance(dt)
+        el = time.perf_counter() - t0
+        o.close()
+    rate = w["n"] * w["n"] * steps / el
+    return rate, el
+
+
+def bench_reference(args, rank):
+    """--impl reference: the reference algorithm on the host cores (rank 0 only)."""
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    w = WORKLOADS[args.workload]
+    # bounded sample: at most ~120 s of CPU time whatever --steps says
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    rate1, el1 = run_cpu_baseline(args.workload, 1, threads)
+    steps = max(1, min(args.steps, int(120.0 / max(el1, 1e-3))))
+    rate, el = run_cpu_baseline(args.workload, steps, threads) if steps > 1 else (rate1, el1)
+    line = {
+        "metric": "fp64_zone_updates_per_s", "value": rate, "unit": "zone-updates/s", "n_gpus": args.gpus,
+        "steps": steps, "warmup": 1, "ms_per_step": el / steps * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": args.workload, "desc": w["desc"], "fp": "fma (release-like)"},
+        "impl": "reference",
+        "cpu_baseline": {"value": rate, "unit": "zone-updates/s", "cores": threads, "kind": "port",
+                         "sample": f"{steps} full RK3 steps of {args.workload} after 1 warm-up step, "
+                                   f"CPU oracle (C++ restatement of the Fortran, OpenMP, -O3 AVX2/FMA)"},
+        "e2e": {"value": rate, "unit": "zone-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def bench_ours(args, rank, world, local):
+    import numpy as np
+    import torch
+
+    m = load_pkg()
+    torch.cuda.set_device(local)
+    m.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    w = WORKLOADS[args.workload]
+    fp = m.FP_FAST if args.fp == "fast" else m.FP_STRICT
+    with tempfile.TemporaryDirectory() as d:
+        par = par_for(args.workload, d)
+        params, run = m.par_load(par)
+        params.fp_mode = fp
+        pv, qw, st = m.par_gp(par, params.max_radius)
+        U0, V0 = m.ic_set(par, params)
+    sol = m.Solver(params, pv, qw, st)
+    sol.upload(U0, V0)
+    stream = torch.cuda.ExternalStream(sol.stream())
+    zones = w["n"] * w["n"]
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # warm-up
+    for _ in range(args.warmup):
+        sol.timeStep_advanceSolution(sol.cfl_computedt())
+    barrier()
+    sol.profile(True)
+    sol.profile_read(reset=True)
+    clocks = ClockSampler(local)
+    clocks.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    passes = 0
+    for _ in range(args.steps):
+        sol.timeStep_advanceSolution(sol.cfl_computedt())
+        passes += sol.stats()["mood_passes"]
+    e1.record(stream)
+    e1.synchronize()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    p1_ms, p1_n, launches = sol.profile_read(reset=True)
+    sol.profile(False)
+    barrier()
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * zones * args.steps / (ms / 1e3)
+
+    # end to end through the C ABI with host buffers: upload U,V from pinned
+    # memory, cfl, advance, download U,V -- every step
+    Uh = torch.from_numpy(np.ascontiguousarray(U0)).pin_memory().numpy()
+    Vh = torch.from_numpy(np.ascontiguousarray(V0)).pin_memory().numpy()
+    e2e_steps = max(1, min(args.steps, 5))
+    barrier()
+    f0 = torch.cuda.Event(enable_timing=True)
+    f1 = torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    for _ in range(e2e_steps):
+        sol.upload(Uh, Vh)
+        sol.timeStep_advanceSolution(sol.cfl_computedt())
+        sol.download(Uh, Vh, with_scheme=False)
+    f1.record(stream)
+    f1.synchronize()
+    e2e_ms = f0.elapsed_time(f1)
+    if dist is not None:
+        t = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    barrier()
+    e2e = {"value": world * zones * e2e_steps / (e2e_ms / 1e3), "unit": "zone-updates/s",
+           "h2d_bytes_per_step": U0.nbytes + V0.nbytes, "d2h_bytes_per_step": U0.nbytes + V0.nbytes,
+           "steps": e2e_steps, "ms_per_step": e2e_ms / e2e_steps}
+    sol.close()
+
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+    hbm, hbm_kind = peaks()
+    p1_avg = p1_ms / max(p1_n, 1)
+    bytes1 = pass1_bytes(w["n"], w["radius"])
+    achieved = bytes1 / (p1_avg / 1e3) / 1e9
+    roofline = {"bound": "hbm", "kernel": "k_face_pass1", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                "frac": achieved / hbm, "traffic": None, "peak_kind": hbm_kind,
+                "kernel_ms": p1_avg, "kernel_launches": p1_n,
+                "note": "FP64 CUDA-core kernel; HBM line shown as the contract requires"}
+    line = {
+        "metric": "fp64_zone_updates_per_s", "value": value, "unit": "zone-updates/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": args.workload, "desc": w["desc"], "fp": args.fp, "parallelism": f"replicas{world}",
+                   "l2": "inputs larger than L2 (U alone 270 MB at 2048^2)", "mood_passes": passes},
+        "gpu_launches": launches, "clocks": clk, "roofline": roofline, "e2e": e2e,
+    }
+    if not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        rate, el = run_cpu_baseline(args.workload, 1, threads)
+        line["cpu_baseline"] = {"value": rate, "unit": "zone-updates/s", "cores": threads, "kind": "port",
+                                "sample": f"1 full RK3 step of {args.workload} after 1 warm-up step, CPU oracle "
+                                          f"(C++ restatement, OpenMP, -O3 AVX2/FMA), {el:.1f} s"}
+    print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="ot2048_r2", choices=sorted(WORKLOADS))
+    ap.add_argument("--fp", default="strict", choices=["strict", "fast"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        bench_reference(args, rank)
+    else:
+        bench_ours(args, rank, world, local)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,333 @@
+"""hosono-2DMHD time-step path on B200: Python binding of libhosono_gpu.so.
+
+The native library (include/hosono_gpu.h) replaces the reference's
+``cfl_computedt`` (src/cfl.f90:14-52) and ``timeStep_advanceSolution``
+(src/timeStep.f90:22-43) with FP64 CUDA kernels for sm_100a.  This module
+is a thin ctypes layer over that C ABI; the compute path is the native one
+only, and every entry point raises if the library or a GPU is missing.
+
+Host arrays use the reference's layout, shaped (nyTot, nxTot, nvar) in numpy
+(Fortran ``U(var, i, j)`` with var fastest), guard cells included.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+PKG_DIR = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG_DIR, "libhosono_gpu.so")
+
+OK, EINVAL, ENOMEM, ECUDA, ENANDT, EMOODCAP, ETIMEOUT, EPAR, ENOTBUILT = range(9)
+BC_OUTFLOW, BC_PERIODIC = 0, 1
+FP_STRICT, FP_FAST = 0, 1
+STATUS_NAMES = {OK: "OK", EINVAL: "EINVAL", ENOMEM: "ENOMEM", ECUDA: "ECUDA", ENANDT: "ENANDT",
+                EMOODCAP: "EMOODCAP", ETIMEOUT: "ETIMEOUT", EPAR: "EPAR", ENOTBUILT: "ENOTBUILT"}
+
+
+class HosonoError(RuntimeError):
+    def __init__(self, code, msg=""):
+        super().__init__(f"{STATUS_NAMES.get(code, code)}: {msg}")
+        self.code = code
+
+
+class Params(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("ngc", ctypes.c_int), ("max_radius", ctypes.c_int),
+                ("bc", ctypes.c_int), ("force_hydro", ctypes.c_int), ("riemann_solver", ctypes.c_int),
+                ("fp_mode", ctypes.c_int), ("dx", ctypes.c_double), ("dy", ctypes.c_double),
+                ("mindxdy", ctypes.c_double), ("maxdxdy", ctypes.c_double), ("gamma", ctypes.c_double),
+                ("small_pressure", ctypes.c_double), ("small_density", ctypes.c_double),
+                ("small_energy", ctypes.c_double), ("small_b", ctypes.c_double), ("cfl", ctypes.c_double)]
+
+
+class RunInfo(ctypes.Structure):
+    _fields_ = [("tmax", ctypes.c_double), ("nstepmax", ctypes.c_int), ("output_freq_step", ctypes.c_int),
+                ("output_freq_time", ctypes.c_double), ("ell_over_delta", ctypes.c_double),
+                ("x_beg", ctypes.c_double), ("x_end", ctypes.c_double), ("y_beg", ctypes.c_double),
+                ("y_end", ctypes.c_double), ("nx_tot", ctypes.c_int), ("ny_tot", ctypes.c_int),
+                ("ic_type", ctypes.c_char * 32), ("data_file_base", ctypes.c_char * 256)]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [("stages", ctypes.c_int), ("mood_passes", ctypes.c_int), ("max_passes", ctypes.c_int),
+                ("detect_lowered", ctypes.c_longlong), ("inner_lowered", ctypes.c_longlong),
+                ("cascade_iters", ctypes.c_int)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+# Every symbol the C ABI exports (include/hosono_gpu.h), with its signature.
+_dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int)
+_vp = ctypes.c_void_p
+_cp = ctypes.c_char_p
+_i = ctypes.c_int
+_d = ctypes.c_double
+SIGNATURES = {
+    "hosono_gp_build": [_i, _cp, _cp, _i, _cp, _cp, _i, _cp, _dp, _dp, _ip],
+    "hosono_par_load": [_cp, ctypes.POINTER(Params), ctypes.POINTER(RunInfo), _cp, _i],
+    "hosono_par_gp": [_cp, _dp, _dp, _ip, _cp, _i],
+    "hosono_ic_set": [_cp, ctypes.POINTER(Params), _dp, _dp, _cp, _i],
+    "hosono_gpu_create": [ctypes.POINTER(Params), _dp, _dp, _ip, ctypes.POINTER(_vp)],
+    "hosono_gpu_destroy": [_vp],
+    "hosono_gpu_upload": [_vp, _dp, _dp],
+    "hosono_gpu_download": [_vp, _dp, _dp, _ip],
+    "hosono_gpu_cfl": [_vp, _dp],
+    "hosono_gpu_advance": [_vp, _d],
+    "hosono_gpu_run": [_vp, _d, _i, _i, _dp, _ip],
+    "hosono_gpu_advance_host": [_vp, _d, _dp, _dp],
+    "hosono_gpu_stats": [_vp, ctypes.POINTER(Stats)],
+    "hosono_gpu_last_error": [_vp, _cp, _i],
+    "hosono_gpu_trace_enable": [_vp, _i],
+    "hosono_gpu_trace_count": [_vp],
+    "hosono_gpu_trace_get": [_vp, _i, _ip, _vp, _vp],
+    "hosono_gpu_trace_clear": [_vp],
+    "hosono_gpu_state_layout": [_vp, ctypes.POINTER(_vp), _ip, ctypes.POINTER(ctypes.c_longlong)],
+    "hosono_gpu_build_info": [_ip, _ip],
+    "hosono_gpu_set_device": [_i],
+    "hosono_gpu_stream": [_vp, ctypes.POINTER(_vp)],
+    "hosono_gpu_profile": [_vp, _i],
+    "hosono_gpu_profile_read": [_vp, _dp, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong), _i],
+}
+
+
+def set_device(device):
+    """Select the CUDA device the library creates its next handles on."""
+    rc = load_library().hosono_gpu_set_device(int(device))
+    if rc:
+        raise HosonoError(rc, f"cudaSetDevice({device})")
+
+_lib = None
+
+
+def load_library(path=LIB_PATH):
+    """Load libhosono_gpu.so; raise if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise HosonoError(ENOTBUILT, f"{path} is missing; run __graft_entry__.build() or "
+                                     f"python hosono-2dmhd_b200/build.py")
+    lib = ctypes.CDLL(path)
+    for name, args in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = ctypes.c_int
+    _lib = lib
+    return lib
+
+
+def build(verbose=False, force=False):
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("hosono_build", os.path.join(PKG_DIR, "build.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod.build(verbose=verbose, force=force)
+
+
+def _p(a, t=ctypes.c_double):
+    return a.ctypes.data_as(ctypes.POINTER(t))
+
+
+def gp_build(radius, x_beg, x_end, nx, y_beg, y_end, ny, ell_over_delta):
+    """GP_init: (pv, qw, stenc) in Fortran order from .par strings."""
+    lib = load_library()
+    ns, nq = 1 + 2 * radius * (radius + 1), radius + 1
+    pv = np.zeros(ns * nq * 4 * radius)
+    qw = np.zeros(nq * radius)
+    st = np.zeros(2 * ns * radius, dtype=np.int32)
+    rc = lib.hosono_gp_build(radius, str(x_beg).encode(), str(x_end).encode(), nx, str(y_beg).encode(),
+                             str(y_end).encode(), ny, str(ell_over_delta).encode(), _p(pv), _p(qw),
+                             _p(st, ctypes.c_int))
+    if rc:
+        raise HosonoError(rc, "hosono_gp_build")
+    return pv, qw, st
+
+
+def par_load(parfile):
+    """simulation_init + grid_init: (Params, RunInfo) from a .par file."""
+    lib = load_library()
+    p, r = Params(), RunInfo()
+    err = ctypes.create_string_buffer(512)
+    rc = lib.hosono_par_load(os.fsencode(parfile), ctypes.byref(p), ctypes.byref(r), err, 512)
+    if rc:
+        raise HosonoError(rc, err.value.decode())
+    return p, r
+
+
+def par_gp(parfile, radius):
+    lib = load_library()
+    ns, nq = 1 + 2 * radius * (radius + 1), radius + 1
+    pv = np.zeros(ns * nq * 4 * radius)
+    qw = np.zeros(nq * radius)
+    st = np.zeros(2 * ns * radius, dtype=np.int32)
+    err = ctypes.create_string_buffer(512)
+    rc = lib.hosono_par_gp(os.fsencode(parfile), _p(pv), _p(qw), _p(st, ctypes.c_int), err, 512)
+    if rc:
+        raise HosonoError(rc, err.value.decode())
+    return pv, qw, st
+
+
+def ic_set(parfile, params):
+    """initialCondition_set: (U, V) host arrays shaped (nyTot, nxTot, 8|10)."""
+    lib = load_library()
+    nxt, nyt = params.nx + 2 * params.ngc, params.ny + 2 * params.ngc
+    U = np.zeros((nyt, nxt, 8))
+    V = np.zeros((nyt, nxt, 10))
+    err = ctypes.create_string_buffer(512)
+    rc = lib.hosono_ic_set(os.fsencode(parfile), ctypes.byref(params), _p(U), _p(V), err, 512)
+    if rc:
+        raise HosonoError(rc, err.value.decode())
+    return U, V
+
+
+class Solver:
+    """One block advanced on the GPU (gridBlock_t + gridState_t resident in HBM)."""
+
+    def __init__(self, params, pv, qw, stenc):
+        self.lib = load_library()
+        self.params = params
+        self.nxt = params.nx + 2 * params.ngc
+        self.nyt = params.ny + 2 * params.ngc
+        self._pv = np.ascontiguousarray(pv, dtype=np.float64)
+        self._qw = np.ascontiguousarray(qw, dtype=np.float64)
+        self._st = np.ascontiguousarray(stenc, dtype=np.int32)
+        h = ctypes.c_void_p()
+        rc = self.lib.hosono_gpu_create(ctypes.byref(params), _p(self._pv), _p(self._qw),
+                                        _p(self._st, ctypes.c_int), ctypes.byref(h))
+        if rc:
+            raise HosonoError(rc, "hosono_gpu_create")
+        self.h = h
+
+    @classmethod
+    def from_par(cls, parfile, fp_mode=FP_STRICT):
+        """simulation_init + GP_init + grid_init + initialCondition_set, then upload."""
+        p, run = par_load(parfile)
+        p.fp_mode = fp_mode
+        pv, qw, st = par_gp(parfile, p.max_radius)
+        s = cls(p, pv, qw, st)
+        s.run_info = run
+        U, V = ic_set(parfile, p)
+        s.upload(U, V)
+        return s
+
+    def _check(self, rc, what):
+        if rc:
+            buf = ctypes.create_string_buffer(512)
+            self.lib.hosono_gpu_last_error(self.h, buf, 512)
+            raise HosonoError(rc, f"{what}: {buf.value.decode()}")
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.hosono_gpu_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def upload(self, U, V=None):
+        U = np.ascontiguousarray(U, dtype=np.float64)
+        assert U.size == self.nxt * self.nyt * 8
+        Vp = None
+        if V is not None:
+            V = np.ascontiguousarray(V, dtype=np.float64)
+            assert V.size == self.nxt * self.nyt * 10
+            Vp = _p(V)
+        self._check(self.lib.hosono_gpu_upload(self.h, _p(U), Vp), "upload")
+
+    def download(self, U=None, V=None, with_scheme=True):
+        """(U, V, scheme); pass U/V (C-contiguous float64) to fill them in place."""
+        U = np.zeros((self.nyt, self.nxt, 8)) if U is None else U
+        V = np.zeros((self.nyt, self.nxt, 10)) if V is None else V
+        assert U.flags.c_contiguous and V.flags.c_contiguous
+        S = np.zeros((self.nyt, self.nxt), dtype=np.int32) if with_scheme else None
+        self._check(self.lib.hosono_gpu_download(self.h, _p(U), _p(V), _p(S, ctypes.c_int) if with_scheme else None),
+                    "download")
+        return U, V, S
+
+    def cfl_computedt(self):
+        dt = ctypes.c_double()
+        self._check(self.lib.hosono_gpu_cfl(self.h, ctypes.byref(dt)), "cfl")
+        return dt.value
+
+    def timeStep_advanceSolution(self, dt):
+        self._check(self.lib.hosono_gpu_advance(self.h, float(dt)), "advance")
+
+    def advance_host(self, dt, U, V=None):
+        """Drop-in on host arrays: U (and V) in, advanced U (and V) out, in place."""
+        assert U.flags.c_contiguous and U.dtype == np.float64
+        self._check(self.lib.hosono_gpu_advance_host(self.h, float(dt), _p(U), _p(V) if V is not None else None),
+                    "advance_host")
+
+    def run(self, tmax=None, nstepmax=None, max_steps=0):
+        """mhd_driver's time loop (no output)."""
+        ri = getattr(self, "run_info", None)
+        tmax = ri.tmax if tmax is None else tmax
+        nstepmax = (ri.nstepmax if ri is not None else 1 << 30) if nstepmax is None else nstepmax
+        t = ctypes.c_double()
+        n = ctypes.c_int()
+        self._check(self.lib.hosono_gpu_run(self.h, float(tmax), int(nstepmax), int(max_steps), ctypes.byref(t),
+                                            ctypes.byref(n)), "run")
+        return t.value, n.value
+
+    def stats(self):
+        s = Stats()
+        self._check(self.lib.hosono_gpu_stats(self.h, ctypes.byref(s)), "stats")
+        return s.as_dict()
+
+    def trace(self, on=True):
+        self._check(self.lib.hosono_gpu_trace_enable(self.h, 1 if on else 0), "trace")
+
+    def trace_clear(self):
+        self._check(self.lib.hosono_gpu_trace_clear(self.h), "trace_clear")
+
+    def traces(self, masks=True):
+        out = []
+        n = self.nxt * self.nyt
+        for k in range(self.lib.hosono_gpu_trace_count(self.h)):
+            meta = np.zeros(4, dtype=np.int32)
+            inner = np.zeros(n, dtype=np.uint8)
+            det = np.zeros(n, dtype=np.uint8)
+            self._check(self.lib.hosono_gpu_trace_get(self.h, k, _p(meta, ctypes.c_int), inner.ctypes.data,
+                                                      det.ctypes.data), "trace_get")
+            rec = dict(stage=int(meta[0]), mood_pass=int(meta[1]), n_inner=int(meta[2]), n_detect=int(meta[3]))
+            if masks:
+                rec["inner"] = inner.reshape(self.nyt, self.nxt)
+                rec["detect"] = det.reshape(self.nyt, self.nxt)
+            out.append(rec)
+        return out
+
+    def stream(self):
+        """cudaStream_t (as an int) all of this solver's kernels run on."""
+        s = ctypes.c_void_p()
+        self._check(self.lib.hosono_gpu_stream(self.h, ctypes.byref(s)), "stream")
+        return s.value or 0
+
+    def profile(self, on=True):
+        self._check(self.lib.hosono_gpu_profile(self.h, 1 if on else 0), "profile")
+
+    def profile_read(self, reset=True):
+        """(pass-1 kernel ms summed, pass-1 launches, all launches) since the last reset."""
+        ms = ctypes.c_double()
+        n1 = ctypes.c_longlong()
+        n = ctypes.c_longlong()
+        self._check(self.lib.hosono_gpu_profile_read(self.h, ctypes.byref(ms), ctypes.byref(n1), ctypes.byref(n),
+                                                     1 if reset else 0), "profile_read")
+        return ms.value, n1.value, n.value
+
+    def state_layout(self):
+        ptr = ctypes.c_void_p()
+        pitch = ctypes.c_int()
+        plane = ctypes.c_longlong()
+        self._check(self.lib.hosono_gpu_state_layout(self.h, ctypes.byref(ptr), ctypes.byref(pitch),
+                                                     ctypes.byref(plane)), "state_layout")
+        return ptr.value, pitch.value, plane.value

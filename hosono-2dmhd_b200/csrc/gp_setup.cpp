@@ -1,0 +1,194 @@
+// gp_setup.cpp -- GP prediction vectors on the host, in quad precision
+// (GP_init, src/GP.f90:37-200, with the SPD solve of
+// src/linAlgQuadPrecision.f90:107-365).  Built once per (radius, ell/Delta,
+// dx, dy) and uploaded; the per-cell work never touches quad precision.
+//
+// Every quad operation is one correctly rounded libquadmath/soft-float
+// operation in the order the Fortran statement evaluates it, and the final
+// vectors are rounded to FP64 exactly once, so the tables equal the
+// reference's GP_predictionVectors bit for bit whenever erfq/expq agree.
+
+#include "hosono_gpu.h"
+
+#include <quadmath.h>
+
+#include <cmath>
+#include <cstdlib>
+#include <string>
+#include <vector>
+
+namespace {
+
+using quad = __float128;
+
+quad quad_from_text(const char* s) {
+    std::string t(s ? s : "0");
+    for (char& c : t)
+        if (c == 'd' || c == 'D') c = 'e';  // Fortran exponent letter
+    return strtoflt128(t.c_str(), nullptr);
+}
+
+// Square-exponential covariance of two cell averages (GP.f90:216-280).
+struct SqExpKernel {
+    quad dl[2];
+    quad ell;
+    quad rt2ell, twoEll2, rtpiEll2, rtpi, rtHalfPi;
+
+    SqExpKernel(quad dx, quad dy, quad ell_) : ell(ell_) {
+        dl[0] = dx;
+        dl[1] = dy;
+        rt2ell = sqrtq((quad)2) * ell;
+        twoEll2 = (quad)2 * (ell * ell);
+        rtpi = sqrtq(M_PIq);
+        rtpiEll2 = rtpi * (ell * ell);
+        rtHalfPi = sqrtq(M_PIq / (quad)2);
+    }
+
+    quad avg_avg(const quad* a, const quad* b) const {
+        quad k = (quad)1;
+        for (int d = 0; d < 2; d++) {
+            const quad sep = a[d] - b[d];
+            const quad sp = sep + dl[d], sm = sep - dl[d];
+            const quad r1 = sp / rt2ell, r2 = sm / rt2ell, r5 = sep / rt2ell;
+            const quad e3 = expq(-((sp * sp) / twoEll2));
+            const quad e4 = expq(-((sm * sm) / twoEll2));
+            const quad e6 = expq(-((sep * sep) / twoEll2));
+            const quad t = ((r1 * erfq(r1) + r2 * erfq(r2)) + (e3 + e4) / rtpi) - (quad)2 * (r5 * erfq(r5) + e6 / rtpi);
+            k = ((k * rtpiEll2) / (dl[d] * dl[d])) * t;
+        }
+        return k;
+    }
+
+    // covariance of a cell average with a point value (GP.f90:282-335)
+    quad avg_point(const quad* a, const quad* x) const {
+        quad k = (quad)1;
+        for (int d = 0; d < 2; d++) {
+            const quad half = dl[d] / (quad)2;
+            const quad sep = a[d] - x[d];
+            k = ((k * rtHalfPi) * (ell / dl[d])) * (erfq((sep + half) / rt2ell) - erfq((sep - half) / rt2ell));
+        }
+        return k;
+    }
+};
+
+// A x = B for SPD A (m x m) and B (m x n), row-major; Cholesky A = R^T R,
+// then R^T y = B and R x = y (linAlgQuadPrecision.f90:107-235, :336-365).
+bool spd_solve(int m, int n, std::vector<quad> A, const std::vector<quad>& B, std::vector<quad>& X) {
+    for (int r = 1; r < m; r++)
+        for (int c = 0; c < r; c++) A[r * m + c] = 0;
+    for (int k = 0; k < m; k++) {
+        const quad piv = A[k * m + k];
+        if (!(piv > 0)) return false;
+        for (int r = k + 1; r < m; r++) {
+            const quad akr = A[k * m + r];
+            for (int c = r; c < m; c++) A[r * m + c] = A[r * m + c] - (A[k * m + c] * akr) / piv;
+        }
+        const quad root = sqrtq(piv);
+        for (int c = k; c < m; c++) A[k * m + c] = A[k * m + c] / root;
+    }
+    std::vector<quad> Y((size_t)m * n), acc(n);
+    for (int c = 0; c < n; c++) Y[c] = B[c] / A[0];
+    for (int r = 1; r < m; r++) {
+        for (int c = 0; c < n; c++) acc[c] = 0;
+        for (int k = 0; k < r; k++)
+            for (int c = 0; c < n; c++) acc[c] = acc[c] + A[k * m + r] * Y[k * n + c];
+        for (int c = 0; c < n; c++) Y[r * n + c] = (B[r * n + c] - acc[c]) / A[r * m + r];
+    }
+    X.assign((size_t)m * n, 0);
+    for (int c = 0; c < n; c++) X[(m - 1) * n + c] = Y[(m - 1) * n + c] / A[(m - 1) * m + (m - 1)];
+    for (int r = m - 2; r >= 0; r--) {
+        for (int c = 0; c < n; c++) acc[c] = 0;
+        for (int k = r + 1; k < m; k++)
+            for (int c = 0; c < n; c++) acc[c] = acc[c] + A[r * m + k] * X[k * n + c];
+        for (int c = 0; c < n; c++) X[r * n + c] = (Y[r * n + c] - acc[c]) / A[r * m + r];
+    }
+    return true;
+}
+
+// Gauss-Legendre nodes on [-1/2, 1/2] (quad) and weights (FP64), GP.f90:119-148
+void quadrature(int rr, std::vector<quad>& x, double* w) {
+    const quad half = (quad)1 / (quad)2;
+    if (rr == 1) {
+        x = {half / sqrtq((quad)3)};
+        x.push_back(-x[0]);
+        w[0] = 1.0 / 2.0;
+        w[1] = w[0];
+    } else if (rr == 2) {
+        const quad a = half * sqrtq((quad)3 / (quad)5);
+        x = {a, (quad)0, -a};
+        w[0] = 5.0 / 18.0;
+        w[1] = 8.0 / 18.0;
+        w[2] = w[0];
+    } else {
+        const quad s = (quad)2 / (quad)7 * sqrtq((quad)6 / (quad)5);
+        const quad a = half * sqrtq((quad)3 / (quad)7 + s), b = half * sqrtq((quad)3 / (quad)7 - s);
+        x = {a, b, -b, -a};
+        w[0] = (18.0 - std::sqrt(30.0)) / 72.0;
+        w[1] = (18.0 + std::sqrt(30.0)) / 72.0;
+        w[2] = w[1];
+        w[3] = w[0];
+    }
+}
+
+}  // namespace
+
+extern "C" int hosono_gp_build(int R, const char* x_beg, const char* x_end, int nx, const char* y_beg,
+                               const char* y_end, int ny, const char* ell_over_delta, double* pv, double* qw,
+                               int* stenc) {
+    if (R < 1 || R > 3 || nx < 1 || ny < 1 || !pv || !qw || !stenc) return HOSONO_EINVAL;
+    const quad dx = (quad_from_text(x_end) - quad_from_text(x_beg)) / (quad)nx;
+    const quad dy = (quad_from_text(y_end) - quad_from_text(y_beg)) / (quad)ny;
+    const quad ell = quad_from_text(ell_over_delta) * (dx < dy ? dx : dy);
+    if (!(dx > 0) || !(dy > 0) || !(ell > 0)) return HOSONO_EINVAL;
+    const int nsMax = 1 + 2 * R * (R + 1), nqMax = R + 1;
+    const SqExpKernel K(dx, dy, ell);
+    for (size_t t = 0; t < (size_t)nsMax * nqMax * 4 * R; t++) pv[t] = 0.0;
+    for (size_t t = 0; t < (size_t)nqMax * R; t++) qw[t] = 0.0;
+    for (size_t t = 0; t < (size_t)2 * nsMax * R; t++) stenc[t] = 0;
+    for (int rr = 1; rr <= R; rr++) {
+        // stencil |i|+|j| <= rr, i outer (GP.f90:85-95); training inputs at cell centres
+        std::vector<quad> X;
+        int ns = 0;
+        for (int a = -rr; a <= rr; a++)
+            for (int b = -rr; b <= rr; b++)
+                if (std::abs(a) + std::abs(b) <= rr) {
+                    stenc[0 + 2 * (ns + nsMax * (rr - 1))] = a;
+                    stenc[1 + 2 * (ns + nsMax * (rr - 1))] = b;
+                    X.push_back((quad)a * dx);
+                    X.push_back((quad)b * dy);
+                    ns++;
+                }
+        std::vector<quad> xq;
+        quadrature(rr, xq, qw + nqMax * (rr - 1));
+        const int nq = rr + 1, np = 4 * nq;
+        // prediction points: north, south, east, west faces (GP.f90:155-165)
+        std::vector<quad> P;
+        for (int f = 0; f < 4; f++)
+            for (int q = 0; q < nq; q++) {
+                quad px, py;
+                if (f == 0) { px = xq[q] * dx; py = dy / (quad)2; }
+                else if (f == 1) { px = xq[q] * dx; py = -(dy / (quad)2); }
+                else if (f == 2) { px = dx / (quad)2; py = xq[q] * dy; }
+                else { px = -(dx / (quad)2); py = xq[q] * dy; }
+                P.push_back(px);
+                P.push_back(py);
+            }
+        std::vector<quad> Kcov((size_t)ns * ns), Kstr((size_t)ns * np), W;
+        for (int r = 0; r < ns; r++)
+            for (int c = 0; c < ns; c++) Kcov[r * ns + c] = K.avg_avg(&X[2 * r], &X[2 * c]);
+        for (int r = 0; r < ns; r++)
+            for (int c = 0; c < np; c++) Kstr[r * np + c] = K.avg_point(&X[2 * r], &P[2 * c]);
+        if (!spd_solve(ns, np, Kcov, Kstr, W)) return HOSONO_EINVAL;
+        // unit 1-norm per vector (GP.f90:171-173), then one rounding to FP64
+        for (int c = 0; c < np; c++) {
+            quad sum = 0;
+            for (int r = 0; r < ns; r++) sum = sum + W[r * np + c];
+            for (int r = 0; r < ns; r++) W[r * np + c] = W[r * np + c] / sum;
+        }
+        for (int f = 0; f < 4; f++)
+            for (int q = 0; q < nq; q++)
+                for (int k = 0; k < ns; k++)
+                    pv[k + nsMax * (q + nqMax * (f + 4 * (rr - 1)))] = (double)W[k * np + f * nq + q];
+    }
+    return HOSONO_OK;
+}

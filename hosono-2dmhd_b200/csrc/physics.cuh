@@ -1,0 +1,208 @@
+// physics.cuh -- pointwise ideal-MHD physics on the device (FP64).
+//
+// Each function keeps the operation order of the reference Fortran routine
+// it cites, so that a build without FMA contraction (--fmad=false) rounds
+// exactly like the reference's arithmetic statement by statement.  Fortran
+// MAX/MIN become fmax/fmin (the non-NaN argument wins).
+#pragma once
+
+#include <cstdint>
+
+namespace hosono {
+
+// variable indices, src/definitions.f90:18-35 (0-based)
+enum : int { DENS = 0, MOMX = 1, MOMY = 2, MOMZ = 3, ENER = 4, MAGX = 5, MAGY = 6, MAGZ = 7 };
+enum : int { VELX = 1, VELY = 2, VELZ = 3, PRES = 4, EINT = 8, GAMM = 9 };
+enum : int { XDIR = 0, YDIR = 1 };
+enum : int { NORTH = 0, SOUTH = 1, EAST = 2, WEST = 3 };
+constexpr int NCONS = 8;
+constexpr int NPRIM = 10;
+
+struct Phys {
+    double gamma;
+    double small_pressure;
+    double small_density;
+    int force_hydro;
+};
+
+// src/eos.f90:9-26 (pressure floor)
+__device__ __forceinline__ double eos_pres(const Phys& s, double dens, double eint) {
+    double pres = (s.gamma - 1.0) * dens * eint;
+    if (pres < s.small_pressure) pres = s.small_pressure;
+    return pres;
+}
+
+// src/convert.f90:198-234
+__device__ __forceinline__ void cons2prim(const Phys& s, const double* U, double* V) {
+    double Bp;
+    if (s.force_hydro)
+        Bp = 0.0;
+    else
+        Bp = 0.5 * (U[MAGX] * U[MAGX] + U[MAGY] * U[MAGY] + U[MAGZ] * U[MAGZ]);
+    const double density = U[DENS];
+    const double velx = U[MOMX] / density;
+    const double vely = U[MOMY] / density;
+    const double velz = U[MOMZ] / density;
+    const double eint = (U[ENER] - Bp) / density - 0.5 * (velx * velx + vely * vely + velz * velz);
+    V[DENS] = density;
+    V[VELX] = velx;
+    V[VELY] = vely;
+    V[VELZ] = velz;
+    if (s.force_hydro) {
+        V[MAGX] = 0.0;
+        V[MAGY] = 0.0;
+        V[MAGZ] = 0.0;
+    } else {
+        V[MAGX] = U[MAGX];
+        V[MAGY] = U[MAGY];
+        V[MAGZ] = U[MAGZ];
+    }
+    V[PRES] = eos_pres(s, density, eint);
+    V[EINT] = eint;
+    V[GAMM] = s.gamma;
+}
+
+// src/convert.f90:236-254 (not floored; SUM starts from zero)
+__device__ __forceinline__ double cons2pres(const Phys& s, const double* U) {
+    double Bp;
+    if (s.force_hydro)
+        Bp = 0.0;
+    else
+        Bp = 0.5 * ((0.0 + U[MAGX] * U[MAGX]) + U[MAGY] * U[MAGY] + U[MAGZ] * U[MAGZ]);
+    const double msq = (0.0 + U[MOMX] * U[MOMX]) + U[MOMY] * U[MOMY] + U[MOMZ] * U[MOMZ];
+    return (s.gamma - 1.0) * (U[ENER] - Bp - 0.5 * msq / U[DENS]);
+}
+
+// src/convert.f90:28-92
+__device__ __forceinline__ void cons2flux(const Phys& s, const double* U, const double* V, int dir, double* F) {
+    double Bp = 0.0;
+    if (!s.force_hydro) Bp = 0.5 * (U[MAGX] * U[MAGX] + U[MAGY] * U[MAGY] + U[MAGZ] * U[MAGZ]);
+    const double E = U[ENER];
+    const double Ptot = V[PRES] + Bp;
+    const int mN = dir == XDIR ? MOMX : MOMY, mT1 = dir == XDIR ? MOMY : MOMX, mT2 = MOMZ;
+    const int vN = mN, vT1 = mT1, vT2 = mT2;  // velocity indices equal momentum indices
+    const int bN = dir == XDIR ? MAGX : MAGY, bT1 = dir == XDIR ? MAGY : MAGX, bT2 = MAGZ;
+#pragma unroll
+    for (int v = 0; v < NCONS; v++) F[v] = 0.0;
+    F[DENS] = U[mN];
+    F[mN] = U[mN] * U[mN] / U[DENS] + Ptot;
+    F[mT1] = U[mN] * V[vT1];
+    F[mT2] = U[mN] * V[vT2];
+    F[ENER] = (E + Ptot) * V[vN];
+    if (!s.force_hydro) {
+        F[mN] = F[mN] - V[bN] * V[bN];
+        F[mT1] = F[mT1] - V[bT1] * V[bN];
+        F[mT2] = F[mT2] - V[bT2] * V[bN];
+        F[bT1] = V[vN] * V[bT1] - V[vT1] * V[bN];
+        F[bT2] = V[vN] * V[bT2] - V[vT2] * V[bN];
+        F[ENER] = F[ENER] - V[bN] * (V[VELX] * V[MAGX] + V[VELY] * V[MAGY] + V[VELZ] * V[MAGZ]);
+    }
+}
+
+// src/eigen.f90:305-321 (Ryu & Jones 1995, eqs. 2.18-2.19)
+__device__ __forceinline__ double c_fs(double gam, double rho, double p, double BB, double B_N, double pm) {
+    double c = (gam * p + BB) / rho;
+    c = 0.5 * (c + pm * sqrt(c * c - 4.0 * gam * p * (B_N * B_N) / (rho * rho)));
+    return sqrt(fmax(1.0e-14, c));
+}
+
+// src/eigen.f90:257-303, eigenvalues 1 and 7 (the only ones HLLC uses)
+__device__ __forceinline__ void fast_speeds(const Phys& s, const double* V, int dir, double& lam1, double& lam7) {
+    const double rho = fmax(V[DENS], s.small_density);
+    const double velN = V[VELX + dir];
+    const double B_N = V[MAGX + dir];
+    const double p = fmax(V[PRES], s.small_pressure);
+    const double gam = V[GAMM];
+    const double BB = V[MAGX] * V[MAGX] + V[MAGY] * V[MAGY] + V[MAGZ] * V[MAGZ];
+    const double cf = c_fs(gam, rho, p, BB, B_N, +1.0);
+    lam1 = velN - cf;
+    lam7 = velN + cf;
+}
+
+__device__ __forceinline__ double dot3(double a0, double a1, double a2, double b0, double b1, double b2) {
+    return (0.0 + a0 * b0) + a1 * b1 + a2 * b2;
+}
+
+// src/riemannSolver.f90:68-221 (HLLC for MHD, Li 2005)
+__device__ __forceinline__ void hllc(const Phys& s, const double* uL, const double* uR, int dir, double* flux) {
+    double vL[NPRIM], vR[NPRIM];
+    cons2prim(s, uL, vL);
+    cons2prim(s, uR, vR);
+    const int vN = dir == XDIR ? VELX : VELY, vT1 = dir == XDIR ? VELY : VELX, vT2 = VELZ;
+    const int bN = dir == XDIR ? MAGX : MAGY, bT1 = dir == XDIR ? MAGY : MAGX, bT2 = MAGZ;
+    const int mN = vN, mT1 = vT1, mT2 = vT2;
+    double eL1, eL7, eR1, eR7, eA1, eA7;
+    fast_speeds(s, vL, dir, eL1, eL7);
+    fast_speeds(s, vR, dir, eR1, eR7);
+    {
+        double vA[NPRIM];
+#pragma unroll
+        for (int v = 0; v < NPRIM; v++) vA[v] = (vL[v] + vR[v]) / 2.0;
+        fast_speeds(s, vA, dir, eA1, eA7);
+    }
+    const double sL = fmin(eL1, eA1);
+    const double sR = fmax(eA7, eR7);
+    double fL[NCONS], fR[NCONS];
+    cons2flux(s, uL, vL, dir, fL);
+    cons2flux(s, uR, vR, dir, fR);
+    double uHLL[NCONS];
+#pragma unroll
+    for (int v = 0; v < NCONS; v++) uHLL[v] = (sR * uR[v] - sL * uL[v] + fL[v] - fR[v]) / (sR - sL);
+    const double velHx = uHLL[MOMX] / uHLL[DENS];
+    const double velHy = uHLL[MOMY] / uHLL[DENS];
+    const double velHz = uHLL[MOMZ] / uHLL[DENS];
+    const double magDotVelHLL = dot3(uHLL[MAGX], uHLL[MAGY], uHLL[MAGZ], velHx, velHy, velHz);
+    const double magDotVelL = dot3(vL[MAGX], vL[MAGY], vL[MAGZ], vL[VELX], vL[VELY], vL[VELZ]);
+    const double magDotVelR = dot3(vR[MAGX], vR[MAGY], vR[MAGZ], vR[VELX], vR[VELY], vR[VELZ]);
+    const double velNL = vL[vN], velNR = vR[vN];
+    const double magNL = vL[bN], magNR = vR[bN], magNHLL = uHLL[bN];
+    const double rhoL = vL[DENS], rhoR = vR[DENS];
+    const double pTotL = vL[PRES] + 0.5 * dot3(vL[MAGX], vL[MAGY], vL[MAGZ], vL[MAGX], vL[MAGY], vL[MAGZ]);
+    const double pTotR = vR[PRES] + 0.5 * dot3(vR[MAGX], vR[MAGY], vR[MAGZ], vR[MAGX], vR[MAGY], vR[MAGZ]);
+    const double dL = sL - velNL, dR = sR - velNR;
+    const double sStr = (uR[mN] * dR - uL[mN] * dL + pTotL - pTotR - magNL * magNL + magNR * magNR) /
+                        (rhoR * dR - rhoL * dL);
+    const double pStr = rhoL * dL * (sStr - velNL) + pTotL - magNL * magNL + magNHLL * magNHLL;
+    if (0.0 < sL) {
+#pragma unroll
+        for (int v = 0; v < NCONS; v++) flux[v] = fL[v];
+    } else if ((sL <= 0.0) && (0.0 < sStr)) {
+        double uStr[NCONS];
+        uStr[DENS] = rhoL * dL / (sL - sStr);
+        uStr[mN] = uStr[DENS] * sStr;
+        uStr[mT1] = uStr[DENS] * vL[vT1] - (magNHLL * uHLL[bT1] - magNL * vL[bT1]) / (sL - sStr);
+        uStr[mT2] = uStr[DENS] * vL[vT2] - (magNHLL * uHLL[bT2] - magNL * vL[bT2]) / (sL - sStr);
+        uStr[bN] = magNHLL;
+        uStr[bT1] = uHLL[bT1];
+        uStr[bT2] = uHLL[bT2];
+        uStr[ENER] = uL[ENER] * dL + pStr * sStr - pTotL * velNL - magNHLL * magDotVelHLL + magNL * magDotVelL;
+        uStr[ENER] = uStr[ENER] / (sL - sStr);
+#pragma unroll
+        for (int v = 0; v < NCONS; v++) flux[v] = fL[v] + sL * (uStr[v] - uL[v]);
+    } else if ((sStr <= 0.0) && (0.0 <= sR)) {
+        double uStr[NCONS];
+        uStr[DENS] = rhoR * dR / (sR - sStr);
+        uStr[mN] = uStr[DENS] * sStr;
+        uStr[mT1] = uStr[DENS] * vR[vT1] - (magNHLL * uHLL[bT1] - magNR * vR[bT1]) / (sR - sStr);
+        uStr[mT2] = uStr[DENS] * vR[vT2] - (magNHLL * uHLL[bT2] - magNR * vR[bT2]) / (sR - sStr);
+        uStr[bN] = magNHLL;
+        uStr[bT1] = uHLL[bT1];
+        uStr[bT2] = uHLL[bT2];
+        uStr[ENER] = uR[ENER] * dR + pStr * sStr - pTotR * velNR - magNHLL * magDotVelHLL + magNR * magDotVelR;
+        uStr[ENER] = uStr[ENER] / (sR - sStr);
+#pragma unroll
+        for (int v = 0; v < NCONS; v++) flux[v] = fR[v] + sR * (uStr[v] - uR[v]);
+    } else {
+#pragma unroll
+        for (int v = 0; v < NCONS; v++) flux[v] = fR[v];
+    }
+}
+
+// src/detect.f90:250-265 (CAD) and :238-248 (PAD)
+__device__ __forceinline__ bool admissible(double dens, double pres) {
+    const bool cad = !(isnan(dens) || isnan(pres) || !isfinite(dens) || !isfinite(pres));
+    const bool pad = (dens > 0.0) && (pres > 0.0);
+    return cad && pad;
+}
+
+}  // namespace hosono

@@ -1,0 +1,191 @@
+/*
+ * hosono_gpu.h -- C ABI of the B200 (sm_100a, FP64) time-step path of
+ * hosono-2DMHD.
+ *
+ * The library replaces the reference's hot path behind its module
+ * interfaces:
+ *   cfl_computedt(blk, state)                 src/cfl.f90:14-52
+ *   timeStep_advanceSolution(dt, blk, state)  src/timeStep.f90:22-43
+ * and, inside it, reconstruct_faceValsWithGP (src/reconstruct.f90:18-175),
+ * getFluxes_ (src/getFluxes.f90:16-90), riemannSolver_* (src/riemannSolver.f90),
+ * FLICDdivB_fluxCorrections (src/FLICDdivB.f90:13-70), detect_ALL
+ * (src/detect.f90:18-236), gridBlock_lowerOrder (src/gridBlock.f90:194-235),
+ * boundaryConditions_applyBlk/applyMOOD (src/boundaryConditions.f90) and
+ * timeStep_RK3/forwardEuler (src/timeStep.f90:45-171).
+ *
+ * All entry points are extern "C", take plain pointers and sizes, return an
+ * int status (HOSONO_OK = 0) and never abort the process.  Host arrays use
+ * the reference's Fortran order with guard cells:
+ *     U(var=1..8, i=1..nx+2*NGC, j=1..ny+2*NGC), var fastest,
+ *     V(var=1..10, i, j), scheme(i, j) (int).
+ * One host thread per handle.
+ */
+#ifndef HOSONO_GPU_H
+#define HOSONO_GPU_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define HOSONO_OK 0
+#define HOSONO_EINVAL 1     /* bad argument (sizes, radius, boundary id)          */
+#define HOSONO_ENOMEM 2     /* device allocation failed                           */
+#define HOSONO_ECUDA 3      /* a CUDA call failed (message in last_error)         */
+#define HOSONO_ENANDT 4     /* dt is NaN, infinite or negative (validTimeStep)    */
+#define HOSONO_EMOODCAP 5   /* MOOD loop exceeded its pass cap                    */
+#define HOSONO_ETIMEOUT 6   /* a bounded device wait gave up                      */
+#define HOSONO_EPAR 7       /* .par file missing a key or holding a bad value     */
+#define HOSONO_ENOTBUILT 8  /* library loaded without device code for this GPU    */
+
+/* boundary ids (sim_BC, src/simulation.f90:62) */
+#define HOSONO_BC_OUTFLOW 0
+#define HOSONO_BC_PERIODIC 1
+
+/* arithmetic modes */
+#define HOSONO_FP_STRICT 0  /* no FMA contraction: bit-identical to the oracle   */
+#define HOSONO_FP_FAST 1    /* FMA contraction allowed                            */
+
+/* POD copy of the run settings: sim_* of src/simulation.f90:9-31 and the
+ * index/geometry fields of gridBlock_t (src/gridBlock.f90:36-45). */
+typedef struct hosono_params {
+    int nx, ny;            /* interior cells (grid_Nx, grid_Ny)                  */
+    int ngc;               /* guard cells, must be max_radius + 2 (grid.f90:71)  */
+    int max_radius;        /* GP_maxRadius, 1..3                                  */
+    int bc;                /* HOSONO_BC_*                                         */
+    int force_hydro;       /* sim_forceHydro                                      */
+    int riemann_solver;    /* sim_riemannSolverID; 1 = HLLC-MHD                   */
+    int fp_mode;           /* HOSONO_FP_*                                         */
+    double dx, dy;         /* blk%dl                                              */
+    double mindxdy, maxdxdy;
+    double gamma;          /* sim_gamma                                           */
+    double small_pressure, small_density, small_energy, small_b;
+    double cfl;            /* sim_cfl                                             */
+} hosono_params;
+
+typedef struct hosono_handle hosono_handle;
+
+/* Per-handle counters of the last advance (MOOD activity). */
+typedef struct hosono_stats {
+    int stages;            /* forward-Euler stages run                           */
+    int mood_passes;       /* MOOD passes summed over the stages                  */
+    int max_passes;        /* largest pass count of one stage                     */
+    long long detect_lowered;  /* cells lowered by detect_ALL                      */
+    long long inner_lowered;   /* cells lowered by the reconstruct face cascade    */
+    int cascade_iters;     /* inner cascade iterations                            */
+} hosono_stats;
+
+/* ---------------------------------------------------------------- set-up */
+
+/* GP_init (src/GP.f90:37-200): quad-precision GP prediction vectors and
+ * quadrature weights, rounded to FP64.  Real inputs are decimal strings
+ * parsed in quad precision like readParamFile_quadPrecisionReal
+ * (src/readParamFile.f90:67-84).  Outputs in Fortran order:
+ *   pv(nsMax, nqMax, 4, R), qw(nqMax, R), stenc(2, nsMax, R),
+ * nsMax = 1+2R(R+1), nqMax = R+1. */
+int hosono_gp_build(int max_radius, const char* x_beg, const char* x_end, int nx,
+                    const char* y_beg, const char* y_end, int ny, const char* ell_over_delta,
+                    double* pv, double* qw, int* stenc);
+
+/* Run settings of a .par file that are not part of hosono_params. */
+typedef struct hosono_run_info {
+    double tmax;               /* sim_tmax                                      */
+    int nstepmax;              /* sim_nstepmax                                  */
+    int output_freq_step;      /* sim_outputFreqStep                            */
+    double output_freq_time;   /* sim_outputFreqTime                            */
+    double ell_over_delta;     /* GP_ellOverDelta                               */
+    double x_beg, x_end, y_beg, y_end;  /* grid_xBeg .. grid_yEnd               */
+    int nx_tot, ny_tot;        /* nx + 2*NGC, ny + 2*NGC (host array extents)   */
+    char ic_type[32];          /* IC_type                                       */
+    char data_file_base[256];  /* sim_dataFileBaseName                          */
+} hosono_run_info;
+
+/* simulation_init + grid_init (src/simulation.f90:35-78, src/grid.f90:31-103):
+ * read a .par file (format of src/readParamFile.f90:1-9, first matching line
+ * wins) into params and run settings.  fp_mode is set to HOSONO_FP_STRICT. */
+int hosono_par_load(const char* parfile, hosono_params* p, hosono_run_info* run, char* err, int errlen);
+
+/* GP_init from a .par file (grid_* and GP_* keys read in quad precision). */
+int hosono_par_gp(const char* parfile, double* pv, double* qw, int* stenc, char* err, int errlen);
+
+/* initialCondition_set (src/initialCondition.f90:23-84): fills U and V
+ * (Fortran order, nx_tot*ny_tot cells, guards by the boundary condition).
+ * IC types explosion2d, sedov2d, OrszagTang2d.  Optional keys beyond the
+ * reference, whose defaults reproduce it: IC_B0 and IC_pres for
+ * OrszagTang2d (default 1/gamma), IC_magx/IC_magy/IC_magz for explosion2d
+ * (default 0). */
+int hosono_ic_set(const char* parfile, const hosono_params* p, double* U, double* V, char* err, int errlen);
+
+/* ---------------------------------------------------------------- solver */
+
+/* Allocate a device instance (gridBlock_t + gridState_t of grid.f90:88-89
+ * and the GP tables of GP.f90:99-101).  pv/qw/stenc as produced by
+ * hosono_gp_build.  The handle owns its device buffers and CUDA stream. */
+int hosono_gpu_create(const hosono_params* p, const double* pv, const double* qw, const int* stenc,
+                      hosono_handle** out);
+int hosono_gpu_destroy(hosono_handle* h);
+
+/* Host <-> device state (Fortran order, guards included).  V may be NULL
+ * on upload (then V = cons2prim(U) on every cell).  Any download pointer
+ * may be NULL. */
+int hosono_gpu_upload(hosono_handle* h, const double* U, const double* V);
+int hosono_gpu_download(hosono_handle* h, double* U, double* V, int* scheme);
+
+/* cfl_computedt (src/cfl.f90:14-52) on the resident state. */
+int hosono_gpu_cfl(hosono_handle* h, double* dt);
+
+/* timeStep_advanceSolution (src/timeStep.f90:22-43) on the resident state. */
+int hosono_gpu_advance(hosono_handle* h, double dt);
+
+/* The mhd_driver time loop (src/mhd_driver.f90:198-217 with validTimeStep
+ * :239-266) on the resident state, without output: steps until t >= tmax,
+ * nstep >= nstepmax or max_steps steps (max_steps <= 0: no extra limit). */
+int hosono_gpu_run(hosono_handle* h, double tmax, int nstepmax, int max_steps, double* t_out, int* nstep_out);
+
+/* Drop-in with host buffers: upload U (and V if not NULL), advance by dt,
+ * download U and V.  The form a Fortran caller that keeps grid_state on
+ * the host binds (timeStep_advanceSolution with state%U/state%V). */
+int hosono_gpu_advance_host(hosono_handle* h, double dt, double* U, double* V);
+
+int hosono_gpu_stats(hosono_handle* h, hosono_stats* s);
+
+/* Copies the last error message into buf; returns its status code. */
+int hosono_gpu_last_error(hosono_handle* h, char* buf, int len);
+
+/* MOOD trace for parity tests: one record per MOOD pass.  meta[0..3] =
+ * stage, pass, inner-cascade lowerings, detect lowerings; masks hold
+ * per-cell lowering counts of that pass (nxTot*nyTot bytes, may be NULL). */
+int hosono_gpu_trace_enable(hosono_handle* h, int on);
+int hosono_gpu_trace_count(hosono_handle* h);
+int hosono_gpu_trace_get(hosono_handle* h, int k, int* meta, unsigned char* inner_mask,
+                         unsigned char* detect_mask);
+int hosono_gpu_trace_clear(hosono_handle* h);
+
+/* Device-resident access for callers that manage their own buffers
+ * (benchmarks, batching): device pointer of the first U plane; planes are
+ * pitch*nyTot doubles apart, rows pitch doubles apart. */
+int hosono_gpu_state_layout(hosono_handle* h, double** U_dev, int* pitch, long long* plane);
+
+/* Library identification: fills the compiled device architecture (e.g. 100
+ * for sm_100a) and returns HOSONO_OK. */
+int hosono_gpu_build_info(int* sm_arch, int* has_fast_mode);
+
+/* Select the CUDA device for handles created afterwards on this thread. */
+int hosono_gpu_set_device(int device);
+
+/* The cudaStream_t every kernel of this handle runs on (for events). */
+int hosono_gpu_stream(hosono_handle* h, void** stream);
+
+/* Kernel timing: when on, CUDA events bracket every launch of the MOOD
+ * pass-1 kernel; times[0] = summed milliseconds, counts[0] = launches since
+ * the last reset.  launches = kernels launched by this handle since reset. */
+int hosono_gpu_profile(hosono_handle* h, int on);
+int hosono_gpu_profile_read(hosono_handle* h, double* pass1_ms, long long* pass1_launches, long long* launches,
+                            int reset);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

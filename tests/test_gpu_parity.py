@@ -1,0 +1,98 @@
+"""GPU path (through the C ABI) against the oracle on identical inputs.
+
+Strict arithmetic (no FMA contraction) must reproduce the oracle bit for bit:
+U, V, the MOOD scheme and every pass's troubled-cell masks.  The FMA build
+must stay within the parity tolerance of 1e-12 relative L1 after one step.
+"""
+import numpy as np
+import pytest
+
+import oracle
+import parfiles
+import pkg
+
+CASES = {
+    "ot32_r1": lambda: parfiles.orszag_tang(32, 1),
+    "ot32_r2": lambda: parfiles.orszag_tang(32, 2),
+    "ot24_r3_refic": lambda: parfiles.orszag_tang(24, 3, standard=False),
+    "sedov32_r2": lambda: parfiles.sedov(32, 2),
+    "sedov33x40_r1": lambda: dict(parfiles.sedov(33, 1), grid_Ny="40", grid_yEnd="0.7"),
+    "blast40_r2": lambda: parfiles.blast(40, 2, p_ratio=1000.0, theta=0.3),
+    "blast36_r3": lambda: parfiles.blast(36, 3, p_ratio=100.0, theta=1.2),
+}
+
+
+def rel_l1(a, b):
+    return np.abs(a - b).sum() / max(np.abs(b).sum(), 1e-300)
+
+
+def compare_traces(gt, ot):
+    assert len(gt) == len(ot), (len(gt), len(ot))
+    for g, o in zip(gt, ot):
+        assert (g["stage"], g["mood_pass"], g["n_inner"], g["n_detect"]) == \
+               (o["stage"], o["mood_pass"], o["n_inner"], o["n_detect"]), (g, o)
+        np.testing.assert_array_equal(g["detect"], o["detect"])
+        np.testing.assert_array_equal(g["inner"], o["inner"])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", sorted(CASES))
+def test_strict_bitwise_steps(case, tmp_par_dir):
+    m = pkg.load()
+    par = parfiles.make(tmp_par_dir, case, CASES[case]())
+    o = oracle.Oracle(par)
+    s = m.Solver.from_par(par, fp_mode=m.FP_STRICT)
+    o.trace(True)
+    s.trace(True)
+    nsteps = 6
+    for step in range(nsteps):
+        dt_o = o.cfl()
+        dt_g = s.cfl_computedt()
+        assert dt_g == dt_o, (step, dt_g, dt_o)
+        o.advance(dt_o)
+        s.timeStep_advanceSolution(dt_g)
+        U, V, S = s.download()
+        np.testing.assert_array_equal(U, o.U())
+        np.testing.assert_array_equal(V, o.V())
+        np.testing.assert_array_equal(S, o.scheme())
+    compare_traces(s.traces(), o.traces())
+    s.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", ["ot32_r2", "blast40_r2", "sedov32_r2"])
+def test_fast_one_step_tolerance(case, tmp_par_dir):
+    """FMA build: one RK3 step within 1e-12 relative L1 on all 8 variables."""
+    m = pkg.load()
+    par = parfiles.make(tmp_par_dir, case, CASES[case]())
+    o = oracle.Oracle(par)
+    s = m.Solver.from_par(par, fp_mode=m.FP_FAST)
+    dt = o.cfl()
+    assert abs(s.cfl_computedt() - dt) <= 1e-14 * dt
+    o.advance(dt)
+    s.timeStep_advanceSolution(dt)
+    U, _, _ = s.download()
+    Uo = o.U()
+    g = o.ngc
+    for v in range(8):
+        a, b = U[g:-g, g:-g, v], Uo[g:-g, g:-g, v]
+        if np.abs(b).sum() > 0:
+            assert rel_l1(a, b) <= 1e-12, (v, rel_l1(a, b))
+    s.close()
+
+
+@pytest.mark.gpu
+def test_orszag_tang_128_r1_to_t_end(tmp_par_dir):
+    """The reference's own runnable case (OT 128^2, R=1, t_end=0.5): strict
+    path bit-identical to the oracle at t_end."""
+    m = pkg.load()
+    par = parfiles.make(tmp_par_dir, "ot128", parfiles.orszag_tang(128, 1))
+    o = oracle.Oracle(par)
+    s = m.Solver.from_par(par, fp_mode=m.FP_STRICT)
+    rc, t_o, n_o = o.run()
+    t_g, n_g = s.run()
+    assert rc == 0 and n_g == n_o and t_g == t_o == 0.5
+    U, V, S = s.download()
+    np.testing.assert_array_equal(U, o.U())
+    np.testing.assert_array_equal(V, o.V())
+    s.close()
