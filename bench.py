@@ -39,6 +39,7 @@ FALLBACK_HBM_GBS = 6650.0
 
 WORKLOADS = {
     "ot2048_r2": dict(n=2048, radius=2, ell=12.0, desc="Orszag-Tang 2048x2048, GP-MOOD R=2 (5th->3rd->1st), ell/dx=12"),
+    "ot1536_r2": dict(n=1536, radius=2, ell=12.0, desc="Orszag-Tang 1536x1536, GP-MOOD R=2 (5th->3rd->1st), ell/dx=12"),
     "ot1024_r2": dict(n=1024, radius=2, ell=12.0, desc="Orszag-Tang 1024x1024, GP-MOOD R=2 (5th->3rd->1st), ell/dx=12"),
     "ot128_r1": dict(n=128, radius=1, ell=6.0, desc="Orszag-Tang 128x128, GP-MOOD R=1 (3rd->1st), ell/dx=6"),
 }
@@ -128,10 +129,26 @@ def pass1_bytes(n, radius):
     return cells_u * 8 * 8 + faces * 18 * 8 + (n + 5) ** 2 * 2
 
 
-def run_cpu_baseline(workload, steps, threads, fast=True):
-    """Time the oracle restatement on the host cores: returns (zone-updates/s, sample text)."""
+def host_has_avx2_fma():
+    try:
+        with open("/proc/cpuinfo") as f:
+            flags = next((ln for ln in f if ln.startswith("flags")), "").split()
+        return "avx2" in flags and "fma" in flags
+    except OSError:
+        return False
+
+
+def oracle_build():
+    return "-O3 AVX2/FMA contraction" if host_has_avx2_fma() else "-O3 SSE2, no contraction"
+
+
+def run_cpu_baseline(workload, steps, threads, fast=None):
+    """Time the oracle restatement on the host cores: returns (zone-updates/s, seconds).
+    fast=None picks the AVX2/FMA build when the host supports it."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
+    if fast is None:
+        fast = host_has_avx2_fma()
     oracle.set_threads(threads, fast=fast)
     w = WORKLOADS[workload]
     with tempfile.TemporaryDirectory() as d:
@@ -168,7 +185,7 @@ def bench_reference(args, rank):
         "impl": "reference",
         "cpu_baseline": {"value": rate, "unit": "zone-updates/s", "cores": threads, "kind": "port",
                          "sample": f"{steps} full RK3 steps of {args.workload} after 1 warm-up step, "
-                                   f"CPU oracle (C++ restatement of the Fortran, OpenMP, -O3 AVX2/FMA)"},
+                                   f"CPU oracle (C++ restatement of the Fortran, OpenMP, {oracle_build()})"},
         "e2e": {"value": rate, "unit": "zone-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -204,14 +221,15 @@ def bench_ours(args, rank, world, local):
             dist.barrier()
         torch.cuda.synchronize()
 
-    # warm-up
+    # warm-up (the clock sampler starts here so it has samples under load
+    # even when the timed region is shorter than its 200 ms period)
+    clocks = ClockSampler(local)
+    clocks.start()
     for _ in range(args.warmup):
         sol.timeStep_advanceSolution(sol.cfl_computedt())
     barrier()
     sol.profile(True)
     sol.profile_read(reset=True)
-    clocks = ClockSampler(local)
-    clocks.start()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
@@ -283,7 +301,7 @@ def bench_ours(args, rank, world, local):
         rate, el = run_cpu_baseline(args.workload, 1, threads)
         line["cpu_baseline"] = {"value": rate, "unit": "zone-updates/s", "cores": threads, "kind": "port",
                                 "sample": f"1 full RK3 step of {args.workload} after 1 warm-up step, CPU oracle "
-                                          f"(C++ restatement, OpenMP, -O3 AVX2/FMA), {el:.1f} s"}
+                                          f"(C++ restatement, OpenMP, {oracle_build()}), {el:.1f} s"}
     print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()

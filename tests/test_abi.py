@@ -1,0 +1,97 @@
+"""The C ABI library loads and exports every symbol include/hosono_gpu.h
+declares; host-side set-up entry points run without a GPU."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+import oracle
+import parfiles
+import pkg
+
+HEADER = os.path.join(pkg.ROOT, "include", "hosono_gpu.h")
+
+
+def declared_functions():
+    src = open(HEADER).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(hosono_\w+)\s*\(", src)))
+
+
+def test_library_exports_every_declared_symbol():
+    m = pkg.load()
+    lib = m.load_library()
+    names = declared_functions()
+    assert len(names) >= 20
+    for n in names:
+        assert hasattr(lib, n), n
+    assert set(names) == set(m.SIGNATURES), set(names) ^ set(m.SIGNATURES)
+
+
+@pytest.mark.parametrize("R", [1, 2, 3])
+def test_gp_tables_bit_identical_to_oracle(R):
+    m = pkg.load()
+    for args in (("0.0", "1.0", 128, "0.0", "1.0", 128, "6.0"), ("-0.5", "0.5", 512, "-0.5", "0.5", 256, "12.0")):
+        a = m.gp_build(R, *args)
+        b = oracle.gp_build(R, *args)
+        for x, y in zip(a, b):
+            np.testing.assert_array_equal(x, y)
+
+
+@pytest.mark.parametrize("name,kv", [
+    ("ot", parfiles.orszag_tang(40, 2)),
+    ("ot_refic", parfiles.orszag_tang(24, 3, standard=False)),
+    ("sedov", parfiles.sedov(36, 2)),
+    ("blast", parfiles.blast(48, 2, p_ratio=300.0, theta=0.7)),
+])
+def test_par_and_initial_condition_match_oracle(name, kv, tmp_par_dir):
+    m = pkg.load()
+    par = parfiles.make(tmp_par_dir, name, kv)
+    p, run = m.par_load(par)
+    U, V = m.ic_set(par, p)
+    o = oracle.Oracle(par)
+    np.testing.assert_array_equal(U, o.U())
+    np.testing.assert_array_equal(V, o.V())
+    assert (p.nx, p.ny, p.ngc, p.max_radius) == (o.nx, o.ny, o.ngc, o.R)
+    assert p.dx == o.dx and p.dy == o.dy and p.mindxdy == o.mindxdy and p.maxdxdy == o.maxdxdy
+    assert run.tmax == o.tmax
+
+
+def test_par_missing_key_is_reported(tmp_par_dir):
+    m = pkg.load()
+    kv = parfiles.orszag_tang(16, 1)
+    del kv["sim_cfl"]
+    par = parfiles.make(tmp_par_dir, "missing", kv)
+    with pytest.raises(m.HosonoError) as e:
+        m.par_load(par)
+    assert e.value.code == m.EPAR and "sim_cfl" in str(e.value)
+
+
+def test_par_first_match_and_comments(tmp_par_dir):
+    """readParamFile.f90:150-175: comment lines skipped, text after '#'
+    dropped, first matching key wins, leading blanks make a different key."""
+    m = pkg.load()
+    kv = parfiles.orszag_tang(16, 1)
+    par = parfiles.make(tmp_par_dir, "dup", kv)
+    with open(par) as f:
+        body = f.read()
+    body = "# sim_cfl = 0.1\n   sim_cfl = 0.2\n" + body.replace("sim_cfl = 0.8", "sim_cfl = 0.8 # courant") + \
+        "sim_cfl = 0.3\n"
+    with open(par, "w") as f:
+        f.write(body)
+    p, _ = m.par_load(par)
+    assert p.cfl == 0.8
+
+
+def test_create_rejects_bad_params():
+    m = pkg.load()
+    p = m.Params(nx=8, ny=8, ngc=3, max_radius=2, bc=1, riemann_solver=1, dx=0.1, dy=0.1)
+    pv, qw, st = m.gp_build(2, "0.0", "1.0", 8, "0.0", "1.0", 8, "6.0")
+    h = ctypes.c_void_p()
+    lib = m.load_library()
+    rc = lib.hosono_gpu_create(ctypes.byref(p), pv.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                               qw.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                               st.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), ctypes.byref(h))
+    assert rc == m.EINVAL  # ngc must be R + 2
