@@ -88,7 +88,9 @@ SIGNATURES = {
     "hosono_gpu_stream": [_vp, ctypes.POINTER(_vp)],
     "hosono_gpu_profile": [_vp, _i],
     "hosono_gpu_profile_read": [_vp, _dp, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong), _i],
+    "hosono_cfl_noalloc": [_vp, _i, _i, _i, _i, ctypes.c_longlong, _d, _d, _d, _i, _vp, _vp],
 }
+NOALLOC_MAX_ROWS = 16384  # HOSONO_NOALLOC_MAX_ROWS
 
 
 def set_device(device):

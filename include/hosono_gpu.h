@@ -178,6 +178,25 @@ int hosono_gpu_set_device(int device);
 /* The cudaStream_t every kernel of this handle runs on (for events). */
 int hosono_gpu_stream(hosono_handle* h, void** stream);
 
+/* CFL time step that allocates nothing.  No counterpart in the reference:
+ * it exists for callers that cannot call cudaMalloc when they need dt (code
+ * inside a CUDA stream capture, where allocation fails; hosts whose device
+ * memory is wholly owned by their own pool allocator; loops that must not
+ * enter the allocator, which may synchronise the device).
+ * Computes dt = cfl * min(dx/max(|u|+c_f), dy/max(|v|+c_f)) over the interior
+ * of a caller-owned device V (10 SoA planes, rows `pitch` doubles apart,
+ * planes `plane` doubles apart, ngc guard cells; the layout of the handle's
+ * own V) and writes it to the caller-owned device double *dt_dev, on
+ * `stream` (NULL = default stream).  Result equal to hosono_gpu_cfl's.
+ * Scratch: a file-scope device array of 2*HOSONO_NOALLOC_MAX_ROWS doubles
+ * (256 KiB) per GPU, held until process exit; ny > HOSONO_NOALLOC_MAX_ROWS
+ * returns HOSONO_EINVAL.  All calls on a device share that array, so calls
+ * whose kernels overlap on the GPU race.  The first call on a device looks
+ * up the array's address; make it before any stream capture. */
+#define HOSONO_NOALLOC_MAX_ROWS 16384
+int hosono_cfl_noalloc(const double* V_dev, int nx, int ny, int ngc, int pitch, long long plane, double dx, double dy,
+                       double cfl, int force_hydro, double* dt_dev, void* stream);
+
 /* Kernel timing: when on, CUDA events bracket every launch of the MOOD
  * pass-1 kernel; times[0] = summed milliseconds, counts[0] = launches since
  * the last reset.  launches = kernels launched by this handle since reset. */
