@@ -89,7 +89,27 @@ SIGNATURES = {
     "hosono_gpu_profile": [_vp, _i],
     "hosono_gpu_profile_read": [_vp, _dp, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong), _i],
     "hosono_cfl_noalloc": [_vp, _i, _i, _i, _i, ctypes.c_longlong, _d, _d, _d, _i, _vp, _vp],
+    "hosono_gpu_set_time": [_vp, _d, _d, _i, _i],
+    "hosono_gpu_step": [_vp, _i, _dp, _ip],
+    "hosono_gpu_set_graphs": [_vp, _i],
+    "hosono_batch_create": [_i, _i, _i, ctypes.POINTER(_vp)],
+    "hosono_batch_destroy": [_vp],
+    "hosono_batch_tiles_for": [ctypes.POINTER(Params)],
+    "hosono_batch_instance_bytes": [ctypes.POINTER(Params)],
+    "hosono_batch_add": [_vp, ctypes.POINTER(Params), _dp, _dp, _ip, _ip],
+    "hosono_batch_remove": [_vp, _i],
+    "hosono_batch_upload": [_vp, _i, _dp, _dp],
+    "hosono_batch_download": [_vp, _i, _dp, _dp, _ip],
+    "hosono_batch_set_time": [_vp, _i, _d, _d, _i, _i],
+    "hosono_batch_run": [_vp, _i],
+    "hosono_batch_status": [_vp, _i, _dp, _dp, _ip, _ip, _ip],
+    "hosono_batch_stats": [_vp, _i, ctypes.POINTER(Stats)],
+    "hosono_batch_stream": [_vp, ctypes.POINTER(_vp)],
+    "hosono_batch_set_graphs": [_vp, _i],
+    "hosono_batch_last_error": [_vp, _cp, _i],
+    "hosono_batch_capacity": [_vp, _ip, _ip, _ip, _ip],
 }
+RESTYPES = {"hosono_batch_instance_bytes": ctypes.c_longlong}
 NOALLOC_MAX_ROWS = 16384  # HOSONO_NOALLOC_MAX_ROWS
 
 
@@ -114,7 +134,7 @@ def load_library(path=LIB_PATH):
     for name, args in SIGNATURES.items():
         fn = getattr(lib, name)
         fn.argtypes = args
-        fn.restype = ctypes.c_int
+        fn.restype = RESTYPES.get(name, ctypes.c_int)
     _lib = lib
     return lib
 
@@ -270,6 +290,22 @@ class Solver:
         self._check(self.lib.hosono_gpu_advance_host(self.h, float(dt), _p(U), _p(V) if V is not None else None),
                     "advance_host")
 
+    def set_graphs(self, on=True):
+        """Run the MOOD loops from the captured CUDA graph (default) or host-driven."""
+        self._check(self.lib.hosono_gpu_set_graphs(self.h, 1 if on else 0), "set_graphs")
+
+    def set_time(self, t, tmax, nstep=0, nstepmax=1 << 30):
+        self._check(self.lib.hosono_gpu_set_time(self.h, float(t), float(tmax), int(nstep), int(nstepmax)),
+                    "set_time")
+
+    def step(self, max_steps=1):
+        """Continue the time loop (cfl + validTimeStep + advance on the device) by
+        up to max_steps steps; returns (t, nstep)."""
+        t = ctypes.c_double()
+        n = ctypes.c_int()
+        self._check(self.lib.hosono_gpu_step(self.h, int(max_steps), ctypes.byref(t), ctypes.byref(n)), "step")
+        return t.value, n.value
+
     def run(self, tmax=None, nstepmax=None, max_steps=0):
         """mhd_driver's time loop (no output)."""
         ri = getattr(self, "run_info", None)
@@ -333,3 +369,120 @@ class Solver:
         self._check(self.lib.hosono_gpu_state_layout(self.h, ctypes.byref(ptr), ctypes.byref(pitch),
                                                      ctypes.byref(plane)), "state_layout")
         return ptr.value, pitch.value, plane.value
+
+
+class Batch:
+    """Many independent blocks advanced together (include/hosono_gpu.h, hosono_batch_*)."""
+
+    def __init__(self, max_instances, max_tiles, fp_mode=FP_STRICT):
+        self.lib = load_library()
+        h = ctypes.c_void_p()
+        rc = self.lib.hosono_batch_create(int(max_instances), int(max_tiles), int(fp_mode), ctypes.byref(h))
+        if rc:
+            raise HosonoError(rc, "hosono_batch_create")
+        self.h = h
+        self.shapes = {}
+        self._keep = {}
+
+    @staticmethod
+    def tiles_for(params):
+        return load_library().hosono_batch_tiles_for(ctypes.byref(params))
+
+    @staticmethod
+    def instance_bytes(params):
+        return load_library().hosono_batch_instance_bytes(ctypes.byref(params))
+
+    def _check(self, rc, what):
+        if rc:
+            buf = ctypes.create_string_buffer(512)
+            self.lib.hosono_batch_last_error(self.h, buf, 512)
+            raise HosonoError(rc, f"{what}: {buf.value.decode()}")
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.hosono_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def add(self, params, pv, qw, stenc):
+        pv = np.ascontiguousarray(pv, dtype=np.float64)
+        qw = np.ascontiguousarray(qw, dtype=np.float64)
+        st = np.ascontiguousarray(stenc, dtype=np.int32)
+        slot = ctypes.c_int()
+        self._check(self.lib.hosono_batch_add(self.h, ctypes.byref(params), _p(pv), _p(qw), _p(st, ctypes.c_int),
+                                              ctypes.byref(slot)), "add")
+        k = slot.value
+        self.shapes[k] = (params.ny + 2 * params.ngc, params.nx + 2 * params.ngc)
+        return k
+
+    def add_par(self, parfile, fp_mode=None):
+        """Set up an instance from a .par file (GP tables, IC, time limits) and upload it."""
+        p, run = par_load(parfile)
+        pv, qw, st = par_gp(parfile, p.max_radius)
+        k = self.add(p, pv, qw, st)
+        U, V = ic_set(parfile, p)
+        self.upload(k, U, V)
+        self.set_time(k, 0.0, run.tmax, 0, run.nstepmax)
+        return k
+
+    def remove(self, slot):
+        self._check(self.lib.hosono_batch_remove(self.h, int(slot)), "remove")
+        self.shapes.pop(slot, None)
+
+    def upload(self, slot, U, V=None):
+        U = np.ascontiguousarray(U, dtype=np.float64)
+        Vp = None
+        if V is not None:
+            V = np.ascontiguousarray(V, dtype=np.float64)
+            Vp = _p(V)
+        self._check(self.lib.hosono_batch_upload(self.h, int(slot), _p(U), Vp), "upload")
+
+    def download(self, slot):
+        nyt, nxt = self.shapes[slot]
+        U = np.zeros((nyt, nxt, 8))
+        V = np.zeros((nyt, nxt, 10))
+        S = np.zeros((nyt, nxt), dtype=np.int32)
+        self._check(self.lib.hosono_batch_download(self.h, int(slot), _p(U), _p(V), _p(S, ctypes.c_int)),
+                    "download")
+        return U, V, S
+
+    def set_time(self, slot, t, tmax, nstep=0, nstepmax=1 << 30):
+        self._check(self.lib.hosono_batch_set_time(self.h, int(slot), float(t), float(tmax), int(nstep),
+                                                   int(nstepmax)), "set_time")
+
+    def run(self, max_steps=0):
+        self._check(self.lib.hosono_batch_run(self.h, int(max_steps)), "run")
+
+    def status(self, slot):
+        t = ctypes.c_double()
+        dt = ctypes.c_double()
+        n = ctypes.c_int()
+        done = ctypes.c_int()
+        err = ctypes.c_int()
+        self._check(self.lib.hosono_batch_status(self.h, int(slot), ctypes.byref(t), ctypes.byref(dt),
+                                                 ctypes.byref(n), ctypes.byref(done), ctypes.byref(err)), "status")
+        return dict(t=t.value, dt=dt.value, nstep=n.value, done=bool(done.value), error=err.value)
+
+    def stats(self, slot):
+        s = Stats()
+        self._check(self.lib.hosono_batch_stats(self.h, int(slot), ctypes.byref(s)), "stats")
+        return s.as_dict()
+
+    def stream(self):
+        s = ctypes.c_void_p()
+        self._check(self.lib.hosono_batch_stream(self.h, ctypes.byref(s)), "stream")
+        return s.value or 0
+
+    def set_graphs(self, on=True):
+        self._check(self.lib.hosono_batch_set_graphs(self.h, 1 if on else 0), "set_graphs")
+
+    def capacity(self):
+        a, b, c, d = (ctypes.c_int() for _ in range(4))
+        self._check(self.lib.hosono_batch_capacity(self.h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c),
+                                                   ctypes.byref(d)), "capacity")
+        return dict(max_instances=a.value, max_tiles=b.value, used_tiles=c.value, live=d.value)

@@ -1,0 +1,148 @@
+// engine.h -- batched solver engine: any number of independent blocks
+// ("instances", each a gridBlock_t + gridState_t of the reference) advanced
+// together by one set of kernel launches.  A plain single solve is a batch of
+// one.
+//
+// Kernels read their work from device tables: InstDev (per-instance geometry,
+// physics and buffer pointers), InstState (per-instance mutable scalars: t,
+// dt, MOOD counters, ...) and a list of 32x8 cell tiles (instance, x0, y0).
+// The tile list and its length live in device memory, so instances can be
+// added or removed between launches without rebuilding a CUDA graph.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+
+#include "physics.cuh"
+
+namespace hosono {
+
+constexpr int TILE_X = 32, TILE_Y = 8;
+
+// Index bookkeeping of gridBlock_t (src/gridBlock.f90:36-45), 0-based:
+// cells i in [0, nxt), interior [g, g+nx); planes are pitch*nyt doubles.
+struct Geo {
+    int nx, ny, g, nxt, nyt, pitch;
+    long long plane;
+    int R;   // GP_maxRadius
+    int bc;  // 0 outflow, 1 periodic
+    int nsMax, nqMax;
+    double dx, dy, mindxdy, maxdxdy;
+};
+
+// Per-instance descriptor (device memory; written by the host at admission).
+struct InstDev {
+    Geo geo;
+    Phys phys;
+    double cfl;
+    const double* pv;  // (nsMax, nqMax, 4, R)
+    const double* qw;  // (nqMax, R)
+    double* U[3];      // state and two stage buffers; roles rotate, see role_ptr
+    double* V;         // 10 planes
+    double* FX;        // fluxRaw x (8 planes): face between (i-1,j) and (i,j)
+    double* FY;        // fluxRaw y (8 planes): face between (i,j-1) and (i,j)
+    double* CTX;       // flux(magy, xdir): FLICD-corrected, or the raw copy
+    double* CTY;       // flux(magx, ydir)
+    int8_t* scheme[2];  // double-buffered MOOD scheme (GP radius per cell)
+    uint8_t* rec;       // blk%recompute
+    uint8_t* recF;      // blk%recomputeFLICD
+    uint8_t* rrRec;     // radius each face was last reconstructed at (2 bits x 4 faces)
+    uint8_t* fail;      // cell failed face CAD/PAD (inner cascade)
+    uint8_t* failX;     // bit0: E side of (i-1,j) failed, bit1: W side of (i,j)
+    uint8_t* failY;     // bit0: N side of (i,j-1) failed, bit1: S side of (i,j)
+    uint8_t* nextPass;  // reconstructNextPass
+    uint8_t* dirty;     // re-reconstructed by the pass-1 cascade
+    uint8_t* lowered;   // lowered by detect in this pass
+    uint8_t* innerCount;  // per-cell inner lowerings of this pass (trace)
+};
+
+// Per-instance mutable scalars (device memory).
+struct InstState {
+    double dt, t, tmax;
+    int nstep, nstepmax;
+    int live;        // slot holds an instance
+    int done;        // time loop finished (t >= tmax or nstep >= nstepmax) or failed
+    int error;       // HOSONO_* status that stopped it
+    int parity;      // which of U[0], U[1] holds the state
+    int schemeSel;   // which scheme buffer is current
+    int stepping;    // takes part in the current step
+    int stageActive;  // MOOD loop of the current stage still running
+    int anyFail;     // face cascade: some cell failed CAD/PAD since the last check
+    int nextIter;    // face cascade: this instance runs the next inner iteration
+    int cascaded;    // face cascade ran in the current pass
+    int cascadeMode;  // CASCADE_FROM_FACES after pass 1's fused kernel, else FROM_CELLS
+    int nInner, nDetect;  // lowerings in the current pass
+    int lastInner, lastDetect;  // lowerings of the last finished pass
+    int passes;      // MOOD passes in the current stage
+    int passCap;     // pass limit (a stage lowers >= 1 cell per pass: R*nx*ny+1 suffices)
+    int maxPasses, stages, cascadeIters, passesTotal;
+    long long innerTotal, detectTotal;
+    unsigned long long cflbits[2];
+};
+
+// Batch-wide flags the graph's conditional nodes are driven by.
+struct BatchFlags {
+    int anyActive;   // some instance's MOOD loop still running
+    int anyFail;     // some instance is in its face cascade
+    int anyLive;     // some instance still stepping (time loop)
+    int error;
+    int stepsLeft;   // step budget of the current run launch
+};
+
+// Roles of the three U buffers: the state lives in U[parity]; A in
+// U[1-parity]; B in U[2].  The final RK combine writes A and flips parity.
+enum : int { ROLE_STATE = 0, ROLE_A = 1, ROLE_B = 2 };
+
+__host__ __device__ inline double* role_ptr(const InstDev& d, int parity, int role) {
+    return role == ROLE_STATE ? d.U[parity] : role == ROLE_A ? d.U[1 - parity] : d.U[2];
+}
+
+// One kernel launch over the batch: tables and the tile list.
+struct Batch {
+    const InstDev* dev;
+    InstState* st;
+    const int4* tiles;   // x: instance, y: x0, z: y0
+    const int* ntiles;   // device counter
+    BatchFlags* flags;
+    int maxTiles;        // grid size of tile launches
+    int maxInst;         // capacity (slots)
+};
+
+enum : int { CASCADE_FROM_FACES = 0, CASCADE_FROM_CELLS = 1 };
+enum : int { FLUX_DIRTY = 0, FLUX_REC = 1 };
+enum : int { MASK_REC = 0, MASK_NEXTPASS = 1 };
+
+// Launchers of one arithmetic build (kernels.cu compiled strict or fast).
+struct KernelSet {
+    const char* name;
+    // time loop: per-instance step begin (cfl -> validated dt) and end
+    void (*cfl_reduce)(const Batch&, cudaStream_t);
+    void (*step_prepare)(const Batch&, int steps, cudaStream_t);
+    void (*step_begin)(const Batch&, int use_host_dt, cudaStream_t);
+    void (*step_end)(const Batch&, cudaGraphConditionalHandle run_cond, cudaStream_t);
+    // forward-Euler stage
+    void (*stage_init)(const Batch&, cudaStream_t);
+    void (*face_pass1)(const Batch&, int uin, cudaStream_t);
+    void (*cascade_cond)(const Batch&, cudaGraphConditionalHandle h, cudaStream_t);
+    void (*cascade_lower)(const Batch&, int mode, cudaStream_t);
+    void (*recon_check)(const Batch&, int uin, int mask, cudaStream_t);
+    void (*flux)(const Batch&, int uin, int mode, cudaStream_t);
+    void (*ct_update_detect)(const Batch&, int uin, int uout, cudaStream_t);
+    void (*mood_flags)(const Batch&, cudaStream_t);
+    void (*pass_end)(const Batch&, cudaGraphConditionalHandle h, cudaStream_t);
+    // RK3 combines and boundary conditions
+    void (*bc_fill)(const Batch&, int role, cudaStream_t);
+    void (*rk_combine2)(const Batch&, cudaStream_t);
+    void (*rk_final)(const Batch&, cudaStream_t);
+    void (*cons2prim_all)(const Batch&, cudaStream_t);
+};
+
+const KernelSet* kernelset_strict();
+const KernelSet* kernelset_fast();
+
+// layout conversions for one instance (no arithmetic; one build)
+void launch_aos_to_soa(const Geo& G, const double* aos, double* soa, int nvar, cudaStream_t s);
+void launch_soa_to_aos(const Geo& G, const double* soa, double* aos, int nvar, cudaStream_t s);
+void launch_scheme_to_int(const Geo& G, const int8_t* scheme, int* out, cudaStream_t s);
+
+}  // namespace hosono

@@ -1,0 +1,110 @@
+// engine_host.h -- host side of the batched engine (engine.cu).
+#pragma once
+
+#include "engine.h"
+#include "hosono_gpu.h"
+
+#include <string>
+#include <vector>
+
+namespace hosono {
+
+struct TraceRec {
+    int slot, stage, pass, nInner, nDetect;
+    std::vector<unsigned char> inner, detect;  // nxt*nyt, i fastest
+};
+
+class Engine {
+  public:
+    Engine() = default;
+    ~Engine();
+    Engine(const Engine&) = delete;
+    Engine& operator=(const Engine&) = delete;
+
+    // capacity: instance slots and 32x8 tiles over all instances
+    int init(int max_inst, int max_tiles, int fp_mode);
+    int add(const hosono_params& p, const double* pv, const double* qw, int* slot);
+    int remove(int slot);
+    int upload(int slot, const double* U, const double* V);
+    int download(int slot, double* U, double* V, int* scheme);
+    int set_time(int slot, double t, double tmax, int nstep, int nstepmax);
+    int state(int slot, InstState* out);
+    // cfl_computedt of one instance (dt to the host)
+    int cfl(int slot, double* dt);
+    // timeStep_advanceSolution of one instance with a host dt
+    int advance(int slot, double dt);
+    // time loop of every live instance: up to max_steps steps (<=0: until done)
+    int run(int max_steps);
+    // one step of every live instance with the pass-1 kernel bracketed by events
+    int run_profiled_step(double* pass1_ms, int* pass1_launches);
+
+    int tiles_of(const hosono_params& p) const;
+    int live_count() const;
+    size_t instance_bytes(const hosono_params& p) const;
+    const hosono_params& params(int slot) const { return slots_[slot].p; }
+    const Geo& geo(int slot) const { return slots_[slot].dev.geo; }
+    const InstDev& dev(int slot) const { return slots_[slot].dev; }
+    cudaStream_t stream() const { return s_; }
+    int max_inst() const { return maxInst_; }
+    int max_tiles() const { return maxTiles_; }
+    int used_tiles() const { return (int)tiles_.size(); }
+
+    bool use_graphs = true;
+    bool trace = false;
+    std::vector<TraceRec> traces;
+    std::vector<int> traceStageBase;
+    long long launches = 0;  // kernels launched (eager) or executed (graph, counted per node)
+
+    int err = HOSONO_OK;
+    std::string msg;
+    int fail(int code, const char* fmt, ...);
+
+  private:
+    struct Slot {
+        bool live = false;
+        hosono_params p{};
+        InstDev dev{};
+        std::vector<void*> allocs;
+        int ntiles = 0;
+    };
+    class Rec;
+    friend class Rec;
+
+    Batch batch() const;
+    int upload_tables();
+    int write_state_field(int slot, size_t offset, const void* src, size_t n);
+    template <typename T>
+    int write_field(int slot, T InstState::*field, T value) {
+        const InstState* z = nullptr;
+        return write_state_field(slot, (size_t)((const char*)&(z->*field) - (const char*)z), &value, sizeof(T));
+    }
+    int record_stage(Rec& r, int uin, int uout, cudaEvent_t ev0, cudaEvent_t ev1);
+    int record_step(Rec& r, bool host_dt, cudaGraphConditionalHandle run_cond, bool profile);
+    int build_graphs();
+    int launch(cudaGraphExec_t g);
+    int sync();
+    int check_errors();
+    int trace_before_pass();
+    int trace_after_pass();
+
+    const KernelSet* K_ = nullptr;
+    cudaStream_t s_ = nullptr;
+    int maxInst_ = 0, maxTiles_ = 0;
+    InstDev* d_dev_ = nullptr;
+    InstState* d_st_ = nullptr;
+    int4* d_tiles_ = nullptr;
+    int* d_ntiles_ = nullptr;
+    BatchFlags* d_flags_ = nullptr;
+    BatchFlags* h_flags_ = nullptr;  // pinned
+    InstState* h_st_ = nullptr;      // pinned
+    double* staging_ = nullptr;
+    size_t stagingCells_ = 0;
+    int* schemeInt_ = nullptr;
+    std::vector<Slot> slots_;
+    std::vector<int4> tiles_;
+    cudaGraphExec_t gAdvance_ = nullptr, gRun_ = nullptr, gProf_ = nullptr;
+    cudaEvent_t profEv_[6] = {};
+    std::vector<long long> tracePassesSeen_;
+};
+
+}  // namespace hosono

@@ -1,353 +1,77 @@
-// hosono_gpu.cu -- device instance, MOOD-loop orchestration and the C ABI of
-// include/hosono_gpu.h.
+// hosono_gpu.cu -- the C ABI of include/hosono_gpu.h over the batched engine.
 //
-// One handle = one block (gridBlock_t + gridState_t of the reference) resident
-// in HBM.  The forward-Euler stage follows timeStep.f90:45-130: every pass
-// reconstructs, fluxes, corrects (FLICD), updates and detects the flagged
-// cells until detect lowers nothing; the face cascade of reconstruct.f90:73-173
-// runs inside each pass until every high-order face state is admissible.
+// hosono_gpu_* : one block (the reference's grid_block + grid_state), i.e. an
+//                engine holding one instance.
+// hosono_batch_*: many independent blocks of any sizes advanced together.
 
+#include "engine_host.h"
 #include "hosono_gpu.h"
-#include "kernels.h"
-
-#include <cuda_runtime.h>
 
 #include <cmath>
-#include <cstdlib>
-#include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <new>
-#include <string>
-#include <utility>
-#include <vector>
 
 using namespace hosono;
 
-namespace {
-
-struct TraceRec {
-    int stage, pass, nInner, nDetect;
-    std::vector<unsigned char> inner, detect;  // Fortran order (i fastest), nxt*nyt
-};
-
-}  // namespace
-
 struct hosono_handle {
-    hosono_params p{};
-    Geo geo{};
-    Phys phys{};
-    const KernelTable* kt = nullptr;
-    cudaStream_t stream = nullptr;
-    int device = 0;
-    size_t ncellp = 0;  // pitch * nyt
-    // state and stage buffers (SoA planes)
-    double *Un = nullptr, *A = nullptr, *B = nullptr, *V = nullptr;
-    double *FX = nullptr, *FY = nullptr, *CTX = nullptr, *CTY = nullptr;
-    double *pv = nullptr, *qw = nullptr;
-    double* staging = nullptr;  // AoS <-> SoA conversions
-    int* scheme_int = nullptr;
-    int8_t *scheme = nullptr, *scheme_next = nullptr;
-    uint8_t *rec = nullptr, *recF = nullptr, *rrRec = nullptr, *fail = nullptr, *failX = nullptr, *failY = nullptr;
-    uint8_t *nextPass = nullptr, *dirty = nullptr, *lowered = nullptr, *innerCount = nullptr;
-    int* counters = nullptr;
-    int* h_counters = nullptr;  // pinned
-    unsigned long long* cflbits = nullptr;
-    unsigned long long* h_cflbits = nullptr;  // pinned
-    std::vector<void*> allocations;
+    Engine eng;
+    int slot = 0;
     hosono_stats stats{};
-    // launch accounting / pass-1 timing
-    long long launches = 0;
     bool profile = false;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    bool evPending = false;
     double pass1Ms = 0.0;
     long long pass1Count = 0;
-    bool trace = false;
-    int traceStage = 0;
-    std::vector<TraceRec> traces;
-    int err = HOSONO_OK;
-    std::string msg;
+};
+
+struct hosono_batch {
+    Engine eng;
 };
 
 namespace {
 
-int set_err(hosono_handle* h, int code, const char* fmt, ...) {
-    char buf[512];
-    va_list ap;
-    va_start(ap, fmt);
-    std::vsnprintf(buf, sizeof buf, fmt, ap);
-    va_end(ap);
-    if (h) {
-        h->err = code;
-        h->msg = buf;
+// the kernels hard-code the stencil order of GP.f90:85-95; check the table
+bool stencil_ok(int R, const int* stenc) {
+    if (!stenc) return true;
+    const int nsMax = 1 + 2 * R * (R + 1);
+    for (int rr = 1; rr <= R; rr++) {
+        int k = 0;
+        for (int a = -rr; a <= rr; a++)
+            for (int b = -rr; b <= rr; b++)
+                if (std::abs(a) + std::abs(b) <= rr) {
+                    if (stenc[0 + 2 * (k + nsMax * (rr - 1))] != a || stenc[1 + 2 * (k + nsMax * (rr - 1))] != b)
+                        return false;
+                    k++;
+                }
     }
-    return code;
+    return true;
 }
 
-#define CU(h, call)                                                                                   \
-    do {                                                                                              \
-        cudaError_t e_ = (call);                                                                      \
-        if (e_ != cudaSuccess)                                                                        \
-            return set_err((h), HOSONO_ECUDA, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), \
-                           __FILE__, __LINE__);                                                       \
-    } while (0)
-
-template <typename T>
-int dalloc(hosono_handle* h, T** p, size_t count) {
-    void* q = nullptr;
-    cudaError_t e = cudaMalloc(&q, count * sizeof(T));
-    if (e != cudaSuccess) {
-        cudaGetLastError();
-        return set_err(h, HOSONO_ENOMEM, "cudaMalloc of %zu bytes failed: %s", count * sizeof(T),
-                       cudaGetErrorString(e));
-    }
-    h->allocations.push_back(q);
-    *p = static_cast<T*>(q);
-    return HOSONO_OK;
+// the checks Engine::add repeats, done before any CUDA call
+bool params_ok(const hosono_params& p) {
+    const int R = p.max_radius;
+    return R >= 1 && R <= 3 && p.ngc == R + 2 && p.nx >= 2 * p.ngc && p.ny >= 2 * p.ngc &&
+           (p.bc == HOSONO_BC_OUTFLOW || p.bc == HOSONO_BC_PERIODIC) && p.riemann_solver == 1 && p.dx > 0 &&
+           p.dy > 0;
 }
 
-StageArgs stage_args(hosono_handle* h, const double* Uin, double* Uout, double dt) {
-    StageArgs a{};
-    a.geo = h->geo;
-    a.phys = h->phys;
-    a.pv = h->pv;
-    a.qw = h->qw;
-    a.Uin = Uin;
-    a.Uout = Uout;
-    a.FX = h->FX;
-    a.FY = h->FY;
-    a.CTX = h->CTX;
-    a.CTY = h->CTY;
-    a.scheme = h->scheme;
-    a.scheme_next = h->scheme_next;
-    a.rec = h->rec;
-    a.recF = h->recF;
-    a.rrRec = h->rrRec;
-    a.fail = h->fail;
-    a.failX = h->failX;
-    a.failY = h->failY;
-    a.nextPass = h->nextPass;
-    a.dirty = h->dirty;
-    a.lowered = h->lowered;
-    a.innerCount = h->innerCount;
-    a.counters = h->counters;
-    a.dt = dt;
-    a.trace = h->trace ? 1 : 0;
-    return a;
+hosono_stats stats_delta(const InstState& a, const InstState& b) {
+    hosono_stats s{};
+    s.stages = b.stages - a.stages;
+    s.mood_passes = b.passesTotal - a.passesTotal;
+    s.max_passes = b.maxPasses;
+    s.detect_lowered = b.detectTotal - a.detectTotal;
+    s.inner_lowered = b.innerTotal - a.innerTotal;
+    s.cascade_iters = b.cascadeIters - a.cascadeIters;
+    return s;
 }
 
-int read_counters(hosono_handle* h) {
-    CU(h, cudaMemcpyAsync(h->h_counters, h->counters, sizeof(int) * CNT_N, cudaMemcpyDeviceToHost, h->stream));
-    CU(h, cudaStreamSynchronize(h->stream));
-    return HOSONO_OK;
-}
-
-int check_launch(hosono_handle* h, const char* what) {
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return set_err(h, HOSONO_ECUDA, "launch of %s failed: %s", what, cudaGetErrorString(e));
-    return HOSONO_OK;
-}
-
-#define LAUNCH(h, what, stmt)                  \
-    do {                                       \
-        stmt;                                  \
-        (h)->launches++;                       \
-        int rc_ = check_launch((h), (what));   \
-        if (rc_) return rc_;                   \
-    } while (0)
-
-// accumulate the pass-1 kernel time once its bracketing events completed
-int harvest_profile(hosono_handle* h) {
-    if (!h->evPending) return HOSONO_OK;
-    float ms = 0.f;
-    CU(h, cudaEventSynchronize(h->ev1));
-    CU(h, cudaEventElapsedTime(&ms, h->ev0, h->ev1));
-    h->pass1Ms += ms;
-    h->pass1Count++;
-    h->evPending = false;
-    return HOSONO_OK;
-}
-
-#define TRY(x)              \
-    do {                    \
-        int rc_ = (x);      \
-        if (rc_) return rc_; \
-    } while (0)
-
-int record_trace(hosono_handle* h, int stage, int pass, int nInner, int nDetect) {
-    const Geo& G = h->geo;
-    TraceRec t;
-    t.stage = stage;
-    t.pass = pass;
-    t.nInner = nInner;
-    t.nDetect = nDetect;
-    std::vector<unsigned char> a(h->ncellp), b(h->ncellp);
-    CU(h, cudaMemcpyAsync(a.data(), h->innerCount, h->ncellp, cudaMemcpyDeviceToHost, h->stream));
-    CU(h, cudaMemcpyAsync(b.data(), h->lowered, h->ncellp, cudaMemcpyDeviceToHost, h->stream));
-    CU(h, cudaStreamSynchronize(h->stream));
-    t.inner.resize((size_t)G.nxt * G.nyt);
-    t.detect.resize((size_t)G.nxt * G.nyt);
-    for (int j = 0; j < G.nyt; j++)
-        for (int i = 0; i < G.nxt; i++) {
-            t.inner[(size_t)j * G.nxt + i] = a[(size_t)j * G.pitch + i];
-            t.detect[(size_t)j * G.nxt + i] = b[(size_t)j * G.pitch + i];
-        }
-    h->traces.push_back(std::move(t));
-    return HOSONO_OK;
-}
-
-// timeStep_forwardEuler (timeStep.f90:45-130): Uin (guards filled) -> Uout (interior)
-int forward_euler(hosono_handle* h, const double* Uin, double* Uout, double dt) {
-    const Geo& G = h->geo;
-    const KernelTable* K = h->kt;
-    cudaStream_t s = h->stream;
-    const size_t n = h->ncellp;
-    const uint8_t rrAll = (uint8_t)(G.R | (G.R << 2) | (G.R << 4) | (G.R << 6));
-    // scheme = R, recompute = recomputeFLICD = .true. on every cell (:79-81)
-    CU(h, cudaMemsetAsync(h->scheme, G.R, n, s));
-    CU(h, cudaMemsetAsync(h->rec, 1, n, s));
-    CU(h, cudaMemsetAsync(h->recF, 1, n, s));
-    CU(h, cudaMemsetAsync(h->rrRec, rrAll, n, s));
-    CU(h, cudaMemsetAsync(h->dirty, 0, n, s));
-    const int stage = h->traceStage++;
-    const long long passCap = (long long)G.R * G.nx * G.ny + 2;
-    const long long innerCap = (long long)G.R * (G.nx + 4) * (G.ny + 4) + 2;
-    int pass = 0;
-    for (;;) {
-        if (pass >= passCap) return set_err(h, HOSONO_EMOODCAP, "MOOD loop exceeded %lld passes", passCap);
-        CU(h, cudaMemsetAsync(h->counters, 0, sizeof(int) * CNT_N, s));
-        if (h->trace) CU(h, cudaMemsetAsync(h->innerCount, 0, n, s));
-        StageArgs a = stage_args(h, Uin, Uout, dt);
-        // reconstruct_faceValsWithGP, first inner pass
-        if (pass == 0) {
-            if (h->profile) CU(h, cudaEventRecord(h->ev0, s));
-            LAUNCH(h, "face_pass1", K->face_pass1(a, s));
-            if (h->profile) {
-                CU(h, cudaEventRecord(h->ev1, s));
-                h->evPending = true;
-            }
-        } else {
-            CU(h, cudaMemsetAsync(h->fail, 0, n, s));
-            LAUNCH(h, "recon_check", K->recon_check(a, h->rec, s));
-        }
-        TRY(read_counters(h));
-        TRY(harvest_profile(h));
-        // inner cascade (reconstruct.f90:146-171)
-        bool cascaded = false;
-        int mode = pass == 0 ? CASCADE_FROM_FACES : CASCADE_FROM_CELLS;
-        long long iters = 0;
-        while (h->h_counters[CNT_ANYFAIL]) {
-            if (++iters > innerCap) return set_err(h, HOSONO_EMOODCAP, "face cascade exceeded %lld passes", innerCap);
-            cascaded = true;
-            CU(h, cudaMemsetAsync(h->nextPass, 0, n, s));
-            LAUNCH(h, "cascade_lower", K->cascade_lower(a, mode, s));
-            CU(h, cudaMemsetAsync(h->fail, 0, n, s));
-            CU(h, cudaMemsetAsync(h->counters + CNT_ANYFAIL, 0, sizeof(int), s));
-            LAUNCH(h, "recon_check", K->recon_check(a, h->nextPass, s));
-            TRY(read_counters(h));
-            mode = CASCADE_FROM_CELLS;
-            h->stats.cascade_iters++;
-        }
-        // getFluxes_
-        if (pass == 0) {
-            if (cascaded) LAUNCH(h, "flux", K->flux(a, FLUX_DIRTY, s));
-        } else {
-            LAUNCH(h, "flux", K->flux(a, FLUX_REC, s));
-        }
-        // FLICD + update + detect_ALL + applyMOOD
-        CU(h, cudaMemsetAsync(h->lowered, 0, n, s));
-        LAUNCH(h, "ct_update_detect", K->ct_update_detect(a, s));
-        LAUNCH(h, "mood_flags", K->mood_flags(a, s));
-        std::swap(h->scheme, h->scheme_next);
-        TRY(read_counters(h));
-        const int nInner = h->h_counters[CNT_INNER], nDetect = h->h_counters[CNT_DETECT];
-        h->stats.inner_lowered += nInner;
-        h->stats.detect_lowered += nDetect;
-        if (h->trace) TRY(record_trace(h, stage, pass, nInner, nDetect));
-        pass++;
-        if (nDetect == 0) break;
-    }
-    h->stats.stages++;
-    h->stats.mood_passes += pass;
-    if (pass > h->stats.max_passes) h->stats.max_passes = pass;
-    return HOSONO_OK;
-}
-
-// timeStep_advanceSolution + timeStep_RK3 (timeStep.f90:22-43, :132-171)
-int advance(hosono_handle* h, double dt) {
-    const Geo& G = h->geo;
-    const KernelTable* K = h->kt;
-    cudaStream_t s = h->stream;
-    h->stats = hosono_stats{};
-    TRY(forward_euler(h, h->Un, h->A, dt));                     // U1 = FE(U)
-    LAUNCH(h, "bc_fill", K->bc_fill(G, h->A, NCONS, s));        // BC(U1)
-    TRY(forward_euler(h, h->A, h->B, dt));                      // U2 = FE(U1)
-    LAUNCH(h, "rk_combine2", K->rk_combine2(G, h->Un, h->B, h->A, s));  // U2 = (3U+U2)/4, BC
-    TRY(forward_euler(h, h->A, h->B, dt));                      // U3 = FE(U2)
-    LAUNCH(h, "rk_final", K->rk_final(G, h->phys, h->Un, h->B, h->A, h->V, s));  // (U+2U3)/3, V, BC
-    std::swap(h->Un, h->A);
-    return HOSONO_OK;
-}
-
-int cfl(hosono_handle* h, double* dt) {
-    CU(h, cudaMemsetAsync(h->cflbits, 0, 2 * sizeof(unsigned long long), h->stream));
-    LAUNCH(h, "cfl_max", h->kt->cfl_max(h->geo, h->phys, h->V, h->cflbits, h->stream));
-    CU(h, cudaMemcpyAsync(h->h_cflbits, h->cflbits, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
-                          h->stream));
-    CU(h, cudaStreamSynchronize(h->stream));
-    double xm, ym;
-    std::memcpy(&xm, &h->h_cflbits[0], sizeof(double));
-    std::memcpy(&ym, &h->h_cflbits[1], sizeof(double));
-    // cfl.f90:50
-    *dt = h->p.cfl * std::fmin(h->geo.dx / xm, h->geo.dy / ym);
-    return HOSONO_OK;
-}
-
-int upload(hosono_handle* h, const double* U, const double* V) {
-    const Geo& G = h->geo;
-    const size_t cells = (size_t)G.nxt * G.nyt;
-    CU(h, cudaMemcpyAsync(h->staging, U, cells * NCONS * sizeof(double), cudaMemcpyHostToDevice, h->stream));
-    LAUNCH(h, "aos_to_soa", launch_aos_to_soa(G, h->staging, h->Un, NCONS, h->stream));
-    if (V) {
-        CU(h, cudaMemcpyAsync(h->staging, V, cells * NPRIM * sizeof(double), cudaMemcpyHostToDevice, h->stream));
-        LAUNCH(h, "aos_to_soa", launch_aos_to_soa(G, h->staging, h->V, NPRIM, h->stream));
-    } else {
-        LAUNCH(h, "cons2prim_all", h->kt->cons2prim_all(G, h->phys, h->Un, h->V, h->stream));
-    }
-    CU(h, cudaStreamSynchronize(h->stream));
-    return HOSONO_OK;
-}
-
-int download(hosono_handle* h, double* U, double* V, int* scheme) {
-    const Geo& G = h->geo;
-    const size_t cells = (size_t)G.nxt * G.nyt;
-    if (U) {
-        LAUNCH(h, "soa_to_aos", launch_soa_to_aos(G, h->Un, h->staging, NCONS, h->stream));
-        CU(h, cudaMemcpyAsync(U, h->staging, cells * NCONS * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-        CU(h, cudaStreamSynchronize(h->stream));
-    }
-    if (V) {
-        LAUNCH(h, "soa_to_aos", launch_soa_to_aos(G, h->V, h->staging, NPRIM, h->stream));
-        CU(h, cudaMemcpyAsync(V, h->staging, cells * NPRIM * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-        CU(h, cudaStreamSynchronize(h->stream));
-    }
-    if (scheme) {
-        LAUNCH(h, "scheme_to_int", launch_scheme_to_int(G, h->scheme, h->scheme_int, h->stream));
-        CU(h, cudaMemcpyAsync(scheme, h->scheme_int, cells * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
-        CU(h, cudaStreamSynchronize(h->stream));
-    }
-    return HOSONO_OK;
-}
-
-void release(hosono_handle* h) {
-    for (void* p : h->allocations) cudaFree(p);
-    h->allocations.clear();
-    if (h->ev0) cudaEventDestroy(h->ev0);
-    if (h->ev1) cudaEventDestroy(h->ev1);
-    if (h->h_counters) cudaFreeHost(h->h_counters);
-    if (h->h_cflbits) cudaFreeHost(h->h_cflbits);
-    if (h->stream) cudaStreamDestroy(h->stream);
+// kernels one graph execution launched, from the work counters: per step 4
+// time-loop kernels (cfl path) or 1 (host dt), 3 RK kernels; per stage 7;
+// per cascade iteration 4; per further MOOD pass 6.
+long long graph_launches(const hosono_stats& s, int steps, bool host_dt) {
+    return (long long)steps * ((host_dt ? 1 : 4) + 3) + 7LL * s.stages + 4LL * s.cascade_iters +
+           6LL * (s.mood_passes - s.stages);
 }
 
 }  // namespace
@@ -358,155 +82,99 @@ int hosono_gpu_create(const hosono_params* p, const double* pv, const double* qw
                       hosono_handle** out) {
     if (!p || !pv || !qw || !out) return HOSONO_EINVAL;
     *out = nullptr;
-    const int R = p->max_radius;
-    if (R < 1 || R > 3) return HOSONO_EINVAL;
-    if (p->ngc != R + 2) return HOSONO_EINVAL;
-    if (p->nx < 2 * p->ngc || p->ny < 2 * p->ngc) return HOSONO_EINVAL;  // periodic images must not overlap
-    if (p->bc != HOSONO_BC_OUTFLOW && p->bc != HOSONO_BC_PERIODIC) return HOSONO_EINVAL;
-    if (p->riemann_solver != 1) return HOSONO_EINVAL;
-    if (!(p->dx > 0) || !(p->dy > 0)) return HOSONO_EINVAL;
-    if (stenc) {  // the kernels hard-code the stencil order of GP.f90:85-95; check it
-        const int nsMax = 1 + 2 * R * (R + 1);
-        for (int rr = 1; rr <= R; rr++) {
-            int k = 0;
-            for (int a = -rr; a <= rr; a++)
-                for (int b = -rr; b <= rr; b++)
-                    if (std::abs(a) + std::abs(b) <= rr) {
-                        if (stenc[0 + 2 * (k + nsMax * (rr - 1))] != a || stenc[1 + 2 * (k + nsMax * (rr - 1))] != b)
-                            return HOSONO_EINVAL;
-                        k++;
-                    }
-        }
-    }
+    if (!params_ok(*p) || !stencil_ok(p->max_radius, stenc)) return HOSONO_EINVAL;
     hosono_handle* h = new (std::nothrow) hosono_handle();
     if (!h) return HOSONO_ENOMEM;
-    h->p = *p;
-    h->kt = p->fp_mode == HOSONO_FP_FAST ? kernels_fast() : kernels_strict();
-    Geo& G = h->geo;
-    G.nx = p->nx;
-    G.ny = p->ny;
-    G.g = p->ngc;
-    G.nxt = p->nx + 2 * p->ngc;
-    G.nyt = p->ny + 2 * p->ngc;
-    G.pitch = (G.nxt + 31) / 32 * 32;
-    G.plane = (long long)G.pitch * G.nyt;
-    G.R = R;
-    G.bc = p->bc;
-    G.nsMax = 1 + 2 * R * (R + 1);
-    G.nqMax = R + 1;
-    G.dx = p->dx;
-    G.dy = p->dy;
-    G.mindxdy = p->mindxdy;
-    G.maxdxdy = p->maxdxdy;
-    h->phys.gamma = p->gamma;
-    h->phys.small_pressure = p->small_pressure;
-    h->phys.small_density = p->small_density;
-    h->phys.force_hydro = p->force_hydro ? 1 : 0;
-    h->ncellp = (size_t)G.plane;
-    const size_t n = h->ncellp;
-    const size_t cells = (size_t)G.nxt * G.nyt;
-    int rc = HOSONO_OK;
-    auto fail = [&](int code) {
-        release(h);
+    int rc = h->eng.init(1, h->eng.tiles_of(*p), p->fp_mode);
+    if (!rc) rc = h->eng.add(*p, pv, qw, &h->slot);
+    if (rc) {
         delete h;
-        return code;
-    };
-    if (cudaGetDevice(&h->device) != cudaSuccess) return fail(HOSONO_ECUDA);
-    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) return fail(HOSONO_ECUDA);
-    if ((rc = dalloc(h, &h->Un, n * NCONS)) || (rc = dalloc(h, &h->A, n * NCONS)) ||
-        (rc = dalloc(h, &h->B, n * NCONS)) || (rc = dalloc(h, &h->V, n * NPRIM)) ||
-        (rc = dalloc(h, &h->FX, n * NCONS)) || (rc = dalloc(h, &h->FY, n * NCONS)) ||
-        (rc = dalloc(h, &h->CTX, n)) || (rc = dalloc(h, &h->CTY, n)) ||
-        (rc = dalloc(h, &h->pv, (size_t)G.nsMax * G.nqMax * 4 * R)) || (rc = dalloc(h, &h->qw, (size_t)G.nqMax * R)) ||
-        (rc = dalloc(h, &h->staging, cells * NPRIM)) || (rc = dalloc(h, &h->scheme_int, cells)) ||
-        (rc = dalloc(h, &h->scheme, n)) || (rc = dalloc(h, &h->scheme_next, n)) || (rc = dalloc(h, &h->rec, n)) ||
-        (rc = dalloc(h, &h->recF, n)) || (rc = dalloc(h, &h->rrRec, n)) || (rc = dalloc(h, &h->fail, n)) ||
-        (rc = dalloc(h, &h->failX, n)) || (rc = dalloc(h, &h->failY, n)) || (rc = dalloc(h, &h->nextPass, n)) ||
-        (rc = dalloc(h, &h->dirty, n)) || (rc = dalloc(h, &h->lowered, n)) || (rc = dalloc(h, &h->innerCount, n)) ||
-        (rc = dalloc(h, &h->counters, CNT_N)) || (rc = dalloc(h, &h->cflbits, 2)))
-        return fail(rc);
-    if (cudaMallocHost(&h->h_counters, sizeof(int) * CNT_N) != cudaSuccess) return fail(HOSONO_ENOMEM);
-    if (cudaMallocHost(&h->h_cflbits, sizeof(unsigned long long) * 2) != cudaSuccess) return fail(HOSONO_ENOMEM);
-    // every plane starts zeroed, like gridBlock_alloc / gridState_alloc
-    for (void* q : {(void*)h->Un, (void*)h->A, (void*)h->B, (void*)h->FX, (void*)h->FY})
-        if (cudaMemsetAsync(q, 0, n * NCONS * sizeof(double), h->stream) != cudaSuccess) return fail(HOSONO_ECUDA);
-    if (cudaMemsetAsync(h->V, 0, n * NPRIM * sizeof(double), h->stream) != cudaSuccess) return fail(HOSONO_ECUDA);
-    if (cudaMemsetAsync(h->CTX, 0, n * sizeof(double), h->stream) != cudaSuccess) return fail(HOSONO_ECUDA);
-    if (cudaMemsetAsync(h->CTY, 0, n * sizeof(double), h->stream) != cudaSuccess) return fail(HOSONO_ECUDA);
-    for (uint8_t* q : {(uint8_t*)h->scheme, (uint8_t*)h->scheme_next, h->rec, h->recF, h->rrRec, h->fail, h->failX,
-                       h->failY, h->nextPass, h->dirty, h->lowered, h->innerCount})
-        if (cudaMemsetAsync(q, 0, n, h->stream) != cudaSuccess) return fail(HOSONO_ECUDA);
-    if (cudaMemcpyAsync(h->pv, pv, sizeof(double) * G.nsMax * G.nqMax * 4 * R, cudaMemcpyHostToDevice, h->stream) !=
-            cudaSuccess ||
-        cudaMemcpyAsync(h->qw, qw, sizeof(double) * G.nqMax * R, cudaMemcpyHostToDevice, h->stream) != cudaSuccess)
-        return fail(HOSONO_ECUDA);
-    if (cudaStreamSynchronize(h->stream) != cudaSuccess) return fail(HOSONO_ECUDA);
+        return rc;
+    }
     *out = h;
     return HOSONO_OK;
 }
 
 int hosono_gpu_destroy(hosono_handle* h) {
-    if (!h) return HOSONO_OK;
-    cudaStreamSynchronize(h->stream);
-    release(h);
     delete h;
     return HOSONO_OK;
 }
 
 int hosono_gpu_upload(hosono_handle* h, const double* U, const double* V) {
     if (!h || !U) return HOSONO_EINVAL;
-    return upload(h, U, V);
+    return h->eng.upload(h->slot, U, V);
 }
 
 int hosono_gpu_download(hosono_handle* h, double* U, double* V, int* scheme) {
     if (!h) return HOSONO_EINVAL;
-    return download(h, U, V, scheme);
+    return h->eng.download(h->slot, U, V, scheme);
 }
 
 int hosono_gpu_cfl(hosono_handle* h, double* dt) {
     if (!h || !dt) return HOSONO_EINVAL;
-    return cfl(h, dt);
+    return h->eng.cfl(h->slot, dt);
 }
 
 int hosono_gpu_advance(hosono_handle* h, double dt) {
     if (!h) return HOSONO_EINVAL;
-    if (!(dt >= 0.0) || !std::isfinite(dt)) return set_err(h, HOSONO_ENANDT, "dt = %g is not a valid time step", dt);
-    TRY(advance(h, dt));
-    CU(h, cudaStreamSynchronize(h->stream));
+    InstState a, b;
+    int rc = h->eng.state(h->slot, &a);
+    if (!rc) rc = h->eng.advance(h->slot, dt);
+    if (!rc) rc = h->eng.state(h->slot, &b);
+    if (!rc) {
+        h->stats = stats_delta(a, b);
+        if (h->eng.use_graphs && !h->eng.trace) h->eng.launches += graph_launches(h->stats, 1, true);
+    }
+    return rc;
+}
+
+int hosono_gpu_set_time(hosono_handle* h, double t, double tmax, int nstep, int nstepmax) {
+    if (!h) return HOSONO_EINVAL;
+    return h->eng.set_time(h->slot, t, tmax, nstep, nstepmax);
+}
+
+int hosono_gpu_step(hosono_handle* h, int max_steps, double* t_out, int* nstep_out) {
+    if (!h) return HOSONO_EINVAL;
+    InstState a, b;
+    int rc = h->eng.state(h->slot, &a);
+    if (rc) return rc;
+    if (h->profile) {
+        for (int k = 0; k < (max_steps > 0 ? max_steps : 1) && !rc; k++) {
+            InstState c;
+            rc = h->eng.state(h->slot, &c);
+            if (rc || c.done) break;
+            double ms = 0;
+            int n = 0;
+            rc = h->eng.run_profiled_step(&ms, &n);
+            h->pass1Ms += ms;
+            h->pass1Count += n;
+        }
+    } else {
+        rc = h->eng.run(max_steps);
+    }
+    if (rc) return rc;
+    rc = h->eng.state(h->slot, &b);
+    if (rc) return rc;
+    h->stats = stats_delta(a, b);
+    if (h->eng.use_graphs && !h->eng.trace) h->eng.launches += graph_launches(h->stats, b.nstep - a.nstep, false);
+    if (t_out) *t_out = b.t;
+    if (nstep_out) *nstep_out = b.nstep;
     return HOSONO_OK;
 }
 
 int hosono_gpu_run(hosono_handle* h, double tmax, int nstepmax, int max_steps, double* t_out, int* nstep_out) {
     if (!h) return HOSONO_EINVAL;
-    int nStep = 0;
-    double t = 0.0;
-    int rc = HOSONO_OK;
-    while ((t < tmax) && (nStep < nstepmax)) {
-        if (max_steps > 0 && nStep >= max_steps) break;
-        double dt = 0;
-        if ((rc = cfl(h, &dt))) break;
-        // validTimeStep (mhd_driver.f90:239-266): clamp first, then check
-        if (t + dt > tmax)
-            dt = tmax - t;
-        else if (dt < 0.0 || std::isnan(dt) || !std::isfinite(dt)) {
-            rc = set_err(h, HOSONO_ENANDT, "dt = %g is not a valid time step", dt);
-            break;
-        }
-        if ((rc = advance(h, dt))) break;
-        t = t + dt;
-        nStep = nStep + 1;
-    }
-    if (!rc && cudaStreamSynchronize(h->stream) != cudaSuccess) rc = set_err(h, HOSONO_ECUDA, "stream sync failed");
-    if (t_out) *t_out = t;
-    if (nstep_out) *nstep_out = nStep;
-    return rc;
+    int rc = h->eng.set_time(h->slot, 0.0, tmax, 0, nstepmax);
+    if (rc) return rc;
+    return hosono_gpu_step(h, max_steps, t_out, nstep_out);
 }
 
 int hosono_gpu_advance_host(hosono_handle* h, double dt, double* U, double* V) {
     if (!h || !U) return HOSONO_EINVAL;
-    TRY(upload(h, U, V));
-    TRY(hosono_gpu_advance(h, dt));
-    return download(h, U, V, nullptr);
+    int rc = h->eng.upload(h->slot, U, V);
+    if (!rc) rc = hosono_gpu_advance(h, dt);
+    if (!rc) rc = h->eng.download(h->slot, U, V, nullptr);
+    return rc;
 }
 
 int hosono_gpu_stats(hosono_handle* h, hosono_stats* s) {
@@ -517,19 +185,19 @@ int hosono_gpu_stats(hosono_handle* h, hosono_stats* s) {
 
 int hosono_gpu_last_error(hosono_handle* h, char* buf, int len) {
     if (!h) return HOSONO_EINVAL;
-    if (buf && len > 0) std::snprintf(buf, (size_t)len, "%s", h->msg.c_str());
-    return h->err;
+    if (buf && len > 0) std::snprintf(buf, (size_t)len, "%s", h->eng.msg.c_str());
+    return h->eng.err;
 }
 
 int hosono_gpu_trace_enable(hosono_handle* h, int on) {
     if (!h) return HOSONO_EINVAL;
-    h->trace = on != 0;
+    h->eng.trace = on != 0;
     return HOSONO_OK;
 }
-int hosono_gpu_trace_count(hosono_handle* h) { return h ? (int)h->traces.size() : 0; }
+int hosono_gpu_trace_count(hosono_handle* h) { return h ? (int)h->eng.traces.size() : 0; }
 int hosono_gpu_trace_get(hosono_handle* h, int k, int* meta, unsigned char* inner, unsigned char* detect) {
-    if (!h || k < 0 || k >= (int)h->traces.size()) return HOSONO_EINVAL;
-    const TraceRec& t = h->traces[k];
+    if (!h || k < 0 || k >= (int)h->eng.traces.size()) return HOSONO_EINVAL;
+    const TraceRec& t = h->eng.traces[k];
     if (meta) {
         meta[0] = t.stage;
         meta[1] = t.pass;
@@ -542,16 +210,22 @@ int hosono_gpu_trace_get(hosono_handle* h, int k, int* meta, unsigned char* inne
 }
 int hosono_gpu_trace_clear(hosono_handle* h) {
     if (!h) return HOSONO_EINVAL;
-    h->traces.clear();
-    h->traceStage = 0;
-    return HOSONO_OK;
+    h->eng.traces.clear();
+    InstState st;
+    int rc = h->eng.state(h->slot, &st);
+    if (!rc) h->eng.traceStageBase[h->slot] = st.stages;
+    return rc;
 }
 
 int hosono_gpu_state_layout(hosono_handle* h, double** U_dev, int* pitch, long long* plane) {
     if (!h) return HOSONO_EINVAL;
-    if (U_dev) *U_dev = h->Un;
-    if (pitch) *pitch = h->geo.pitch;
-    if (plane) *plane = h->geo.plane;
+    InstState st;
+    int rc = h->eng.state(h->slot, &st);
+    if (rc) return rc;
+    const Geo& G = h->eng.geo(h->slot);
+    if (pitch) *pitch = G.pitch;
+    if (plane) *plane = G.plane;
+    if (U_dev) *U_dev = h->eng.dev(h->slot).U[st.parity];
     return HOSONO_OK;
 }
 
@@ -561,22 +235,22 @@ int hosono_gpu_build_info(int* sm_arch, int* has_fast_mode) {
     return HOSONO_OK;
 }
 
-int hosono_gpu_set_device(int device) {
-    return cudaSetDevice(device) == cudaSuccess ? HOSONO_OK : HOSONO_ECUDA;
-}
+int hosono_gpu_set_device(int device) { return cudaSetDevice(device) == cudaSuccess ? HOSONO_OK : HOSONO_ECUDA; }
 
 int hosono_gpu_stream(hosono_handle* h, void** stream) {
     if (!h || !stream) return HOSONO_EINVAL;
-    *stream = (void*)h->stream;
+    *stream = (void*)h->eng.stream();
+    return HOSONO_OK;
+}
+
+int hosono_gpu_set_graphs(hosono_handle* h, int on) {
+    if (!h) return HOSONO_EINVAL;
+    h->eng.use_graphs = on != 0;
     return HOSONO_OK;
 }
 
 int hosono_gpu_profile(hosono_handle* h, int on) {
     if (!h) return HOSONO_EINVAL;
-    if (on && !h->ev0) {
-        CU(h, cudaEventCreate(&h->ev0));
-        CU(h, cudaEventCreate(&h->ev1));
-    }
     h->profile = on != 0;
     return HOSONO_OK;
 }
@@ -584,15 +258,124 @@ int hosono_gpu_profile(hosono_handle* h, int on) {
 int hosono_gpu_profile_read(hosono_handle* h, double* pass1_ms, long long* pass1_launches, long long* launches,
                             int reset) {
     if (!h) return HOSONO_EINVAL;
-    TRY(harvest_profile(h));
     if (pass1_ms) *pass1_ms = h->pass1Ms;
     if (pass1_launches) *pass1_launches = h->pass1Count;
-    if (launches) *launches = h->launches;
+    if (launches) *launches = h->eng.launches;
     if (reset) {
         h->pass1Ms = 0.0;
         h->pass1Count = 0;
-        h->launches = 0;
+        h->eng.launches = 0;
     }
+    return HOSONO_OK;
+}
+
+// ---------------------------------------------------------------- batches
+
+int hosono_batch_create(int max_instances, int max_tiles, int fp_mode, hosono_batch** out) {
+    if (!out || max_instances < 1 || max_tiles < 1) return HOSONO_EINVAL;
+    *out = nullptr;
+    hosono_batch* b = new (std::nothrow) hosono_batch();
+    if (!b) return HOSONO_ENOMEM;
+    int rc = b->eng.init(max_instances, max_tiles, fp_mode);
+    if (rc) {
+        delete b;
+        return rc;
+    }
+    *out = b;
+    return HOSONO_OK;
+}
+
+int hosono_batch_destroy(hosono_batch* b) {
+    delete b;
+    return HOSONO_OK;
+}
+
+int hosono_batch_tiles_for(const hosono_params* p) {
+    if (!p) return -1;
+    const int nxt = p->nx + 2 * p->ngc, nyt = p->ny + 2 * p->ngc;
+    return ((nxt + TILE_X - 1) / TILE_X) * ((nyt + TILE_Y - 1) / TILE_Y);
+}
+
+long long hosono_batch_instance_bytes(const hosono_params* p) {
+    if (!p) return -1;
+    Engine e;
+    return (long long)e.instance_bytes(*p);
+}
+
+int hosono_batch_add(hosono_batch* b, const hosono_params* p, const double* pv, const double* qw, const int* stenc,
+                     int* slot) {
+    if (!b || !p || !slot) return HOSONO_EINVAL;
+    if (!params_ok(*p) || !stencil_ok(p->max_radius, stenc)) return HOSONO_EINVAL;
+    return b->eng.add(*p, pv, qw, slot);
+}
+
+int hosono_batch_remove(hosono_batch* b, int slot) { return b ? b->eng.remove(slot) : HOSONO_EINVAL; }
+
+int hosono_batch_upload(hosono_batch* b, int slot, const double* U, const double* V) {
+    return b ? b->eng.upload(slot, U, V) : HOSONO_EINVAL;
+}
+
+int hosono_batch_download(hosono_batch* b, int slot, double* U, double* V, int* scheme) {
+    return b ? b->eng.download(slot, U, V, scheme) : HOSONO_EINVAL;
+}
+
+int hosono_batch_set_time(hosono_batch* b, int slot, double t, double tmax, int nstep, int nstepmax) {
+    return b ? b->eng.set_time(slot, t, tmax, nstep, nstepmax) : HOSONO_EINVAL;
+}
+
+int hosono_batch_run(hosono_batch* b, int max_steps) { return b ? b->eng.run(max_steps) : HOSONO_EINVAL; }
+
+int hosono_batch_status(hosono_batch* b, int slot, double* t, double* dt, int* nstep, int* done, int* error) {
+    if (!b) return HOSONO_EINVAL;
+    InstState st;
+    int rc = b->eng.state(slot, &st);
+    if (rc) return rc;
+    if (t) *t = st.t;
+    if (dt) *dt = st.dt;
+    if (nstep) *nstep = st.nstep;
+    if (done) *done = st.done;
+    if (error) *error = st.error;
+    return HOSONO_OK;
+}
+
+int hosono_batch_stats(hosono_batch* b, int slot, hosono_stats* s) {
+    if (!b || !s) return HOSONO_EINVAL;
+    InstState st;
+    int rc = b->eng.state(slot, &st);
+    if (rc) return rc;
+    s->stages = st.stages;
+    s->mood_passes = st.passesTotal;
+    s->max_passes = st.maxPasses;
+    s->detect_lowered = st.detectTotal;
+    s->inner_lowered = st.innerTotal;
+    s->cascade_iters = st.cascadeIters;
+    return HOSONO_OK;
+}
+
+int hosono_batch_stream(hosono_batch* b, void** stream) {
+    if (!b || !stream) return HOSONO_EINVAL;
+    *stream = (void*)b->eng.stream();
+    return HOSONO_OK;
+}
+
+int hosono_batch_set_graphs(hosono_batch* b, int on) {
+    if (!b) return HOSONO_EINVAL;
+    b->eng.use_graphs = on != 0;
+    return HOSONO_OK;
+}
+
+int hosono_batch_last_error(hosono_batch* b, char* buf, int len) {
+    if (!b) return HOSONO_EINVAL;
+    if (buf && len > 0) std::snprintf(buf, (size_t)len, "%s", b->eng.msg.c_str());
+    return b->eng.err;
+}
+
+int hosono_batch_capacity(hosono_batch* b, int* max_instances, int* max_tiles, int* used_tiles, int* live) {
+    if (!b) return HOSONO_EINVAL;
+    if (max_instances) *max_instances = b->eng.max_inst();
+    if (max_tiles) *max_tiles = b->eng.max_tiles();
+    if (used_tiles) *used_tiles = b->eng.used_tiles();
+    if (live) *live = b->eng.live_count();
     return HOSONO_OK;
 }
 

@@ -1,24 +1,25 @@
-// kernels.cu -- FP64 stage kernels of the hosono-2DMHD time step for sm_100a.
+// kernels.cu -- FP64 stage kernels of the hosono-2DMHD time step for sm_100a,
+// batched: every launch walks a list of 32x8 cell tiles that may belong to
+// any number of independent instances (engine.h).
 //
 // Compiled twice: with -DHOSONO_FAST=0 --fmad=false (strict: every operation
 // rounded on its own, bit-identical to the oracle) and with -DHOSONO_FAST=1
-// --fmad=true (FMA contraction allowed).  Each object exports one KernelTable.
+// --fmad=true (FMA contraction allowed).  Each object exports one KernelSet.
 //
 // Data layout in HBM: structure of arrays, one plane per conserved variable
 // (and per primitive variable for V), rows of `pitch` doubles (a multiple of
 // 32, i.e. 256-byte rows), guard cells included.  Cell (i,j) 0-based at
-// j*pitch+i; the interior is [g, g+nx) x [g, g+ny), g = NGC = R+2.
-// MOOD state is one byte per cell per flag.
+// j*pitch+i; the interior is [g, g+nx) x [g, g+ny), g = NGC = R+2.  MOOD
+// state is one byte per cell per flag.
 //
 // Index ranges (0-based) of the reference loops:
-//   reconstruct  [strt-2, stop+2]  -> [g-2, g+n+1]   (reconstruct.f90:81-82)
-//   getFluxes    [strt-1, stop+2]  -> [g-1, g+n+1]   (getFluxes.f90:204-205)
-//   FLICD        [strt,   stop+1]  -> [g,   g+n]     (FLICDdivB.f90:301-302)
-//   update/detect [strt,  stop]    -> [g,   g+n-1]   (timeStep.f90:108-109, detect.f90:81-82)
+//   reconstruct   [strt-2, stop+2] -> [g-2, g+n+1]   (reconstruct.f90:81-82)
+//   getFluxes     [strt-1, stop+2] -> [g-1, g+n+1]   (getFluxes.f90:204-205)
+//   FLICD         [strt,   stop+1] -> [g,   g+n]     (FLICDdivB.f90:301-302)
+//   update/detect [strt,   stop]   -> [g,   g+n-1]   (timeStep.f90:108-109, detect.f90:81-82)
 
-#include "kernels.h"
-
-#include <cstdio>
+#include "engine.h"
+#include "hosono_gpu.h"
 
 #ifndef HOSONO_FAST
 #error "HOSONO_FAST must be defined (0 strict, 1 fast)"
@@ -30,15 +31,36 @@
 #define KNS kstrict
 #endif
 
+// resident 256-thread blocks per SM the pass-1 register budget aims at
+#ifndef HOSONO_PASS1_MIN_BLOCKS
+#define HOSONO_PASS1_MIN_BLOCKS 2
+#endif
+
 namespace hosono {
 namespace KNS {
 
-constexpr int BX = 32, BY = 8;
+constexpr int NTHREADS = TILE_X * TILE_Y;
 
 __device__ __forceinline__ int iabs_c(int a) { return a < 0 ? -a : a; }
 
+// Tile prologue: the instance and cell a thread works on.  Returns false for
+// blocks past the tile count (uniform per block).
+struct Cell {
+    int k, i, j;
+};
+__device__ __forceinline__ bool tile_cell(const Batch& B, Cell& c) {
+    if ((int)blockIdx.x >= __ldg(B.ntiles)) return false;
+    const int4 t = B.tiles[blockIdx.x];
+    c.k = t.x;
+    c.i = t.y + threadIdx.x;
+    c.j = t.z + threadIdx.y;
+    return true;
+}
+// the one thread per instance that owns cell (0,0) (every instance has a tile at its origin)
+__device__ __forceinline__ bool first_tile_thread(const Cell& c) { return c.i == 0 && c.j == 0; }
+
 // GP prediction at quadrature point q of face f of cell (i,j), radius RR:
-// sum_k pv(k,q,f,RR) * U(:, stencil_k)  in stencil order k=1..ns
+// sum_k pv(k,q,f,RR) * U(:, stencil_k), stencil order k=1..ns
 // (reconstruct.f90:109-124; stencil order of GP.f90:85-95).
 template <int RR>
 __device__ __forceinline__ void gp_face(const double* __restrict__ U, long long plane, int pitch, int i, int j,
@@ -61,60 +83,59 @@ __device__ __forceinline__ void gp_face(const double* __restrict__ U, long long 
     }
 }
 
-__device__ __forceinline__ const double* pv_ptr(const StageArgs& a, int rr, int f, int q) {
-    return a.pv + (long long)a.geo.nsMax * (q + a.geo.nqMax * (f + 4 * (rr - 1)));
+__device__ __forceinline__ const double* pv_ptr(const InstDev& d, int rr, int f, int q) {
+    return d.pv + (long long)d.geo.nsMax * (q + d.geo.nqMax * (f + 4 * (rr - 1)));
+}
+__device__ __forceinline__ double qw_at(const InstDev& d, int rr, int q) {
+    return __ldg(d.qw + q + d.geo.nqMax * (rr - 1));
 }
 
-__device__ __forceinline__ double qw_at(const StageArgs& a, int rr, int q) { return __ldg(a.qw + q + a.geo.nqMax * (rr - 1)); }
-
 // face value with a run-time radius; rr == 0 is the first-order copy of U
-__device__ __forceinline__ void face_value(const StageArgs& a, int rr, int i, int j, int f, int q, double out[NCONS]) {
-    const Geo& G = a.geo;
+__device__ __forceinline__ void face_value(const InstDev& d, const double* __restrict__ U, int rr, int i, int j, int f,
+                                           int q, double out[NCONS]) {
+    const Geo& G = d.geo;
     if (rr == 0) {
         const long long idx = (long long)j * G.pitch + i;
 #pragma unroll
-        for (int v = 0; v < NCONS; v++) out[v] = __ldg(a.Uin + v * G.plane + idx);
+        for (int v = 0; v < NCONS; v++) out[v] = __ldg(U + v * G.plane + idx);
         return;
     }
-    const double* pvq = pv_ptr(a, rr, f, q);
+    const double* pvq = pv_ptr(d, rr, f, q);
     if (rr == 1)
-        gp_face<1>(a.Uin, G.plane, G.pitch, i, j, pvq, out);
+        gp_face<1>(U, G.plane, G.pitch, i, j, pvq, out);
     else if (rr == 2)
-        gp_face<2>(a.Uin, G.plane, G.pitch, i, j, pvq, out);
+        gp_face<2>(U, G.plane, G.pitch, i, j, pvq, out);
     else
-        gp_face<3>(a.Uin, G.plane, G.pitch, i, j, pvq, out);
+        gp_face<3>(U, G.plane, G.pitch, i, j, pvq, out);
 }
 
-__device__ __forceinline__ void warp_flag(int* counter, bool flag) {
-    const unsigned m = __ballot_sync(0xffffffffu, flag);
-    if (m && (threadIdx.x & 31) == 0) atomicOr(counter, 1);
+__device__ __forceinline__ void warp_flag(int* flag, bool v) {
+    const unsigned m = __ballot_sync(0xffffffffu, v);
+    if (m && (threadIdx.x & 31) == 0) atomicOr(flag, 1);
 }
-
-__device__ __forceinline__ void warp_count(int* counter, bool flag) {
-    const unsigned m = __ballot_sync(0xffffffffu, flag);
+__device__ __forceinline__ void warp_count(int* counter, bool v) {
+    const unsigned m = __ballot_sync(0xffffffffu, v);
     if (m && (threadIdx.x & 31) == 0) atomicAdd(counter, __popc(m));
 }
 
-// ------------------------------------------------------------------------
+// ======================================================================
 // MOOD pass 1 (every scheme == R): reconstruct_faceValsWithGP + face CAD/PAD
-// + getFluxes_ fused.  One thread per cell (i,j) owns the x-face between
-// (i-1,j) and (i,j) and the y-face between (i,j-1) and (i,j).  Face values are
-// recomputed per quadrature point and never stored.  A cell fails when any of
-// its four faces fails; the four verdicts are kept per face side in failX /
-// failY and combined by cascade_lower.  Fluxes of faces next to a failing
-// cell are recomputed after the cascade (flux, FLUX_DIRTY).
+// + getFluxes_ fused.  A thread owns the x-face between (i-1,j) and (i,j) and
+// the y-face between (i,j-1) and (i,j).  Face values are recomputed per
+// quadrature point and never stored.  A cell fails when any of its four
+// faces fails; the verdicts are kept per face side in failX / failY and
+// combined by cascade_lower.  Fluxes next to a cell the cascade
+// re-reconstructs are recomputed after it (flux, FLUX_DIRTY).
 template <int R>
-__global__ void __launch_bounds__(BX* BY) k_face_pass1(StageArgs a) {
-    const Geo& G = a.geo;
+__device__ __forceinline__ bool pass1_body(const InstDev& d, const double* __restrict__ U, int i, int j) {
+    const Geo& G = d.geo;
+    const Phys& P = d.phys;
     const int g = G.g;
-    const int i = g - 2 + blockIdx.x * BX + threadIdx.x;
-    const int j = g - 2 + blockIdx.y * BY + threadIdx.y;
     const int clo = g - 2, cxhi = g + G.nx + 1, cyhi = g + G.ny + 1;  // reconstruct range
     const int flo = g - 1, fxhi = g + G.nx + 1, fyhi = g + G.ny + 1;  // flux range
     const long long c = (long long)j * G.pitch + i;
     constexpr int NQ = R + 1;
     bool bad = false;
-
     // x-face
     if (i >= clo && i <= cxhi + 1 && j >= clo && j <= cyhi) {
         const bool needL = (i - 1 >= clo);
@@ -128,27 +149,27 @@ __global__ void __launch_bounds__(BX* BY) k_face_pass1(StageArgs a) {
         for (int q = 0; q < NQ; q++) {
             double uL[NCONS], uR[NCONS];
             if (needL) {
-                gp_face<R>(a.Uin, G.plane, G.pitch, i - 1, j, pv_ptr(a, R, EAST, q), uL);
-                if (!admissible(uL[DENS], cons2pres(a.phys, uL))) bits |= 1;
+                gp_face<R>(U, G.plane, G.pitch, i - 1, j, pv_ptr(d, R, EAST, q), uL);
+                if (!admissible(uL[DENS], cons2pres(P, uL))) bits |= 1;
             }
             if (needR) {
-                gp_face<R>(a.Uin, G.plane, G.pitch, i, j, pv_ptr(a, R, WEST, q), uR);
-                if (!admissible(uR[DENS], cons2pres(a.phys, uR))) bits |= 2;
+                gp_face<R>(U, G.plane, G.pitch, i, j, pv_ptr(d, R, WEST, q), uR);
+                if (!admissible(uR[DENS], cons2pres(P, uR))) bits |= 2;
             }
             if (doFlux) {
                 double F[NCONS];
-                hllc(a.phys, uL, uR, XDIR, F);
-                const double w = qw_at(a, R, q);
+                hllc(P, uL, uR, XDIR, F);
+                const double w = qw_at(d, R, q);
 #pragma unroll
                 for (int v = 0; v < NCONS; v++) acc[v] = acc[v] + w * F[v];
             }
         }
-        a.failX[c] = bits;
+        d.failX[c] = bits;
         bad |= bits != 0;
         if (doFlux) {
 #pragma unroll
-            for (int v = 0; v < NCONS; v++) a.FX[v * G.plane + c] = acc[v];
-            a.CTX[c] = acc[MAGY];
+            for (int v = 0; v < NCONS; v++) d.FX[v * G.plane + c] = acc[v];
+            d.CTX[c] = acc[MAGY];
         }
     }
     // y-face
@@ -164,194 +185,267 @@ __global__ void __launch_bounds__(BX* BY) k_face_pass1(StageArgs a) {
         for (int q = 0; q < NQ; q++) {
             double uL[NCONS], uR[NCONS];
             if (needB) {
-                gp_face<R>(a.Uin, G.plane, G.pitch, i, j - 1, pv_ptr(a, R, NORTH, q), uL);
-                if (!admissible(uL[DENS], cons2pres(a.phys, uL))) bits |= 1;
+                gp_face<R>(U, G.plane, G.pitch, i, j - 1, pv_ptr(d, R, NORTH, q), uL);
+                if (!admissible(uL[DENS], cons2pres(P, uL))) bits |= 1;
             }
             if (needT) {
-                gp_face<R>(a.Uin, G.plane, G.pitch, i, j, pv_ptr(a, R, SOUTH, q), uR);
-                if (!admissible(uR[DENS], cons2pres(a.phys, uR))) bits |= 2;
+                gp_face<R>(U, G.plane, G.pitch, i, j, pv_ptr(d, R, SOUTH, q), uR);
+                if (!admissible(uR[DENS], cons2pres(P, uR))) bits |= 2;
             }
             if (doFlux) {
                 double F[NCONS];
-                hllc(a.phys, uL, uR, YDIR, F);
-                const double w = qw_at(a, R, q);
+                hllc(P, uL, uR, YDIR, F);
+                const double w = qw_at(d, R, q);
 #pragma unroll
                 for (int v = 0; v < NCONS; v++) acc[v] = acc[v] + w * F[v];
             }
         }
-        a.failY[c] = bits;
+        d.failY[c] = bits;
         bad |= bits != 0;
         if (doFlux) {
 #pragma unroll
-            for (int v = 0; v < NCONS; v++) a.FY[v * G.plane + c] = acc[v];
-            a.CTY[c] = acc[MAGX];
+            for (int v = 0; v < NCONS; v++) d.FY[v * G.plane + c] = acc[v];
+            d.CTY[c] = acc[MAGX];
         }
     }
-    warp_flag(a.counters + CNT_ANYFAIL, bad);
+    return bad;
 }
 
-// ------------------------------------------------------------------------
-// Serial lowering pass of reconstruct.f90:146-169 (order independent: a cell
-// only lowers its own scheme; every flag write is a set): for each failing
+// One launch per radius: blocks of instances with another GP radius leave at once.
+template <int R>
+__global__ void __launch_bounds__(NTHREADS, HOSONO_PASS1_MIN_BLOCKS) k_face_pass1(Batch B, int uin) {
+    Cell c;
+    if (!tile_cell(B, c)) return;
+    InstState& S = B.st[c.k];
+    if (!S.stepping) return;
+    const InstDev& d = B.dev[c.k];
+    if (d.geo.R != R) return;
+    const double* U = role_ptr(d, S.parity, uin);
+    if (first_tile_thread(c)) S.cascadeMode = CASCADE_FROM_FACES;
+    bool bad = false;
+    if (c.i < d.geo.nxt && c.j < d.geo.nyt) bad = pass1_body<R>(d, U, c.i, c.j);
+    warp_flag(&S.anyFail, bad);
+}
+
+// ======================================================================
+// Face cascade (reconstruct.f90:143-171).
+// cascade_cond: per instance, whether it entered (or stays in) the cascade;
+// sets the batch condition.  Single block, one thread per slot.
+__global__ void k_cascade_cond(Batch B, cudaGraphConditionalHandle h, int set_handle) {
+    __shared__ int any;
+    if (threadIdx.x == 0) any = 0;
+    __syncthreads();
+    for (int k = threadIdx.x; k < B.maxInst; k += blockDim.x) {
+        InstState& S = B.st[k];
+        const int in = (S.stepping && S.stageActive && S.anyFail) ? 1 : 0;
+        S.anyFail = 0;
+        S.nextIter = in;
+        if (in) {
+            S.cascaded = 1;
+            S.cascadeIters++;
+            any = 1;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        B.flags->anyFail = any;
+        if (set_handle) cudaGraphSetConditional(h, any ? 1u : 0u);
+    }
+}
+
+// the serial lowering loop of reconstruct.f90:146-169 (order independent: a
+// cell lowers only its own scheme; every flag write sets): for each failing
 // cell in [g-2, g+n+1]^2, gridBlock_lowerOrder (gridBlock.f90:194-235) and
-// mark the cross for the next inner pass.
-__global__ void __launch_bounds__(BX* BY) k_cascade_lower(StageArgs a, int mode) {
-    const Geo& G = a.geo;
+// mark the cross for the next inner pass.  nextPass is cleared first.
+__global__ void __launch_bounds__(NTHREADS) k_clear_nextpass(Batch B) {
+    Cell c;
+    if (!tile_cell(B, c)) return;
+    const InstState& S = B.st[c.k];
+    if (!S.nextIter) return;
+    const InstDev& d = B.dev[c.k];
+    if (c.i < d.geo.nxt && c.j < d.geo.nyt) d.nextPass[(long long)c.j * d.geo.pitch + c.i] = 0;
+}
+
+__global__ void __launch_bounds__(NTHREADS) k_cascade_lower(Batch B) {
+    Cell c;
+    if (!tile_cell(B, c)) return;
+    InstState& S = B.st[c.k];
+    if (!S.nextIter) return;
+    const InstDev& d = B.dev[c.k];
+    const Geo& G = d.geo;
     const int g = G.g;
-    const int i = g - 2 + blockIdx.x * BX + threadIdx.x;
-    const int j = g - 2 + blockIdx.y * BY + threadIdx.y;
+    const int i = c.i, j = c.j;
     bool f = false;
-    if (i <= g + G.nx + 1 && j <= g + G.ny + 1) {
-        const long long c = (long long)j * G.pitch + i;
-        if (mode == CASCADE_FROM_FACES)
-            f = ((a.failX[c] & 2) | (a.failX[c + 1] & 1) | (a.failY[c] & 2) | (a.failY[c + G.pitch] & 1)) != 0;
+    if (i >= g - 2 && j >= g - 2 && i <= g + G.nx + 1 && j <= g + G.ny + 1) {
+        const long long cc = (long long)j * G.pitch + i;
+        if (S.cascadeMode == CASCADE_FROM_FACES)
+            f = ((d.failX[cc] & 2) | (d.failX[cc + 1] & 1) | (d.failY[cc] & 2) | (d.failY[cc + G.pitch] & 1)) != 0;
         else
-            f = a.fail[c] != 0;
+            f = d.fail[cc] != 0;
         if (f) {
-            const int s = a.scheme[c];
-            a.scheme[c] = (int8_t)(s - 1 > 0 ? s - 1 : 0);
-            a.rec[c] = 1;
-            a.rec[c + 1] = 1;
-            a.rec[c - 1] = 1;
-            a.rec[c + G.pitch] = 1;
-            a.rec[c - G.pitch] = 1;
+            int8_t* sch = d.scheme[S.schemeSel];
+            const int s = sch[cc];
+            sch[cc] = (int8_t)(s - 1 > 0 ? s - 1 : 0);
+            d.rec[cc] = 1;
+            d.rec[cc + 1] = 1;
+            d.rec[cc - 1] = 1;
+            d.rec[cc + G.pitch] = 1;
+            d.rec[cc - G.pitch] = 1;
             for (int jj = j - 2; jj <= j + 2; jj++) {
                 if (jj < 0 || jj >= G.nyt) continue;
                 for (int ii = i - 2; ii <= i + 2; ii++) {
                     if (ii < 0 || ii >= G.nxt) continue;
-                    if (iabs_c(ii - i) + iabs_c(jj - j) <= 2) a.recF[(long long)jj * G.pitch + ii] = 1;
+                    if (iabs_c(ii - i) + iabs_c(jj - j) <= 2) d.recF[(long long)jj * G.pitch + ii] = 1;
                 }
             }
-            a.nextPass[c] = 1;
-            a.nextPass[c + 1] = 1;
-            a.nextPass[c - 1] = 1;
-            a.nextPass[c + G.pitch] = 1;
-            a.nextPass[c - G.pitch] = 1;
-            if (a.trace) a.innerCount[c] = (uint8_t)(a.innerCount[c] + 1);
+            d.nextPass[cc] = 1;
+            d.nextPass[cc + 1] = 1;
+            d.nextPass[cc - 1] = 1;
+            d.nextPass[cc + G.pitch] = 1;
+            d.nextPass[cc - G.pitch] = 1;
+            d.innerCount[cc] = (uint8_t)(d.innerCount[cc] + 1);
         }
     }
-    warp_count(a.counters + CNT_INNER, f);
+    warp_count(&S.nInner, f);
 }
 
-// ------------------------------------------------------------------------
-// One inner pass of reconstruct_faceValsWithGP on the cells flagged in mask:
-// all four faces at rr = min(scheme(c), scheme(nbr)) (EDP1), CAD/PAD on every
-// quadrature point.  The radius used per face is recorded in rrRec so the
-// flux kernel can rebuild exactly these face values later.
-__global__ void __launch_bounds__(BX* BY) k_recon_check(StageArgs a, const uint8_t* __restrict__ mask) {
-    const Geo& G = a.geo;
+// One inner pass of reconstruct_faceValsWithGP on flagged cells (mask = rec at
+// the start of a later MOOD pass, nextPass inside the cascade): all four faces
+// at rr = min(scheme(c), scheme(nbr)) (EDP1), CAD/PAD at every quadrature
+// point.  The radius used per face is recorded in rrRec.  The verdict plane
+// `fail` is written on the whole reconstruct range.
+__global__ void __launch_bounds__(NTHREADS) k_recon_check(Batch B, int uin, int maskSel) {
+    Cell c;
+    if (!tile_cell(B, c)) return;
+    InstState& S = B.st[c.k];
+    const bool run = maskSel == MASK_REC ? (S.stepping && S.stageActive) : (S.nextIter != 0);
+    if (!run) return;
+    const InstDev& d = B.dev[c.k];
+    const Geo& G = d.geo;
     const int g = G.g;
-    const int i = g - 2 + blockIdx.x * BX + threadIdx.x;
-    const int j = g - 2 + blockIdx.y * BY + threadIdx.y;
+    const int i = c.i, j = c.j;
+    if (first_tile_thread(c)) S.cascadeMode = CASCADE_FROM_CELLS;
     bool bad = false;
-    if (i <= g + G.nx + 1 && j <= g + G.ny + 1) {
-        const long long c = (long long)j * G.pitch + i;
-        if (mask[c]) {
-            a.dirty[c] = 1;
-            const int s = a.scheme[c];
+    if (i >= g - 2 && j >= g - 2 && i <= g + G.nx + 1 && j <= g + G.ny + 1) {
+        const long long cc = (long long)j * G.pitch + i;
+        const uint8_t* mask = maskSel == MASK_REC ? d.rec : d.nextPass;
+        if (mask[cc]) {
+            const double* U = role_ptr(d, S.parity, uin);
+            const int8_t* sch = d.scheme[S.schemeSel];
+            d.dirty[cc] = 1;
+            const int s = sch[cc];
             int rr[4];
-            rr[NORTH] = min(s, (int)a.scheme[c + G.pitch]);
-            rr[SOUTH] = min(s, (int)a.scheme[c - G.pitch]);
-            rr[EAST] = min(s, (int)a.scheme[c + 1]);
-            rr[WEST] = min(s, (int)a.scheme[c - 1]);
-            a.rrRec[c] = (uint8_t)(rr[0] | (rr[1] << 2) | (rr[2] << 4) | (rr[3] << 6));
+            rr[NORTH] = min(s, (int)sch[cc + G.pitch]);
+            rr[SOUTH] = min(s, (int)sch[cc - G.pitch]);
+            rr[EAST] = min(s, (int)sch[cc + 1]);
+            rr[WEST] = min(s, (int)sch[cc - 1]);
+            d.rrRec[cc] = (uint8_t)(rr[0] | (rr[1] << 2) | (rr[2] << 4) | (rr[3] << 6));
 #pragma unroll 1
             for (int f = 0; f < 4 && !bad; f++) {
                 if (rr[f] == 0) continue;
 #pragma unroll 1
                 for (int q = 0; q <= rr[f] && !bad; q++) {
                     double u[NCONS];
-                    face_value(a, rr[f], i, j, f, q, u);
-                    if (!admissible(u[DENS], cons2pres(a.phys, u))) bad = true;
+                    face_value(d, U, rr[f], i, j, f, q, u);
+                    if (!admissible(u[DENS], cons2pres(d.phys, u))) bad = true;
                 }
             }
-            if (bad) a.fail[c] = 1;
         }
+        d.fail[cc] = bad ? 1 : 0;
     }
-    warp_flag(a.counters + CNT_ANYFAIL, bad);
+    warp_flag(&S.anyFail, bad);
 }
 
-// ------------------------------------------------------------------------
+// ======================================================================
 // getFluxes_ (getFluxes.f90:16-90) on flagged faces.  Face values are rebuilt
 // from U at the radius each side was last reconstructed with (rrRec); the
 // quadrature uses the face's current radius (riemannSolver.f90:23-47).
-__device__ __forceinline__ void face_flux(const StageArgs& a, int dir, int iL, int jL, int fL, int rrL, int iR, int jR,
-                                          int fR, int rrR, int rr, double flux[NCONS]) {
+__device__ __forceinline__ void face_flux(const InstDev& d, const double* __restrict__ U, int dir, int iL, int jL,
+                                          int fL, int rrL, int iR, int jR, int fR, int rrR, int rr,
+                                          double flux[NCONS]) {
     double uL[NCONS], uR[NCONS];
     if (rr == 0) {
-        face_value(a, rrL, iL, jL, fL, 0, uL);
-        face_value(a, rrR, iR, jR, fR, 0, uR);
-        hllc(a.phys, uL, uR, dir, flux);
+        face_value(d, U, rrL, iL, jL, fL, 0, uL);
+        face_value(d, U, rrR, iR, jR, fR, 0, uR);
+        hllc(d.phys, uL, uR, dir, flux);
         return;
     }
 #pragma unroll
     for (int v = 0; v < NCONS; v++) flux[v] = 0.0;
 #pragma unroll 1
     for (int q = 0; q <= rr; q++) {
-        face_value(a, rrL, iL, jL, fL, q, uL);
-        face_value(a, rrR, iR, jR, fR, q, uR);
+        face_value(d, U, rrL, iL, jL, fL, q, uL);
+        face_value(d, U, rrR, iR, jR, fR, q, uR);
         double F[NCONS];
-        hllc(a.phys, uL, uR, dir, F);
-        const double w = qw_at(a, rr, q);
+        hllc(d.phys, uL, uR, dir, F);
+        const double w = qw_at(d, rr, q);
 #pragma unroll
         for (int v = 0; v < NCONS; v++) flux[v] = flux[v] + w * F[v];
     }
 }
 
-__global__ void __launch_bounds__(BX* BY) k_flux(StageArgs a, int mode) {
-    const Geo& G = a.geo;
+__global__ void __launch_bounds__(NTHREADS) k_flux(Batch B, int uin, int mode) {
+    Cell c;
+    if (!tile_cell(B, c)) return;
+    const InstState& S = B.st[c.k];
+    if (!(S.stepping && S.stageActive)) return;
+    if (mode == FLUX_DIRTY && !S.cascaded) return;
+    const InstDev& d = B.dev[c.k];
+    const Geo& G = d.geo;
     const int g = G.g;
-    const int i = g - 1 + blockIdx.x * BX + threadIdx.x;
-    const int j = g - 1 + blockIdx.y * BY + threadIdx.y;
-    if (i > g + G.nx + 1 || j > g + G.ny + 1) return;
-    const long long c = (long long)j * G.pitch + i;
-    const long long cw = c - 1, cs = c - G.pitch;
-    const bool doX = mode == FLUX_DIRTY ? (a.dirty[c] | a.dirty[cw]) != 0 : (a.rec[c] | a.rec[cw]) != 0;
-    const bool doY = mode == FLUX_DIRTY ? (a.dirty[c] | a.dirty[cs]) != 0 : (a.rec[c] | a.rec[cs]) != 0;
+    const int i = c.i, j = c.j;
+    if (i < g - 1 || j < g - 1 || i > g + G.nx + 1 || j > g + G.ny + 1) return;
+    const long long cc = (long long)j * G.pitch + i;
+    const long long cw = cc - 1, cs = cc - G.pitch;
+    const bool doX = mode == FLUX_DIRTY ? (d.dirty[cc] | d.dirty[cw]) != 0 : (d.rec[cc] | d.rec[cw]) != 0;
+    const bool doY = mode == FLUX_DIRTY ? (d.dirty[cc] | d.dirty[cs]) != 0 : (d.rec[cc] | d.rec[cs]) != 0;
+    if (!doX && !doY) return;
+    const double* U = role_ptr(d, S.parity, uin);
+    const int8_t* sch = d.scheme[S.schemeSel];
     if (doX) {
-        const int rr = min((int)a.scheme[c], (int)a.scheme[cw]);
-        const int rrL = (a.rrRec[cw] >> (2 * EAST)) & 3;
-        const int rrR = (a.rrRec[c] >> (2 * WEST)) & 3;
+        const int rr = min((int)sch[cc], (int)sch[cw]);
+        const int rrL = (d.rrRec[cw] >> (2 * EAST)) & 3;
+        const int rrR = (d.rrRec[cc] >> (2 * WEST)) & 3;
         double F[NCONS];
-        face_flux(a, XDIR, i - 1, j, EAST, rrL, i, j, WEST, rrR, rr, F);
+        face_flux(d, U, XDIR, i - 1, j, EAST, rrL, i, j, WEST, rrR, rr, F);
 #pragma unroll
-        for (int v = 0; v < NCONS; v++) a.FX[v * G.plane + c] = F[v];
-        a.CTX[c] = F[MAGY];
+        for (int v = 0; v < NCONS; v++) d.FX[v * G.plane + cc] = F[v];
+        d.CTX[cc] = F[MAGY];
     }
     if (doY) {
-        const int rr = min((int)a.scheme[c], (int)a.scheme[cs]);
-        const int rrL = (a.rrRec[cs] >> (2 * NORTH)) & 3;
-        const int rrR = (a.rrRec[c] >> (2 * SOUTH)) & 3;
+        const int rr = min((int)sch[cc], (int)sch[cs]);
+        const int rrL = (d.rrRec[cs] >> (2 * NORTH)) & 3;
+        const int rrR = (d.rrRec[cc] >> (2 * SOUTH)) & 3;
         double F[NCONS];
-        face_flux(a, YDIR, i, j - 1, NORTH, rrL, i, j, SOUTH, rrR, rr, F);
+        face_flux(d, U, YDIR, i, j - 1, NORTH, rrL, i, j, SOUTH, rrR, rr, F);
 #pragma unroll
-        for (int v = 0; v < NCONS; v++) a.FY[v * G.plane + c] = F[v];
-        a.CTY[c] = F[MAGX];
+        for (int v = 0; v < NCONS; v++) d.FY[v * G.plane + cc] = F[v];
+        d.CTY[cc] = F[MAGX];
     }
 }
 
-// ------------------------------------------------------------------------
+// ======================================================================
 // FLICDdivB_fluxCorrections (FLICDdivB.f90:13-70) from fluxRaw.
-__device__ __forceinline__ double flicd_x(const StageArgs& a, long long c) {
-    const Geo& G = a.geo;
-    const double* fxy = a.FX + MAGY * G.plane;
-    const double* fyx = a.FY + MAGX * G.plane;
+__device__ __forceinline__ double flicd_x(const InstDev& d, long long c) {
+    const Geo& G = d.geo;
+    const double* fxy = d.FX + MAGY * G.plane;
+    const double* fyx = d.FY + MAGX * G.plane;
     const long long p = G.pitch;
     return (2 * fxy[c] + fxy[c + 1] + fxy[c - 1] - fyx[c + p] - fyx[c] - fyx[c - 1] - fyx[c - 1 + p]) / 8.0;
 }
-__device__ __forceinline__ double flicd_y(const StageArgs& a, long long c) {
-    const Geo& G = a.geo;
-    const double* fxy = a.FX + MAGY * G.plane;
-    const double* fyx = a.FY + MAGX * G.plane;
+__device__ __forceinline__ double flicd_y(const InstDev& d, long long c) {
+    const Geo& G = d.geo;
+    const double* fxy = d.FX + MAGY * G.plane;
+    const double* fyx = d.FY + MAGX * G.plane;
     const long long p = G.pitch;
     return (2 * fyx[c] + fyx[c + p] + fyx[c - p] - fxy[c + 1] - fxy[c] - fxy[c - p] - fxy[c + 1 - p]) / 8.0;
 }
 
 // detect_ALL's per-cell test (detect.f90:84-213): true when the cell must be lowered.
-__device__ __forceinline__ bool detect_cell(const StageArgs& a, long long c, const double un[NCONS]) {
-    const Geo& G = a.geo;
-    const Phys& s = a.phys;
-    const double* U = a.Uin;
+__device__ __forceinline__ bool detect_cell(const InstDev& d, const double* __restrict__ U, long long c,
+                                            const double un[NCONS]) {
+    const Geo& G = d.geo;
+    const Phys& s = d.phys;
     const long long P = G.plane, p = G.pitch;
     const double presNew = cons2pres(s, un);
     if (!admissible(un[DENS], presNew)) return true;
@@ -430,24 +524,33 @@ __device__ __forceinline__ bool detect_cell(const StageArgs& a, long long c, con
 // unsplit update of timeStep.f90:107-118 and detect_ALL.  A corrected flux a
 // neighbour needs is recomputed locally when the neighbour is flagged (it
 // writes the same value) and read from memory otherwise (nobody writes it).
-__global__ void __launch_bounds__(BX* BY) k_ct_update_detect(StageArgs a) {
-    const Geo& G = a.geo;
+// `lowered` is written on the whole interior every pass.
+__global__ void __launch_bounds__(NTHREADS) k_ct_update_detect(Batch B, int uin, int uout) {
+    Cell c;
+    if (!tile_cell(B, c)) return;
+    InstState& S = B.st[c.k];
+    if (!(S.stepping && S.stageActive)) return;
+    const InstDev& d = B.dev[c.k];
+    const Geo& G = d.geo;
     const int g = G.g;
-    const int i = g + blockIdx.x * BX + threadIdx.x;
-    const int j = g + blockIdx.y * BY + threadIdx.y;
+    const int i = c.i, j = c.j;
     bool low = false;
-    if (i <= g + G.nx && j <= g + G.ny) {
-        const long long c = (long long)j * G.pitch + i;
-        if (a.recF[c]) {
-            const double ctx = flicd_x(a, c);
-            const double cty = flicd_y(a, c);
-            a.CTX[c] = ctx;
-            a.CTY[c] = cty;
-            if (i < g + G.nx && j < g + G.ny) {
-                const long long ce = c + 1, cn = c + G.pitch;
-                const double ctx_e = a.recF[ce] ? flicd_x(a, ce) : a.CTX[ce];
-                const double cty_n = a.recF[cn] ? flicd_y(a, cn) : a.CTY[cn];
-                const double dtdx = a.dt / G.dx, dtdy = a.dt / G.dy;
+    if (i >= g && j >= g && i <= g + G.nx && j <= g + G.ny) {
+        const long long cc = (long long)j * G.pitch + i;
+        const bool interior = i < g + G.nx && j < g + G.ny;
+        if (d.recF[cc]) {
+            const double ctx = flicd_x(d, cc);
+            const double cty = flicd_y(d, cc);
+            d.CTX[cc] = ctx;
+            d.CTY[cc] = cty;
+            if (interior) {
+                const double* U = role_ptr(d, S.parity, uin);
+                double* Uo = role_ptr(d, S.parity, uout);
+                const long long ce = cc + 1, cn = cc + G.pitch;
+                const double ctx_e = d.recF[ce] ? flicd_x(d, ce) : d.CTX[ce];
+                const double cty_n = d.recF[cn] ? flicd_y(d, cn) : d.CTY[cn];
+                const double dt = S.dt;
+                const double dtdx = dt / G.dx, dtdy = dt / G.dy;
                 double un[NCONS];
 #pragma unroll
                 for (int v = 0; v < NCONS; v++) {
@@ -463,44 +566,42 @@ __global__ void __launch_bounds__(BX* BY) k_ct_update_detect(StageArgs a) {
                         g0 = 0.0;
                         g1 = 0.0;
                     } else {
-                        f0 = a.FX[v * G.plane + c];
-                        f1 = a.FX[v * G.plane + ce];
-                        g0 = a.FY[v * G.plane + c];
-                        g1 = a.FY[v * G.plane + cn];
+                        f0 = d.FX[v * G.plane + cc];
+                        f1 = d.FX[v * G.plane + ce];
+                        g0 = d.FY[v * G.plane + cc];
+                        g1 = d.FY[v * G.plane + cn];
                     }
-                    un[v] = a.Uin[v * G.plane + c] - dtdx * (f1 - f0) - dtdy * (g1 - g0);
-                    a.Uout[v * G.plane + c] = un[v];
+                    un[v] = U[v * G.plane + cc] - dtdx * (f1 - f0) - dtdy * (g1 - g0);
+                    Uo[v * G.plane + cc] = un[v];
                 }
-                if (a.scheme[c] > 0) {
-                    low = detect_cell(a, c, un);
-                    if (low) a.lowered[c] = 1;
-                }
+                if (d.scheme[S.schemeSel][cc] > 0) low = detect_cell(d, U, cc, un);
             }
         }
+        if (interior) d.lowered[cc] = low ? 1 : 0;
     }
-    warp_count(a.counters + CNT_DETECT, low);
+    warp_count(&S.nDetect, low);
 }
 
-// ------------------------------------------------------------------------
+// ======================================================================
 // After detect: recompute = cross of lowered cells, recomputeFLICD = radius-2
 // diamond (gridBlock_lowerOrder), scheme lowered by one where lowered; then
 // boundaryConditions_applyMOOD's periodic sync, which (x sweep over all rows,
 // then y sweep over all columns, N >= 2*NGC) makes every cell the OR (flags) /
 // MIN (scheme) over its translates by multiples of N that lie in the array.
-__device__ __forceinline__ bool lowered_at(const StageArgs& a, int i, int j) {
-    const Geo& G = a.geo;
-    if (i < 0 || j < 0 || i >= G.nxt || j >= G.nyt) return false;
-    return a.lowered[(long long)j * G.pitch + i] != 0;
-}
-
-__global__ void __launch_bounds__(BX* BY) k_mood_flags(StageArgs a) {
-    const Geo& G = a.geo;
-    const int i = blockIdx.x * BX + threadIdx.x;
-    const int j = blockIdx.y * BY + threadIdx.y;
+__global__ void __launch_bounds__(NTHREADS) k_mood_flags(Batch B) {
+    Cell c;
+    if (!tile_cell(B, c)) return;
+    const InstState& S = B.st[c.k];
+    if (!(S.stepping && S.stageActive)) return;
+    const InstDev& d = B.dev[c.k];
+    const Geo& G = d.geo;
+    const int i = c.i, j = c.j;
     if (i >= G.nxt || j >= G.nyt) return;
+    const int8_t* sch = d.scheme[S.schemeSel];
+    int8_t* schN = d.scheme[1 - S.schemeSel];
     const int reach = G.bc == 1 ? 1 : 0;
     bool rec = false, recF = false;
-    int sch = 127;
+    int s = 127;
     for (int b = -reach; b <= reach; b++) {
         const int jo = j + b * G.ny;
         if (jo < 0 || jo >= G.nyt) continue;
@@ -508,28 +609,99 @@ __global__ void __launch_bounds__(BX* BY) k_mood_flags(StageArgs a) {
             const int io = i + t * G.nx;
             if (io < 0 || io >= G.nxt) continue;
             const long long co = (long long)jo * G.pitch + io;
-            const int lo = a.lowered[co];
-            const int so = a.scheme[co] - lo;
-            sch = min(sch, so > 0 ? so : 0);
+            const int lo = d.lowered[co];
+            const int so = sch[co] - lo;
+            s = min(s, so > 0 ? so : 0);
             for (int dj = -2; dj <= 2; dj++) {
+                const int jj = jo + dj;
+                if (jj < 0 || jj >= G.nyt) continue;
                 for (int di = -2; di <= 2; di++) {
-                    const int d = iabs_c(di) + iabs_c(dj);
-                    if (d > 2) continue;
-                    if (lowered_at(a, io + di, jo + dj)) {
+                    const int dd = iabs_c(di) + iabs_c(dj);
+                    const int ii = io + di;
+                    if (dd > 2 || ii < 0 || ii >= G.nxt) continue;
+                    if (d.lowered[(long long)jj * G.pitch + ii]) {
                         recF = true;
-                        if (d <= 1) rec = true;
+                        if (dd <= 1) rec = true;
                     }
                 }
             }
         }
     }
-    const long long c = (long long)j * G.pitch + i;
-    a.rec[c] = rec;
-    a.recF[c] = recF;
-    a.scheme_next[c] = (int8_t)sch;
+    const long long cc = (long long)j * G.pitch + i;
+    d.rec[cc] = rec;
+    d.recF[cc] = recF;
+    schN[cc] = (int8_t)s;
 }
 
-// ------------------------------------------------------------------------
+// End of a MOOD pass (timeStep.f90:86-128 loop test): an instance whose detect
+// lowered nothing leaves the loop.  Single block, one thread per slot.
+__global__ void k_pass_end(Batch B, cudaGraphConditionalHandle h, int set_handle) {
+    __shared__ int any;
+    if (threadIdx.x == 0) any = 0;
+    __syncthreads();
+    for (int k = threadIdx.x; k < B.maxInst; k += blockDim.x) {
+        InstState& S = B.st[k];
+        if (!(S.stepping && S.stageActive)) continue;
+        S.schemeSel = 1 - S.schemeSel;  // k_mood_flags wrote the other buffer
+        S.passes++;
+        S.passesTotal++;
+        S.innerTotal += S.nInner;
+        S.detectTotal += S.nDetect;
+        S.lastInner = S.nInner;
+        S.lastDetect = S.nDetect;
+        if (S.nDetect == 0) {
+            S.stageActive = 0;
+            if (S.passes > S.maxPasses) S.maxPasses = S.passes;
+        } else if (S.passes >= S.passCap) {
+            S.stageActive = 0;
+            S.stepping = 0;
+            S.done = 1;
+            S.error = HOSONO_EMOODCAP;
+        } else {
+            any = 1;
+        }
+        S.nInner = 0;
+        S.nDetect = 0;
+        S.cascaded = 0;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        B.flags->anyActive = any;
+        if (set_handle) cudaGraphSetConditional(h, any ? 1u : 0u);
+    }
+}
+
+// timeStep_forwardEuler's reset (timeStep.f90:79-81) on every cell:
+// scheme = R, recompute = recomputeFLICD = .true.; plus the per-instance
+// stage scalars.
+__global__ void __launch_bounds__(NTHREADS) k_stage_init(Batch B) {
+    Cell c;
+    if (!tile_cell(B, c)) return;
+    InstState& S = B.st[c.k];
+    if (!S.stepping) return;
+    const InstDev& d = B.dev[c.k];
+    const Geo& G = d.geo;
+    if (first_tile_thread(c)) {
+        S.stageActive = 1;
+        S.passes = 0;
+        S.nInner = 0;
+        S.nDetect = 0;
+        S.anyFail = 0;
+        S.cascaded = 0;
+        S.stages++;
+    }
+    if (c.i >= G.nxt || c.j >= G.nyt) return;
+    const long long cc = (long long)c.j * G.pitch + c.i;
+    const int R = G.R;
+    d.scheme[S.schemeSel][cc] = (int8_t)R;
+    d.rec[cc] = 1;
+    d.recF[cc] = 1;
+    d.rrRec[cc] = (uint8_t)(R | (R << 2) | (R << 4) | (R << 6));
+    d.dirty[cc] = 0;
+    d.innerCount[cc] = 0;
+}
+
+// ======================================================================
 // boundary conditions (boundaryConditions.f90:291-360) as a gather
 __device__ __forceinline__ int bc_src(int i, int n, int g, int bc) {
     if (i < g) return bc == 1 ? i + n : g;
@@ -537,166 +709,255 @@ __device__ __forceinline__ int bc_src(int i, int n, int g, int bc) {
     return i;
 }
 
-__global__ void k_bc_fill(Geo G, double* A, int nvar) {
-    const int i = blockIdx.x * BX + threadIdx.x;
-    const int j = blockIdx.y * BY + threadIdx.y;
-    if (i >= G.nxt || j >= G.nyt) return;
-    const int si = bc_src(i, G.nx, G.g, G.bc), sj = bc_src(j, G.ny, G.g, G.bc);
-    if (si == i && sj == j) return;
-    const long long c = (long long)j * G.pitch + i, s = (long long)sj * G.pitch + si;
-    for (int v = 0; v < nvar; v++) A[v * G.plane + c] = A[v * G.plane + s];
-}
-
-// timeStep.f90:165 over every cell (guards from their images)
-__global__ void k_rk_combine2(Geo G, const double* __restrict__ Un, const double* __restrict__ B, double* __restrict__ out) {
-    const int i = blockIdx.x * BX + threadIdx.x;
-    const int j = blockIdx.y * BY + threadIdx.y;
-    if (i >= G.nxt || j >= G.nyt) return;
-    const int si = bc_src(i, G.nx, G.g, G.bc), sj = bc_src(j, G.ny, G.g, G.bc);
-    const long long c = (long long)j * G.pitch + i, s = (long long)sj * G.pitch + si;
+__global__ void __launch_bounds__(NTHREADS) k_bc_fill(Batch B, int role) {
+    Cell c;
+    if (!tile_cell(B, c)) return;
+    const InstState& S = B.st[c.k];
+    if (!S.stepping) return;
+    const InstDev& d = B.dev[c.k];
+    const Geo& G = d.geo;
+    if (c.i >= G.nxt || c.j >= G.nyt) return;
+    const int si = bc_src(c.i, G.nx, G.g, G.bc), sj = bc_src(c.j, G.ny, G.g, G.bc);
+    if (si == c.i && sj == c.j) return;
+    double* A = role_ptr(d, S.parity, role);
+    const long long cc = (long long)c.j * G.pitch + c.i, s = (long long)sj * G.pitch + si;
 #pragma unroll
-    for (int v = 0; v < NCONS; v++) out[v * G.plane + c] = (3 * Un[v * G.plane + s] + B[v * G.plane + s]) / 4.0;
+    for (int v = 0; v < NCONS; v++) A[v * G.plane + cc] = A[v * G.plane + s];
 }
 
-// timeStep.f90:169 and :32-41 (V = cons2prim(U), boundary conditions on U and V)
-__global__ void k_rk_final(Geo G, Phys P, const double* __restrict__ Un, const double* __restrict__ B,
-                           double* __restrict__ outU, double* __restrict__ outV) {
-    const int i = blockIdx.x * BX + threadIdx.x;
-    const int j = blockIdx.y * BY + threadIdx.y;
-    if (i >= G.nxt || j >= G.nyt) return;
-    const int si = bc_src(i, G.nx, G.g, G.bc), sj = bc_src(j, G.ny, G.g, G.bc);
-    const long long c = (long long)j * G.pitch + i, s = (long long)sj * G.pitch + si;
+// timeStep.f90:165-166 over every cell (guards from their images): A = (3 U + B)/4
+__global__ void __launch_bounds__(NTHREADS) k_rk_combine2(Batch B) {
+    Cell c;
+    if (!tile_cell(B, c)) return;
+    const InstState& S = B.st[c.k];
+    if (!S.stepping) return;
+    const InstDev& d = B.dev[c.k];
+    const Geo& G = d.geo;
+    if (c.i >= G.nxt || c.j >= G.nyt) return;
+    const int si = bc_src(c.i, G.nx, G.g, G.bc), sj = bc_src(c.j, G.ny, G.g, G.bc);
+    const long long cc = (long long)c.j * G.pitch + c.i, s = (long long)sj * G.pitch + si;
+    const double* Un = role_ptr(d, S.parity, ROLE_STATE);
+    const double* Bb = role_ptr(d, S.parity, ROLE_B);
+    double* out = role_ptr(d, S.parity, ROLE_A);
+#pragma unroll
+    for (int v = 0; v < NCONS; v++) out[v * G.plane + cc] = (3 * Un[v * G.plane + s] + Bb[v * G.plane + s]) / 4.0;
+}
+
+// timeStep.f90:169 and :32-41: A = (U + 2 B)/3, V = cons2prim(A), on every
+// cell (guards from their images).  step_end makes A the state.
+__global__ void __launch_bounds__(NTHREADS) k_rk_final(Batch B) {
+    Cell c;
+    if (!tile_cell(B, c)) return;
+    const InstState& S = B.st[c.k];
+    if (!S.stepping) return;
+    const InstDev& d = B.dev[c.k];
+    const Geo& G = d.geo;
+    if (c.i >= G.nxt || c.j >= G.nyt) return;
+    const int si = bc_src(c.i, G.nx, G.g, G.bc), sj = bc_src(c.j, G.ny, G.g, G.bc);
+    const long long cc = (long long)c.j * G.pitch + c.i, s = (long long)sj * G.pitch + si;
+    const double* Un = role_ptr(d, S.parity, ROLE_STATE);
+    const double* Bb = role_ptr(d, S.parity, ROLE_B);
+    double* out = role_ptr(d, S.parity, ROLE_A);
     double u[NCONS], V[NPRIM];
 #pragma unroll
     for (int v = 0; v < NCONS; v++) {
-        u[v] = (Un[v * G.plane + s] + 2 * B[v * G.plane + s]) / 3.0;
-        outU[v * G.plane + c] = u[v];
+        u[v] = (Un[v * G.plane + s] + 2 * Bb[v * G.plane + s]) / 3.0;
+        out[v * G.plane + cc] = u[v];
     }
-    cons2prim(P, u, V);
+    cons2prim(d.phys, u, V);
 #pragma unroll
-    for (int v = 0; v < NPRIM; v++) outV[v * G.plane + c] = V[v];
+    for (int v = 0; v < NPRIM; v++) d.V[v * G.plane + cc] = V[v];
 }
 
-__global__ void k_cons2prim_all(Geo G, Phys P, const double* __restrict__ U, double* __restrict__ V) {
-    const int i = blockIdx.x * BX + threadIdx.x;
-    const int j = blockIdx.y * BY + threadIdx.y;
-    if (i >= G.nxt || j >= G.nyt) return;
-    const long long c = (long long)j * G.pitch + i;
+// V = cons2prim(state) on every cell (upload without V)
+__global__ void __launch_bounds__(NTHREADS) k_cons2prim_all(Batch B) {
+    Cell c;
+    if (!tile_cell(B, c)) return;
+    const InstState& S = B.st[c.k];
+    if (!S.stepping) return;
+    const InstDev& d = B.dev[c.k];
+    const Geo& G = d.geo;
+    if (c.i >= G.nxt || c.j >= G.nyt) return;
+    const long long cc = (long long)c.j * G.pitch + c.i;
+    const double* U = role_ptr(d, S.parity, ROLE_STATE);
     double u[NCONS], w[NPRIM];
 #pragma unroll
-    for (int v = 0; v < NCONS; v++) u[v] = U[v * G.plane + c];
-    cons2prim(P, u, w);
+    for (int v = 0; v < NCONS; v++) u[v] = U[v * G.plane + cc];
+    cons2prim(d.phys, u, w);
 #pragma unroll
-    for (int v = 0; v < NPRIM; v++) V[v * G.plane + c] = w[v];
+    for (int v = 0; v < NPRIM; v++) d.V[v * G.plane + cc] = w[v];
 }
 
-// cfl_computedt (cfl.f90:14-52): max over the interior of |u|+c and |v|+c.
-// Non-negative doubles order like their bit patterns, so the block maxima
-// are combined with an integer atomicMax.
-__global__ void __launch_bounds__(256) k_cfl_max(Geo G, Phys P, const double* __restrict__ V, unsigned long long* out) {
+// ======================================================================
+// cfl_computedt (cfl.f90:14-52): per instance, max of |u|+c and |v|+c over the
+// interior.  Non-negative doubles order like their bit patterns, so block
+// maxima are combined with an integer atomicMax.
+__global__ void __launch_bounds__(NTHREADS) k_cfl_reduce(Batch B) {
+    Cell c;
+    if (!tile_cell(B, c)) return;
+    InstState& S = B.st[c.k];
+    if (!S.stepping) return;
+    const InstDev& d = B.dev[c.k];
+    const Geo& G = d.geo;
     double xm = 0.0, ym = 0.0;
-    const long long n = (long long)G.nx * G.ny;
-    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
-        const int ii = (int)(t % G.nx), jj = (int)(t / G.nx);
-        const long long c = (long long)(jj + G.g) * G.pitch + (ii + G.g);
-        const double rho = V[DENS * G.plane + c], pr = V[PRES * G.plane + c], gam = V[GAMM * G.plane + c];
+    if (c.i >= G.g && c.j >= G.g && c.i < G.g + G.nx && c.j < G.g + G.ny) {
+        const long long cc = (long long)c.j * G.pitch + c.i;
+        const double* V = d.V;
+        const double rho = V[DENS * G.plane + cc], pr = V[PRES * G.plane + cc], gam = V[GAMM * G.plane + cc];
         double cs;
-        if (P.force_hydro) {
+        if (d.phys.force_hydro) {
             cs = sqrt(gam * pr / rho);
         } else {
-            const double bx = V[MAGX * G.plane + c], by = V[MAGY * G.plane + c], bz = V[MAGZ * G.plane + c];
+            const double bx = V[MAGX * G.plane + cc], by = V[MAGY * G.plane + cc], bz = V[MAGZ * G.plane + cc];
             const double BB = bx * bx + by * by + bz * bz;
             const double bmin = fmin(fmin(fabs(bx), fabs(by)), fabs(bz));
             cs = c_fs(gam, rho, pr, BB, bmin, +1.0);
         }
-        xm = fmax(xm, fabs(V[VELX * G.plane + c]) + cs);
-        ym = fmax(ym, fabs(V[VELY * G.plane + c]) + cs);
+        xm = fabs(V[VELX * G.plane + cc]) + cs;
+        ym = fabs(V[VELY * G.plane + cc]) + cs;
     }
     for (int o = 16; o > 0; o >>= 1) {
         xm = fmax(xm, __shfl_xor_sync(0xffffffffu, xm, o));
         ym = fmax(ym, __shfl_xor_sync(0xffffffffu, ym, o));
     }
-    __shared__ double sx[8], sy[8];
-    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-    if (l == 0) {
+    __shared__ double sx[NTHREADS / 32], sy[NTHREADS / 32];
+    const int lane = (threadIdx.y * TILE_X + threadIdx.x) & 31, w = (threadIdx.y * TILE_X + threadIdx.x) >> 5;
+    if (lane == 0) {
         sx[w] = xm;
         sy[w] = ym;
     }
     __syncthreads();
     if (w == 0) {
-        xm = l < (int)(blockDim.x >> 5) ? sx[l] : 0.0;
-        ym = l < (int)(blockDim.x >> 5) ? sy[l] : 0.0;
+        xm = lane < NTHREADS / 32 ? sx[lane] : 0.0;
+        ym = lane < NTHREADS / 32 ? sy[lane] : 0.0;
         for (int o = 16; o > 0; o >>= 1) {
             xm = fmax(xm, __shfl_xor_sync(0xffffffffu, xm, o));
             ym = fmax(ym, __shfl_xor_sync(0xffffffffu, ym, o));
         }
-        if (l == 0) {
-            atomicMax(out + 0, (unsigned long long)__double_as_longlong(xm));
-            atomicMax(out + 1, (unsigned long long)__double_as_longlong(ym));
+        if (lane == 0) {
+            atomicMax(&S.cflbits[0], (unsigned long long)__double_as_longlong(xm));
+            atomicMax(&S.cflbits[1], (unsigned long long)__double_as_longlong(ym));
         }
     }
 }
 
-// ------------------------------------------------------------------------
-inline dim3 grid2(int nx, int ny) { return dim3((nx + BX - 1) / BX, (ny + BY - 1) / BY); }
-const dim3 kBlock(BX, BY);
-
-void face_pass1(const StageArgs& a, cudaStream_t s) {
-    const dim3 grd = grid2(a.geo.nx + 5, a.geo.ny + 5);
-    switch (a.geo.R) {
-        case 1: k_face_pass1<1><<<grd, kBlock, 0, s>>>(a); break;
-        case 2: k_face_pass1<2><<<grd, kBlock, 0, s>>>(a); break;
-        default: k_face_pass1<3><<<grd, kBlock, 0, s>>>(a); break;
+// Step begin: dt = cfl * min(dx/xmax, dy/ymax) (cfl.f90:50) and validTimeStep
+// (mhd_driver.f90:239-266: clamp to tmax first, then reject negative, NaN or
+// infinite dt).  With use_host_dt the host already stored dt.
+__global__ void k_step_begin(Batch B, int use_host_dt) {
+    for (int k = threadIdx.x; k < B.maxInst; k += blockDim.x) {
+        InstState& S = B.st[k];
+        if (!S.stepping) continue;
+        if (use_host_dt) continue;
+        const InstDev& d = B.dev[k];
+        const double xm = __longlong_as_double((long long)S.cflbits[0]);
+        const double ym = __longlong_as_double((long long)S.cflbits[1]);
+        double dt = d.cfl * fmin(d.geo.dx / xm, d.geo.dy / ym);
+        if (S.t + dt > S.tmax) {
+            dt = S.tmax - S.t;
+        } else if (dt < 0.0 || isnan(dt) || !isfinite(dt)) {
+            S.error = HOSONO_ENANDT;
+            S.done = 1;
+            S.stepping = 0;
+        }
+        S.dt = dt;
     }
 }
-void cascade_lower(const StageArgs& a, int mode, cudaStream_t s) {
-    k_cascade_lower<<<grid2(a.geo.nx + 4, a.geo.ny + 4), kBlock, 0, s>>>(a, mode);
-}
-void recon_check(const StageArgs& a, const uint8_t* mask, cudaStream_t s) {
-    k_recon_check<<<grid2(a.geo.nx + 4, a.geo.ny + 4), kBlock, 0, s>>>(a, mask);
-}
-void flux(const StageArgs& a, int mode, cudaStream_t s) {
-    k_flux<<<grid2(a.geo.nx + 3, a.geo.ny + 3), kBlock, 0, s>>>(a, mode);
-}
-void ct_update_detect(const StageArgs& a, cudaStream_t s) {
-    k_ct_update_detect<<<grid2(a.geo.nx + 1, a.geo.ny + 1), kBlock, 0, s>>>(a);
-}
-void mood_flags(const StageArgs& a, cudaStream_t s) { k_mood_flags<<<grid2(a.geo.nxt, a.geo.nyt), kBlock, 0, s>>>(a); }
-void bc_fill(const Geo& G, double* A, int nvar, cudaStream_t s) {
-    k_bc_fill<<<grid2(G.nxt, G.nyt), kBlock, 0, s>>>(G, A, nvar);
-}
-void rk_combine2(const Geo& G, const double* Un, const double* B, double* out, cudaStream_t s) {
-    k_rk_combine2<<<grid2(G.nxt, G.nyt), kBlock, 0, s>>>(G, Un, B, out);
-}
-void rk_final(const Geo& G, const Phys& P, const double* Un, const double* B, double* outU, double* outV,
-              cudaStream_t s) {
-    k_rk_final<<<grid2(G.nxt, G.nyt), kBlock, 0, s>>>(G, P, Un, B, outU, outV);
-}
-void cons2prim_all(const Geo& G, const Phys& P, const double* U, double* V, cudaStream_t s) {
-    k_cons2prim_all<<<grid2(G.nxt, G.nyt), kBlock, 0, s>>>(G, P, U, V);
-}
-void cfl_max(const Geo& G, const Phys& P, const double* V, unsigned long long* out2, cudaStream_t s) {
-    long long n = (long long)G.nx * G.ny;
-    int blocks = (int)((n + 255) / 256);
-    if (blocks > 148 * 8) blocks = 148 * 8;
-    k_cfl_max<<<blocks, 256, 0, s>>>(G, P, V, out2);
+
+// Step start: which instances take part, fresh CFL accumulators.  (The step
+// budget flags->stepsLeft is set by the host before each run launch.)
+__global__ void k_step_prepare(Batch B, int /*unused*/) {
+    for (int k = threadIdx.x; k < B.maxInst; k += blockDim.x) {
+        InstState& S = B.st[k];
+        S.stepping = (S.live && !S.done) ? 1 : 0;
+        S.cflbits[0] = 0;
+        S.cflbits[1] = 0;
+    }
 }
 
-const KernelTable table = {
+// Step end: the new state is buffer A (parity flips), t += dt, nstep += 1,
+// and the time-loop test of mhd_driver.f90:198; next step's participants and
+// the batch condition.
+__global__ void k_step_end(Batch B, cudaGraphConditionalHandle h, int set_handle) {
+    __shared__ int any;
+    if (threadIdx.x == 0) any = 0;
+    __syncthreads();
+    for (int k = threadIdx.x; k < B.maxInst; k += blockDim.x) {
+        InstState& S = B.st[k];
+        if (S.stepping) {
+            S.parity = 1 - S.parity;
+            S.t = S.t + S.dt;
+            S.nstep = S.nstep + 1;
+            if (!((S.t < S.tmax) && (S.nstep < S.nstepmax))) S.done = 1;
+        }
+        S.stepping = 0;  // at rest between launches; step_prepare picks the next participants
+        S.cflbits[0] = 0;
+        S.cflbits[1] = 0;
+        if (S.live && !S.done) any = 1;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const int left = --B.flags->stepsLeft;
+        B.flags->anyLive = any && left > 0;
+        if (set_handle) cudaGraphSetConditional(h, (any && left > 0) ? 1u : 0u);
+    }
+}
+
+// ======================================================================
+inline dim3 tiles_grid(const Batch& B) { return dim3((unsigned)B.maxTiles); }
+const dim3 kTile(TILE_X, TILE_Y);
+
+void l_cfl_reduce(const Batch& B, cudaStream_t s) { k_cfl_reduce<<<tiles_grid(B), kTile, 0, s>>>(B); }
+void l_step_prepare(const Batch& B, int steps, cudaStream_t s) { k_step_prepare<<<1, 128, 0, s>>>(B, steps); }
+void l_step_begin(const Batch& B, int use_host_dt, cudaStream_t s) { k_step_begin<<<1, 128, 0, s>>>(B, use_host_dt); }
+void l_step_end(const Batch& B, cudaGraphConditionalHandle h, cudaStream_t s) {
+    k_step_end<<<1, 128, 0, s>>>(B, h, h != 0);
+}
+void l_stage_init(const Batch& B, cudaStream_t s) { k_stage_init<<<tiles_grid(B), kTile, 0, s>>>(B); }
+void l_face_pass1(const Batch& B, int uin, cudaStream_t s) {
+    k_face_pass1<2><<<tiles_grid(B), kTile, 0, s>>>(B, uin);
+    k_face_pass1<1><<<tiles_grid(B), kTile, 0, s>>>(B, uin);
+    k_face_pass1<3><<<tiles_grid(B), kTile, 0, s>>>(B, uin);
+}
+void l_cascade_cond(const Batch& B, cudaGraphConditionalHandle h, cudaStream_t s) {
+    k_cascade_cond<<<1, 128, 0, s>>>(B, h, h != 0);
+}
+void l_cascade_lower(const Batch& B, int /*mode: per instance*/, cudaStream_t s) {
+    k_clear_nextpass<<<tiles_grid(B), kTile, 0, s>>>(B);
+    k_cascade_lower<<<tiles_grid(B), kTile, 0, s>>>(B);
+}
+void l_recon_check(const Batch& B, int uin, int mask, cudaStream_t s) {
+    k_recon_check<<<tiles_grid(B), kTile, 0, s>>>(B, uin, mask);
+}
+void l_flux(const Batch& B, int uin, int mode, cudaStream_t s) { k_flux<<<tiles_grid(B), kTile, 0, s>>>(B, uin, mode); }
+void l_ct_update_detect(const Batch& B, int uin, int uout, cudaStream_t s) {
+    k_ct_update_detect<<<tiles_grid(B), kTile, 0, s>>>(B, uin, uout);
+}
+void l_mood_flags(const Batch& B, cudaStream_t s) { k_mood_flags<<<tiles_grid(B), kTile, 0, s>>>(B); }
+void l_pass_end(const Batch& B, cudaGraphConditionalHandle h, cudaStream_t s) {
+    k_pass_end<<<1, 128, 0, s>>>(B, h, h != 0);
+}
+void l_bc_fill(const Batch& B, int role, cudaStream_t s) { k_bc_fill<<<tiles_grid(B), kTile, 0, s>>>(B, role); }
+void l_rk_combine2(const Batch& B, cudaStream_t s) { k_rk_combine2<<<tiles_grid(B), kTile, 0, s>>>(B); }
+void l_rk_final(const Batch& B, cudaStream_t s) { k_rk_final<<<tiles_grid(B), kTile, 0, s>>>(B); }
+void l_cons2prim_all(const Batch& B, cudaStream_t s) { k_cons2prim_all<<<tiles_grid(B), kTile, 0, s>>>(B); }
+
+const KernelSet kset = {
 #if HOSONO_FAST
     "fast",
 #else
     "strict",
 #endif
-    face_pass1, cascade_lower, recon_check, flux, ct_update_detect, mood_flags,
-    bc_fill, rk_combine2, rk_final, cons2prim_all, cfl_max};
+    l_cfl_reduce, l_step_prepare, l_step_begin, l_step_end, l_stage_init, l_face_pass1, l_cascade_cond, l_cascade_lower,
+    l_recon_check, l_flux, l_ct_update_detect, l_mood_flags, l_pass_end, l_bc_fill, l_rk_combine2, l_rk_final,
+    l_cons2prim_all};
 
 }  // namespace KNS
 
 #if HOSONO_FAST
-const KernelTable* kernels_fast() { return &kfast::table; }
+const KernelSet* kernelset_fast() { return &kfast::kset; }
 #else
-const KernelTable* kernels_strict() { return &kstrict::table; }
+const KernelSet* kernelset_strict() { return &kstrict::kset; }
 #endif
 
 }  // namespace hosono

@@ -1,7 +1,7 @@
 // layout.cu -- conversions between the reference's Fortran-order AoS host
 // arrays (var fastest, then i, then j; guards included) and the device SoA
 // planes.  Pure data movement: no arithmetic, one build.
-#include "kernels.h"
+#include "engine.h"
 
 namespace hosono {
 

@@ -144,6 +144,18 @@ int hosono_gpu_advance(hosono_handle* h, double dt);
  * nstep >= nstepmax or max_steps steps (max_steps <= 0: no extra limit). */
 int hosono_gpu_run(hosono_handle* h, double tmax, int nstepmax, int max_steps, double* t_out, int* nstep_out);
 
+/* Set the instance's time-loop position (t, nstep) and limits (tmax, nstepmax). */
+int hosono_gpu_set_time(hosono_handle* h, double t, double tmax, int nstep, int nstepmax);
+
+/* Continue the driver's time loop from the current t/nstep: up to max_steps
+ * steps of cfl_computedt + validTimeStep + timeStep_advanceSolution, each one
+ * taken on the device without a host round trip (max_steps <= 0: to tmax). */
+int hosono_gpu_step(hosono_handle* h, int max_steps, double* t_out, int* nstep_out);
+
+/* Run the MOOD loops from a captured CUDA graph (on, the default) or from
+ * host-driven launches (off; always the case while tracing). */
+int hosono_gpu_set_graphs(hosono_handle* h, int on);
+
 /* Drop-in with host buffers: upload U (and V if not NULL), advance by dt,
  * download U and V.  The form a Fortran caller that keeps grid_state on
  * the host binds (timeStep_advanceSolution with state%U/state%V). */
@@ -177,6 +189,37 @@ int hosono_gpu_set_device(int device);
 
 /* The cudaStream_t every kernel of this handle runs on (for events). */
 int hosono_gpu_stream(hosono_handle* h, void** stream);
+
+/* ---------------------------------------------------------------- batches
+ * Many independent blocks (any sizes, radii, boundary conditions, problems)
+ * advanced together: every kernel launch covers all instances' tiles, each
+ * instance keeps its own t, dt (its own cfl_computedt), MOOD loop and time
+ * limits, and hosono_batch_run takes them all to their tmax in one graph
+ * launch.  Instances can be added and removed between runs (continuous
+ * batching); capacity is fixed at creation in slots and 32x8 tiles. */
+typedef struct hosono_batch hosono_batch;
+
+int hosono_batch_create(int max_instances, int max_tiles, int fp_mode, hosono_batch** out);
+int hosono_batch_destroy(hosono_batch* b);
+/* tiles and device bytes one instance with these parameters needs */
+int hosono_batch_tiles_for(const hosono_params* p);
+long long hosono_batch_instance_bytes(const hosono_params* p);
+int hosono_batch_add(hosono_batch* b, const hosono_params* p, const double* pv, const double* qw, const int* stenc,
+                     int* slot);
+int hosono_batch_remove(hosono_batch* b, int slot);
+int hosono_batch_upload(hosono_batch* b, int slot, const double* U, const double* V);
+int hosono_batch_download(hosono_batch* b, int slot, double* U, double* V, int* scheme);
+int hosono_batch_set_time(hosono_batch* b, int slot, double t, double tmax, int nstep, int nstepmax);
+/* every live, unfinished instance steps until its tmax/nstepmax, or at most
+ * max_steps steps (max_steps <= 0: no limit) */
+int hosono_batch_run(hosono_batch* b, int max_steps);
+int hosono_batch_status(hosono_batch* b, int slot, double* t, double* dt, int* nstep, int* done, int* error);
+/* cumulative MOOD counters of one instance */
+int hosono_batch_stats(hosono_batch* b, int slot, hosono_stats* s);
+int hosono_batch_stream(hosono_batch* b, void** stream);
+int hosono_batch_set_graphs(hosono_batch* b, int on);
+int hosono_batch_last_error(hosono_batch* b, char* buf, int len);
+int hosono_batch_capacity(hosono_batch* b, int* max_instances, int* max_tiles, int* used_tiles, int* live);
 
 /* CFL time step that allocates nothing.  No counterpart in the reference:
  * it exists for callers that cannot call cudaMalloc when they need dt (code

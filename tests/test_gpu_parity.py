@@ -60,6 +60,29 @@ def test_strict_bitwise_steps(case, tmp_par_dir):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("case", ["ot32_r1", "ot24_r3_refic", "sedov32_r2", "blast40_r2"])
+def test_strict_bitwise_graph_path(case, tmp_par_dir):
+    """The production path (whole step from a CUDA graph with conditional MOOD
+    loops, dt computed and validated on the device) equals the oracle's
+    driver loop bit for bit."""
+    m = pkg.load()
+    par = parfiles.make(tmp_par_dir, case + "_g", CASES[case]())
+    o = oracle.Oracle(par)
+    s = m.Solver.from_par(par, fp_mode=m.FP_STRICT)
+    s.set_time(0.0, o.tmax, 0, 1 << 30)
+    for chunk in (1, 3, 4):
+        for _ in range(chunk):
+            dt = o.cfl()
+            o.advance(dt)
+        s.step(chunk)
+        U, V, S = s.download()
+        np.testing.assert_array_equal(U, o.U())
+        np.testing.assert_array_equal(V, o.V())
+        np.testing.assert_array_equal(S, o.scheme())
+    s.close()
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("case", ["ot32_r2", "blast40_r2", "sedov32_r2"])
 def test_fast_one_step_tolerance(case, tmp_par_dir):
     """FMA build: one RK3 step within 1e-12 relative L1 on all 8 variables."""
