@@ -213,6 +213,7 @@ def bench_ours(args, rank, world, local):
         U0, V0 = m.ic_set(par, params)
     sol = m.Solver(params, pv, qw, st)
     sol.upload(U0, V0)
+    sol.set_time(0.0, run.tmax, 0, run.nstepmax)
     stream = torch.cuda.ExternalStream(sol.stream())
     zones = w["n"] * w["n"]
 
@@ -221,27 +222,26 @@ def bench_ours(args, rank, world, local):
             dist.barrier()
         torch.cuda.synchronize()
 
-    # warm-up (the clock sampler starts here so it has samples under load
-    # even when the timed region is shorter than its 200 ms period)
+    # warm-up (graph capture happens here; the clock sampler starts here so it
+    # has samples under load even when the timed region is short)
     clocks = ClockSampler(local)
     clocks.start()
-    for _ in range(args.warmup):
-        sol.timeStep_advanceSolution(sol.cfl_computedt())
+    sol.step(max(args.warmup, 1))
     barrier()
+    # timed region: K steps, each one launch of the step graph (cfl, dt,
+    # three MOOD stages, RK3) with CUDA events bracketing the pass-1 kernels
     sol.profile(True)
     sol.profile_read(reset=True)
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    passes = 0
-    for _ in range(args.steps):
-        sol.timeStep_advanceSolution(sol.cfl_computedt())
-        passes += sol.stats()["mood_passes"]
+    t_sim, n_steps = sol.step(args.steps)
     e1.record(stream)
     e1.synchronize()
     clk = clocks.stop()
     ms = e0.elapsed_time(e1)
     p1_ms, p1_n, launches = sol.profile_read(reset=True)
+    passes = sol.stats()["mood_passes"]
     sol.profile(False)
     barrier()
     if dist is not None:
@@ -250,8 +250,8 @@ def bench_ours(args, rank, world, local):
         ms = float(t.item())
     value = world * zones * args.steps / (ms / 1e3)
 
-    # end to end through the C ABI with host buffers: upload U,V from pinned
-    # memory, cfl, advance, download U,V -- every step
+    # end to end through the C ABI with host buffers: every step uploads U,V
+    # from pinned memory, takes the step (dt on the device) and downloads U,V
     Uh = torch.from_numpy(np.ascontiguousarray(U0)).pin_memory().numpy()
     Vh = torch.from_numpy(np.ascontiguousarray(V0)).pin_memory().numpy()
     e2e_steps = max(1, min(args.steps, 5))
@@ -261,7 +261,7 @@ def bench_ours(args, rank, world, local):
     f0.record(stream)
     for _ in range(e2e_steps):
         sol.upload(Uh, Vh)
-        sol.timeStep_advanceSolution(sol.cfl_computedt())
+        sol.step(1)
         sol.download(Uh, Vh, with_scheme=False)
     f1.record(stream)
     f1.synchronize()
@@ -296,6 +296,8 @@ def bench_ours(args, rank, world, local):
                    "l2": "inputs larger than L2 (U alone 270 MB at 2048^2)", "mood_passes": passes},
         "gpu_launches": launches, "clocks": clk, "roofline": roofline, "e2e": e2e,
     }
+    if world == 1 and not args.no_batched:
+        line["batched"] = bench_batched(m, fp, torch)
     if not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         rate, el = run_cpu_baseline(args.workload, 1, threads)
@@ -307,6 +309,72 @@ def bench_ours(args, rank, world, local):
         dist.destroy_process_group()
 
 
+def load_problems():
+    import importlib
+    load_pkg()
+    return importlib.import_module("hosono_2dmhd_b200.problems")
+
+
+def bench_batched(m, fp, torch, manifest="blast64_seed0.json", limit=None):
+    """The 64-instance MHD-blast workload (uneven N in {128..512}) advanced to
+    t_end=0.02 as one batch (one graph launch for the whole run) and, for
+    comparison, as 64 plain single solves one after the other.  Set-up (host
+    initial state, GP tables, upload) and the first step of each (graph
+    capture) are outside the timed regions; zone-updates count the timed steps."""
+    import time as _t
+    problems = load_problems()
+    path = os.path.join(ROOT, "hosono-2dmhd_b200", "workloads", manifest)
+    with open(path) as f:
+        entries = json.load(f)["instances"][:limit]
+    with tempfile.TemporaryDirectory() as d:
+        pars = [problems.make(d, f"i{e['id']}", problems.from_entry(e)) for e in entries]
+        tiles = sum(m.Batch.tiles_for(m.par_load(p)[0]) for p in pars)
+        b = m.Batch(len(pars), tiles, fp_mode=fp)
+        slots = [b.add_par(p) for p in pars]
+        b.run(max_steps=1)
+        n0 = {k: b.status(k)["nstep"] for k in slots}
+        stream = torch.cuda.ExternalStream(b.stream())
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        w0 = _t.perf_counter()
+        e0.record(stream)
+        b.run()
+        e1.record(stream)
+        e1.synchronize()
+        wall_b = _t.perf_counter() - w0
+        ms_b = e0.elapsed_time(e1)
+        zu_b = 0
+        steps = []
+        for k, e in zip(slots, entries):
+            st = b.status(k)
+            assert st["done"] and st["error"] == 0, st
+            zu_b += e["n"] * e["n"] * (st["nstep"] - n0[k])
+            steps.append(st["nstep"])
+        b.close()
+        # plain: one solve after another, each through its own single-instance engine
+        ms_p = 0.0
+        zu_p = 0
+        for p, e in zip(pars, entries):
+            s = m.Solver.from_par(p, fp_mode=fp)
+            s.set_time(0.0, e["tmax"], 0, 1 << 30)
+            s.step(1)
+            st_ = torch.cuda.ExternalStream(s.stream())
+            a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a0.record(st_)
+            _, n = s.step(0)
+            a1.record(st_)
+            a1.synchronize()
+            ms_p += a0.elapsed_time(a1)
+            zu_p += e["n"] * e["n"] * (n - 1)
+            s.close()
+    rate_b = zu_b / (ms_b / 1e3)
+    rate_p = zu_p / (ms_p / 1e3)
+    return {"workload": "blast64: 64 MHD blasts, N in {128..512} (seed 0), R=2, t_end=0.02",
+            "instances": len(entries), "zone_updates": zu_b, "steps_min": min(steps), "steps_max": max(steps),
+            "batched_value": rate_b, "batched_s": ms_b / 1e3, "batched_wall_s": wall_b,
+            "plain_value": rate_p, "plain_s": ms_p / 1e3, "ratio_batched_over_plain": rate_b / rate_p,
+            "unit": "zone-updates/s"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -316,6 +384,7 @@ def main():
     ap.add_argument("--workload", default="ot2048_r2", choices=sorted(WORKLOADS))
     ap.add_argument("--fp", default="strict", choices=["strict", "fast"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batched", action="store_true", help="skip the 64-instance batched-vs-plain measurement")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -43,19 +43,22 @@ constexpr int NTHREADS = TILE_X * TILE_Y;
 
 __device__ __forceinline__ int iabs_c(int a) { return a < 0 ? -a : a; }
 
-// Tile prologue: the instance and cell a thread works on.  Returns false for
-// blocks past the tile count (uniform per block).
+// The instance and cell a thread works on in tile t.
 struct Cell {
     int k, i, j;
 };
-__device__ __forceinline__ bool tile_cell(const Batch& B, Cell& c) {
-    if ((int)blockIdx.x >= __ldg(B.ntiles)) return false;
-    const int4 t = B.tiles[blockIdx.x];
-    c.k = t.x;
-    c.i = t.y + threadIdx.x;
-    c.j = t.z + threadIdx.y;
-    return true;
+__device__ __forceinline__ Cell tile_at(const Batch& B, int t) {
+    const int4 v = B.tiles[t];
+    Cell c;
+    c.k = v.x;
+    c.i = v.y + threadIdx.x;
+    c.j = v.z + threadIdx.y;
+    return c;
 }
+// Kernels walk the tile list grid-stride: the grid is sized to the GPU, the
+// tile count is read from device memory at run time.
+#define FOR_TILES(B, t) for (int t = blockIdx.x, n_ = __ldg((B).ntiles); t < n_; t += gridDim.x)
+
 // the one thread per instance that owns cell (0,0) (every instance has a tile at its origin)
 __device__ __forceinline__ bool first_tile_thread(const Cell& c) { return c.i == 0 && c.j == 0; }
 
@@ -213,9 +216,7 @@ __device__ __forceinline__ bool pass1_body(const InstDev& d, const double* __res
 
 // One launch per radius: blocks of instances with another GP radius leave at once.
 template <int R>
-__global__ void __launch_bounds__(NTHREADS, HOSONO_PASS1_MIN_BLOCKS) k_face_pass1(Batch B, int uin) {
-    Cell c;
-    if (!tile_cell(B, c)) return;
+__device__ __forceinline__ void t_face_pass1(const Batch& B, int uin, const Cell c) {
     InstState& S = B.st[c.k];
     if (!S.stepping) return;
     const InstDev& d = B.dev[c.k];
@@ -225,6 +226,10 @@ __global__ void __launch_bounds__(NTHREADS, HOSONO_PASS1_MIN_BLOCKS) k_face_pass
     bool bad = false;
     if (c.i < d.geo.nxt && c.j < d.geo.nyt) bad = pass1_body<R>(d, U, c.i, c.j);
     warp_flag(&S.anyFail, bad);
+}
+template <int R>
+__global__ void __launch_bounds__(NTHREADS, HOSONO_PASS1_MIN_BLOCKS) k_face_pass1(Batch B, int uin) {
+    FOR_TILES(B, t) t_face_pass1<R>(B, uin, tile_at(B, t));
 }
 
 // ======================================================================
@@ -257,18 +262,17 @@ __global__ void k_cascade_cond(Batch B, cudaGraphConditionalHandle h, int set_ha
 // cell lowers only its own scheme; every flag write sets): for each failing
 // cell in [g-2, g+n+1]^2, gridBlock_lowerOrder (gridBlock.f90:194-235) and
 // mark the cross for the next inner pass.  nextPass is cleared first.
-__global__ void __launch_bounds__(NTHREADS) k_clear_nextpass(Batch B) {
-    Cell c;
-    if (!tile_cell(B, c)) return;
+__device__ __forceinline__ void t_clear_nextpass(const Batch& B, const Cell c) {
     const InstState& S = B.st[c.k];
     if (!S.nextIter) return;
     const InstDev& d = B.dev[c.k];
     if (c.i < d.geo.nxt && c.j < d.geo.nyt) d.nextPass[(long long)c.j * d.geo.pitch + c.i] = 0;
 }
+__global__ void __launch_bounds__(NTHREADS) k_clear_nextpass(Batch B) {
+    FOR_TILES(B, t) t_clear_nextpass(B, tile_at(B, t));
+}
 
-__global__ void __launch_bounds__(NTHREADS) k_cascade_lower(Batch B) {
-    Cell c;
-    if (!tile_cell(B, c)) return;
+__device__ __forceinline__ void t_cascade_lower(const Batch& B, const Cell c) {
     InstState& S = B.st[c.k];
     if (!S.nextIter) return;
     const InstDev& d = B.dev[c.k];
@@ -308,15 +312,16 @@ __global__ void __launch_bounds__(NTHREADS) k_cascade_lower(Batch B) {
     }
     warp_count(&S.nInner, f);
 }
+__global__ void __launch_bounds__(NTHREADS) k_cascade_lower(Batch B) {
+    FOR_TILES(B, t) t_cascade_lower(B, tile_at(B, t));
+}
 
 // One inner pass of reconstruct_faceValsWithGP on flagged cells (mask = rec at
 // the start of a later MOOD pass, nextPass inside the cascade): all four faces
 // at rr = min(scheme(c), scheme(nbr)) (EDP1), CAD/PAD at every quadrature
 // point.  The radius used per face is recorded in rrRec.  The verdict plane
 // `fail` is written on the whole reconstruct range.
-__global__ void __launch_bounds__(NTHREADS) k_recon_check(Batch B, int uin, int maskSel) {
-    Cell c;
-    if (!tile_cell(B, c)) return;
+__device__ __forceinline__ void t_recon_check(const Batch& B, int uin, int maskSel, const Cell c) {
     InstState& S = B.st[c.k];
     const bool run = maskSel == MASK_REC ? (S.stepping && S.stageActive) : (S.nextIter != 0);
     if (!run) return;
@@ -355,6 +360,9 @@ __global__ void __launch_bounds__(NTHREADS) k_recon_check(Batch B, int uin, int 
     }
     warp_flag(&S.anyFail, bad);
 }
+__global__ void __launch_bounds__(NTHREADS) k_recon_check(Batch B, int uin, int maskSel) {
+    FOR_TILES(B, t) t_recon_check(B, uin, maskSel, tile_at(B, t));
+}
 
 // ======================================================================
 // getFluxes_ (getFluxes.f90:16-90) on flagged faces.  Face values are rebuilt
@@ -384,9 +392,7 @@ __device__ __forceinline__ void face_flux(const InstDev& d, const double* __rest
     }
 }
 
-__global__ void __launch_bounds__(NTHREADS) k_flux(Batch B, int uin, int mode) {
-    Cell c;
-    if (!tile_cell(B, c)) return;
+__device__ __forceinline__ void t_flux(const Batch& B, int uin, int mode, const Cell c) {
     const InstState& S = B.st[c.k];
     if (!(S.stepping && S.stageActive)) return;
     if (mode == FLUX_DIRTY && !S.cascaded) return;
@@ -422,6 +428,9 @@ __global__ void __launch_bounds__(NTHREADS) k_flux(Batch B, int uin, int mode) {
         for (int v = 0; v < NCONS; v++) d.FY[v * G.plane + cc] = F[v];
         d.CTY[cc] = F[MAGX];
     }
+}
+__global__ void __launch_bounds__(NTHREADS) k_flux(Batch B, int uin, int mode) {
+    FOR_TILES(B, t) t_flux(B, uin, mode, tile_at(B, t));
 }
 
 // ======================================================================
@@ -525,9 +534,7 @@ __device__ __forceinline__ bool detect_cell(const InstDev& d, const double* __re
 // neighbour needs is recomputed locally when the neighbour is flagged (it
 // writes the same value) and read from memory otherwise (nobody writes it).
 // `lowered` is written on the whole interior every pass.
-__global__ void __launch_bounds__(NTHREADS) k_ct_update_detect(Batch B, int uin, int uout) {
-    Cell c;
-    if (!tile_cell(B, c)) return;
+__device__ __forceinline__ void t_ct_update_detect(const Batch& B, int uin, int uout, const Cell c) {
     InstState& S = B.st[c.k];
     if (!(S.stepping && S.stageActive)) return;
     const InstDev& d = B.dev[c.k];
@@ -581,6 +588,9 @@ __global__ void __launch_bounds__(NTHREADS) k_ct_update_detect(Batch B, int uin,
     }
     warp_count(&S.nDetect, low);
 }
+__global__ void __launch_bounds__(NTHREADS) k_ct_update_detect(Batch B, int uin, int uout) {
+    FOR_TILES(B, t) t_ct_update_detect(B, uin, uout, tile_at(B, t));
+}
 
 // ======================================================================
 // After detect: recompute = cross of lowered cells, recomputeFLICD = radius-2
@@ -588,9 +598,7 @@ __global__ void __launch_bounds__(NTHREADS) k_ct_update_detect(Batch B, int uin,
 // boundaryConditions_applyMOOD's periodic sync, which (x sweep over all rows,
 // then y sweep over all columns, N >= 2*NGC) makes every cell the OR (flags) /
 // MIN (scheme) over its translates by multiples of N that lie in the array.
-__global__ void __launch_bounds__(NTHREADS) k_mood_flags(Batch B) {
-    Cell c;
-    if (!tile_cell(B, c)) return;
+__device__ __forceinline__ void t_mood_flags(const Batch& B, const Cell c) {
     const InstState& S = B.st[c.k];
     if (!(S.stepping && S.stageActive)) return;
     const InstDev& d = B.dev[c.k];
@@ -631,6 +639,9 @@ __global__ void __launch_bounds__(NTHREADS) k_mood_flags(Batch B) {
     d.rec[cc] = rec;
     d.recF[cc] = recF;
     schN[cc] = (int8_t)s;
+}
+__global__ void __launch_bounds__(NTHREADS) k_mood_flags(Batch B) {
+    FOR_TILES(B, t) t_mood_flags(B, tile_at(B, t));
 }
 
 // End of a MOOD pass (timeStep.f90:86-128 loop test): an instance whose detect
@@ -674,9 +685,7 @@ __global__ void k_pass_end(Batch B, cudaGraphConditionalHandle h, int set_handle
 // timeStep_forwardEuler's reset (timeStep.f90:79-81) on every cell:
 // scheme = R, recompute = recomputeFLICD = .true.; plus the per-instance
 // stage scalars.
-__global__ void __launch_bounds__(NTHREADS) k_stage_init(Batch B) {
-    Cell c;
-    if (!tile_cell(B, c)) return;
+__device__ __forceinline__ void t_stage_init(const Batch& B, const Cell c) {
     InstState& S = B.st[c.k];
     if (!S.stepping) return;
     const InstDev& d = B.dev[c.k];
@@ -700,6 +709,9 @@ __global__ void __launch_bounds__(NTHREADS) k_stage_init(Batch B) {
     d.dirty[cc] = 0;
     d.innerCount[cc] = 0;
 }
+__global__ void __launch_bounds__(NTHREADS) k_stage_init(Batch B) {
+    FOR_TILES(B, t) t_stage_init(B, tile_at(B, t));
+}
 
 // ======================================================================
 // boundary conditions (boundaryConditions.f90:291-360) as a gather
@@ -709,9 +721,7 @@ __device__ __forceinline__ int bc_src(int i, int n, int g, int bc) {
     return i;
 }
 
-__global__ void __launch_bounds__(NTHREADS) k_bc_fill(Batch B, int role) {
-    Cell c;
-    if (!tile_cell(B, c)) return;
+__device__ __forceinline__ void t_bc_fill(const Batch& B, int role, const Cell c) {
     const InstState& S = B.st[c.k];
     if (!S.stepping) return;
     const InstDev& d = B.dev[c.k];
@@ -724,11 +734,12 @@ __global__ void __launch_bounds__(NTHREADS) k_bc_fill(Batch B, int role) {
 #pragma unroll
     for (int v = 0; v < NCONS; v++) A[v * G.plane + cc] = A[v * G.plane + s];
 }
+__global__ void __launch_bounds__(NTHREADS) k_bc_fill(Batch B, int role) {
+    FOR_TILES(B, t) t_bc_fill(B, role, tile_at(B, t));
+}
 
 // timeStep.f90:165-166 over every cell (guards from their images): A = (3 U + B)/4
-__global__ void __launch_bounds__(NTHREADS) k_rk_combine2(Batch B) {
-    Cell c;
-    if (!tile_cell(B, c)) return;
+__device__ __forceinline__ void t_rk_combine2(const Batch& B, const Cell c) {
     const InstState& S = B.st[c.k];
     if (!S.stepping) return;
     const InstDev& d = B.dev[c.k];
@@ -742,12 +753,13 @@ __global__ void __launch_bounds__(NTHREADS) k_rk_combine2(Batch B) {
 #pragma unroll
     for (int v = 0; v < NCONS; v++) out[v * G.plane + cc] = (3 * Un[v * G.plane + s] + Bb[v * G.plane + s]) / 4.0;
 }
+__global__ void __launch_bounds__(NTHREADS) k_rk_combine2(Batch B) {
+    FOR_TILES(B, t) t_rk_combine2(B, tile_at(B, t));
+}
 
 // timeStep.f90:169 and :32-41: A = (U + 2 B)/3, V = cons2prim(A), on every
 // cell (guards from their images).  step_end makes A the state.
-__global__ void __launch_bounds__(NTHREADS) k_rk_final(Batch B) {
-    Cell c;
-    if (!tile_cell(B, c)) return;
+__device__ __forceinline__ void t_rk_final(const Batch& B, const Cell c) {
     const InstState& S = B.st[c.k];
     if (!S.stepping) return;
     const InstDev& d = B.dev[c.k];
@@ -768,11 +780,12 @@ __global__ void __launch_bounds__(NTHREADS) k_rk_final(Batch B) {
 #pragma unroll
     for (int v = 0; v < NPRIM; v++) d.V[v * G.plane + cc] = V[v];
 }
+__global__ void __launch_bounds__(NTHREADS) k_rk_final(Batch B) {
+    FOR_TILES(B, t) t_rk_final(B, tile_at(B, t));
+}
 
 // V = cons2prim(state) on every cell (upload without V)
-__global__ void __launch_bounds__(NTHREADS) k_cons2prim_all(Batch B) {
-    Cell c;
-    if (!tile_cell(B, c)) return;
+__device__ __forceinline__ void t_cons2prim_all(const Batch& B, const Cell c) {
     const InstState& S = B.st[c.k];
     if (!S.stepping) return;
     const InstDev& d = B.dev[c.k];
@@ -787,14 +800,15 @@ __global__ void __launch_bounds__(NTHREADS) k_cons2prim_all(Batch B) {
 #pragma unroll
     for (int v = 0; v < NPRIM; v++) d.V[v * G.plane + cc] = w[v];
 }
+__global__ void __launch_bounds__(NTHREADS) k_cons2prim_all(Batch B) {
+    FOR_TILES(B, t) t_cons2prim_all(B, tile_at(B, t));
+}
 
 // ======================================================================
 // cfl_computedt (cfl.f90:14-52): per instance, max of |u|+c and |v|+c over the
 // interior.  Non-negative doubles order like their bit patterns, so block
 // maxima are combined with an integer atomicMax.
-__global__ void __launch_bounds__(NTHREADS) k_cfl_reduce(Batch B) {
-    Cell c;
-    if (!tile_cell(B, c)) return;
+__device__ __forceinline__ void t_cfl_reduce(const Batch& B, const Cell c) {
     InstState& S = B.st[c.k];
     if (!S.stepping) return;
     const InstDev& d = B.dev[c.k];
@@ -839,6 +853,10 @@ __global__ void __launch_bounds__(NTHREADS) k_cfl_reduce(Batch B) {
             atomicMax(&S.cflbits[1], (unsigned long long)__double_as_longlong(ym));
         }
     }
+    __syncthreads();  // sx/sy are reused by the block's next tile
+}
+__global__ void __launch_bounds__(NTHREADS) k_cfl_reduce(Batch B) {
+    FOR_TILES(B, t) t_cfl_reduce(B, tile_at(B, t));
 }
 
 // Step begin: dt = cfl * min(dx/xmax, dy/ymax) (cfl.f90:50) and validTimeStep
@@ -904,43 +922,69 @@ __global__ void k_step_end(Batch B, cudaGraphConditionalHandle h, int set_handle
 }
 
 // ======================================================================
-inline dim3 tiles_grid(const Batch& B) { return dim3((unsigned)B.maxTiles); }
 const dim3 kTile(TILE_X, TILE_Y);
 
-void l_cfl_reduce(const Batch& B, cudaStream_t s) { k_cfl_reduce<<<tiles_grid(B), kTile, 0, s>>>(B); }
+// Grid of a tile kernel: as many blocks as fit on the GPU at once (the
+// kernels loop over the tile list), and never more than the tile capacity.
+int resident_blocks(const void* kernel) {
+    static const void* keys[64];
+    static int vals[64];
+    static int n = 0;
+    for (int k = 0; k < n; k++)
+        if (keys[k] == kernel) return vals[k];
+    int dev = 0, sms = 148, per = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, TILE_X * TILE_Y, 0);
+    const int v = sms * (per > 0 ? per : 1);
+    if (n < 64) {
+        keys[n] = kernel;
+        vals[n] = v;
+        n++;
+    }
+    return v;
+}
+template <typename K>
+dim3 grid_for(K kernel, const Batch& B) {
+    const int r = resident_blocks((const void*)kernel);
+    return dim3((unsigned)(r < B.maxTiles ? r : B.maxTiles));
+}
+#define TILE_LAUNCH(kern, B, s, ...) kern<<<grid_for(kern, B), kTile, 0, s>>>(B, ##__VA_ARGS__)
+
+void l_cfl_reduce(const Batch& B, cudaStream_t s) { TILE_LAUNCH(k_cfl_reduce, B, s); }
 void l_step_prepare(const Batch& B, int steps, cudaStream_t s) { k_step_prepare<<<1, 128, 0, s>>>(B, steps); }
 void l_step_begin(const Batch& B, int use_host_dt, cudaStream_t s) { k_step_begin<<<1, 128, 0, s>>>(B, use_host_dt); }
 void l_step_end(const Batch& B, cudaGraphConditionalHandle h, cudaStream_t s) {
     k_step_end<<<1, 128, 0, s>>>(B, h, h != 0);
 }
-void l_stage_init(const Batch& B, cudaStream_t s) { k_stage_init<<<tiles_grid(B), kTile, 0, s>>>(B); }
+void l_stage_init(const Batch& B, cudaStream_t s) { TILE_LAUNCH(k_stage_init, B, s); }
 void l_face_pass1(const Batch& B, int uin, cudaStream_t s) {
-    k_face_pass1<2><<<tiles_grid(B), kTile, 0, s>>>(B, uin);
-    k_face_pass1<1><<<tiles_grid(B), kTile, 0, s>>>(B, uin);
-    k_face_pass1<3><<<tiles_grid(B), kTile, 0, s>>>(B, uin);
+    TILE_LAUNCH(k_face_pass1<2>, B, s, uin);
+    TILE_LAUNCH(k_face_pass1<1>, B, s, uin);
+    TILE_LAUNCH(k_face_pass1<3>, B, s, uin);
 }
 void l_cascade_cond(const Batch& B, cudaGraphConditionalHandle h, cudaStream_t s) {
     k_cascade_cond<<<1, 128, 0, s>>>(B, h, h != 0);
 }
 void l_cascade_lower(const Batch& B, int /*mode: per instance*/, cudaStream_t s) {
-    k_clear_nextpass<<<tiles_grid(B), kTile, 0, s>>>(B);
-    k_cascade_lower<<<tiles_grid(B), kTile, 0, s>>>(B);
+    TILE_LAUNCH(k_clear_nextpass, B, s);
+    TILE_LAUNCH(k_cascade_lower, B, s);
 }
 void l_recon_check(const Batch& B, int uin, int mask, cudaStream_t s) {
-    k_recon_check<<<tiles_grid(B), kTile, 0, s>>>(B, uin, mask);
+    TILE_LAUNCH(k_recon_check, B, s, uin, mask);
 }
-void l_flux(const Batch& B, int uin, int mode, cudaStream_t s) { k_flux<<<tiles_grid(B), kTile, 0, s>>>(B, uin, mode); }
+void l_flux(const Batch& B, int uin, int mode, cudaStream_t s) { TILE_LAUNCH(k_flux, B, s, uin, mode); }
 void l_ct_update_detect(const Batch& B, int uin, int uout, cudaStream_t s) {
-    k_ct_update_detect<<<tiles_grid(B), kTile, 0, s>>>(B, uin, uout);
+    TILE_LAUNCH(k_ct_update_detect, B, s, uin, uout);
 }
-void l_mood_flags(const Batch& B, cudaStream_t s) { k_mood_flags<<<tiles_grid(B), kTile, 0, s>>>(B); }
+void l_mood_flags(const Batch& B, cudaStream_t s) { TILE_LAUNCH(k_mood_flags, B, s); }
 void l_pass_end(const Batch& B, cudaGraphConditionalHandle h, cudaStream_t s) {
     k_pass_end<<<1, 128, 0, s>>>(B, h, h != 0);
 }
-void l_bc_fill(const Batch& B, int role, cudaStream_t s) { k_bc_fill<<<tiles_grid(B), kTile, 0, s>>>(B, role); }
-void l_rk_combine2(const Batch& B, cudaStream_t s) { k_rk_combine2<<<tiles_grid(B), kTile, 0, s>>>(B); }
-void l_rk_final(const Batch& B, cudaStream_t s) { k_rk_final<<<tiles_grid(B), kTile, 0, s>>>(B); }
-void l_cons2prim_all(const Batch& B, cudaStream_t s) { k_cons2prim_all<<<tiles_grid(B), kTile, 0, s>>>(B); }
+void l_bc_fill(const Batch& B, int role, cudaStream_t s) { TILE_LAUNCH(k_bc_fill, B, s, role); }
+void l_rk_combine2(const Batch& B, cudaStream_t s) { TILE_LAUNCH(k_rk_combine2, B, s); }
+void l_rk_final(const Batch& B, cudaStream_t s) { TILE_LAUNCH(k_rk_final, B, s); }
+void l_cons2prim_all(const Batch& B, cudaStream_t s) { TILE_LAUNCH(k_cons2prim_all, B, s); }
 
 const KernelSet kset = {
 #if HOSONO_FAST
