@@ -94,7 +94,8 @@ class Engine::Rec {
     }
     int event(cudaEvent_t ev) {
         TRYE(begin());
-        cudaError_t r = cudaEventRecord(ev, e_->s_);
+        // External: under capture this becomes an event-record node of the graph
+        cudaError_t r = g_ ? cudaEventRecordWithFlags(ev, e_->s_, cudaEventRecordExternal) : cudaEventRecord(ev, e_->s_);
         if (r != cudaSuccess) return e_->fail(HOSONO_ECUDA, "event record: %s", cudaGetErrorString(r));
         return HOSONO_OK;
     }
@@ -159,7 +160,8 @@ Engine::~Engine() {
     for (cudaEvent_t ev : profEv_)
         if (ev) cudaEventDestroy(ev);
     for (void* p : {(void*)d_dev_, (void*)d_st_, (void*)d_tiles_, (void*)d_ntiles_, (void*)d_flags_, (void*)staging_,
-                    (void*)schemeInt_})
+                    (void*)schemeInt_, (void*)lists_.rec, (void*)lists_.face, (void*)lists_.recF, (void*)lists_.low,
+                    (void*)lists_.counts})
         if (p) cudaFree(p);
     if (h_flags_) cudaFreeHost(h_flags_);
     if (h_st_) cudaFreeHost(h_st_);
@@ -177,6 +179,13 @@ int Engine::init(int max_inst, int max_tiles, int fp_mode) {
     CUE(cudaMalloc(&d_tiles_, sizeof(int4) * maxTiles_));
     CUE(cudaMalloc(&d_ntiles_, sizeof(int)));
     CUE(cudaMalloc(&d_flags_, sizeof(BatchFlags)));
+    lists_.cap = (long long)maxTiles_ * TILE_X * TILE_Y;
+    CUE(cudaMalloc(&lists_.rec, sizeof(int2) * lists_.cap));
+    CUE(cudaMalloc(&lists_.face, sizeof(int2) * 2 * lists_.cap));
+    CUE(cudaMalloc(&lists_.recF, sizeof(int2) * lists_.cap));
+    CUE(cudaMalloc(&lists_.low, sizeof(int2) * lists_.cap));
+    CUE(cudaMalloc(&lists_.counts, sizeof(int) * (LIST_N + 1)));
+    CUE(cudaMemsetAsync(lists_.counts, 0, sizeof(int) * (LIST_N + 1), s_));
     CUE(cudaMallocHost(&h_flags_, sizeof(BatchFlags)));
     CUE(cudaMallocHost(&h_st_, sizeof(InstState) * maxInst_));
     CUE(cudaMemsetAsync(d_dev_, 0, sizeof(InstDev) * maxInst_, s_));
@@ -199,6 +208,7 @@ Batch Engine::batch() const {
     B.tiles = d_tiles_;
     B.ntiles = d_ntiles_;
     B.flags = d_flags_;
+    B.L = lists_;
     B.maxTiles = maxTiles_;
     B.maxInst = maxInst_;
     return B;
@@ -486,19 +496,28 @@ int Engine::record_stage(Rec& r, int uin, int uout, cudaEvent_t ev0, cudaEvent_t
     TRYE(r.k([&](cudaStream_t s) { K->flux(B, uin, FLUX_DIRTY, s); }));
     TRYE(r.k([&](cudaStream_t s) { K->ct_update_detect(B, uin, uout, s); }));
     TRYE(r.k([&](cudaStream_t s) { K->mood_flags(B, s); }));
+    if (trace) TRYE(r.host([&] { return trace_snapshot(); }));
+    TRYE(r.k([&](cudaStream_t s) { K->clear_low(B, s); }));
     TRYE(r.cond(&hm, 0));
     TRYE(r.k([&](cudaStream_t s) { K->pass_end(B, hm, s); }));
     if (trace) TRYE(r.host([&] { return trace_after_pass(); }));
+    // later MOOD passes touch the flagged cells only: each step builds a work
+    // list (warp ballot + one atomic per warp) and a list kernel consumes it
     TRYE(r.loop(hm, &BatchFlags::anyActive, cap, [&](Rec& b) -> int {
         if (trace) TRYE(b.host([&] { return trace_before_pass(); }));
-        TRYE(b.k([&](cudaStream_t s) { K->recon_check(B, uin, MASK_REC, s); }));
+        TRYE(b.k([&](cudaStream_t s) { K->compact_rec(B, s); }));
+        TRYE(b.k([&](cudaStream_t s) { K->recon_list(B, uin, s); }));
         cudaGraphConditionalHandle hc2;
         TRYE(b.cond(&hc2, 0));
         TRYE(b.k([&](cudaStream_t s) { K->cascade_cond(B, hc2, s); }));
         TRYE(b.loop(hc2, &BatchFlags::anyFail, cap, cascade_body(hc2)));
-        TRYE(b.k([&](cudaStream_t s) { K->flux(B, uin, FLUX_REC, s); }));
-        TRYE(b.k([&](cudaStream_t s) { K->ct_update_detect(B, uin, uout, s); }));
+        TRYE(b.k([&](cudaStream_t s) { K->compact_faces(B, s); }));
+        TRYE(b.k([&](cudaStream_t s) { K->flux_list(B, uin, s); }));
+        TRYE(b.k([&](cudaStream_t s) { K->compact_recF(B, s); }));
+        TRYE(b.k([&](cudaStream_t s) { K->ct_list(B, uin, uout, s); }));
         TRYE(b.k([&](cudaStream_t s) { K->mood_flags(B, s); }));
+        if (trace) TRYE(b.host([&] { return trace_snapshot(); }));
+        TRYE(b.k([&](cudaStream_t s) { K->clear_low(B, s); }));
         TRYE(b.k([&](cudaStream_t s) { K->pass_end(B, hm, s); }));
         if (trace) TRYE(b.host([&] { return trace_after_pass(); }));
         return HOSONO_OK;
@@ -540,6 +559,10 @@ int Engine::build_graphs() {
         int rc;
         if (which == 0) {
             rc = record_step(r, true, 0, false);
+        } else if (which == 2) {
+            // one step at the graph's top level: event records are not allowed
+            // inside conditional bodies, and pass 1 sits outside the MOOD loops
+            rc = record_step(r, false, 0, true);
         } else {
             cudaGraphConditionalHandle hr;
             rc = r.cond(&hr, 1);
@@ -668,6 +691,22 @@ int Engine::trace_before_pass() {
     return HOSONO_OK;
 }
 
+int Engine::trace_snapshot() {
+    snapInner_.assign(maxInst_, {});
+    snapLow_.assign(maxInst_, {});
+    for (int k = 0; k < maxInst_; k++) {
+        if (!slots_[k].live) continue;
+        const Geo& G = slots_[k].dev.geo;
+        snapInner_[k].resize((size_t)G.plane);
+        snapLow_[k].resize((size_t)G.plane);
+        CUE(cudaMemcpyAsync(snapInner_[k].data(), slots_[k].dev.innerCount, (size_t)G.plane, cudaMemcpyDeviceToHost,
+                            s_));
+        CUE(cudaMemcpyAsync(snapLow_[k].data(), slots_[k].dev.lowered, (size_t)G.plane, cudaMemcpyDeviceToHost, s_));
+    }
+    CUE(cudaStreamSynchronize(s_));
+    return HOSONO_OK;
+}
+
 int Engine::trace_after_pass() {
     CUE(cudaMemcpyAsync(h_st_, d_st_, sizeof(InstState) * maxInst_, cudaMemcpyDeviceToHost, s_));
     CUE(cudaStreamSynchronize(s_));
@@ -683,10 +722,8 @@ int Engine::trace_after_pass() {
         t.pass = S.passes - 1;
         t.nInner = S.lastInner;
         t.nDetect = S.lastDetect;
-        std::vector<unsigned char> a((size_t)G.plane), b((size_t)G.plane);
-        CUE(cudaMemcpyAsync(a.data(), slots_[k].dev.innerCount, (size_t)G.plane, cudaMemcpyDeviceToHost, s_));
-        CUE(cudaMemcpyAsync(b.data(), slots_[k].dev.lowered, (size_t)G.plane, cudaMemcpyDeviceToHost, s_));
-        CUE(cudaStreamSynchronize(s_));
+        const std::vector<unsigned char>& a = snapInner_[k];
+        const std::vector<unsigned char>& b = snapLow_[k];
         t.inner.resize((size_t)G.nxt * G.nyt);
         t.detect.resize((size_t)G.nxt * G.nyt);
         for (int j = 0; j < G.nyt; j++)

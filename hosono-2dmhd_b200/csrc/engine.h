@@ -97,6 +97,18 @@ __host__ __device__ inline double* role_ptr(const InstDev& d, int parity, int ro
     return role == ROLE_STATE ? d.U[parity] : role == ROLE_A ? d.U[1 - parity] : d.U[2];
 }
 
+// Work lists of the later MOOD passes (compacted by warp ballot): entries are
+// (instance, cell index j*pitch+i); face entries carry 2*cell+dir.
+enum : int { LIST_REC = 0, LIST_FACE = 1, LIST_RECF = 2, LIST_LOW = 3, LIST_N = 4, LIST_OVERFLOW = 4 };
+struct Lists {
+    int2* rec;    // cells to re-reconstruct (recompute set)
+    int2* face;   // faces to re-flux
+    int2* recF;   // cells to FLICD + update + detect (recomputeFLICD set)
+    int2* low;    // cells detect lowered this pass (to clear `lowered` after use)
+    int* counts;  // [LIST_*] entries, [LIST_OVERFLOW] set if a list overflowed
+    long long cap;  // entries per list (the face list holds 2*cap)
+};
+
 // One kernel launch over the batch: tables and the tile list.
 struct Batch {
     const InstDev* dev;
@@ -104,7 +116,8 @@ struct Batch {
     const int4* tiles;   // x: instance, y: x0, z: y0
     const int* ntiles;   // device counter
     BatchFlags* flags;
-    int maxTiles;        // grid size of tile launches
+    Lists L;
+    int maxTiles;        // capacity of the tile list
     int maxInst;         // capacity (slots)
 };
 
@@ -130,6 +143,14 @@ struct KernelSet {
     void (*ct_update_detect)(const Batch&, int uin, int uout, cudaStream_t);
     void (*mood_flags)(const Batch&, cudaStream_t);
     void (*pass_end)(const Batch&, cudaGraphConditionalHandle h, cudaStream_t);
+    // later MOOD passes on compacted work lists
+    void (*compact_rec)(const Batch&, cudaStream_t);
+    void (*recon_list)(const Batch&, int uin, cudaStream_t);
+    void (*compact_faces)(const Batch&, cudaStream_t);
+    void (*flux_list)(const Batch&, int uin, cudaStream_t);
+    void (*compact_recF)(const Batch&, cudaStream_t);
+    void (*ct_list)(const Batch&, int uin, int uout, cudaStream_t);
+    void (*clear_low)(const Batch&, cudaStream_t);
     // RK3 combines and boundary conditions
     void (*bc_fill)(const Batch&, int role, cudaStream_t);
     void (*rk_combine2)(const Batch&, cudaStream_t);

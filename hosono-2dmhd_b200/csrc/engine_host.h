@@ -85,6 +85,7 @@ class Engine {
     int sync();
     int check_errors();
     int trace_before_pass();
+    int trace_snapshot();
     int trace_after_pass();
 
     const KernelSet* K_ = nullptr;
@@ -95,6 +96,7 @@ class Engine {
     int4* d_tiles_ = nullptr;
     int* d_ntiles_ = nullptr;
     BatchFlags* d_flags_ = nullptr;
+    Lists lists_{};
     BatchFlags* h_flags_ = nullptr;  // pinned
     InstState* h_st_ = nullptr;      // pinned
     double* staging_ = nullptr;
@@ -105,6 +107,7 @@ class Engine {
     cudaGraphExec_t gAdvance_ = nullptr, gRun_ = nullptr, gProf_ = nullptr;
     cudaEvent_t profEv_[6] = {};
     std::vector<long long> tracePassesSeen_;
+    std::vector<std::vector<unsigned char>> snapInner_, snapLow_;
 };
 
 }  // namespace hosono

@@ -129,107 +129,132 @@ __device__ __forceinline__ void warp_count(int* counter, bool v) {
 // faces fails; the verdicts are kept per face side in failX / failY and
 // combined by cascade_lower.  Fluxes next to a cell the cascade
 // re-reconstructs are recomputed after it (flux, FLUX_DIRTY).
+//
+// The block stages its tile's stencil box -- x in [x0-4, x0+36), y in
+// [y0-1-R, y0+9+R), all 8 planes -- in shared memory (16-byte vector loads,
+// 256-byte rows), so every GP dot product reads shared memory at offsets
+// known at compile time.
 template <int R>
-__device__ __forceinline__ bool pass1_body(const InstDev& d, const double* __restrict__ U, int i, int j) {
-    const Geo& G = d.geo;
-    const Phys& P = d.phys;
-    const int g = G.g;
-    const int clo = g - 2, cxhi = g + G.nx + 1, cyhi = g + G.ny + 1;  // reconstruct range
-    const int flo = g - 1, fxhi = g + G.nx + 1, fyhi = g + G.ny + 1;  // flux range
-    const long long c = (long long)j * G.pitch + i;
-    constexpr int NQ = R + 1;
-    bool bad = false;
-    // x-face
-    if (i >= clo && i <= cxhi + 1 && j >= clo && j <= cyhi) {
-        const bool needL = (i - 1 >= clo);
-        const bool needR = (i <= cxhi);
-        const bool doFlux = (i >= flo && i <= fxhi && j >= flo && j <= fyhi);
-        uint8_t bits = 0;
-        double acc[NCONS];
+struct P1Box {
+    static constexpr int SX = TILE_X + 8;          // [x0-4, x0+36)
+    static constexpr int SY = TILE_Y + 2 * R + 1;  // [y0-1-R, y0+8+R)
+    static constexpr int PLANE = SX * SY;
+    static constexpr int DOUBLES = NCONS * PLANE;
+    static constexpr int OX = 4, OY = 1 + R;       // shared coordinates of the tile origin
+};
+
+// GP prediction from the shared box: sum_k pv(k,q,f,RR) * U(:, stencil_k)
+// around shared coordinates (sx, sy), stencil order k=1..ns
+template <int RR, int R>
+__device__ __forceinline__ void gp_face_s(const double* __restrict__ sU, int sx, int sy,
+                                          const double* __restrict__ pvq, double out[NCONS]) {
+    constexpr int SX = P1Box<R>::SX, PL = P1Box<R>::PLANE;
+    const double* base = sU + sy * SX + sx;
 #pragma unroll
-        for (int v = 0; v < NCONS; v++) acc[v] = 0.0;
-#pragma unroll 1
-        for (int q = 0; q < NQ; q++) {
-            double uL[NCONS], uR[NCONS];
-            if (needL) {
-                gp_face<R>(U, G.plane, G.pitch, i - 1, j, pv_ptr(d, R, EAST, q), uL);
-                if (!admissible(uL[DENS], cons2pres(P, uL))) bits |= 1;
-            }
-            if (needR) {
-                gp_face<R>(U, G.plane, G.pitch, i, j, pv_ptr(d, R, WEST, q), uR);
-                if (!admissible(uR[DENS], cons2pres(P, uR))) bits |= 2;
-            }
-            if (doFlux) {
-                double F[NCONS];
-                hllc(P, uL, uR, XDIR, F);
-                const double w = qw_at(d, R, q);
+    for (int v = 0; v < NCONS; v++) out[v] = 0.0;
+    int k = 0;
 #pragma unroll
-                for (int v = 0; v < NCONS; v++) acc[v] = acc[v] + w * F[v];
-            }
-        }
-        d.failX[c] = bits;
-        bad |= bits != 0;
-        if (doFlux) {
+    for (int a = -RR; a <= RR; a++) {
 #pragma unroll
-            for (int v = 0; v < NCONS; v++) d.FX[v * G.plane + c] = acc[v];
-            d.CTX[c] = acc[MAGY];
+        for (int b = -RR; b <= RR; b++) {
+            if (iabs_c(a) + iabs_c(b) <= RR) {
+                const double p = __ldg(pvq + k);
+#pragma unroll
+                for (int v = 0; v < NCONS; v++) out[v] = out[v] + p * base[v * PL + b * SX + a];
+                k++;
+            }
         }
     }
-    // y-face
-    if (i >= clo && i <= cxhi && j >= clo && j <= cyhi + 1) {
-        const bool needB = (j - 1 >= clo);
-        const bool needT = (j <= cyhi);
-        const bool doFlux = (i >= flo && i <= fxhi && j >= flo && j <= fyhi);
-        uint8_t bits = 0;
-        double acc[NCONS];
-#pragma unroll
-        for (int v = 0; v < NCONS; v++) acc[v] = 0.0;
-#pragma unroll 1
-        for (int q = 0; q < NQ; q++) {
-            double uL[NCONS], uR[NCONS];
-            if (needB) {
-                gp_face<R>(U, G.plane, G.pitch, i, j - 1, pv_ptr(d, R, NORTH, q), uL);
-                if (!admissible(uL[DENS], cons2pres(P, uL))) bits |= 1;
-            }
-            if (needT) {
-                gp_face<R>(U, G.plane, G.pitch, i, j, pv_ptr(d, R, SOUTH, q), uR);
-                if (!admissible(uR[DENS], cons2pres(P, uR))) bits |= 2;
-            }
-            if (doFlux) {
-                double F[NCONS];
-                hllc(P, uL, uR, YDIR, F);
-                const double w = qw_at(d, R, q);
-#pragma unroll
-                for (int v = 0; v < NCONS; v++) acc[v] = acc[v] + w * F[v];
-            }
-        }
-        d.failY[c] = bits;
-        bad |= bits != 0;
-        if (doFlux) {
-#pragma unroll
-            for (int v = 0; v < NCONS; v++) d.FY[v * G.plane + c] = acc[v];
-            d.CTY[c] = acc[MAGX];
-        }
-    }
-    return bad;
 }
 
-// One launch per radius: blocks of instances with another GP radius leave at once.
-template <int R>
-__device__ __forceinline__ void t_face_pass1(const Batch& B, int uin, const Cell c) {
-    InstState& S = B.st[c.k];
-    if (!S.stepping) return;
-    const InstDev& d = B.dev[c.k];
-    if (d.geo.R != R) return;
-    const double* U = role_ptr(d, S.parity, uin);
-    if (first_tile_thread(c)) S.cascadeMode = CASCADE_FROM_FACES;
-    bool bad = false;
-    if (c.i < d.geo.nxt && c.j < d.geo.nyt) bad = pass1_body<R>(d, U, c.i, c.j);
-    warp_flag(&S.anyFail, bad);
+// one face (both sides, every quadrature point); returns the side verdict bits
+template <int R, int DIR>
+__device__ __forceinline__ uint8_t pass1_face(const InstDev& d, const double* __restrict__ sU, int sx, int sy,
+                                              bool needL, bool needR, bool doFlux, long long c) {
+    const Geo& G = d.geo;
+    const Phys& P = d.phys;
+    constexpr int NQ = R + 1;
+    constexpr int FL = DIR == XDIR ? EAST : NORTH, FR = DIR == XDIR ? WEST : SOUTH;
+    const int lx = DIR == XDIR ? sx - 1 : sx, ly = DIR == XDIR ? sy : sy - 1;
+    uint8_t bits = 0;
+    double acc[NCONS];
+#pragma unroll
+    for (int v = 0; v < NCONS; v++) acc[v] = 0.0;
+#pragma unroll 1
+    for (int q = 0; q < NQ; q++) {
+        double uL[NCONS], uR[NCONS];
+        if (needL) {
+            gp_face_s<R, R>(sU, lx, ly, pv_ptr(d, R, FL, q), uL);
+            if (!admissible(uL[DENS], cons2pres(P, uL))) bits |= 1;
+        }
+        if (needR) {
+            gp_face_s<R, R>(sU, sx, sy, pv_ptr(d, R, FR, q), uR);
+            if (!admissible(uR[DENS], cons2pres(P, uR))) bits |= 2;
+        }
+        if (doFlux) {
+            double F[NCONS];
+            hllc(P, uL, uR, DIR, F);
+            const double w = qw_at(d, R, q);
+#pragma unroll
+            for (int v = 0; v < NCONS; v++) acc[v] = acc[v] + w * F[v];
+        }
+    }
+    if (doFlux) {
+        double* Fo = DIR == XDIR ? d.FX : d.FY;
+#pragma unroll
+        for (int v = 0; v < NCONS; v++) Fo[v * G.plane + c] = acc[v];
+        (DIR == XDIR ? d.CTX : d.CTY)[c] = DIR == XDIR ? acc[MAGY] : acc[MAGX];
+    }
+    return bits;
 }
+
+// One launch per radius: blocks of instances with another GP radius skip the tile.
 template <int R>
 __global__ void __launch_bounds__(NTHREADS, HOSONO_PASS1_MIN_BLOCKS) k_face_pass1(Batch B, int uin) {
-    FOR_TILES(B, t) t_face_pass1<R>(B, uin, tile_at(B, t));
+    extern __shared__ double sU[];
+    using Box = P1Box<R>;
+    const int tid = threadIdx.y * TILE_X + threadIdx.x;
+    FOR_TILES(B, t) {
+        const Cell c = tile_at(B, t);
+        InstState& S = B.st[c.k];
+        const InstDev& d = B.dev[c.k];
+        if (!S.stepping || d.geo.R != R) continue;  // uniform over the block
+        const Geo& G = d.geo;
+        const double* __restrict__ U = role_ptr(d, S.parity, uin);
+        const int x0 = c.i - threadIdx.x - Box::OX, y0 = c.j - threadIdx.y - Box::OY;
+        __syncthreads();  // the previous tile's reads of sU are done
+        for (int e = tid; e < NCONS * Box::SY * (Box::SX / 2); e += NTHREADS) {
+            const int v = e / (Box::SY * (Box::SX / 2));
+            const int r = e - v * (Box::SY * (Box::SX / 2));
+            const int yy = r / (Box::SX / 2), xx = 2 * (r - yy * (Box::SX / 2));
+            const int gx = x0 + xx, gy = y0 + yy;
+            double2 val = make_double2(0.0, 0.0);
+            if (gx >= 0 && gx < G.pitch && gy >= 0 && gy < G.nyt)
+                val = __ldg(reinterpret_cast<const double2*>(U + v * G.plane + (long long)gy * G.pitch + gx));
+            *reinterpret_cast<double2*>(sU + v * Box::PLANE + yy * Box::SX + xx) = val;
+        }
+        __syncthreads();
+        if (first_tile_thread(c)) S.cascadeMode = CASCADE_FROM_FACES;
+        const int i = c.i, j = c.j;
+        const int g = G.g;
+        const int clo = g - 2, cxhi = g + G.nx + 1, cyhi = g + G.ny + 1;  // reconstruct range
+        const int flo = g - 1, fxhi = g + G.nx + 1, fyhi = g + G.ny + 1;  // flux range
+        const int sx = threadIdx.x + Box::OX, sy = threadIdx.y + Box::OY;
+        const long long cc = (long long)j * G.pitch + i;
+        const bool inF = i >= flo && i <= fxhi && j >= flo && j <= fyhi;
+        bool bad = false;
+        if (i >= clo && i <= cxhi + 1 && j >= clo && j <= cyhi) {  // x-face
+            const uint8_t bits = pass1_face<R, XDIR>(d, sU, sx, sy, i - 1 >= clo, i <= cxhi, inF, cc);
+            d.failX[cc] = bits;
+            bad |= bits != 0;
+        }
+        if (i >= clo && i <= cxhi && j >= clo && j <= cyhi + 1) {  // y-face
+            const uint8_t bits = pass1_face<R, YDIR>(d, sU, sx, sy, j - 1 >= clo, j <= cyhi, inF, cc);
+            d.failY[cc] = bits;
+            bad |= bits != 0;
+        }
+        warp_flag(&S.anyFail, bad);
+    }
 }
 
 // ======================================================================
@@ -272,6 +297,36 @@ __global__ void __launch_bounds__(NTHREADS) k_clear_nextpass(Batch B) {
     FOR_TILES(B, t) t_clear_nextpass(B, tile_at(B, t));
 }
 
+// gridBlock_lowerOrder (gridBlock.f90:194-235) of cell (i,j) plus the mark of
+// its cross for the next inner pass
+__device__ __forceinline__ void lower_cell(const InstDev& d, const InstState& S, int i, int j, long long cc) {
+    const Geo& G = d.geo;
+    int8_t* sch = d.scheme[S.schemeSel];
+    const int s = sch[cc];
+    sch[cc] = (int8_t)(s - 1 > 0 ? s - 1 : 0);
+    d.rec[cc] = 1;
+    d.rec[cc + 1] = 1;
+    d.rec[cc - 1] = 1;
+    d.rec[cc + G.pitch] = 1;
+    d.rec[cc - G.pitch] = 1;
+    for (int jj = j - 2; jj <= j + 2; jj++) {
+        if (jj < 0 || jj >= G.nyt) continue;
+        for (int ii = i - 2; ii <= i + 2; ii++) {
+            if (ii < 0 || ii >= G.nxt) continue;
+            if (iabs_c(ii - i) + iabs_c(jj - j) <= 2) d.recF[(long long)jj * G.pitch + ii] = 1;
+        }
+    }
+    d.nextPass[cc] = 1;
+    d.nextPass[cc + 1] = 1;
+    d.nextPass[cc - 1] = 1;
+    d.nextPass[cc + G.pitch] = 1;
+    d.nextPass[cc - G.pitch] = 1;
+    d.innerCount[cc] = (uint8_t)(d.innerCount[cc] + 1);
+}
+
+// For each cell of [g-2, g+n+1]^2 that failed (face verdicts of pass 1, or the
+// `fail` plane of a re-reconstruction, which is cleared as it is consumed):
+// lower it.
 __device__ __forceinline__ void t_cascade_lower(const Batch& B, const Cell c) {
     InstState& S = B.st[c.k];
     if (!S.nextIter) return;
@@ -282,33 +337,13 @@ __device__ __forceinline__ void t_cascade_lower(const Batch& B, const Cell c) {
     bool f = false;
     if (i >= g - 2 && j >= g - 2 && i <= g + G.nx + 1 && j <= g + G.ny + 1) {
         const long long cc = (long long)j * G.pitch + i;
-        if (S.cascadeMode == CASCADE_FROM_FACES)
+        if (S.cascadeMode == CASCADE_FROM_FACES) {
             f = ((d.failX[cc] & 2) | (d.failX[cc + 1] & 1) | (d.failY[cc] & 2) | (d.failY[cc + G.pitch] & 1)) != 0;
-        else
+        } else {
             f = d.fail[cc] != 0;
-        if (f) {
-            int8_t* sch = d.scheme[S.schemeSel];
-            const int s = sch[cc];
-            sch[cc] = (int8_t)(s - 1 > 0 ? s - 1 : 0);
-            d.rec[cc] = 1;
-            d.rec[cc + 1] = 1;
-            d.rec[cc - 1] = 1;
-            d.rec[cc + G.pitch] = 1;
-            d.rec[cc - G.pitch] = 1;
-            for (int jj = j - 2; jj <= j + 2; jj++) {
-                if (jj < 0 || jj >= G.nyt) continue;
-                for (int ii = i - 2; ii <= i + 2; ii++) {
-                    if (ii < 0 || ii >= G.nxt) continue;
-                    if (iabs_c(ii - i) + iabs_c(jj - j) <= 2) d.recF[(long long)jj * G.pitch + ii] = 1;
-                }
-            }
-            d.nextPass[cc] = 1;
-            d.nextPass[cc + 1] = 1;
-            d.nextPass[cc - 1] = 1;
-            d.nextPass[cc + G.pitch] = 1;
-            d.nextPass[cc - G.pitch] = 1;
-            d.innerCount[cc] = (uint8_t)(d.innerCount[cc] + 1);
+            if (f) d.fail[cc] = 0;
         }
+        if (f) lower_cell(d, S, i, j, cc);
     }
     warp_count(&S.nInner, f);
 }
@@ -316,15 +351,43 @@ __global__ void __launch_bounds__(NTHREADS) k_cascade_lower(Batch B) {
     FOR_TILES(B, t) t_cascade_lower(B, tile_at(B, t));
 }
 
-// One inner pass of reconstruct_faceValsWithGP on flagged cells (mask = rec at
-// the start of a later MOOD pass, nextPass inside the cascade): all four faces
-// at rr = min(scheme(c), scheme(nbr)) (EDP1), CAD/PAD at every quadrature
-// point.  The radius used per face is recorded in rrRec.  The verdict plane
-// `fail` is written on the whole reconstruct range.
-__device__ __forceinline__ void t_recon_check(const Batch& B, int uin, int maskSel, const Cell c) {
+// One cell of an inner pass of reconstruct_faceValsWithGP: all four faces at
+// rr = min(scheme(c), scheme(nbr)) (EDP1), CAD/PAD at every quadrature point;
+// the radius used per face is recorded in rrRec.  Returns true if a face
+// state is inadmissible.
+__device__ __forceinline__ bool recon_cell(const InstDev& d, const InstState& S, int uin, int i, int j,
+                                           long long cc) {
+    const Geo& G = d.geo;
+    const double* U = role_ptr(d, S.parity, uin);
+    const int8_t* sch = d.scheme[S.schemeSel];
+    d.dirty[cc] = 1;
+    const int s = sch[cc];
+    int rr[4];
+    rr[NORTH] = min(s, (int)sch[cc + G.pitch]);
+    rr[SOUTH] = min(s, (int)sch[cc - G.pitch]);
+    rr[EAST] = min(s, (int)sch[cc + 1]);
+    rr[WEST] = min(s, (int)sch[cc - 1]);
+    d.rrRec[cc] = (uint8_t)(rr[0] | (rr[1] << 2) | (rr[2] << 4) | (rr[3] << 6));
+    bool bad = false;
+#pragma unroll 1
+    for (int f = 0; f < 4 && !bad; f++) {
+        if (rr[f] == 0) continue;
+#pragma unroll 1
+        for (int q = 0; q <= rr[f] && !bad; q++) {
+            double u[NCONS];
+            face_value(d, U, rr[f], i, j, f, q, u);
+            if (!admissible(u[DENS], cons2pres(d.phys, u))) bad = true;
+        }
+    }
+    if (bad) d.fail[cc] = 1;
+    return bad;
+}
+
+// Inner cascade pass over the cells marked in nextPass (dense over the tiles
+// of instances in their cascade).
+__device__ __forceinline__ void t_recon_check(const Batch& B, int uin, int /*maskSel*/, const Cell c) {
     InstState& S = B.st[c.k];
-    const bool run = maskSel == MASK_REC ? (S.stepping && S.stageActive) : (S.nextIter != 0);
-    if (!run) return;
+    if (!S.nextIter) return;
     const InstDev& d = B.dev[c.k];
     const Geo& G = d.geo;
     const int g = G.g;
@@ -333,35 +396,119 @@ __device__ __forceinline__ void t_recon_check(const Batch& B, int uin, int maskS
     bool bad = false;
     if (i >= g - 2 && j >= g - 2 && i <= g + G.nx + 1 && j <= g + G.ny + 1) {
         const long long cc = (long long)j * G.pitch + i;
-        const uint8_t* mask = maskSel == MASK_REC ? d.rec : d.nextPass;
-        if (mask[cc]) {
-            const double* U = role_ptr(d, S.parity, uin);
-            const int8_t* sch = d.scheme[S.schemeSel];
-            d.dirty[cc] = 1;
-            const int s = sch[cc];
-            int rr[4];
-            rr[NORTH] = min(s, (int)sch[cc + G.pitch]);
-            rr[SOUTH] = min(s, (int)sch[cc - G.pitch]);
-            rr[EAST] = min(s, (int)sch[cc + 1]);
-            rr[WEST] = min(s, (int)sch[cc - 1]);
-            d.rrRec[cc] = (uint8_t)(rr[0] | (rr[1] << 2) | (rr[2] << 4) | (rr[3] << 6));
-#pragma unroll 1
-            for (int f = 0; f < 4 && !bad; f++) {
-                if (rr[f] == 0) continue;
-#pragma unroll 1
-                for (int q = 0; q <= rr[f] && !bad; q++) {
-                    double u[NCONS];
-                    face_value(d, U, rr[f], i, j, f, q, u);
-                    if (!admissible(u[DENS], cons2pres(d.phys, u))) bad = true;
-                }
-            }
-        }
-        d.fail[cc] = bad ? 1 : 0;
+        if (d.nextPass[cc]) bad = recon_cell(d, S, uin, i, j, cc);
     }
     warp_flag(&S.anyFail, bad);
 }
 __global__ void __launch_bounds__(NTHREADS) k_recon_check(Batch B, int uin, int maskSel) {
     FOR_TILES(B, t) t_recon_check(B, uin, maskSel, tile_at(B, t));
+}
+
+// ----------------------------------------------------------------------
+// Work lists of the later MOOD passes.  Appends are warp-aggregated: one
+// atomicAdd per warp reserves the slots, each active lane writes at its rank.
+__device__ __forceinline__ void warp_append(const Lists& L, int which, int2* list, long long cap, bool pred,
+                                            int2 item) {
+    const unsigned m = __ballot_sync(0xffffffffu, pred);
+    if (!m) return;
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(m) - 1;
+    int base = 0;
+    if (lane == leader) base = atomicAdd(L.counts + which, __popc(m));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    const long long pos = (long long)base + __popc(m & ((1u << lane) - 1));
+    if (pred) {
+        if (pos < cap)
+            list[pos] = item;
+        else
+            L.counts[LIST_OVERFLOW] = 1;
+    }
+}
+
+__device__ __forceinline__ int2 entry(int k, long long cc) { return make_int2(k, (int)cc); }
+
+// cells with recompute in the reconstruct range (reconstruct.f90:83)
+__device__ __forceinline__ void t_compact_rec(const Batch& B, const Cell c) {
+    InstState& S = B.st[c.k];
+    if (!(S.stepping && S.stageActive)) return;
+    const InstDev& d = B.dev[c.k];
+    const Geo& G = d.geo;
+    const int g = G.g;
+    if (first_tile_thread(c)) S.cascadeMode = CASCADE_FROM_CELLS;
+    bool p = false;
+    long long cc = 0;
+    if (c.i >= g - 2 && c.j >= g - 2 && c.i <= g + G.nx + 1 && c.j <= g + G.ny + 1) {
+        cc = (long long)c.j * G.pitch + c.i;
+        p = d.rec[cc] != 0;
+    }
+    warp_append(B.L, LIST_REC, B.L.rec, B.L.cap, p, entry(c.k, cc));
+}
+__global__ void __launch_bounds__(NTHREADS) k_compact_rec(Batch B) {
+    FOR_TILES(B, t) t_compact_rec(B, tile_at(B, t));
+}
+
+// faces getFluxes_ recomputes: x-face (i,j) if recompute(i,j) or (i-1,j),
+// y-face if recompute(i,j) or (i,j-1), on [g-1, g+n+1]^2 (getFluxes.f90:204-250)
+__device__ __forceinline__ void t_compact_faces(const Batch& B, const Cell c) {
+    const InstState& S = B.st[c.k];
+    if (!(S.stepping && S.stageActive)) return;
+    const InstDev& d = B.dev[c.k];
+    const Geo& G = d.geo;
+    const int g = G.g;
+    bool px = false, py = false;
+    long long cc = 0;
+    if (c.i >= g - 1 && c.j >= g - 1 && c.i <= g + G.nx + 1 && c.j <= g + G.ny + 1) {
+        cc = (long long)c.j * G.pitch + c.i;
+        const bool r = d.rec[cc] != 0;
+        px = r || d.rec[cc - 1] != 0;
+        py = r || d.rec[cc - G.pitch] != 0;
+    }
+    warp_append(B.L, LIST_FACE, B.L.face, 2 * B.L.cap, px, make_int2(c.k, (int)(2 * cc + XDIR)));
+    warp_append(B.L, LIST_FACE, B.L.face, 2 * B.L.cap, py, make_int2(c.k, (int)(2 * cc + YDIR)));
+}
+__global__ void __launch_bounds__(NTHREADS) k_compact_faces(Batch B) {
+    FOR_TILES(B, t) t_compact_faces(B, tile_at(B, t));
+}
+
+// cells with recomputeFLICD in the FLICD range [g, g+n]^2
+__device__ __forceinline__ void t_compact_recF(const Batch& B, const Cell c) {
+    const InstState& S = B.st[c.k];
+    if (!(S.stepping && S.stageActive)) return;
+    const InstDev& d = B.dev[c.k];
+    const Geo& G = d.geo;
+    const int g = G.g;
+    bool p = false;
+    long long cc = 0;
+    if (c.i >= g && c.j >= g && c.i <= g + G.nx && c.j <= g + G.ny) {
+        cc = (long long)c.j * G.pitch + c.i;
+        p = d.recF[cc] != 0;
+    }
+    warp_append(B.L, LIST_RECF, B.L.recF, B.L.cap, p, entry(c.k, cc));
+}
+__global__ void __launch_bounds__(NTHREADS) k_compact_recF(Batch B) {
+    FOR_TILES(B, t) t_compact_recF(B, tile_at(B, t));
+}
+
+// List kernels walk their list grid-stride in whole-warp steps, so warp
+// collectives see every lane.
+#define FOR_LIST(n, e, act)                                                                               \
+    for (int base_ = (blockIdx.x * blockDim.x + threadIdx.x) & ~31, e = base_ + (threadIdx.x & 31);      \
+         base_ < (n); base_ += gridDim.x * blockDim.x, e = base_ + (threadIdx.x & 31))                   \
+        for (bool act = e < (n), once_ = true; once_; once_ = false)
+
+// re-reconstruction of the rec list (first inner pass of a later MOOD pass)
+__global__ void __launch_bounds__(256) k_recon_list(Batch B, int uin) {
+    const int n = min(B.L.counts[LIST_REC], (int)B.L.cap);
+    FOR_LIST(n, e, act) {
+        if (act) {
+            const int2 it = B.L.rec[e];
+            InstState& S = B.st[it.x];
+            const InstDev& d = B.dev[it.x];
+            const long long cc = it.y;
+            const int j = (int)(cc / d.geo.pitch), i = (int)(cc - (long long)j * d.geo.pitch);
+            if (recon_cell(d, S, uin, i, j, cc)) atomicOr(&S.anyFail, 1);
+        }
+    }
 }
 
 // ======================================================================
@@ -431,6 +578,41 @@ __device__ __forceinline__ void t_flux(const Batch& B, int uin, int mode, const 
 }
 __global__ void __launch_bounds__(NTHREADS) k_flux(Batch B, int uin, int mode) {
     FOR_TILES(B, t) t_flux(B, uin, mode, tile_at(B, t));
+}
+
+// getFluxes_ on the face list of a later MOOD pass
+__device__ __forceinline__ void flux_face(const InstDev& d, const InstState& S, int uin, long long cc, int dir) {
+    const Geo& G = d.geo;
+    const int j = (int)(cc / G.pitch), i = (int)(cc - (long long)j * G.pitch);
+    const double* U = role_ptr(d, S.parity, uin);
+    const int8_t* sch = d.scheme[S.schemeSel];
+    double F[NCONS];
+    if (dir == XDIR) {
+        const long long cw = cc - 1;
+        const int rr = min((int)sch[cc], (int)sch[cw]);
+        const int rrL = (d.rrRec[cw] >> (2 * EAST)) & 3;
+        const int rrR = (d.rrRec[cc] >> (2 * WEST)) & 3;
+        face_flux(d, U, XDIR, i - 1, j, EAST, rrL, i, j, WEST, rrR, rr, F);
+#pragma unroll
+        for (int v = 0; v < NCONS; v++) d.FX[v * G.plane + cc] = F[v];
+        d.CTX[cc] = F[MAGY];
+    } else {
+        const long long cs = cc - G.pitch;
+        const int rr = min((int)sch[cc], (int)sch[cs]);
+        const int rrL = (d.rrRec[cs] >> (2 * NORTH)) & 3;
+        const int rrR = (d.rrRec[cc] >> (2 * SOUTH)) & 3;
+        face_flux(d, U, YDIR, i, j - 1, NORTH, rrL, i, j, SOUTH, rrR, rr, F);
+#pragma unroll
+        for (int v = 0; v < NCONS; v++) d.FY[v * G.plane + cc] = F[v];
+        d.CTY[cc] = F[MAGX];
+    }
+}
+__global__ void __launch_bounds__(256) k_flux_list(Batch B, int uin) {
+    const int n = min(B.L.counts[LIST_FACE], (int)(2 * B.L.cap));
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+        const int2 it = B.L.face[e];
+        flux_face(B.dev[it.x], B.st[it.x], uin, (long long)(it.y >> 1), it.y & 1);
+    }
 }
 
 // ======================================================================
@@ -533,63 +715,99 @@ __device__ __forceinline__ bool detect_cell(const InstDev& d, const double* __re
 // unsplit update of timeStep.f90:107-118 and detect_ALL.  A corrected flux a
 // neighbour needs is recomputed locally when the neighbour is flagged (it
 // writes the same value) and read from memory otherwise (nobody writes it).
-// `lowered` is written on the whole interior every pass.
+// A lowered cell sets `lowered` (cleared again after the flags are rebuilt)
+// and is appended to the lowered list.
+__device__ __forceinline__ bool ct_cell(const InstDev& d, const InstState& S, int uin, int uout, int i, int j,
+                                        long long cc) {
+    const Geo& G = d.geo;
+    const int g = G.g;
+    if (!d.recF[cc]) return false;
+    const double ctx = flicd_x(d, cc);
+    const double cty = flicd_y(d, cc);
+    d.CTX[cc] = ctx;
+    d.CTY[cc] = cty;
+    if (i >= g + G.nx || j >= g + G.ny) return false;  // FLICD-only row and column
+    const double* U = role_ptr(d, S.parity, uin);
+    double* Uo = role_ptr(d, S.parity, uout);
+    const long long ce = cc + 1, cn = cc + G.pitch;
+    const double ctx_e = d.recF[ce] ? flicd_x(d, ce) : d.CTX[ce];
+    const double cty_n = d.recF[cn] ? flicd_y(d, cn) : d.CTY[cn];
+    const double dt = S.dt;
+    const double dtdx = dt / G.dx, dtdy = dt / G.dy;
+    double un[NCONS];
+#pragma unroll
+    for (int v = 0; v < NCONS; v++) {
+        double f0, f1, g0, g1;
+        if (v == MAGX) {
+            f0 = 0.0;
+            f1 = 0.0;
+            g0 = cty;
+            g1 = cty_n;
+        } else if (v == MAGY) {
+            f0 = ctx;
+            f1 = ctx_e;
+            g0 = 0.0;
+            g1 = 0.0;
+        } else {
+            f0 = d.FX[v * G.plane + cc];
+            f1 = d.FX[v * G.plane + ce];
+            g0 = d.FY[v * G.plane + cc];
+            g1 = d.FY[v * G.plane + cn];
+        }
+        un[v] = U[v * G.plane + cc] - dtdx * (f1 - f0) - dtdy * (g1 - g0);
+        Uo[v * G.plane + cc] = un[v];
+    }
+    bool low = false;
+    if (d.scheme[S.schemeSel][cc] > 0) low = detect_cell(d, U, cc, un);
+    if (low) d.lowered[cc] = 1;
+    return low;
+}
+
 __device__ __forceinline__ void t_ct_update_detect(const Batch& B, int uin, int uout, const Cell c) {
     InstState& S = B.st[c.k];
     if (!(S.stepping && S.stageActive)) return;
     const InstDev& d = B.dev[c.k];
     const Geo& G = d.geo;
     const int g = G.g;
-    const int i = c.i, j = c.j;
     bool low = false;
-    if (i >= g && j >= g && i <= g + G.nx && j <= g + G.ny) {
-        const long long cc = (long long)j * G.pitch + i;
-        const bool interior = i < g + G.nx && j < g + G.ny;
-        if (d.recF[cc]) {
-            const double ctx = flicd_x(d, cc);
-            const double cty = flicd_y(d, cc);
-            d.CTX[cc] = ctx;
-            d.CTY[cc] = cty;
-            if (interior) {
-                const double* U = role_ptr(d, S.parity, uin);
-                double* Uo = role_ptr(d, S.parity, uout);
-                const long long ce = cc + 1, cn = cc + G.pitch;
-                const double ctx_e = d.recF[ce] ? flicd_x(d, ce) : d.CTX[ce];
-                const double cty_n = d.recF[cn] ? flicd_y(d, cn) : d.CTY[cn];
-                const double dt = S.dt;
-                const double dtdx = dt / G.dx, dtdy = dt / G.dy;
-                double un[NCONS];
-#pragma unroll
-                for (int v = 0; v < NCONS; v++) {
-                    double f0, f1, g0, g1;
-                    if (v == MAGX) {
-                        f0 = 0.0;
-                        f1 = 0.0;
-                        g0 = cty;
-                        g1 = cty_n;
-                    } else if (v == MAGY) {
-                        f0 = ctx;
-                        f1 = ctx_e;
-                        g0 = 0.0;
-                        g1 = 0.0;
-                    } else {
-                        f0 = d.FX[v * G.plane + cc];
-                        f1 = d.FX[v * G.plane + ce];
-                        g0 = d.FY[v * G.plane + cc];
-                        g1 = d.FY[v * G.plane + cn];
-                    }
-                    un[v] = U[v * G.plane + cc] - dtdx * (f1 - f0) - dtdy * (g1 - g0);
-                    Uo[v * G.plane + cc] = un[v];
-                }
-                if (d.scheme[S.schemeSel][cc] > 0) low = detect_cell(d, U, cc, un);
-            }
-        }
-        if (interior) d.lowered[cc] = low ? 1 : 0;
+    long long cc = 0;
+    if (c.i >= g && c.j >= g && c.i <= g + G.nx && c.j <= g + G.ny) {
+        cc = (long long)c.j * G.pitch + c.i;
+        low = ct_cell(d, S, uin, uout, c.i, c.j, cc);
     }
     warp_count(&S.nDetect, low);
+    warp_append(B.L, LIST_LOW, B.L.low, B.L.cap, low, entry(c.k, cc));
 }
 __global__ void __launch_bounds__(NTHREADS) k_ct_update_detect(Batch B, int uin, int uout) {
     FOR_TILES(B, t) t_ct_update_detect(B, uin, uout, tile_at(B, t));
+}
+
+// the same on the recomputeFLICD list of a later MOOD pass
+__global__ void __launch_bounds__(256) k_ct_list(Batch B, int uin, int uout) {
+    const int n = min(B.L.counts[LIST_RECF], (int)B.L.cap);
+    FOR_LIST(n, e, act) {
+        bool low = false;
+        int2 it = make_int2(0, 0);
+        if (act) {
+            it = B.L.recF[e];
+            InstState& S = B.st[it.x];
+            const InstDev& d = B.dev[it.x];
+            const long long cc = it.y;
+            const int j = (int)(cc / d.geo.pitch), i = (int)(cc - (long long)j * d.geo.pitch);
+            low = ct_cell(d, S, uin, uout, i, j, cc);
+            if (low) atomicAdd(&S.nDetect, 1);
+        }
+        warp_append(B.L, LIST_LOW, B.L.low, B.L.cap, low, it);
+    }
+}
+
+// `lowered` back to zero on the cells this pass lowered
+__global__ void __launch_bounds__(256) k_clear_low(Batch B) {
+    const int n = min(B.L.counts[LIST_LOW], (int)B.L.cap);
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+        const int2 it = B.L.low[e];
+        B.dev[it.x].lowered[it.y] = 0;
+    }
 }
 
 // ======================================================================
@@ -678,6 +896,8 @@ __global__ void k_pass_end(Batch B, cudaGraphConditionalHandle h, int set_handle
     __syncthreads();
     if (threadIdx.x == 0) {
         B.flags->anyActive = any;
+        if (B.L.counts[LIST_OVERFLOW]) B.flags->error = HOSONO_EINVAL;
+        for (int w = 0; w < LIST_N; w++) B.L.counts[w] = 0;  // the next pass builds its lists afresh
         if (set_handle) cudaGraphSetConditional(h, any ? 1u : 0u);
     }
 }
@@ -926,7 +1146,7 @@ const dim3 kTile(TILE_X, TILE_Y);
 
 // Grid of a tile kernel: as many blocks as fit on the GPU at once (the
 // kernels loop over the tile list), and never more than the tile capacity.
-int resident_blocks(const void* kernel) {
+int resident_blocks(const void* kernel, int smem = 0) {
     static const void* keys[64];
     static int vals[64];
     static int n = 0;
@@ -935,7 +1155,7 @@ int resident_blocks(const void* kernel) {
     int dev = 0, sms = 148, per = 1;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, TILE_X * TILE_Y, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, TILE_X * TILE_Y, smem);
     const int v = sms * (per > 0 ? per : 1);
     if (n < 64) {
         keys[n] = kernel;
@@ -958,10 +1178,16 @@ void l_step_end(const Batch& B, cudaGraphConditionalHandle h, cudaStream_t s) {
     k_step_end<<<1, 128, 0, s>>>(B, h, h != 0);
 }
 void l_stage_init(const Batch& B, cudaStream_t s) { TILE_LAUNCH(k_stage_init, B, s); }
+template <int R>
+void launch_pass1(const Batch& B, int uin, cudaStream_t s) {
+    constexpr int smem = P1Box<R>::DOUBLES * (int)sizeof(double);
+    const int r = resident_blocks((const void*)k_face_pass1<R>, smem);
+    k_face_pass1<R><<<dim3((unsigned)(r < B.maxTiles ? r : B.maxTiles)), kTile, smem, s>>>(B, uin);
+}
 void l_face_pass1(const Batch& B, int uin, cudaStream_t s) {
-    TILE_LAUNCH(k_face_pass1<2>, B, s, uin);
-    TILE_LAUNCH(k_face_pass1<1>, B, s, uin);
-    TILE_LAUNCH(k_face_pass1<3>, B, s, uin);
+    launch_pass1<2>(B, uin, s);
+    launch_pass1<1>(B, uin, s);
+    launch_pass1<3>(B, uin, s);
 }
 void l_cascade_cond(const Batch& B, cudaGraphConditionalHandle h, cudaStream_t s) {
     k_cascade_cond<<<1, 128, 0, s>>>(B, h, h != 0);
@@ -981,6 +1207,14 @@ void l_mood_flags(const Batch& B, cudaStream_t s) { TILE_LAUNCH(k_mood_flags, B,
 void l_pass_end(const Batch& B, cudaGraphConditionalHandle h, cudaStream_t s) {
     k_pass_end<<<1, 128, 0, s>>>(B, h, h != 0);
 }
+void l_compact_rec(const Batch& B, cudaStream_t s) { TILE_LAUNCH(k_compact_rec, B, s); }
+void l_compact_faces(const Batch& B, cudaStream_t s) { TILE_LAUNCH(k_compact_faces, B, s); }
+void l_compact_recF(const Batch& B, cudaStream_t s) { TILE_LAUNCH(k_compact_recF, B, s); }
+#define LIST_LAUNCH(kern, B, s, ...) kern<<<dim3((unsigned)resident_blocks((const void*)kern)), dim3(256), 0, s>>>(B, ##__VA_ARGS__)
+void l_recon_list(const Batch& B, int uin, cudaStream_t s) { LIST_LAUNCH(k_recon_list, B, s, uin); }
+void l_flux_list(const Batch& B, int uin, cudaStream_t s) { LIST_LAUNCH(k_flux_list, B, s, uin); }
+void l_ct_list(const Batch& B, int uin, int uout, cudaStream_t s) { LIST_LAUNCH(k_ct_list, B, s, uin, uout); }
+void l_clear_low(const Batch& B, cudaStream_t s) { LIST_LAUNCH(k_clear_low, B, s); }
 void l_bc_fill(const Batch& B, int role, cudaStream_t s) { TILE_LAUNCH(k_bc_fill, B, s, role); }
 void l_rk_combine2(const Batch& B, cudaStream_t s) { TILE_LAUNCH(k_rk_combine2, B, s); }
 void l_rk_final(const Batch& B, cudaStream_t s) { TILE_LAUNCH(k_rk_final, B, s); }
@@ -993,7 +1227,8 @@ const KernelSet kset = {
     "strict",
 #endif
     l_cfl_reduce, l_step_prepare, l_step_begin, l_step_end, l_stage_init, l_face_pass1, l_cascade_cond, l_cascade_lower,
-    l_recon_check, l_flux, l_ct_update_detect, l_mood_flags, l_pass_end, l_bc_fill, l_rk_combine2, l_rk_final,
+    l_recon_check, l_flux, l_ct_update_detect, l_mood_flags, l_pass_end, l_compact_rec, l_recon_list,
+    l_compact_faces, l_flux_list, l_compact_recF, l_ct_list, l_clear_low, l_bc_fill, l_rk_combine2, l_rk_final,
     l_cons2prim_all};
 
 }  // namespace KNS

@@ -163,39 +163,47 @@ __device__ __forceinline__ void hllc(const Phys& s, const double* uL, const doub
     const double sStr = (uR[mN] * dR - uL[mN] * dL + pTotL - pTotR - magNL * magNL + magNR * magNR) /
                         (rhoR * dR - rhoL * dL);
     const double pStr = rhoL * dL * (sStr - velNL) + pTotL - magNL * magNL + magNHLL * magNHLL;
-    if (0.0 < sL) {
+    // final choice (riemannSolver.f90:189-219): fL if 0 < sL; left star state
+    // if sL <= 0 < sStr; right star state if sStr <= 0 <= sR; fR otherwise.
+    // The star state is evaluated once, on the operands of the chosen side,
+    // with the statement order of the reference's branch for that side.
+    int side;
+    if (0.0 < sL)
+        side = 0;
+    else if ((sL <= 0.0) && (0.0 < sStr))
+        side = 1;
+    else if ((sStr <= 0.0) && (0.0 <= sR))
+        side = 2;
+    else
+        side = 3;
+    if (side == 0 || side == 3) {
 #pragma unroll
-        for (int v = 0; v < NCONS; v++) flux[v] = fL[v];
-    } else if ((sL <= 0.0) && (0.0 < sStr)) {
-        double uStr[NCONS];
-        uStr[DENS] = rhoL * dL / (sL - sStr);
-        uStr[mN] = uStr[DENS] * sStr;
-        uStr[mT1] = uStr[DENS] * vL[vT1] - (magNHLL * uHLL[bT1] - magNL * vL[bT1]) / (sL - sStr);
-        uStr[mT2] = uStr[DENS] * vL[vT2] - (magNHLL * uHLL[bT2] - magNL * vL[bT2]) / (sL - sStr);
-        uStr[bN] = magNHLL;
-        uStr[bT1] = uHLL[bT1];
-        uStr[bT2] = uHLL[bT2];
-        uStr[ENER] = uL[ENER] * dL + pStr * sStr - pTotL * velNL - magNHLL * magDotVelHLL + magNL * magDotVelL;
-        uStr[ENER] = uStr[ENER] / (sL - sStr);
-#pragma unroll
-        for (int v = 0; v < NCONS; v++) flux[v] = fL[v] + sL * (uStr[v] - uL[v]);
-    } else if ((sStr <= 0.0) && (0.0 <= sR)) {
-        double uStr[NCONS];
-        uStr[DENS] = rhoR * dR / (sR - sStr);
-        uStr[mN] = uStr[DENS] * sStr;
-        uStr[mT1] = uStr[DENS] * vR[vT1] - (magNHLL * uHLL[bT1] - magNR * vR[bT1]) / (sR - sStr);
-        uStr[mT2] = uStr[DENS] * vR[vT2] - (magNHLL * uHLL[bT2] - magNR * vR[bT2]) / (sR - sStr);
-        uStr[bN] = magNHLL;
-        uStr[bT1] = uHLL[bT1];
-        uStr[bT2] = uHLL[bT2];
-        uStr[ENER] = uR[ENER] * dR + pStr * sStr - pTotR * velNR - magNHLL * magDotVelHLL + magNR * magDotVelR;
-        uStr[ENER] = uStr[ENER] / (sR - sStr);
-#pragma unroll
-        for (int v = 0; v < NCONS; v++) flux[v] = fR[v] + sR * (uStr[v] - uR[v]);
-    } else {
-#pragma unroll
-        for (int v = 0; v < NCONS; v++) flux[v] = fR[v];
+        for (int v = 0; v < NCONS; v++) flux[v] = side == 0 ? fL[v] : fR[v];
+        return;
     }
+    const bool left = side == 1;
+    const double sK = left ? sL : sR;
+    const double rhoK = left ? rhoL : rhoR;
+    const double dK = left ? dL : dR;
+    const double velNK = left ? velNL : velNR;
+    const double pTotK = left ? pTotL : pTotR;
+    const double magNK = left ? magNL : magNR;
+    const double magDotVelK = left ? magDotVelL : magDotVelR;
+    const double vT1K = left ? vL[vT1] : vR[vT1], vT2K = left ? vL[vT2] : vR[vT2];
+    const double bT1K = left ? vL[bT1] : vR[bT1], bT2K = left ? vL[bT2] : vR[bT2];
+    const double eK = left ? uL[ENER] : uR[ENER];
+    double uStr[NCONS];
+    uStr[DENS] = rhoK * dK / (sK - sStr);
+    uStr[mN] = uStr[DENS] * sStr;
+    uStr[mT1] = uStr[DENS] * vT1K - (magNHLL * uHLL[bT1] - magNK * bT1K) / (sK - sStr);
+    uStr[mT2] = uStr[DENS] * vT2K - (magNHLL * uHLL[bT2] - magNK * bT2K) / (sK - sStr);
+    uStr[bN] = magNHLL;
+    uStr[bT1] = uHLL[bT1];
+    uStr[bT2] = uHLL[bT2];
+    uStr[ENER] = eK * dK + pStr * sStr - pTotK * velNK - magNHLL * magDotVelHLL + magNK * magDotVelK;
+    uStr[ENER] = uStr[ENER] / (sK - sStr);
+#pragma unroll
+    for (int v = 0; v < NCONS; v++) flux[v] = (left ? fL[v] : fR[v]) + sK * (uStr[v] - (left ? uL[v] : uR[v]));
 }
 
 // src/detect.f90:250-265 (CAD) and :238-248 (PAD)
