@@ -233,7 +233,7 @@ int Engine::live_count() const {
 
 namespace {
 constexpr int kDoublePlanes = 3 * NCONS + NPRIM + 2 * NCONS + 2;  // U x3, V, FX, FY, CTX, CTY
-constexpr int kBytePlanes = 12;
+constexpr int kBytePlanes = 13;
 size_t plane_of(const hosono_params& p) {
     const size_t nxt = p.nx + 2 * p.ngc, nyt = p.ny + 2 * p.ngc;
     const size_t pitch = (nxt + 31) / 32 * 32;
@@ -351,7 +351,8 @@ int Engine::add(const hosono_params& p, const double* pv, const double* qw, int*
     sl.dev.scheme[1] = (int8_t*)(b + plane);
     b += 2 * plane;
     uint8_t** bp[] = {&sl.dev.rec, &sl.dev.recF, &sl.dev.rrRec, &sl.dev.fail, &sl.dev.failX,
-                      &sl.dev.failY, &sl.dev.nextPass, &sl.dev.dirty, &sl.dev.lowered, &sl.dev.innerCount};
+                      &sl.dev.failY, &sl.dev.nextPass, &sl.dev.dirty, &sl.dev.lowered, &sl.dev.innerCount,
+                      &sl.dev.detMask};
     for (uint8_t** pp : bp) {
         *pp = b;
         b += plane;
@@ -477,6 +478,7 @@ int Engine::record_stage(Rec& r, int uin, int uout, cudaEvent_t ev0, cudaEvent_t
     const KernelSet* K = K_;
     const long long cap = (long long)INT_MAX;
     TRYE(r.k([&](cudaStream_t s) { K->stage_init(B, s); }));
+    TRYE(r.k([&](cudaStream_t s) { K->detect_prep(B, uin, s); }));
     if (ev0) TRYE(r.event(ev0));
     TRYE(r.k([&](cudaStream_t s) { K->face_pass1(B, uin, s); }));
     if (ev1) TRYE(r.event(ev1));
@@ -493,7 +495,8 @@ int Engine::record_stage(Rec& r, int uin, int uout, cudaEvent_t ev0, cudaEvent_t
         };
     };
     TRYE(r.loop(hc1, &BatchFlags::anyFail, cap, cascade_body(hc1)));
-    TRYE(r.k([&](cudaStream_t s) { K->flux(B, uin, FLUX_DIRTY, s); }));
+    TRYE(r.k([&](cudaStream_t s) { K->compact_dirty(B, s); }));
+    TRYE(r.k([&](cudaStream_t s) { K->flux_list(B, uin, s); }));
     TRYE(r.k([&](cudaStream_t s) { K->ct_update_detect(B, uin, uout, s); }));
     TRYE(r.k([&](cudaStream_t s) { K->mood_flags(B, s); }));
     if (trace) TRYE(r.host([&] { return trace_snapshot(); }));
@@ -511,9 +514,8 @@ int Engine::record_stage(Rec& r, int uin, int uout, cudaEvent_t ev0, cudaEvent_t
         TRYE(b.cond(&hc2, 0));
         TRYE(b.k([&](cudaStream_t s) { K->cascade_cond(B, hc2, s); }));
         TRYE(b.loop(hc2, &BatchFlags::anyFail, cap, cascade_body(hc2)));
-        TRYE(b.k([&](cudaStream_t s) { K->compact_faces(B, s); }));
+        TRYE(b.k([&](cudaStream_t s) { K->compact_post(B, s); }));
         TRYE(b.k([&](cudaStream_t s) { K->flux_list(B, uin, s); }));
-        TRYE(b.k([&](cudaStream_t s) { K->compact_recF(B, s); }));
         TRYE(b.k([&](cudaStream_t s) { K->ct_list(B, uin, uout, s); }));
         TRYE(b.k([&](cudaStream_t s) { K->mood_flags(B, s); }));
         if (trace) TRYE(b.host([&] { return trace_snapshot(); }));

@@ -54,6 +54,7 @@ struct InstDev {
     uint8_t* dirty;     // re-reconstructed by the pass-1 cascade
     uint8_t* lowered;   // lowered by detect in this pass
     uint8_t* innerCount;  // per-cell inner lowerings of this pass (trace)
+    uint8_t* detMask;     // per-stage detect_ALL terms (shock, plateau, u2 smooth)
 };
 
 // Per-instance mutable scalars (device memory).
@@ -146,9 +147,10 @@ struct KernelSet {
     // later MOOD passes on compacted work lists
     void (*compact_rec)(const Batch&, cudaStream_t);
     void (*recon_list)(const Batch&, int uin, cudaStream_t);
-    void (*compact_faces)(const Batch&, cudaStream_t);
+    void (*compact_post)(const Batch&, cudaStream_t);   // faces and recomputeFLICD cells
+    void (*compact_dirty)(const Batch&, cudaStream_t);  // pass-1 faces next to re-reconstructed cells
+    void (*detect_prep)(const Batch&, int uin, cudaStream_t);  // per-stage part of detect_ALL
     void (*flux_list)(const Batch&, int uin, cudaStream_t);
-    void (*compact_recF)(const Batch&, cudaStream_t);
     void (*ct_list)(const Batch&, int uin, int uout, cudaStream_t);
     void (*clear_low)(const Batch&, cudaStream_t);
     // RK3 combines and boundary conditions

@@ -447,11 +447,38 @@ __global__ void __launch_bounds__(NTHREADS) k_compact_rec(Batch B) {
     FOR_TILES(B, t) t_compact_rec(B, tile_at(B, t));
 }
 
-// faces getFluxes_ recomputes: x-face (i,j) if recompute(i,j) or (i-1,j),
-// y-face if recompute(i,j) or (i,j-1), on [g-1, g+n+1]^2 (getFluxes.f90:204-250)
-__device__ __forceinline__ void t_compact_faces(const Batch& B, const Cell c) {
+// After the face cascade of a later MOOD pass: the faces getFluxes_ recomputes
+// (x-face (i,j) if recompute(i,j) or (i-1,j), y-face if recompute(i,j) or
+// (i,j-1), on [g-1, g+n+1]^2, getFluxes.f90:204-250) and the cells FLICD,
+// the update and detect visit (recomputeFLICD on [g, g+n]^2).
+__device__ __forceinline__ void t_compact_post(const Batch& B, const Cell c) {
     const InstState& S = B.st[c.k];
     if (!(S.stepping && S.stageActive)) return;
+    const InstDev& d = B.dev[c.k];
+    const Geo& G = d.geo;
+    const int g = G.g;
+    bool px = false, py = false, pf = false;
+    long long cc = 0;
+    if (c.i >= g - 1 && c.j >= g - 1 && c.i <= g + G.nx + 1 && c.j <= g + G.ny + 1) {
+        cc = (long long)c.j * G.pitch + c.i;
+        const bool r = d.rec[cc] != 0;
+        px = r || d.rec[cc - 1] != 0;
+        py = r || d.rec[cc - G.pitch] != 0;
+        pf = c.i >= g && c.j >= g && c.i <= g + G.nx && c.j <= g + G.ny && d.recF[cc] != 0;
+    }
+    warp_append(B.L, LIST_FACE, B.L.face, 2 * B.L.cap, px, make_int2(c.k, (int)(2 * cc + XDIR)));
+    warp_append(B.L, LIST_FACE, B.L.face, 2 * B.L.cap, py, make_int2(c.k, (int)(2 * cc + YDIR)));
+    warp_append(B.L, LIST_RECF, B.L.recF, B.L.cap, pf, entry(c.k, cc));
+}
+__global__ void __launch_bounds__(NTHREADS) k_compact_post(Batch B) {
+    FOR_TILES(B, t) t_compact_post(B, tile_at(B, t));
+}
+
+// Pass 1 after a face cascade: the faces next to a re-reconstructed cell
+// (their pass-1 flux used face values that have since changed).
+__device__ __forceinline__ void t_compact_dirty(const Batch& B, const Cell c) {
+    const InstState& S = B.st[c.k];
+    if (!(S.stepping && S.stageActive && S.cascaded)) return;
     const InstDev& d = B.dev[c.k];
     const Geo& G = d.geo;
     const int g = G.g;
@@ -459,34 +486,15 @@ __device__ __forceinline__ void t_compact_faces(const Batch& B, const Cell c) {
     long long cc = 0;
     if (c.i >= g - 1 && c.j >= g - 1 && c.i <= g + G.nx + 1 && c.j <= g + G.ny + 1) {
         cc = (long long)c.j * G.pitch + c.i;
-        const bool r = d.rec[cc] != 0;
-        px = r || d.rec[cc - 1] != 0;
-        py = r || d.rec[cc - G.pitch] != 0;
+        const bool r = d.dirty[cc] != 0;
+        px = r || d.dirty[cc - 1] != 0;
+        py = r || d.dirty[cc - G.pitch] != 0;
     }
     warp_append(B.L, LIST_FACE, B.L.face, 2 * B.L.cap, px, make_int2(c.k, (int)(2 * cc + XDIR)));
     warp_append(B.L, LIST_FACE, B.L.face, 2 * B.L.cap, py, make_int2(c.k, (int)(2 * cc + YDIR)));
 }
-__global__ void __launch_bounds__(NTHREADS) k_compact_faces(Batch B) {
-    FOR_TILES(B, t) t_compact_faces(B, tile_at(B, t));
-}
-
-// cells with recomputeFLICD in the FLICD range [g, g+n]^2
-__device__ __forceinline__ void t_compact_recF(const Batch& B, const Cell c) {
-    const InstState& S = B.st[c.k];
-    if (!(S.stepping && S.stageActive)) return;
-    const InstDev& d = B.dev[c.k];
-    const Geo& G = d.geo;
-    const int g = G.g;
-    bool p = false;
-    long long cc = 0;
-    if (c.i >= g && c.j >= g && c.i <= g + G.nx && c.j <= g + G.ny) {
-        cc = (long long)c.j * G.pitch + c.i;
-        p = d.recF[cc] != 0;
-    }
-    warp_append(B.L, LIST_RECF, B.L.recF, B.L.cap, p, entry(c.k, cc));
-}
-__global__ void __launch_bounds__(NTHREADS) k_compact_recF(Batch B) {
-    FOR_TILES(B, t) t_compact_recF(B, tile_at(B, t));
+__global__ void __launch_bounds__(NTHREADS) k_compact_dirty(Batch B) {
+    FOR_TILES(B, t) t_compact_dirty(B, tile_at(B, t));
 }
 
 // List kernels walk their list grid-stride in whole-warp steps, so warp
@@ -632,83 +640,131 @@ __device__ __forceinline__ double flicd_y(const InstDev& d, long long c) {
     return (2 * fyx[c] + fyx[c + p] + fyx[c - p] - fxy[c + 1] - fxy[c] - fxy[c - p] - fxy[c + 1 - p]) / 8.0;
 }
 
-// detect_ALL's per-cell test (detect.f90:84-213): true when the cell must be lowered.
+// detect_ALL (detect.f90:84-213).  Everything but CAD, PAD and the DMP reads
+// only the stage input U, so it is the same in every MOOD pass of a stage:
+// k_detect_prep evaluates it once per stage into detMask --
+//   bit 0: shock1 && shock2 && shock3 (:115-146), bit 1: plateau (:161),
+//   bit 2: u2 smoothness accepts (:177-213, option 3) --
+// and the per-pass test keeps the reference's order of decisions.
+enum : int { DM_SHOCK = 1, DM_PLATEAU = 2, DM_SMOOTH = 4 };
+
 __device__ __forceinline__ bool detect_cell(const InstDev& d, const double* __restrict__ U, long long c,
                                             const double un[NCONS]) {
     const Geo& G = d.geo;
-    const Phys& s = d.phys;
-    const long long P = G.plane, p = G.pitch;
-    const double presNew = cons2pres(s, un);
-    if (!admissible(un[DENS], presNew)) return true;
-    double u[NCONS], V[NPRIM], Vip[NPRIM], Vim[NPRIM], Vjp[NPRIM], Vjm[NPRIM];
-#pragma unroll
-    for (int v = 0; v < NCONS; v++) u[v] = U[v * P + c];
-    cons2prim(s, u, V);
-#pragma unroll
-    for (int v = 0; v < NCONS; v++) u[v] = U[v * P + c + 1];
-    cons2prim(s, u, Vip);
-#pragma unroll
-    for (int v = 0; v < NCONS; v++) u[v] = U[v * P + c - 1];
-    cons2prim(s, u, Vim);
-#pragma unroll
-    for (int v = 0; v < NCONS; v++) u[v] = U[v * P + c + p];
-    cons2prim(s, u, Vjp);
-#pragma unroll
-    for (int v = 0; v < NCONS; v++) u[v] = U[v * P + c - p];
-    cons2prim(s, u, Vjm);
-    const double dx = G.dx, dy = G.dy;
-    double div_vel = (Vip[VELX] - Vim[VELX]) / (2 * dx);
-    div_vel = div_vel + (Vjp[VELY] - Vjm[VELY]) / (2 * dy);
-    const bool shock1 = div_vel < -(1.0 * (G.maxdxdy * G.maxdxdy));
-    double mach = V[VELX] * V[VELX] + V[VELY] * V[VELY];
-    mach = V[DENS] * mach / (V[GAMM] * V[PRES]);
-    mach = sqrt(mach);
-    const bool shock2 = mach > 0.2;
-    double pg = fabs(Vip[PRES] - Vim[PRES]) / (fmin(Vip[PRES], Vim[PRES]));
-    pg = pg + fabs(Vjp[PRES] - Vjm[PRES]) / (fmin(Vjp[PRES], Vjm[PRES]));
-    const bool shock3 = pg > 10.0 * G.maxdxdy;
-    if (!(shock1 && shock2 && shock3)) return false;
-    const double* rho = U + DENS * P;
+    const double presNew = cons2pres(d.phys, un);
+    if (!admissible(un[DENS], presNew)) return true;  // CAD, PAD
+    const int m = d.detMask[c];
+    if (!(m & DM_SHOCK)) return false;
+    if (m & DM_PLATEAU) return false;
+    const double* rho = U + DENS * G.plane;
+    const long long p = G.pitch;
     const double d1 = rho[c], d2 = rho[c + 1], d3 = rho[c - 1], d4 = rho[c + p], d5 = rho[c - p];
     const double mn = fmin(fmin(fmin(fmin(d1, d2), d3), d4), d5);
     const double mx = fmax(fmax(fmax(fmax(d1, d2), d3), d4), d5);
-    if (mx - mn < G.mindxdy * G.mindxdy * G.mindxdy) return false;
     const double dn = un[DENS];
-    if ((mn <= dn) && (dn <= mx)) return false;
-    // u2 smoothness (detect.f90:177-213, option 3)
-    double mnx = 0, mxx = 0, mny = 0, mxy = 0;
-    int k = 0;
+    if ((mn <= dn) && (dn <= mx)) return false;  // DMP
+    return !(m & DM_SMOOTH);
+}
+
+// Per-stage part of detect_ALL on the interior.  The primitive variables of
+// the tile and a one-cell halo are computed once into shared memory.
+constexpr int DP_SX = TILE_X + 2, DP_SY = TILE_Y + 2;
+__device__ __forceinline__ void t_detect_prep(const Batch& B, int uin, const Cell c, double* sV) {
+    const InstState& S = B.st[c.k];
+    if (!S.stepping) return;
+    const InstDev& d = B.dev[c.k];
+    const Geo& G = d.geo;
+    const Phys& P = d.phys;
+    const double* U = role_ptr(d, S.parity, uin);
+    const int x0 = c.i - (int)threadIdx.x - 1, y0 = c.j - (int)threadIdx.y - 1;
+    const int tid = threadIdx.y * TILE_X + threadIdx.x;
+    __syncthreads();  // the previous tile's reads of sV are done
+    for (int e = tid; e < DP_SX * DP_SY; e += TILE_X * TILE_Y) {
+        const int ey = e / DP_SX, ex = e - ey * DP_SX;
+        const int gx = x0 + ex, gy = y0 + ey;
+        double vx = 0.0, vy = 0.0, pr = 1.0, rho = 1.0;
+        if (gx >= 0 && gx < G.nxt && gy >= 0 && gy < G.nyt) {
+            double u[NCONS], V[NPRIM];
+            const long long g = (long long)gy * G.pitch + gx;
 #pragma unroll
-    for (int ii = -1; ii <= 1; ii++) {
+            for (int v = 0; v < NCONS; v++) u[v] = U[v * G.plane + g];
+            cons2prim(P, u, V);
+            vx = V[VELX];
+            vy = V[VELY];
+            pr = V[PRES];
+            rho = V[DENS];
+        }
+        sV[0 * DP_SX * DP_SY + e] = vx;
+        sV[1 * DP_SX * DP_SY + e] = vy;
+        sV[2 * DP_SX * DP_SY + e] = pr;
+        sV[3 * DP_SX * DP_SY + e] = rho;
+    }
+    __syncthreads();
+    const int g = G.g;
+    if (!(c.i >= g && c.j >= g && c.i < g + G.nx && c.j < g + G.ny)) return;
+    const int e = (threadIdx.y + 1) * DP_SX + threadIdx.x + 1;
+    const double* svx = sV;
+    const double* svy = sV + DP_SX * DP_SY;
+    const double* spr = sV + 2 * DP_SX * DP_SY;
+    const double* srho = sV + 3 * DP_SX * DP_SY;
+    const double dx = G.dx, dy = G.dy;
+    double div_vel = (svx[e + 1] - svx[e - 1]) / (2 * dx);
+    div_vel = div_vel + (svy[e + DP_SX] - svy[e - DP_SX]) / (2 * dy);
+    const bool shock1 = div_vel < -(1.0 * (G.maxdxdy * G.maxdxdy));
+    double mach = svx[e] * svx[e] + svy[e] * svy[e];
+    mach = srho[e] * mach / (P.gamma * spr[e]);
+    mach = sqrt(mach);
+    const bool shock2 = mach > 0.2;
+    double pg = fabs(spr[e + 1] - spr[e - 1]) / (fmin(spr[e + 1], spr[e - 1]));
+    pg = pg + fabs(spr[e + DP_SX] - spr[e - DP_SX]) / (fmin(spr[e + DP_SX], spr[e - DP_SX]));
+    const bool shock3 = pg > 10.0 * G.maxdxdy;
+    const long long cc = (long long)c.j * G.pitch + c.i;
+    int m = 0;
+    if (shock1 && shock2 && shock3) {
+        m |= DM_SHOCK;
+        const double* rho = U + DENS * G.plane;
+        const long long p = G.pitch;
+        const double d1 = rho[cc], d2 = rho[cc + 1], d3 = rho[cc - 1], d4 = rho[cc + p], d5 = rho[cc - p];
+        const double mn = fmin(fmin(fmin(fmin(d1, d2), d3), d4), d5);
+        const double mx = fmax(fmax(fmax(fmax(d1, d2), d3), d4), d5);
+        if (mx - mn < G.mindxdy * G.mindxdy * G.mindxdy) m |= DM_PLATEAU;
+        double mnx = 0, mxx = 0, mny = 0, mxy = 0;
+        int k = 0;
 #pragma unroll
-        for (int jj = -1; jj <= 1; jj++) {
-            if (iabs_c(ii) + iabs_c(jj) <= 1) {
-                const long long cc = c + ii + jj * p;
-                const double ddx = (rho[cc + 1] - 2 * rho[cc] + rho[cc - 1]) / (dx * dx);
-                const double ddy = (rho[cc + p] - 2 * rho[cc] + rho[cc - p]) / (dy * dy);
-                if (k == 0) {
-                    mnx = mxx = ddx;
-                    mny = mxy = ddy;
-                } else {
-                    mnx = fmin(mnx, ddx);
-                    mxx = fmax(mxx, ddx);
-                    mny = fmin(mny, ddy);
-                    mxy = fmax(mxy, ddy);
+        for (int ii = -1; ii <= 1; ii++) {
+#pragma unroll
+            for (int jj = -1; jj <= 1; jj++) {
+                if (iabs_c(ii) + iabs_c(jj) <= 1) {
+                    const long long q = cc + ii + jj * p;
+                    const double ddx = (rho[q + 1] - 2 * rho[q] + rho[q - 1]) / (dx * dx);
+                    const double ddy = (rho[q + p] - 2 * rho[q] + rho[q - p]) / (dy * dy);
+                    if (k == 0) {
+                        mnx = mxx = ddx;
+                        mny = mxy = ddy;
+                    } else {
+                        mnx = fmin(mnx, ddx);
+                        mxx = fmax(mxx, ddx);
+                        mny = fmin(mny, ddy);
+                        mxy = fmax(mxy, ddy);
+                    }
+                    k++;
                 }
-                k++;
             }
         }
+        const double mm = G.mindxdy;
+        const bool sx1 = (mnx * mxx > -mm);
+        const bool sy1 = (mny * mxy > -mm);
+        const bool sx2 = (fmax(fabs(mnx), fabs(mxx)) < mm);
+        const bool sy2 = (fmax(fabs(mny), fabs(mxy)) < mm);
+        const bool sx3 = (fmin(fabs(mnx), fabs(mxx)) >= 0.5 * fmax(fabs(mnx), fabs(mxx)));
+        const bool sy3 = (fmin(fabs(mny), fabs(mxy)) >= 0.5 * fmax(fabs(mny), fabs(mxy)));
+        if ((sx1 && sx2 && sy1 && sy2) || (sx1 && sx3 && sy1 && sy3)) m |= DM_SMOOTH;
     }
-    const double m = G.mindxdy;
-    const bool sx1 = (mnx * mxx > -m);
-    const bool sy1 = (mny * mxy > -m);
-    const bool sx2 = (fmax(fabs(mnx), fabs(mxx)) < m);
-    const bool sy2 = (fmax(fabs(mny), fabs(mxy)) < m);
-    const bool sx3 = (fmin(fabs(mnx), fabs(mxx)) >= 0.5 * fmax(fabs(mnx), fabs(mxx)));
-    const bool sy3 = (fmin(fabs(mny), fabs(mxy)) >= 0.5 * fmax(fabs(mny), fabs(mxy)));
-    const bool smooth1 = sx1 && sx2 && sy1 && sy2;
-    const bool smooth2 = sx1 && sx3 && sy1 && sy3;
-    return !(smooth1 || smooth2);
+    d.detMask[cc] = (uint8_t)m;
+}
+__global__ void __launch_bounds__(NTHREADS) k_detect_prep(Batch B, int uin) {
+    __shared__ double sV[4 * DP_SX * DP_SY];
+    FOR_TILES(B, t) t_detect_prep(B, uin, tile_at(B, t), sV);
 }
 
 // FLICD on [g, g+n]^2 where recomputeFLICD; then, on the interior, the
@@ -1208,8 +1264,9 @@ void l_pass_end(const Batch& B, cudaGraphConditionalHandle h, cudaStream_t s) {
     k_pass_end<<<1, 128, 0, s>>>(B, h, h != 0);
 }
 void l_compact_rec(const Batch& B, cudaStream_t s) { TILE_LAUNCH(k_compact_rec, B, s); }
-void l_compact_faces(const Batch& B, cudaStream_t s) { TILE_LAUNCH(k_compact_faces, B, s); }
-void l_compact_recF(const Batch& B, cudaStream_t s) { TILE_LAUNCH(k_compact_recF, B, s); }
+void l_compact_post(const Batch& B, cudaStream_t s) { TILE_LAUNCH(k_compact_post, B, s); }
+void l_compact_dirty(const Batch& B, cudaStream_t s) { TILE_LAUNCH(k_compact_dirty, B, s); }
+void l_detect_prep(const Batch& B, int uin, cudaStream_t s) { TILE_LAUNCH(k_detect_prep, B, s, uin); }
 #define LIST_LAUNCH(kern, B, s, ...) kern<<<dim3((unsigned)resident_blocks((const void*)kern)), dim3(256), 0, s>>>(B, ##__VA_ARGS__)
 void l_recon_list(const Batch& B, int uin, cudaStream_t s) { LIST_LAUNCH(k_recon_list, B, s, uin); }
 void l_flux_list(const Batch& B, int uin, cudaStream_t s) { LIST_LAUNCH(k_flux_list, B, s, uin); }
@@ -1228,7 +1285,7 @@ const KernelSet kset = {
 #endif
     l_cfl_reduce, l_step_prepare, l_step_begin, l_step_end, l_stage_init, l_face_pass1, l_cascade_cond, l_cascade_lower,
     l_recon_check, l_flux, l_ct_update_detect, l_mood_flags, l_pass_end, l_compact_rec, l_recon_list,
-    l_compact_faces, l_flux_list, l_compact_recF, l_ct_list, l_clear_low, l_bc_fill, l_rk_combine2, l_rk_final,
+    l_compact_post, l_compact_dirty, l_detect_prep, l_flux_list, l_ct_list, l_clear_low, l_bc_fill, l_rk_combine2, l_rk_final,
     l_cons2prim_all};
 
 }  // namespace KNS
