@@ -123,50 +123,100 @@ __device__ __forceinline__ double dot3(double a0, double a1, double a2, double b
     return (0.0 + a0 * b0) + a1 * b1 + a2 * b2;
 }
 
-// src/riemannSolver.f90:68-221 (HLLC for MHD, Li 2005)
-__device__ __forceinline__ void hllc(const Phys& s, const double* uL, const double* uR, int dir, double* flux) {
-    double vL[NPRIM], vR[NPRIM];
-    cons2prim(s, uL, vL);
-    cons2prim(s, uR, vR);
-    const int vN = dir == XDIR ? VELX : VELY, vT1 = dir == XDIR ? VELY : VELX, vT2 = VELZ;
+// The primitive variables HLLC reads from one side: cons2prim
+// (convert.f90:198-234) without eint; b* are zero for a hydro run.
+struct Side {
+    double rho, vx, vy, vz, p, bx, by, bz;
+};
+__device__ __forceinline__ void side_prim(const Phys& s, const double* U, Side& V) {
+    double Bp;
+    if (s.force_hydro)
+        Bp = 0.0;
+    else
+        Bp = 0.5 * (U[MAGX] * U[MAGX] + U[MAGY] * U[MAGY] + U[MAGZ] * U[MAGZ]);
+    const double density = U[DENS];
+    V.rho = density;
+    V.vx = U[MOMX] / density;
+    V.vy = U[MOMY] / density;
+    V.vz = U[MOMZ] / density;
+    const double eint = (U[ENER] - Bp) / density - 0.5 * (V.vx * V.vx + V.vy * V.vy + V.vz * V.vz);
+    V.p = eos_pres(s, density, eint);
+    V.bx = s.force_hydro ? 0.0 : U[MAGX];
+    V.by = s.force_hydro ? 0.0 : U[MAGY];
+    V.bz = s.force_hydro ? 0.0 : U[MAGZ];
+}
+__device__ __forceinline__ double side_vel(const Side& V, int c) { return c == 0 ? V.vx : c == 1 ? V.vy : V.vz; }
+__device__ __forceinline__ double side_mag(const Side& V, int c) { return c == 0 ? V.bx : c == 1 ? V.by : V.bz; }
+
+// fast magnetosonic speed of one side or of the average state (eigen.f90:257-303)
+__device__ __forceinline__ double side_cf(const Phys& s, double rho0, double p0, double bx, double by, double bz,
+                                          double bN) {
+    const double rho = fmax(rho0, s.small_density);
+    const double p = fmax(p0, s.small_pressure);
+    const double BB = bx * bx + by * by + bz * bz;
+    return c_fs(s.gamma, rho, p, BB, bN, +1.0);
+}
+
+// cons2flux (convert.f90:28-92) of one side
+__device__ __forceinline__ void side_flux(const Phys& s, const double* U, const Side& V, int dir, double* F) {
+    double Bp = 0.0;
+    if (!s.force_hydro) Bp = 0.5 * (U[MAGX] * U[MAGX] + U[MAGY] * U[MAGY] + U[MAGZ] * U[MAGZ]);
+    const double E = U[ENER];
+    const double Ptot = V.p + Bp;
+    const int mN = dir == XDIR ? MOMX : MOMY, mT1 = dir == XDIR ? MOMY : MOMX, mT2 = MOMZ;
     const int bN = dir == XDIR ? MAGX : MAGY, bT1 = dir == XDIR ? MAGY : MAGX, bT2 = MAGZ;
-    const int mN = vN, mT1 = vT1, mT2 = vT2;
-    double eL1, eL7, eR1, eR7, eA1, eA7;
-    fast_speeds(s, vL, dir, eL1, eL7);
-    fast_speeds(s, vR, dir, eR1, eR7);
-    {
-        double vA[NPRIM];
-#pragma unroll
-        for (int v = 0; v < NPRIM; v++) vA[v] = (vL[v] + vR[v]) / 2.0;
-        fast_speeds(s, vA, dir, eA1, eA7);
+    const double vN = side_vel(V, dir), vT1 = side_vel(V, 1 - dir), vT2 = V.vz;
+    const double BN = side_mag(V, dir), BT1 = side_mag(V, 1 - dir), BT2 = V.bz;
+    F[DENS] = U[mN];
+    F[mN] = U[mN] * U[mN] / U[DENS] + Ptot;
+    F[mT1] = U[mN] * vT1;
+    F[mT2] = U[mN] * vT2;
+    F[ENER] = (E + Ptot) * vN;
+    F[bN] = 0.0;
+    F[bT1] = 0.0;
+    F[bT2] = 0.0;
+    if (!s.force_hydro) {
+        F[mN] = F[mN] - BN * BN;
+        F[mT1] = F[mT1] - BT1 * BN;
+        F[mT2] = F[mT2] - BT2 * BN;
+        F[bT1] = vN * BT1 - vT1 * BN;
+        F[bT2] = vN * BT2 - vT2 * BN;
+        F[ENER] = F[ENER] - BN * (V.vx * V.bx + V.vy * V.by + V.vz * V.bz);
     }
-    const double sL = fmin(eL1, eA1);
-    const double sR = fmax(eA7, eR7);
-    double fL[NCONS], fR[NCONS];
-    cons2flux(s, uL, vL, dir, fL);
-    cons2flux(s, uR, vR, dir, fR);
-    double uHLL[NCONS];
-#pragma unroll
-    for (int v = 0; v < NCONS; v++) uHLL[v] = (sR * uR[v] - sL * uL[v] + fL[v] - fR[v]) / (sR - sL);
-    const double velHx = uHLL[MOMX] / uHLL[DENS];
-    const double velHy = uHLL[MOMY] / uHLL[DENS];
-    const double velHz = uHLL[MOMZ] / uHLL[DENS];
-    const double magDotVelHLL = dot3(uHLL[MAGX], uHLL[MAGY], uHLL[MAGZ], velHx, velHy, velHz);
-    const double magDotVelL = dot3(vL[MAGX], vL[MAGY], vL[MAGZ], vL[VELX], vL[VELY], vL[VELZ]);
-    const double magDotVelR = dot3(vR[MAGX], vR[MAGY], vR[MAGZ], vR[VELX], vR[VELY], vR[VELZ]);
-    const double velNL = vL[vN], velNR = vR[vN];
-    const double magNL = vL[bN], magNR = vR[bN], magNHLL = uHLL[bN];
-    const double rhoL = vL[DENS], rhoR = vR[DENS];
-    const double pTotL = vL[PRES] + 0.5 * dot3(vL[MAGX], vL[MAGY], vL[MAGZ], vL[MAGX], vL[MAGY], vL[MAGZ]);
-    const double pTotR = vR[PRES] + 0.5 * dot3(vR[MAGX], vR[MAGY], vR[MAGZ], vR[MAGX], vR[MAGY], vR[MAGZ]);
+}
+
+// src/riemannSolver.f90:68-221 (HLLC for MHD, Li 2005).  Every value keeps
+// the reference's expression; what the chosen branch does not read is not
+// computed: a supersonic face (flux = fL or fR) evaluates one physical flux
+// and no HLL or star state, and the star state is evaluated once, on the
+// operands of the chosen side.
+__device__ __forceinline__ void hllc(const Phys& s, const double* uL, const double* uR, int dir, double* flux) {
+    Side L, R;
+    side_prim(s, uL, L);
+    side_prim(s, uR, R);
+    const int mN = dir == XDIR ? MOMX : MOMY, mT1 = dir == XDIR ? MOMY : MOMX, mT2 = MOMZ;
+    const int bN = dir == XDIR ? MAGX : MAGY, bT1 = dir == XDIR ? MAGY : MAGX, bT2 = MAGZ;
+    const double velNL = side_vel(L, dir), velNR = side_vel(R, dir);
+    const double magNL = side_mag(L, dir), magNR = side_mag(R, dir);
+    // eigenvalues 1 and 7 of L, R and the arithmetic average (riemannSolver.f90:84-96)
+    const double eL1 = velNL - side_cf(s, L.rho, L.p, L.bx, L.by, L.bz, magNL);
+    const double eR7 = velNR + side_cf(s, R.rho, R.p, R.bx, R.by, R.bz, magNR);
+    double sL, sR;
+    {
+        const double vNA = (velNL + velNR) / 2.0;
+        const double cfA = side_cf(s, (L.rho + R.rho) / 2.0, (L.p + R.p) / 2.0, (L.bx + R.bx) / 2.0,
+                                   (L.by + R.by) / 2.0, (L.bz + R.bz) / 2.0, (magNL + magNR) / 2.0);
+        sL = fmin(eL1, vNA - cfA);
+        sR = fmax(vNA + cfA, eR7);
+    }
+    const double rhoL = L.rho, rhoR = R.rho;
+    const double pTotL = L.p + 0.5 * dot3(L.bx, L.by, L.bz, L.bx, L.by, L.bz);
+    const double pTotR = R.p + 0.5 * dot3(R.bx, R.by, R.bz, R.bx, R.by, R.bz);
     const double dL = sL - velNL, dR = sR - velNR;
     const double sStr = (uR[mN] * dR - uL[mN] * dL + pTotL - pTotR - magNL * magNL + magNR * magNR) /
                         (rhoR * dR - rhoL * dL);
-    const double pStr = rhoL * dL * (sStr - velNL) + pTotL - magNL * magNL + magNHLL * magNHLL;
     // final choice (riemannSolver.f90:189-219): fL if 0 < sL; left star state
     // if sL <= 0 < sStr; right star state if sStr <= 0 <= sR; fR otherwise.
-    // The star state is evaluated once, on the operands of the chosen side,
-    // with the statement order of the reference's branch for that side.
     int side;
     if (0.0 < sL)
         side = 0;
@@ -177,23 +227,38 @@ __device__ __forceinline__ void hllc(const Phys& s, const double* uL, const doub
     else
         side = 3;
     if (side == 0 || side == 3) {
-#pragma unroll
-        for (int v = 0; v < NCONS; v++) flux[v] = side == 0 ? fL[v] : fR[v];
+        if (side == 0)
+            side_flux(s, uL, L, dir, flux);
+        else
+            side_flux(s, uR, R, dir, flux);
         return;
     }
+    double fL[NCONS], fR[NCONS];
+    side_flux(s, uL, L, dir, fL);
+    side_flux(s, uR, R, dir, fR);
+    double uHLL[NCONS];
+#pragma unroll
+    for (int v = 0; v < NCONS; v++)
+        if (v != ENER) uHLL[v] = (sR * uR[v] - sL * uL[v] + fL[v] - fR[v]) / (sR - sL);
+    const double velHx = uHLL[MOMX] / uHLL[DENS];
+    const double velHy = uHLL[MOMY] / uHLL[DENS];
+    const double velHz = uHLL[MOMZ] / uHLL[DENS];
+    const double magDotVelHLL = dot3(uHLL[MAGX], uHLL[MAGY], uHLL[MAGZ], velHx, velHy, velHz);
+    const double magNHLL = uHLL[bN];
+    const double pStr = rhoL * dL * (sStr - velNL) + pTotL - magNL * magNL + magNHLL * magNHLL;
     const bool left = side == 1;
+    const Side& K = left ? L : R;
     const double sK = left ? sL : sR;
-    const double rhoK = left ? rhoL : rhoR;
     const double dK = left ? dL : dR;
     const double velNK = left ? velNL : velNR;
     const double pTotK = left ? pTotL : pTotR;
     const double magNK = left ? magNL : magNR;
-    const double magDotVelK = left ? magDotVelL : magDotVelR;
-    const double vT1K = left ? vL[vT1] : vR[vT1], vT2K = left ? vL[vT2] : vR[vT2];
-    const double bT1K = left ? vL[bT1] : vR[bT1], bT2K = left ? vL[bT2] : vR[bT2];
+    const double magDotVelK = dot3(K.bx, K.by, K.bz, K.vx, K.vy, K.vz);
+    const double vT1K = side_vel(K, 1 - dir), vT2K = K.vz;
+    const double bT1K = side_mag(K, 1 - dir), bT2K = K.bz;
     const double eK = left ? uL[ENER] : uR[ENER];
     double uStr[NCONS];
-    uStr[DENS] = rhoK * dK / (sK - sStr);
+    uStr[DENS] = K.rho * dK / (sK - sStr);
     uStr[mN] = uStr[DENS] * sStr;
     uStr[mT1] = uStr[DENS] * vT1K - (magNHLL * uHLL[bT1] - magNK * bT1K) / (sK - sStr);
     uStr[mT2] = uStr[DENS] * vT2K - (magNHLL * uHLL[bT2] - magNK * bT2K) / (sK - sStr);
