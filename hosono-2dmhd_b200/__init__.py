@@ -17,11 +17,12 @@ import numpy as np
 PKG_DIR = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(PKG_DIR, "libhosono_gpu.so")
 
-OK, EINVAL, ENOMEM, ECUDA, ENANDT, EMOODCAP, ETIMEOUT, EPAR, ENOTBUILT = range(9)
+OK, EINVAL, ENOMEM, ECUDA, ENANDT, EMOODCAP, ETIMEOUT, EPAR, ENOTBUILT, ECANCELED = range(10)
 BC_OUTFLOW, BC_PERIODIC = 0, 1
 FP_STRICT, FP_FAST = 0, 1
 STATUS_NAMES = {OK: "OK", EINVAL: "EINVAL", ENOMEM: "ENOMEM", ECUDA: "ECUDA", ENANDT: "ENANDT",
-                EMOODCAP: "EMOODCAP", ETIMEOUT: "ETIMEOUT", EPAR: "EPAR", ENOTBUILT: "ENOTBUILT"}
+                EMOODCAP: "EMOODCAP", ETIMEOUT: "ETIMEOUT", EPAR: "EPAR", ENOTBUILT: "ENOTBUILT",
+                ECANCELED: "ECANCELED"}
 
 
 class HosonoError(RuntimeError):
@@ -55,6 +56,36 @@ class Stats(ctypes.Structure):
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
+
+class ServeConfig(ctypes.Structure):
+    _fields_ = [("memory_budget", ctypes.c_longlong), ("max_resident", ctypes.c_int), ("fp_mode", ctypes.c_int),
+                ("chunk_ms", ctypes.c_double), ("max_chunk_steps", ctypes.c_int), ("pad", ctypes.c_int)]
+
+
+class RequestInfo(ctypes.Structure):
+    _fields_ = [("id", ctypes.c_longlong), ("state", ctypes.c_int), ("status", ctypes.c_int),
+                ("nstep", ctypes.c_int), ("slot", ctypes.c_int), ("t", ctypes.c_double),
+                ("zone_updates", ctypes.c_longlong), ("device_bytes", ctypes.c_longlong),
+                ("submit_s", ctypes.c_double), ("admit_s", ctypes.c_double), ("finish_s", ctypes.c_double),
+                ("mood", Stats)]
+
+    def as_dict(self):
+        d = {k: getattr(self, k) for k, _ in self._fields_ if k != "mood"}
+        d["mood"] = self.mood.as_dict()
+        return d
+
+
+class ServeTotals(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_longlong) for k in ("submitted", "completed", "failed", "queued", "resident",
+                                                  "zone_updates", "chunks", "steps", "peak_resident",
+                                                  "budget_bytes", "used_bytes", "peak_bytes", "head_blocked")] + \
+               [("busy_s", ctypes.c_double), ("admin_s", ctypes.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+REQ_QUEUED, REQ_RUNNING, REQ_DONE = 0, 1, 2
 
 # Every symbol the C ABI exports (include/hosono_gpu.h), with its signature.
 _dp = ctypes.POINTER(ctypes.c_double)
@@ -108,8 +139,20 @@ SIGNATURES = {
     "hosono_batch_set_graphs": [_vp, _i],
     "hosono_batch_last_error": [_vp, _cp, _i],
     "hosono_batch_capacity": [_vp, _ip, _ip, _ip, _ip],
+    "hosono_serve_clock": [],
+    "hosono_serve_create": [ctypes.POINTER(ServeConfig), ctypes.POINTER(_vp)],
+    "hosono_serve_destroy": [_vp],
+    "hosono_serve_submit": [_vp, ctypes.POINTER(Params), _dp, _dp, _ip, _dp, _dp, _d, _i, _dp, _dp, _ip,
+                            ctypes.POINTER(ctypes.c_longlong)],
+    "hosono_serve_wait": [_vp, ctypes.c_longlong, _d, ctypes.POINTER(RequestInfo)],
+    "hosono_serve_poll": [_vp, ctypes.POINTER(ctypes.c_longlong), _i, _ip],
+    "hosono_serve_info": [_vp, ctypes.c_longlong, ctypes.POINTER(RequestInfo)],
+    "hosono_serve_snapshot": [_vp, ctypes.c_longlong, _dp, _dp, _ip, _dp, _ip],
+    "hosono_serve_drain": [_vp, _d],
+    "hosono_serve_stats": [_vp, ctypes.POINTER(ServeTotals)],
+    "hosono_serve_last_error": [_vp, _cp, _i],
 }
-RESTYPES = {"hosono_batch_instance_bytes": ctypes.c_longlong}
+RESTYPES = {"hosono_batch_instance_bytes": ctypes.c_longlong, "hosono_serve_clock": ctypes.c_double}
 NOALLOC_MAX_ROWS = 16384  # HOSONO_NOALLOC_MAX_ROWS
 
 

@@ -154,7 +154,7 @@ class Engine::Rec {
 Engine::~Engine() {
     if (s_) cudaStreamSynchronize(s_);
     for (auto& sl : slots_)
-        for (void* p : sl.allocs) cudaFree(p);
+        for (void* p : sl.allocs) dfree(p);
     for (cudaGraphExec_t g : {gAdvance_, gRun_, gProf_})
         if (g) cudaGraphExecDestroy(g);
     for (cudaEvent_t ev : profEv_)
@@ -276,7 +276,39 @@ int Engine::state(int slot, InstState* out) {
     return HOSONO_OK;
 }
 
-int Engine::add(const hosono_params& p, const double* pv, const double* qw, int* slot_out) {
+void* Engine::dalloc(size_t bytes) {
+    if (alloc_) return alloc_->alloc(bytes);
+    void* p = nullptr;
+    if (cudaMalloc(&p, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    return p;
+}
+
+void Engine::dfree(void* p) {
+    if (!p) return;
+    if (alloc_)
+        alloc_->release(p);
+    else
+        cudaFree(p);
+}
+
+int Engine::reserve_staging(size_t cells) {
+    if (cells <= stagingCells_) return HOSONO_OK;
+    CUE(cudaStreamSynchronize(s_));
+    if (staging_) cudaFree(staging_);
+    if (schemeInt_) cudaFree(schemeInt_);
+    staging_ = nullptr;
+    schemeInt_ = nullptr;
+    stagingCells_ = 0;
+    CUE(cudaMalloc(&staging_, sizeof(double) * cells * NPRIM));
+    CUE(cudaMalloc(&schemeInt_, sizeof(int) * cells));
+    stagingCells_ = cells;
+    return HOSONO_OK;
+}
+
+int Engine::add(const hosono_params& p, const double* pv, const double* qw, int* slot_out, bool commit) {
     const int R = p.max_radius;
     if (R < 1 || R > 3 || p.ngc != R + 2 || p.nx < 2 * p.ngc || p.ny < 2 * p.ngc ||
         (p.bc != HOSONO_BC_OUTFLOW && p.bc != HOSONO_BC_PERIODIC) || p.riemann_solver != 1 || !(p.dx > 0) ||
@@ -315,19 +347,13 @@ int Engine::add(const hosono_params& p, const double* pv, const double* qw, int*
     sl.dev.cfl = p.cfl;
     const size_t plane = (size_t)G.plane;
     const size_t npv = (size_t)G.nsMax * G.nqMax * 4 * R, nqw = (size_t)G.nqMax * R;
-    double* dbl = nullptr;
-    uint8_t* byt = nullptr;
-    cudaError_t e1 = cudaMalloc(&dbl, sizeof(double) * (plane * kDoublePlanes + npv + nqw));
-    if (e1 != cudaSuccess) {
-        cudaGetLastError();
-        return fail(HOSONO_ENOMEM, "cudaMalloc of instance state failed: %s", cudaGetErrorString(e1));
-    }
+    double* dbl = (double*)dalloc(sizeof(double) * (plane * kDoublePlanes + npv + nqw));
+    if (!dbl) return fail(HOSONO_ENOMEM, "no device memory for the instance state");
     sl.allocs.push_back(dbl);
-    e1 = cudaMalloc(&byt, plane * kBytePlanes);
-    if (e1 != cudaSuccess) {
-        cudaGetLastError();
-        cudaFree(dbl);
-        return fail(HOSONO_ENOMEM, "cudaMalloc of instance flags failed: %s", cudaGetErrorString(e1));
+    uint8_t* byt = (uint8_t*)dalloc(plane * kBytePlanes);
+    if (!byt) {
+        dfree(dbl);
+        return fail(HOSONO_ENOMEM, "no device memory for the instance flags");
     }
     sl.allocs.push_back(byt);
     double* q = dbl;
@@ -373,29 +399,21 @@ int Engine::add(const hosono_params& p, const double* pv, const double* qw, int*
     slots_[k] = sl;
     traceStageBase[k] = 0;
     tracePassesSeen_[k] = 0;
-    TRYE(upload_tables());
-    const size_t cells = (size_t)G.nxt * G.nyt;
-    if (cells > stagingCells_) {
-        if (staging_) cudaFree(staging_);
-        if (schemeInt_) cudaFree(schemeInt_);
-        staging_ = nullptr;
-        schemeInt_ = nullptr;
-        CUE(cudaMalloc(&staging_, sizeof(double) * cells * NPRIM));
-        CUE(cudaMalloc(&schemeInt_, sizeof(int) * cells));
-        stagingCells_ = cells;
-    }
+    if (commit) TRYE(upload_tables());
+    TRYE(reserve_staging((size_t)G.nxt * G.nyt));
     *slot_out = k;
     return HOSONO_OK;
 }
 
-int Engine::remove(int slot) {
+int Engine::remove(int slot, bool commit) {
     if (slot < 0 || slot >= maxInst_ || !slots_[slot].live) return fail(HOSONO_EINVAL, "bad slot %d", slot);
     CUE(cudaStreamSynchronize(s_));
     InstState st{};
     CUE(cudaMemcpyAsync(d_st_ + slot, &st, sizeof(InstState), cudaMemcpyHostToDevice, s_));
     slots_[slot].live = false;
-    TRYE(upload_tables());
-    for (void* p : slots_[slot].allocs) cudaFree(p);
+    if (commit) TRYE(upload_tables());
+    CUE(cudaStreamSynchronize(s_));  // no kernel of this stream still reads the memory
+    for (void* p : slots_[slot].allocs) dfree(p);
     slots_[slot] = Slot{};
     return HOSONO_OK;
 }
@@ -594,7 +612,10 @@ int Engine::launch(cudaGraphExec_t g) {
 
 int Engine::check_errors() {
     CUE(cudaMemcpyAsync(h_st_, d_st_, sizeof(InstState) * maxInst_, cudaMemcpyDeviceToHost, s_));
+    CUE(cudaMemcpyAsync(h_flags_, d_flags_, sizeof(BatchFlags), cudaMemcpyDeviceToHost, s_));
     CUE(cudaStreamSynchronize(s_));
+    if (h_flags_->error) return fail(h_flags_->error, "a MOOD work list overflowed its capacity");
+    if (!instance_errors_fatal) return HOSONO_OK;
     for (int k = 0; k < maxInst_; k++)
         if (slots_[k].live && h_st_[k].error)
             return fail(h_st_[k].error, "instance %d stopped: %s", k,

@@ -14,6 +14,14 @@ struct TraceRec {
     std::vector<unsigned char> inner, detect;  // nxt*nyt, i fastest
 };
 
+// Where an engine takes instance memory from: cudaMalloc by default, or a
+// caller's pool (the server's arena).
+struct DeviceAllocator {
+    virtual ~DeviceAllocator() = default;
+    virtual void* alloc(size_t bytes) = 0;  // nullptr when it does not fit
+    virtual void release(void* p) = 0;
+};
+
 class Engine {
   public:
     Engine() = default;
@@ -23,8 +31,14 @@ class Engine {
 
     // capacity: instance slots and 32x8 tiles over all instances
     int init(int max_inst, int max_tiles, int fp_mode);
-    int add(const hosono_params& p, const double* pv, const double* qw, int* slot);
-    int remove(int slot);
+    // commit_tables = false defers the tile-list upload to commit_tables(),
+    // so that many admissions or retirements rebuild it once
+    int add(const hosono_params& p, const double* pv, const double* qw, int* slot, bool commit_tables = true);
+    int remove(int slot, bool commit_tables = true);
+    int commit_tables() { return upload_tables(); }
+    // staging for upload/download of instances up to `cells` cells
+    int reserve_staging(size_t cells);
+    void set_allocator(DeviceAllocator* a) { alloc_ = a; }
     int upload(int slot, const double* U, const double* V);
     int download(int slot, double* U, double* V, int* scheme);
     int set_time(int slot, double t, double tmax, int nstep, int nstepmax);
@@ -47,8 +61,17 @@ class Engine {
     cudaStream_t stream() const { return s_; }
     int max_inst() const { return maxInst_; }
     int max_tiles() const { return maxTiles_; }
-    int used_tiles() const { return (int)tiles_.size(); }
+    int used_tiles() const {  // of every live slot, committed to the tile list or not
+        int n = 0;
+        for (const auto& sl : slots_) n += sl.live ? sl.ntiles : 0;
+        return n;
+    }
 
+    // run() fails when an instance stopped with an error; when false, the
+    // instance just ends (done, with its error code) and the others go on
+    bool instance_errors_fatal = true;
+    // per-slot states as of the end of the last run() (pinned host copy)
+    const InstState* host_states() const { return h_st_; }
     bool use_graphs = true;
     bool trace = false;
     std::vector<TraceRec> traces;
@@ -88,6 +111,10 @@ class Engine {
     int trace_snapshot();
     int trace_after_pass();
 
+    void* dalloc(size_t bytes);
+    void dfree(void* p);
+
+    DeviceAllocator* alloc_ = nullptr;
     const KernelSet* K_ = nullptr;
     cudaStream_t s_ = nullptr;
     int maxInst_ = 0, maxTiles_ = 0;

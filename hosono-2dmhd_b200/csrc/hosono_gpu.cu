@@ -4,6 +4,7 @@
 //                engine holding one instance.
 // hosono_batch_*: many independent blocks of any sizes advanced together.
 
+#include "checks.h"
 #include "engine_host.h"
 #include "hosono_gpu.h"
 
@@ -30,31 +31,6 @@ struct hosono_batch {
 
 namespace {
 
-// the kernels hard-code the stencil order of GP.f90:85-95; check the table
-bool stencil_ok(int R, const int* stenc) {
-    if (!stenc) return true;
-    const int nsMax = 1 + 2 * R * (R + 1);
-    for (int rr = 1; rr <= R; rr++) {
-        int k = 0;
-        for (int a = -rr; a <= rr; a++)
-            for (int b = -rr; b <= rr; b++)
-                if (std::abs(a) + std::abs(b) <= rr) {
-                    if (stenc[0 + 2 * (k + nsMax * (rr - 1))] != a || stenc[1 + 2 * (k + nsMax * (rr - 1))] != b)
-                        return false;
-                    k++;
-                }
-    }
-    return true;
-}
-
-// the checks Engine::add repeats, done before any CUDA call
-bool params_ok(const hosono_params& p) {
-    const int R = p.max_radius;
-    return R >= 1 && R <= 3 && p.ngc == R + 2 && p.nx >= 2 * p.ngc && p.ny >= 2 * p.ngc &&
-           (p.bc == HOSONO_BC_OUTFLOW || p.bc == HOSONO_BC_PERIODIC) && p.riemann_solver == 1 && p.dx > 0 &&
-           p.dy > 0;
-}
-
 hosono_stats stats_delta(const InstState& a, const InstState& b) {
     hosono_stats s{};
     s.stages = b.stages - a.stages;
@@ -67,11 +43,12 @@ hosono_stats stats_delta(const InstState& a, const InstState& b) {
 }
 
 // kernels one graph execution launched, from the work counters: per step 4
-// time-loop kernels (cfl path) or 1 (host dt), 3 RK kernels; per stage 7;
-// per cascade iteration 4; per further MOOD pass 6.
+// time-loop kernels (cfl path) or 1 (host dt), 3 RK kernels; per stage 12
+// (MOOD pass 1, three of them the per-radius face kernels); per cascade
+// iteration 4; per further MOOD pass 9.
 long long graph_launches(const hosono_stats& s, int steps, bool host_dt) {
-    return (long long)steps * ((host_dt ? 1 : 4) + 3) + 7LL * s.stages + 4LL * s.cascade_iters +
-           6LL * (s.mood_passes - s.stages);
+    return (long long)steps * ((host_dt ? 1 : 4) + 3) + 12LL * s.stages + 4LL * s.cascade_iters +
+           9LL * (s.mood_passes - s.stages);
 }
 
 }  // namespace

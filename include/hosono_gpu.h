@@ -39,6 +39,7 @@ extern "C" {
 #define HOSONO_ETIMEOUT 6   /* a bounded device wait gave up                      */
 #define HOSONO_EPAR 7       /* .par file missing a key or holding a bad value     */
 #define HOSONO_ENOTBUILT 8  /* library loaded without device code for this GPU    */
+#define HOSONO_ECANCELED 9  /* served solve ended by the server's shutdown        */
 
 /* boundary ids (sim_BC, src/simulation.f90:62) */
 #define HOSONO_BC_OUTFLOW 0
@@ -246,6 +247,90 @@ int hosono_cfl_noalloc(const double* V_dev, int nx, int ny, int ngc, int pitch, 
 int hosono_gpu_profile(hosono_handle* h, int on);
 int hosono_gpu_profile_read(hosono_handle* h, double* pass1_ms, long long* pass1_launches, long long* launches,
                             int reset);
+
+/* ---------------------------------------------------------------- serving
+ * No counterpart in the reference, which runs one solve per process.  A
+ * server owns one batch on the current GPU and a scheduler thread.  Solves
+ * are submitted at any time from any thread and wait in a FIFO queue.  The
+ * head of the queue is admitted when an instance slot, tile capacity and a
+ * free range of the server's device-memory budget are available: the budget
+ * is one device allocation made at start-up, so admission and retirement
+ * never call cudaMalloc.  An admitted solve advances with every other
+ * resident solve in the same batched launches (continuous batching), each at
+ * its own dt, until its tmax or nstepmax; then its final state is copied to
+ * the caller's buffers and its memory returns to the budget.  A solve's
+ * result does not depend on what else is resident.  Between launches the
+ * scheduler admits, retires and serves snapshots. */
+typedef struct hosono_server hosono_server;
+
+typedef struct hosono_serve_config {
+    long long memory_budget; /* device bytes for resident solves; <= 0: 55% of free memory  */
+    int max_resident;        /* instance slots; <= 0: 1024                                  */
+    int fp_mode;             /* HOSONO_FP_*                                                 */
+    double chunk_ms;         /* target GPU time of one batched launch; <= 0: 25 ms          */
+    int max_chunk_steps;     /* time steps per batched launch at most; <= 0: 64             */
+    int pad;
+} hosono_serve_config;
+
+#define HOSONO_REQ_QUEUED 0
+#define HOSONO_REQ_RUNNING 1
+#define HOSONO_REQ_DONE 2
+
+typedef struct hosono_request_info {
+    long long id;
+    int state;                /* HOSONO_REQ_*                                                */
+    int status;               /* HOSONO_OK, or what ended it (ENANDT, EMOODCAP, ECANCELED...) */
+    int nstep;                /* time steps taken                                            */
+    int slot;                 /* batch slot while resident, else -1                          */
+    double t;                 /* simulation time reached                                     */
+    long long zone_updates;   /* nx*ny*nstep                                                 */
+    long long device_bytes;   /* budget bytes held while resident                            */
+    double submit_s, admit_s, finish_s; /* hosono_serve_clock() at each event; 0 = not yet    */
+    hosono_stats mood;        /* MOOD counters over the solve                                */
+} hosono_request_info;
+
+typedef struct hosono_serve_totals {
+    long long submitted, completed, failed, queued, resident;
+    long long zone_updates;   /* of completed solves                                         */
+    long long chunks, steps;  /* batched launches; batch time steps                          */
+    long long peak_resident;
+    long long budget_bytes, used_bytes, peak_bytes;
+    long long head_blocked;   /* admission rounds that stopped at a head that did not fit    */
+    double busy_s;            /* wall time inside batched launches                           */
+    double admin_s;           /* wall time admitting, retiring and snapshotting              */
+} hosono_serve_totals;
+
+/* seconds on the server clock (steady, shared by all servers of the process) */
+double hosono_serve_clock(void);
+int hosono_serve_create(const hosono_serve_config* cfg, hosono_server** out);
+/* stops the scheduler after its current launch; queued and resident solves
+ * end with HOSONO_ECANCELED.  Threads blocked in hosono_serve_wait, _drain
+ * or _snapshot on this server return before it is freed; no other call on
+ * it may overlap this one. */
+int hosono_serve_destroy(hosono_server* s);
+/* Queue one solve: parameters, GP tables (as hosono_gpu_create), the initial
+ * U and V (host, Fortran order with guards, as initialCondition_set leaves
+ * them; copied, so they may be freed on return; V may be NULL: then
+ * V = cons2prim(U) on the device, as hosono_gpu_upload), its tmax and
+ * nstepmax.  U_out (8 doubles/cell), V_out (10) and scheme_out
+ * (int) are filled with the final state when the solve ends; each may be
+ * NULL and must stay valid until hosono_serve_wait/poll reports the solve
+ * done.  A solve larger than the whole budget or the tile capacity is
+ * refused with HOSONO_ENOMEM. */
+int hosono_serve_submit(hosono_server* s, const hosono_params* p, const double* pv, const double* qw, const int* stenc,
+                        const double* U, const double* V, double tmax, int nstepmax, double* U_out, double* V_out,
+                        int* scheme_out, long long* id);
+/* block until the solve is done (HOSONO_ETIMEOUT after timeout_s; < 0: no limit) */
+int hosono_serve_wait(hosono_server* s, long long id, double timeout_s, hosono_request_info* info);
+/* ids of solves finished since the last poll (up to cap) */
+int hosono_serve_poll(hosono_server* s, long long* ids, int cap, int* n);
+int hosono_serve_info(hosono_server* s, long long id, hosono_request_info* info);
+/* current state of a resident solve, taken between batched launches */
+int hosono_serve_snapshot(hosono_server* s, long long id, double* U, double* V, int* scheme, double* t, int* nstep);
+/* block until no solve is queued or resident (HOSONO_ETIMEOUT after timeout_s) */
+int hosono_serve_drain(hosono_server* s, double timeout_s);
+int hosono_serve_stats(hosono_server* s, hosono_serve_totals* st);
+int hosono_serve_last_error(hosono_server* s, char* buf, int len);
 
 #ifdef __cplusplus
 }

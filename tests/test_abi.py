@@ -95,3 +95,18 @@ def test_create_rejects_bad_params():
                                qw.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
                                st.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), ctypes.byref(h))
     assert rc == m.EINVAL  # ngc must be R + 2
+
+
+def test_serve_create_without_gpu_fails_cleanly():
+    """hosono_serve_create on a machine without a usable GPU returns an error
+    status (the scheduler thread starts, fails its CUDA set-up and exits)."""
+    import importlib
+    m = pkg.load()
+    srv = importlib.import_module("hosono_2dmhd_b200.serve")
+    try:
+        s = srv.Server(memory_budget=1 << 26)
+    except m.HosonoError as e:
+        assert e.code in (m.ECUDA, m.ENOMEM)
+        return
+    s.close()
+    pytest.skip("a GPU is present")
