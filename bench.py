@@ -212,6 +212,8 @@ def bench_ours(args, rank, world, local):
         pv, qw, st = m.par_gp(par, params.max_radius)
         U0, V0 = m.ic_set(par, params)
     sol = m.Solver(params, pv, qw, st)
+    if args.eager:
+        sol.set_graphs(False)
     sol.upload(U0, V0)
     sol.set_time(0.0, run.tmax, 0, run.nstepmax)
     stream = torch.cuda.ExternalStream(sol.stream())
@@ -230,7 +232,8 @@ def bench_ours(args, rank, world, local):
     barrier()
     # timed region: K steps, each one launch of the step graph (cfl, dt,
     # three MOOD stages, RK3) with CUDA events bracketing the pass-1 kernels
-    sol.profile(True)
+    if not args.eager:  # the pass-1 events live in the profiled step graph
+        sol.profile(True)
     sol.profile_read(reset=True)
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
@@ -283,9 +286,9 @@ def bench_ours(args, rank, world, local):
     hbm, hbm_kind = peaks()
     p1_avg = p1_ms / max(p1_n, 1)
     bytes1 = pass1_bytes(w["n"], w["radius"])
-    achieved = bytes1 / (p1_avg / 1e3) / 1e9
+    achieved = bytes1 / (p1_avg / 1e3) / 1e9 if p1_avg > 0 else None
     roofline = {"bound": "hbm", "kernel": "k_face_pass1", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                "frac": achieved / hbm, "traffic": None, "peak_kind": hbm_kind,
+                "frac": achieved / hbm if achieved else None, "traffic": None, "peak_kind": hbm_kind,
                 "kernel_ms": p1_avg, "kernel_launches": p1_n,
                 "note": "FP64 CUDA-core kernel; HBM line shown as the contract requires"}
     line = {
@@ -298,12 +301,17 @@ def bench_ours(args, rank, world, local):
     }
     if world == 1 and not args.no_batched:
         line["batched"] = bench_batched(m, fp, torch)
+    served_kept = {}
+    if world == 1 and args.serve_requests > 0:
+        line["served"], served_kept = bench_served(m, fp, args.serve_requests, args.serve_check)
     if not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         rate, el = run_cpu_baseline(args.workload, 1, threads)
         line["cpu_baseline"] = {"value": rate, "unit": "zone-updates/s", "cores": threads, "kind": "port",
                                 "sample": f"1 full RK3 step of {args.workload} after 1 warm-up step, CPU oracle "
                                           f"(C++ restatement, OpenMP, {oracle_build()}), {el:.1f} s"}
+        if served_kept:
+            line["served"]["accuracy"] = cpu_baseline_served_check(served_kept)
     print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
@@ -375,6 +383,64 @@ def bench_batched(m, fp, torch, manifest="blast64_seed0.json", limit=None):
             "unit": "zone-updates/s"}
 
 
+def bench_served(m, fp, requests, check):
+    """The served request stream (workloads/served2000_seed1.json, first
+    `requests` requests): first closed loop (all submitted at once) to measure
+    the batched capacity in requests/s, then open loop with the manifest's
+    seeded exponential gaps scaled to 80% of that capacity.  Latency is
+    submit -> final state on the host.  Returns the report and the final U of
+    the `check` requests with the least work (for the accuracy check)."""
+    import importlib
+    load_pkg()
+    srv = importlib.import_module("hosono_2dmhd_b200.serve")
+    path = os.path.join(ROOT, "hosono-2dmhd_b200", "workloads", "served2000_seed1.json")
+    with open(path) as f:
+        entries = json.load(f)["requests"][:requests]
+    with srv.Server(fp_mode=fp) as s:
+        closed, _, cinfos = srv.run_stream(entries, 1.0, s, fp_mode=fp, closed=True)
+    cap = len(entries) / closed["makespan_s"]
+    rate = 0.8 * cap
+    keep = [i["entry"] for i in sorted(cinfos, key=lambda i: i["zone_updates"])[:check]]
+    with srv.Server(fp_mode=fp) as s:
+        rep, kept, infos = srv.run_stream(entries, rate, s, keep=keep, fp_mode=fp)
+    out = {"workload": f"served2000 (seed 1) requests 0..{len(entries) - 1}: Orszag-Tang / Sedov / MHD blast, "
+                       f"N log-uniform in [64,1024], R in {{1,2}}, t_end U[0.1,1] x default",
+           "requests": len(entries), "load": 0.8, "capacity_rps": cap,
+           "closed_loop_zone_updates_per_s": closed["zone_updates_per_s"], "rate_per_s": rate}
+    for k in ("zone_updates", "zone_updates_per_s", "makespan_s", "latency_p50_s", "latency_p99_s", "latency_max_s",
+              "queue_wait_p50_s", "queue_wait_p99_s", "submit_lag_max_s", "peak_resident", "peak_bytes",
+              "budget_bytes", "gpu_busy_frac", "completed", "failed"):
+        out[k] = rep[k]
+    out["unit"] = "zone-updates/s"
+    return out, {e["id"]: (e, kept[e["id"]]) for e in entries if e["id"] in kept}
+
+
+def cpu_baseline_served_check(kept):
+    """Accuracy of served results against the CPU oracle run of the same
+    request to its t_end: relative L1 of each conserved variable over the
+    interior (the worst one reported) and whether the states are identical."""
+    import numpy as np
+    import oracle
+    problems = load_problems()
+    worst, same, checked = 0.0, True, []
+    with tempfile.TemporaryDirectory() as d:
+        for eid, (e, U) in sorted(kept.items()):
+            par = problems.make(d, f"chk{eid}", problems.from_entry(e))
+            o = oracle.Oracle(par)
+            rc, t, n = o.run()
+            Uo = o.U()
+            g = o.ngc
+            a, b = U[g:-g, g:-g, :], Uo[g:-g, g:-g, :]
+            rel = float(max(np.abs(a[..., v] - b[..., v]).sum() / max(np.abs(b[..., v]).sum(), 1e-300)
+                            for v in range(8)))
+            worst = max(worst, rel)
+            same = same and bool(np.array_equal(U, Uo))
+            checked.append(eid)
+            o.close()
+    return {"checked_requests": checked, "max_rel_l1": worst, "identical": same, "tolerance": 1e-8,
+            "reference": "CPU oracle (C++ restatement, strict FP) run to the same t_end"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -385,6 +451,12 @@ def main():
     ap.add_argument("--fp", default="strict", choices=["strict", "fast"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the 64-instance batched-vs-plain measurement")
+    ap.add_argument("--eager", action="store_true",
+                    help="launch the step's kernels one by one instead of as a CUDA graph (for profilers)")
+    ap.add_argument("--serve-requests", type=int, default=20,
+                    help="requests of the served stream to run (0: skip the served measurement)")
+    ap.add_argument("--serve-check", type=int, default=3,
+                    help="served requests (least work first) checked against the CPU oracle")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
