@@ -18,6 +18,8 @@
 //   FLICD         [strt,   stop+1] -> [g,   g+n]     (FLICDdivB.f90:301-302)
 //   update/detect [strt,   stop]   -> [g,   g+n-1]   (timeStep.f90:108-109, detect.f90:81-82)
 
+#include <mutex>
+
 #include "engine.h"
 #include "hosono_gpu.h"
 
@@ -168,18 +170,20 @@ __device__ __forceinline__ void gp_face_s(const double* __restrict__ sU, int sx,
 }
 
 // one face (both sides, every quadrature point); returns the side verdict bits
+// (the Gauss sum of the fluxes accumulates in this thread's column of
+// shared memory, acc[v * NTHREADS], which keeps it out of the registers the
+// Riemann solver needs)
 template <int R, int DIR>
 __device__ __forceinline__ uint8_t pass1_face(const InstDev& d, const double* __restrict__ sU, int sx, int sy,
-                                              bool needL, bool needR, bool doFlux, long long c) {
+                                              bool needL, bool needR, bool doFlux, long long c, double* acc) {
     const Geo& G = d.geo;
     const Phys& P = d.phys;
     constexpr int NQ = R + 1;
     constexpr int FL = DIR == XDIR ? EAST : NORTH, FR = DIR == XDIR ? WEST : SOUTH;
     const int lx = DIR == XDIR ? sx - 1 : sx, ly = DIR == XDIR ? sy : sy - 1;
     uint8_t bits = 0;
-    double acc[NCONS];
 #pragma unroll
-    for (int v = 0; v < NCONS; v++) acc[v] = 0.0;
+    for (int v = 0; v < NCONS; v++) acc[v * NTHREADS] = 0.0;
 #pragma unroll 1
     for (int q = 0; q < NQ; q++) {
         double uL[NCONS], uR[NCONS];
@@ -196,44 +200,87 @@ __device__ __forceinline__ uint8_t pass1_face(const InstDev& d, const double* __
             hllc(P, uL, uR, DIR, F);
             const double w = qw_at(d, R, q);
 #pragma unroll
-            for (int v = 0; v < NCONS; v++) acc[v] = acc[v] + w * F[v];
+            for (int v = 0; v < NCONS; v++) acc[v * NTHREADS] = acc[v * NTHREADS] + w * F[v];
         }
     }
     if (doFlux) {
         double* Fo = DIR == XDIR ? d.FX : d.FY;
 #pragma unroll
-        for (int v = 0; v < NCONS; v++) Fo[v * G.plane + c] = acc[v];
-        (DIR == XDIR ? d.CTX : d.CTY)[c] = DIR == XDIR ? acc[MAGY] : acc[MAGX];
+        for (int v = 0; v < NCONS; v++) Fo[v * G.plane + c] = acc[v * NTHREADS];
+        (DIR == XDIR ? d.CTX : d.CTY)[c] = acc[(DIR == XDIR ? MAGY : MAGX) * NTHREADS];
     }
     return bits;
 }
 
-// One launch per radius: blocks of instances with another GP radius skip the tile.
+// 16-byte asynchronous copy global -> shared (cp.async); src_bytes = 0
+// writes zeros and reads nothing
+__device__ __forceinline__ void cp_async16(void* dst, const void* src, int src_bytes) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(src), "r"(src_bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+// next tile at or after t (stride gridDim.x) that this launch works on
+template <int R>
+__device__ __forceinline__ int pass1_next(const Batch& B, int t, int n) {
+    for (; t < n; t += gridDim.x) {
+        const int k = B.tiles[t].x;
+        if (B.st[k].stepping && B.dev[k].geo.R == R) return t;
+    }
+    return n;
+}
+
+// stage tile t's stencil box (zeros outside the array) into dst
+template <int R>
+__device__ __forceinline__ void pass1_stage(const Batch& B, int uin, int t, double* dst, int tid) {
+    using Box = P1Box<R>;
+    const int4 tl = B.tiles[t];
+    const InstDev& d = B.dev[tl.x];
+    const Geo& G = d.geo;
+    const double* U = role_ptr(d, B.st[tl.x].parity, uin);
+    const int x0 = tl.y - Box::OX, y0 = tl.z - Box::OY;
+    for (int e = tid; e < NCONS * Box::SY * (Box::SX / 2); e += NTHREADS) {
+        const int v = e / (Box::SY * (Box::SX / 2));
+        const int r = e - v * (Box::SY * (Box::SX / 2));
+        const int yy = r / (Box::SX / 2), xx = 2 * (r - yy * (Box::SX / 2));
+        const int gx = x0 + xx, gy = y0 + yy;
+        const bool in = gx >= 0 && gx < G.pitch && gy >= 0 && gy < G.nyt;
+        const double* src = in ? U + v * G.plane + (long long)gy * G.pitch + gx : U;
+        cp_async16(dst + v * Box::PLANE + yy * Box::SX + xx, src, in ? 16 : 0);
+    }
+    cp_async_commit();
+}
+
+// One launch per radius: blocks skip tiles of instances with another GP
+// radius.  Shared memory: two stencil boxes (the next tile's box is copied in
+// asynchronously while the current one is computed) and the per-thread flux
+// accumulators.
 template <int R>
 __global__ void __launch_bounds__(NTHREADS, HOSONO_PASS1_MIN_BLOCKS) k_face_pass1(Batch B, int uin) {
-    extern __shared__ double sU[];
+    extern __shared__ double smem[];
     using Box = P1Box<R>;
     const int tid = threadIdx.y * TILE_X + threadIdx.x;
-    FOR_TILES(B, t) {
+    double* acc = smem + 2 * Box::DOUBLES + tid;
+    const int n = __ldg(B.ntiles);
+    int t = pass1_next<R>(B, blockIdx.x, n);
+    int buf = 0;
+    if (t < n) pass1_stage<R>(B, uin, t, smem, tid);
+    while (t < n) {
+        const int tn = pass1_next<R>(B, t + gridDim.x, n);
+        if (tn < n) {
+            pass1_stage<R>(B, uin, tn, smem + (buf ^ 1) * Box::DOUBLES, tid);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        __syncthreads();  // tile t's box is in place for every thread
+        const double* sU = smem + buf * Box::DOUBLES;
         const Cell c = tile_at(B, t);
         InstState& S = B.st[c.k];
         const InstDev& d = B.dev[c.k];
-        if (!S.stepping || d.geo.R != R) continue;  // uniform over the block
         const Geo& G = d.geo;
-        const double* __restrict__ U = role_ptr(d, S.parity, uin);
-        const int x0 = c.i - threadIdx.x - Box::OX, y0 = c.j - threadIdx.y - Box::OY;
-        __syncthreads();  // the previous tile's reads of sU are done
-        for (int e = tid; e < NCONS * Box::SY * (Box::SX / 2); e += NTHREADS) {
-            const int v = e / (Box::SY * (Box::SX / 2));
-            const int r = e - v * (Box::SY * (Box::SX / 2));
-            const int yy = r / (Box::SX / 2), xx = 2 * (r - yy * (Box::SX / 2));
-            const int gx = x0 + xx, gy = y0 + yy;
-            double2 val = make_double2(0.0, 0.0);
-            if (gx >= 0 && gx < G.pitch && gy >= 0 && gy < G.nyt)
-                val = __ldg(reinterpret_cast<const double2*>(U + v * G.plane + (long long)gy * G.pitch + gx));
-            *reinterpret_cast<double2*>(sU + v * Box::PLANE + yy * Box::SX + xx) = val;
-        }
-        __syncthreads();
         if (first_tile_thread(c)) S.cascadeMode = CASCADE_FROM_FACES;
         const int i = c.i, j = c.j;
         const int g = G.g;
@@ -244,16 +291,19 @@ __global__ void __launch_bounds__(NTHREADS, HOSONO_PASS1_MIN_BLOCKS) k_face_pass
         const bool inF = i >= flo && i <= fxhi && j >= flo && j <= fyhi;
         bool bad = false;
         if (i >= clo && i <= cxhi + 1 && j >= clo && j <= cyhi) {  // x-face
-            const uint8_t bits = pass1_face<R, XDIR>(d, sU, sx, sy, i - 1 >= clo, i <= cxhi, inF, cc);
+            const uint8_t bits = pass1_face<R, XDIR>(d, sU, sx, sy, i - 1 >= clo, i <= cxhi, inF, cc, acc);
             d.failX[cc] = bits;
             bad |= bits != 0;
         }
         if (i >= clo && i <= cxhi && j >= clo && j <= cyhi + 1) {  // y-face
-            const uint8_t bits = pass1_face<R, YDIR>(d, sU, sx, sy, j - 1 >= clo, j <= cyhi, inF, cc);
+            const uint8_t bits = pass1_face<R, YDIR>(d, sU, sx, sy, j - 1 >= clo, j <= cyhi, inF, cc, acc);
             d.failY[cc] = bits;
             bad |= bits != 0;
         }
         warp_flag(&S.anyFail, bad);
+        __syncthreads();  // every read of this box is done before it is refilled
+        buf ^= 1;
+        t = tn;
     }
 }
 
@@ -1203,6 +1253,8 @@ const dim3 kTile(TILE_X, TILE_Y);
 // Grid of a tile kernel: as many blocks as fit on the GPU at once (the
 // kernels loop over the tile list), and never more than the tile capacity.
 int resident_blocks(const void* kernel, int smem = 0) {
+    static std::mutex mu;  // engines on several host threads launch concurrently
+    std::lock_guard<std::mutex> lock(mu);
     static const void* keys[64];
     static int vals[64];
     static int n = 0;
@@ -1236,7 +1288,11 @@ void l_step_end(const Batch& B, cudaGraphConditionalHandle h, cudaStream_t s) {
 void l_stage_init(const Batch& B, cudaStream_t s) { TILE_LAUNCH(k_stage_init, B, s); }
 template <int R>
 void launch_pass1(const Batch& B, int uin, cudaStream_t s) {
-    constexpr int smem = P1Box<R>::DOUBLES * (int)sizeof(double);
+    constexpr int smem = (2 * P1Box<R>::DOUBLES + NCONS * NTHREADS) * (int)sizeof(double);
+    static const bool attr =  // once per process (thread-safe static initialisation)
+        cudaFuncSetAttribute((const void*)k_face_pass1<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) ==
+        cudaSuccess;
+    (void)attr;
     const int r = resident_blocks((const void*)k_face_pass1<R>, smem);
     k_face_pass1<R><<<dim3((unsigned)(r < B.maxTiles ? r : B.maxTiles)), kTile, smem, s>>>(B, uin);
 }

@@ -123,12 +123,63 @@ __device__ __forceinline__ double dot3(double a0, double a1, double a2, double b
     return (0.0 + a0 * b0) + a1 * b1 + a2 * b2;
 }
 
+// Division policies for the Riemann solver.  Most of its quotients come in
+// groups with one denominator (the density of a side, sR - sL, the HLL
+// density, sK - sStar).
+//
+// IeeeDiv divides each one ('/': IEEE, correctly rounded).
+//
+// SharedRecipDiv takes y = RN(1/b) once per group (__drcp_rn, correctly
+// rounded) and each quotient by Markstein's theorem (P. Markstein, "Computation
+// of elementary functions on the IBM RISC System/6000 processor", IBM J. Res.
+// Dev. 34(1), 1990): when y = RN(1/b) and q is within one ulp of a/b, the
+// remainder r = a - b*q is exact and RN(q + r*y) = RN(a/b).  q0 = RN(a*y) is
+// within two ulps of a/b; one correction q1 = RN(q0 + y*RN(a - b*q0)) brings
+// it within one ulp, and a second gives the correctly rounded quotient -- the
+// same bits as '/' (tests/div_check.cu compares the two on the GPU).  The proof assumes no overflow, underflow or subnormal in a, b,
+// a*y and the remainders; every operand outside [2^-500, 2^500] (zero
+// numerators excepted) clears `ok`, and the caller then recomputes the whole
+// solve with IeeeDiv.  Cost per quotient: one multiply and four FMAs, no
+// branch.
+struct IeeeDiv {
+    struct R {
+        double b;
+    };
+    bool ok = true;
+    __device__ __forceinline__ R recip(double b) { return R{b}; }
+    __device__ __forceinline__ double div(double a, const R& r) { return a / r.b; }
+};
+struct SharedRecipDiv {
+    struct R {
+        double b, y;
+    };
+    bool ok = true;
+    __device__ __forceinline__ static bool in_range(double x) {
+        const double ax = fabs(x);
+        return ax >= 0x1p-500 && ax <= 0x1p500;
+    }
+    __device__ __forceinline__ R recip(double b) {
+        ok = ok && in_range(b);
+        return R{b, __drcp_rn(b)};
+    }
+    __device__ __forceinline__ double div(double a, const R& r) {
+        ok = ok && (a == 0.0 || in_range(a));
+        const double q0 = a * r.y;
+        const double q1 = fma(fma(-r.b, q0, a), r.y, q0);
+        const double q2 = fma(fma(-r.b, q1, a), r.y, q1);
+        return a == 0.0 ? q0 : q2;
+    }
+};
+
 // The primitive variables HLLC reads from one side: cons2prim
 // (convert.f90:198-234) without eint; b* are zero for a hydro run.
+template <class D>
 struct Side {
     double rho, vx, vy, vz, p, bx, by, bz;
+    typename D::R rrho;  // the density as a shared denominator
 };
-__device__ __forceinline__ void side_prim(const Phys& s, const double* U, Side& V) {
+template <class D>
+__device__ __forceinline__ void side_prim(const Phys& s, const double* U, Side<D>& V, D& dv) {
     double Bp;
     if (s.force_hydro)
         Bp = 0.0;
@@ -136,17 +187,24 @@ __device__ __forceinline__ void side_prim(const Phys& s, const double* U, Side& 
         Bp = 0.5 * (U[MAGX] * U[MAGX] + U[MAGY] * U[MAGY] + U[MAGZ] * U[MAGZ]);
     const double density = U[DENS];
     V.rho = density;
-    V.vx = U[MOMX] / density;
-    V.vy = U[MOMY] / density;
-    V.vz = U[MOMZ] / density;
-    const double eint = (U[ENER] - Bp) / density - 0.5 * (V.vx * V.vx + V.vy * V.vy + V.vz * V.vz);
+    V.rrho = dv.recip(density);
+    V.vx = dv.div(U[MOMX], V.rrho);
+    V.vy = dv.div(U[MOMY], V.rrho);
+    V.vz = dv.div(U[MOMZ], V.rrho);
+    const double eint = dv.div(U[ENER] - Bp, V.rrho) - 0.5 * (V.vx * V.vx + V.vy * V.vy + V.vz * V.vz);
     V.p = eos_pres(s, density, eint);
     V.bx = s.force_hydro ? 0.0 : U[MAGX];
     V.by = s.force_hydro ? 0.0 : U[MAGY];
     V.bz = s.force_hydro ? 0.0 : U[MAGZ];
 }
-__device__ __forceinline__ double side_vel(const Side& V, int c) { return c == 0 ? V.vx : c == 1 ? V.vy : V.vz; }
-__device__ __forceinline__ double side_mag(const Side& V, int c) { return c == 0 ? V.bx : c == 1 ? V.by : V.bz; }
+template <class D>
+__device__ __forceinline__ double side_vel(const Side<D>& V, int c) {
+    return c == 0 ? V.vx : c == 1 ? V.vy : V.vz;
+}
+template <class D>
+__device__ __forceinline__ double side_mag(const Side<D>& V, int c) {
+    return c == 0 ? V.bx : c == 1 ? V.by : V.bz;
+}
 
 // fast magnetosonic speed of one side or of the average state (eigen.f90:257-303)
 __device__ __forceinline__ double side_cf(const Phys& s, double rho0, double p0, double bx, double by, double bz,
@@ -158,7 +216,9 @@ __device__ __forceinline__ double side_cf(const Phys& s, double rho0, double p0,
 }
 
 // cons2flux (convert.f90:28-92) of one side
-__device__ __forceinline__ void side_flux(const Phys& s, const double* U, const Side& V, int dir, double* F) {
+template <class D>
+__device__ __forceinline__ void side_flux(const Phys& s, const double* U, const Side<D>& V, int dir, double* F,
+                                          D& dv) {
     double Bp = 0.0;
     if (!s.force_hydro) Bp = 0.5 * (U[MAGX] * U[MAGX] + U[MAGY] * U[MAGY] + U[MAGZ] * U[MAGZ]);
     const double E = U[ENER];
@@ -168,7 +228,7 @@ __device__ __forceinline__ void side_flux(const Phys& s, const double* U, const 
     const double vN = side_vel(V, dir), vT1 = side_vel(V, 1 - dir), vT2 = V.vz;
     const double BN = side_mag(V, dir), BT1 = side_mag(V, 1 - dir), BT2 = V.bz;
     F[DENS] = U[mN];
-    F[mN] = U[mN] * U[mN] / U[DENS] + Ptot;
+    F[mN] = dv.div(U[mN] * U[mN], V.rrho) + Ptot;
     F[mT1] = U[mN] * vT1;
     F[mT2] = U[mN] * vT2;
     F[ENER] = (E + Ptot) * vN;
@@ -190,10 +250,12 @@ __device__ __forceinline__ void side_flux(const Phys& s, const double* U, const 
 // computed: a supersonic face (flux = fL or fR) evaluates one physical flux
 // and no HLL or star state, and the star state is evaluated once, on the
 // operands of the chosen side.
-__device__ __forceinline__ void hllc(const Phys& s, const double* uL, const double* uR, int dir, double* flux) {
-    Side L, R;
-    side_prim(s, uL, L);
-    side_prim(s, uR, R);
+template <class D>
+__device__ __forceinline__ void hllc_t(const Phys& s, const double* uL, const double* uR, int dir, double* flux,
+                                       D& dv) {
+    Side<D> L, R;
+    side_prim(s, uL, L, dv);
+    side_prim(s, uR, R, dv);
     const int mN = dir == XDIR ? MOMX : MOMY, mT1 = dir == XDIR ? MOMY : MOMX, mT2 = MOMZ;
     const int bN = dir == XDIR ? MAGX : MAGY, bT1 = dir == XDIR ? MAGY : MAGX, bT2 = MAGZ;
     const double velNL = side_vel(L, dir), velNR = side_vel(R, dir);
@@ -228,26 +290,28 @@ __device__ __forceinline__ void hllc(const Phys& s, const double* uL, const doub
         side = 3;
     if (side == 0 || side == 3) {
         if (side == 0)
-            side_flux(s, uL, L, dir, flux);
+            side_flux(s, uL, L, dir, flux, dv);
         else
-            side_flux(s, uR, R, dir, flux);
+            side_flux(s, uR, R, dir, flux, dv);
         return;
     }
     double fL[NCONS], fR[NCONS];
-    side_flux(s, uL, L, dir, fL);
-    side_flux(s, uR, R, dir, fR);
+    side_flux(s, uL, L, dir, fL, dv);
+    side_flux(s, uR, R, dir, fR, dv);
     double uHLL[NCONS];
+    const typename D::R rS = dv.recip(sR - sL);
 #pragma unroll
     for (int v = 0; v < NCONS; v++)
-        if (v != ENER) uHLL[v] = (sR * uR[v] - sL * uL[v] + fL[v] - fR[v]) / (sR - sL);
-    const double velHx = uHLL[MOMX] / uHLL[DENS];
-    const double velHy = uHLL[MOMY] / uHLL[DENS];
-    const double velHz = uHLL[MOMZ] / uHLL[DENS];
+        if (v != ENER) uHLL[v] = dv.div(sR * uR[v] - sL * uL[v] + fL[v] - fR[v], rS);
+    const typename D::R rH = dv.recip(uHLL[DENS]);
+    const double velHx = dv.div(uHLL[MOMX], rH);
+    const double velHy = dv.div(uHLL[MOMY], rH);
+    const double velHz = dv.div(uHLL[MOMZ], rH);
     const double magDotVelHLL = dot3(uHLL[MAGX], uHLL[MAGY], uHLL[MAGZ], velHx, velHy, velHz);
     const double magNHLL = uHLL[bN];
     const double pStr = rhoL * dL * (sStr - velNL) + pTotL - magNL * magNL + magNHLL * magNHLL;
     const bool left = side == 1;
-    const Side& K = left ? L : R;
+    const Side<D>& K = left ? L : R;
     const double sK = left ? sL : sR;
     const double dK = left ? dL : dR;
     const double velNK = left ? velNL : velNR;
@@ -257,18 +321,33 @@ __device__ __forceinline__ void hllc(const Phys& s, const double* uL, const doub
     const double vT1K = side_vel(K, 1 - dir), vT2K = K.vz;
     const double bT1K = side_mag(K, 1 - dir), bT2K = K.bz;
     const double eK = left ? uL[ENER] : uR[ENER];
+    const typename D::R rK = dv.recip(sK - sStr);
     double uStr[NCONS];
-    uStr[DENS] = K.rho * dK / (sK - sStr);
+    uStr[DENS] = dv.div(K.rho * dK, rK);
     uStr[mN] = uStr[DENS] * sStr;
-    uStr[mT1] = uStr[DENS] * vT1K - (magNHLL * uHLL[bT1] - magNK * bT1K) / (sK - sStr);
-    uStr[mT2] = uStr[DENS] * vT2K - (magNHLL * uHLL[bT2] - magNK * bT2K) / (sK - sStr);
+    uStr[mT1] = uStr[DENS] * vT1K - dv.div(magNHLL * uHLL[bT1] - magNK * bT1K, rK);
+    uStr[mT2] = uStr[DENS] * vT2K - dv.div(magNHLL * uHLL[bT2] - magNK * bT2K, rK);
     uStr[bN] = magNHLL;
     uStr[bT1] = uHLL[bT1];
     uStr[bT2] = uHLL[bT2];
     uStr[ENER] = eK * dK + pStr * sStr - pTotK * velNK - magNHLL * magDotVelHLL + magNK * magDotVelK;
-    uStr[ENER] = uStr[ENER] / (sK - sStr);
+    uStr[ENER] = dv.div(uStr[ENER], rK);
 #pragma unroll
     for (int v = 0; v < NCONS; v++) flux[v] = (left ? fL[v] : fR[v]) + sK * (uStr[v] - (left ? uL[v] : uR[v]));
+}
+
+// the Riemann solver with IEEE division throughout (the rare fallback)
+static __device__ __noinline__ void hllc_ieee(const Phys& s, const double* uL, const double* uR, int dir, double* flux) {
+    IeeeDiv dv;
+    hllc_t(s, uL, uR, dir, flux, dv);
+}
+
+// HLLC with shared reciprocals; any operand outside their proven range sends
+// the whole solve through IEEE division instead (same result bits either way)
+__device__ __forceinline__ void hllc(const Phys& s, const double* uL, const double* uR, int dir, double* flux) {
+    SharedRecipDiv dv;
+    hllc_t(s, uL, uR, dir, flux, dv);
+    if (!dv.ok) hllc_ieee(s, uL, uR, dir, flux);
 }
 
 // src/detect.f90:250-265 (CAD) and :238-248 (PAD)
