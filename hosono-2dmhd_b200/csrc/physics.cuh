@@ -136,8 +136,9 @@ __device__ __forceinline__ double dot3(double a0, double a1, double a2, double b
 // remainder r = a - b*q is exact and RN(q + r*y) = RN(a/b).  q0 = RN(a*y) is
 // within two ulps of a/b; one correction q1 = RN(q0 + y*RN(a - b*q0)) brings
 // it within one ulp, and a second gives the correctly rounded quotient -- the
-// same bits as '/' (tests/div_check.cu compares the two on the GPU).  The proof assumes no overflow, underflow or subnormal in a, b,
-// a*y and the remainders; every operand outside [2^-500, 2^500] (zero
+// same bits as '/' (tests/div_check.cu compares the two on the GPU).  The
+// proof assumes no overflow, underflow or subnormal in a, b, a*y and the
+// remainders; every operand outside [2^-500, 2^501) (zero
 // numerators excepted) clears `ok`, and the caller then recomputes the whole
 // solve with IeeeDiv.  Cost per quotient: one multiply and four FMAs, no
 // branch.
@@ -154,20 +155,21 @@ struct SharedRecipDiv {
         double b, y;
     };
     bool ok = true;
-    __device__ __forceinline__ static bool in_range(double x) {
-        const double ax = fabs(x);
-        return ax >= 0x1p-500 && ax <= 0x1p500;
+    // |x| in [2^-500, 2^501), from the exponent bits (integer pipes)
+    __device__ __forceinline__ static bool in_range(unsigned long long mag) {
+        return (unsigned)((int)(mag >> 52) - (1023 - 500)) <= 1000u;
     }
     __device__ __forceinline__ R recip(double b) {
-        ok = ok && in_range(b);
+        ok = ok && in_range((unsigned long long)__double_as_longlong(b) & 0x7fffffffffffffffull);
         return R{b, __drcp_rn(b)};
     }
     __device__ __forceinline__ double div(double a, const R& r) {
-        ok = ok && (a == 0.0 || in_range(a));
+        const unsigned long long mag = (unsigned long long)__double_as_longlong(a) & 0x7fffffffffffffffull;
+        ok = ok && (mag == 0 || in_range(mag));
         const double q0 = a * r.y;
         const double q1 = fma(fma(-r.b, q0, a), r.y, q0);
         const double q2 = fma(fma(-r.b, q1, a), r.y, q1);
-        return a == 0.0 ? q0 : q2;
+        return mag == 0 ? q0 : q2;  // a = +-0: q0 carries the sign of the IEEE quotient
     }
 };
 
@@ -350,11 +352,15 @@ __device__ __forceinline__ void hllc(const Phys& s, const double* uL, const doub
     if (!dv.ok) hllc_ieee(s, uL, uR, dir, flux);
 }
 
-// src/detect.f90:250-265 (CAD) and :238-248 (PAD)
+// src/detect.f90:250-265 (CAD) and :238-248 (PAD): both finite (not NaN,
+// not infinite) and both > 0, i.e. each bit pattern is a positive, nonzero,
+// finite double (tested on the integer pipes)
+__device__ __forceinline__ bool positive_finite(double x) {
+    const unsigned long long u = (unsigned long long)__double_as_longlong(x);
+    return u - 1ull < 0x7fefffffffffffffull;  // u in [1, 0x7fefffffffffffff]
+}
 __device__ __forceinline__ bool admissible(double dens, double pres) {
-    const bool cad = !(isnan(dens) || isnan(pres) || !isfinite(dens) || !isfinite(pres));
-    const bool pad = (dens > 0.0) && (pres > 0.0);
-    return cad && pad;
+    return positive_finite(dens) && positive_finite(pres);
 }
 
 }  // namespace hosono

@@ -49,8 +49,8 @@ __global__ void check(unsigned long long seed, long long n, unsigned long long* 
         const auto rr = dv.recip(b);
         const double q = dv.div(a, rr);
         const double ref = a / b;
-        const bool in = (fabs(b) >= 0x1p-500 && fabs(b) <= 0x1p500) &&
-                        (a == 0.0 || (fabs(a) >= 0x1p-500 && fabs(a) <= 0x1p500));
+        const bool in = (fabs(b) >= 0x1p-500 && fabs(b) < 0x1p501) &&
+                        (a == 0.0 || (fabs(a) >= 0x1p-500 && fabs(a) < 0x1p501));
         if (dv.ok) {
             unsigned long long x, y;
             memcpy(&x, &q, 8);
