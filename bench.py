@@ -300,7 +300,7 @@ def bench_ours(args, rank, world, local):
         "gpu_launches": launches, "clocks": clk, "roofline": roofline, "e2e": e2e,
     }
     if world == 1 and not args.no_batched:
-        line["batched"] = bench_batched(m, fp, torch)
+        line["batched"] = bench_batched(m, fp, torch, limit=args.batched_limit, eager=args.eager)
     served_kept = {}
     if world == 1 and args.serve_requests > 0:
         line["served"], served_kept = bench_served(m, fp, args.serve_requests, args.serve_check)
@@ -323,7 +323,7 @@ def load_problems():
     return importlib.import_module("hosono_2dmhd_b200.problems")
 
 
-def bench_batched(m, fp, torch, manifest="blast64_seed0.json", limit=None):
+def bench_batched(m, fp, torch, manifest="blast64_seed0.json", limit=None, eager=False):
     """The 64-instance MHD-blast workload (uneven N in {128..512}) advanced to
     t_end=0.02 as one batch (one graph launch for the whole run) and, for
     comparison, as 64 plain single solves one after the other.  Set-up (host
@@ -338,6 +338,8 @@ def bench_batched(m, fp, torch, manifest="blast64_seed0.json", limit=None):
         pars = [problems.make(d, f"i{e['id']}", problems.from_entry(e)) for e in entries]
         tiles = sum(m.Batch.tiles_for(m.par_load(p)[0]) for p in pars)
         b = m.Batch(len(pars), tiles, fp_mode=fp)
+        if eager:
+            b.set_graphs(False)
         slots = [b.add_par(p) for p in pars]
         b.run(max_steps=1)
         n0 = {k: b.status(k)["nstep"] for k in slots}
@@ -376,7 +378,7 @@ def bench_batched(m, fp, torch, manifest="blast64_seed0.json", limit=None):
             s.close()
     rate_b = zu_b / (ms_b / 1e3)
     rate_p = zu_p / (ms_p / 1e3)
-    return {"workload": "blast64: 64 MHD blasts, N in {128..512} (seed 0), R=2, t_end=0.02",
+    return {"workload": f"blast64: {len(entries)} of 64 MHD blasts, N in {{128..512}} (seed 0), R=2, t_end=0.02",
             "instances": len(entries), "zone_updates": zu_b, "steps_min": min(steps), "steps_max": max(steps),
             "batched_value": rate_b, "batched_s": ms_b / 1e3, "batched_wall_s": wall_b,
             "plain_value": rate_p, "plain_s": ms_p / 1e3, "ratio_batched_over_plain": rate_b / rate_p,
@@ -452,7 +454,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the 64-instance batched-vs-plain measurement")
     ap.add_argument("--eager", action="store_true",
-                    help="launch the step's kernels one by one instead of as a CUDA graph (for profilers)")
+                    help="launch kernels one by one instead of as CUDA graphs (the plain and batched legs; for "
+                         "profilers, which do not see inside conditional graph nodes)")
+    ap.add_argument("--batched-limit", type=int, default=64, help="instances of the batched workload to run")
     ap.add_argument("--serve-requests", type=int, default=20,
                     help="requests of the served stream to run (0: skip the served measurement)")
     ap.add_argument("--serve-check", type=int, default=3,

@@ -161,7 +161,7 @@ Engine::~Engine() {
         if (ev) cudaEventDestroy(ev);
     for (void* p : {(void*)d_dev_, (void*)d_st_, (void*)d_tiles_, (void*)d_ntiles_, (void*)d_flags_, (void*)staging_,
                     (void*)schemeInt_, (void*)lists_.rec, (void*)lists_.face, (void*)lists_.recF, (void*)lists_.low,
-                    (void*)lists_.counts})
+                    (void*)lists_.next, (void*)lists_.counts})
         if (p) cudaFree(p);
     if (h_flags_) cudaFreeHost(h_flags_);
     if (h_st_) cudaFreeHost(h_st_);
@@ -184,6 +184,7 @@ int Engine::init(int max_inst, int max_tiles, int fp_mode) {
     CUE(cudaMalloc(&lists_.face, sizeof(int2) * 2 * lists_.cap));
     CUE(cudaMalloc(&lists_.recF, sizeof(int2) * lists_.cap));
     CUE(cudaMalloc(&lists_.low, sizeof(int2) * lists_.cap));
+    CUE(cudaMalloc(&lists_.next, sizeof(int2) * lists_.cap));
     CUE(cudaMalloc(&lists_.counts, sizeof(int) * (LIST_N + 1)));
     CUE(cudaMemsetAsync(lists_.counts, 0, sizeof(int) * (LIST_N + 1), s_));
     CUE(cudaMallocHost(&h_flags_, sizeof(BatchFlags)));

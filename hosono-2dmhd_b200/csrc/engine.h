@@ -100,12 +100,13 @@ __host__ __device__ inline double* role_ptr(const InstDev& d, int parity, int ro
 
 // Work lists of the later MOOD passes (compacted by warp ballot): entries are
 // (instance, cell index j*pitch+i); face entries carry 2*cell+dir.
-enum : int { LIST_REC = 0, LIST_FACE = 1, LIST_RECF = 2, LIST_LOW = 3, LIST_N = 4, LIST_OVERFLOW = 4 };
+enum : int { LIST_REC = 0, LIST_FACE = 1, LIST_RECF = 2, LIST_LOW = 3, LIST_NEXT = 4, LIST_N = 5, LIST_OVERFLOW = 5 };
 struct Lists {
     int2* rec;    // cells to re-reconstruct (recompute set)
     int2* face;   // faces to re-flux
     int2* recF;   // cells to FLICD + update + detect (recomputeFLICD set)
     int2* low;    // cells detect lowered this pass (to clear `lowered` after use)
+    int2* next;   // cells an inner cascade iteration re-reconstructs (nextPass set)
     int* counts;  // [LIST_*] entries, [LIST_OVERFLOW] set if a list overflowed
     long long cap;  // entries per list (the face list holds 2*cap)
 };
@@ -139,7 +140,7 @@ struct KernelSet {
     void (*face_pass1)(const Batch&, int uin, cudaStream_t);
     void (*cascade_cond)(const Batch&, cudaGraphConditionalHandle h, cudaStream_t);
     void (*cascade_lower)(const Batch&, int mode, cudaStream_t);
-    void (*recon_check)(const Batch&, int uin, int mask, cudaStream_t);
+    void (*recon_check)(const Batch&, int uin, int mask, cudaStream_t);  // compact nextPass, re-reconstruct
     void (*flux)(const Batch&, int uin, int mode, cudaStream_t);
     void (*ct_update_detect)(const Batch&, int uin, int uout, cudaStream_t);
     void (*mood_flags)(const Batch&, cudaStream_t);

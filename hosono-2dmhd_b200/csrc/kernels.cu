@@ -329,6 +329,7 @@ __global__ void k_cascade_cond(Batch B, cudaGraphConditionalHandle h, int set_ha
     __syncthreads();
     if (threadIdx.x == 0) {
         B.flags->anyFail = any;
+        B.L.counts[LIST_NEXT] = 0;  // the next cascade iteration compacts its cells afresh
         if (set_handle) cudaGraphSetConditional(h, any ? 1u : 0u);
     }
 }
@@ -401,59 +402,6 @@ __global__ void __launch_bounds__(NTHREADS) k_cascade_lower(Batch B) {
     FOR_TILES(B, t) t_cascade_lower(B, tile_at(B, t));
 }
 
-// One cell of an inner pass of reconstruct_faceValsWithGP: all four faces at
-// rr = min(scheme(c), scheme(nbr)) (EDP1), CAD/PAD at every quadrature point;
-// the radius used per face is recorded in rrRec.  Returns true if a face
-// state is inadmissible.
-__device__ __forceinline__ bool recon_cell(const InstDev& d, const InstState& S, int uin, int i, int j,
-                                           long long cc) {
-    const Geo& G = d.geo;
-    const double* U = role_ptr(d, S.parity, uin);
-    const int8_t* sch = d.scheme[S.schemeSel];
-    d.dirty[cc] = 1;
-    const int s = sch[cc];
-    int rr[4];
-    rr[NORTH] = min(s, (int)sch[cc + G.pitch]);
-    rr[SOUTH] = min(s, (int)sch[cc - G.pitch]);
-    rr[EAST] = min(s, (int)sch[cc + 1]);
-    rr[WEST] = min(s, (int)sch[cc - 1]);
-    d.rrRec[cc] = (uint8_t)(rr[0] | (rr[1] << 2) | (rr[2] << 4) | (rr[3] << 6));
-    bool bad = false;
-#pragma unroll 1
-    for (int f = 0; f < 4 && !bad; f++) {
-        if (rr[f] == 0) continue;
-#pragma unroll 1
-        for (int q = 0; q <= rr[f] && !bad; q++) {
-            double u[NCONS];
-            face_value(d, U, rr[f], i, j, f, q, u);
-            if (!admissible(u[DENS], cons2pres(d.phys, u))) bad = true;
-        }
-    }
-    if (bad) d.fail[cc] = 1;
-    return bad;
-}
-
-// Inner cascade pass over the cells marked in nextPass (dense over the tiles
-// of instances in their cascade).
-__device__ __forceinline__ void t_recon_check(const Batch& B, int uin, int /*maskSel*/, const Cell c) {
-    InstState& S = B.st[c.k];
-    if (!S.nextIter) return;
-    const InstDev& d = B.dev[c.k];
-    const Geo& G = d.geo;
-    const int g = G.g;
-    const int i = c.i, j = c.j;
-    if (first_tile_thread(c)) S.cascadeMode = CASCADE_FROM_CELLS;
-    bool bad = false;
-    if (i >= g - 2 && j >= g - 2 && i <= g + G.nx + 1 && j <= g + G.ny + 1) {
-        const long long cc = (long long)j * G.pitch + i;
-        if (d.nextPass[cc]) bad = recon_cell(d, S, uin, i, j, cc);
-    }
-    warp_flag(&S.anyFail, bad);
-}
-__global__ void __launch_bounds__(NTHREADS) k_recon_check(Batch B, int uin, int maskSel) {
-    FOR_TILES(B, t) t_recon_check(B, uin, maskSel, tile_at(B, t));
-}
-
 // ----------------------------------------------------------------------
 // Work lists of the later MOOD passes.  Appends are warp-aggregated: one
 // atomicAdd per warp reserves the slots, each active lane writes at its rank.
@@ -476,6 +424,91 @@ __device__ __forceinline__ void warp_append(const Lists& L, int which, int2* lis
 }
 
 __device__ __forceinline__ int2 entry(int k, long long cc) { return make_int2(k, (int)cc); }
+
+// Lane groups: list kernels give each item (a cell to re-reconstruct, a face
+// to re-flux) a group of GL lanes that split its independent parts (faces x
+// quadrature points, or quadrature points), so one item costs the latency of
+// one face value instead of a dozen in a row.  The loop runs in whole-warp
+// steps so warp collectives see every lane.
+#define FOR_GROUPS(n, GL, e, sub, act)                                                                        \
+    for (int wbase_ = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * (32 / (GL)), sub = threadIdx.x % (GL), \
+             e = wbase_ + (int)((threadIdx.x & 31) / (GL));                                                   \
+         wbase_ < (n); wbase_ += ((gridDim.x * blockDim.x) >> 5) * (32 / (GL)), e = wbase_ + (int)((threadIdx.x & 31) / (GL))) \
+        for (bool act = e < (n), once_ = true; once_; once_ = false)
+
+// One cell of an inner pass of reconstruct_faceValsWithGP on 16 lanes: lane
+// sub = 4*f + q takes face f at quadrature point q, at rr = min(scheme(c),
+// scheme(nbr)) (EDP1), and tests CAD/PAD there.  The radius used per face is
+// recorded in rrRec; `fail` is set when any face state is inadmissible (the
+// reference's loop stops at the first one; the verdict is the same).
+// Returns the cell's verdict on every lane of the group.
+constexpr int RECON_GL = 16;
+__device__ __forceinline__ bool recon_cell_group(const InstDev& d, const InstState& S, int uin, long long cc,
+                                                 int sub, bool act) {
+    bool bad = false;
+    int i = 0, j = 0;
+    if (act) {
+        const Geo& G = d.geo;
+        j = (int)(cc / G.pitch);
+        i = (int)(cc - (long long)j * G.pitch);
+        const int8_t* sch = d.scheme[S.schemeSel];
+        const int s = sch[cc];
+        const int f = sub >> 2, q = sub & 3;
+        const long long nb = f == NORTH ? cc + G.pitch : f == SOUTH ? cc - G.pitch : f == EAST ? cc + 1 : cc - 1;
+        const int rr = min(s, (int)sch[nb]);
+        if (sub == 0) {
+            const int rN = min(s, (int)sch[cc + G.pitch]), rS = min(s, (int)sch[cc - G.pitch]);
+            const int rE = min(s, (int)sch[cc + 1]), rW = min(s, (int)sch[cc - 1]);
+            d.dirty[cc] = 1;
+            d.rrRec[cc] = (uint8_t)(rN | (rS << 2) | (rE << 4) | (rW << 6));
+        }
+        if (rr > 0 && q <= rr) {
+            double u[NCONS];
+            face_value(d, role_ptr(d, S.parity, uin), rr, i, j, f, q, u);
+            bad = !admissible(u[DENS], cons2pres(d.phys, u));
+        }
+    }
+    const unsigned m = __ballot_sync(0xffffffffu, bad);
+    const unsigned gm = 0xffffu << ((threadIdx.x & 31) & ~15);
+    const bool any = (m & gm) != 0;
+    if (act && sub == 0 && any) d.fail[cc] = 1;
+    return any;
+}
+
+// Inner cascade pass: compact the cells marked in nextPass (dense over the
+// tiles of instances in their cascade) ...
+__device__ __forceinline__ void t_compact_next(const Batch& B, const Cell c) {
+    InstState& S = B.st[c.k];
+    if (!S.nextIter) return;
+    const InstDev& d = B.dev[c.k];
+    const Geo& G = d.geo;
+    const int g = G.g;
+    if (first_tile_thread(c)) S.cascadeMode = CASCADE_FROM_CELLS;
+    bool p = false;
+    long long cc = 0;
+    if (c.i >= g - 2 && c.j >= g - 2 && c.i <= g + G.nx + 1 && c.j <= g + G.ny + 1) {
+        cc = (long long)c.j * G.pitch + c.i;
+        p = d.nextPass[cc] != 0;
+    }
+    warp_append(B.L, LIST_NEXT, B.L.next, B.L.cap, p, entry(c.k, cc));
+}
+__global__ void __launch_bounds__(NTHREADS) k_compact_next(Batch B) {
+    FOR_TILES(B, t) t_compact_next(B, tile_at(B, t));
+}
+// ... and re-reconstruct them (list `which`: LIST_NEXT in the cascade,
+// LIST_REC at the start of a later MOOD pass)
+__global__ void __launch_bounds__(256) k_recon_group(Batch B, int uin, int which) {
+    const int2* list = which == LIST_NEXT ? B.L.next : B.L.rec;
+    const int n = min(B.L.counts[which], (int)B.L.cap);
+    FOR_GROUPS(n, RECON_GL, e, sub, act) {
+        int2 it = make_int2(0, 0);
+        if (act) it = list[e];
+        InstState& S = B.st[it.x];
+        const bool bad = recon_cell_group(B.dev[it.x], S, uin, it.y, sub, act);
+        if (act && sub == 0 && bad) atomicOr(&S.anyFail, 1);
+    }
+}
+
 
 // cells with recompute in the reconstruct range (reconstruct.f90:83)
 __device__ __forceinline__ void t_compact_rec(const Batch& B, const Cell c) {
@@ -553,21 +586,6 @@ __global__ void __launch_bounds__(NTHREADS) k_compact_dirty(Batch B) {
     for (int base_ = (blockIdx.x * blockDim.x + threadIdx.x) & ~31, e = base_ + (threadIdx.x & 31);      \
          base_ < (n); base_ += gridDim.x * blockDim.x, e = base_ + (threadIdx.x & 31))                   \
         for (bool act = e < (n), once_ = true; once_; once_ = false)
-
-// re-reconstruction of the rec list (first inner pass of a later MOOD pass)
-__global__ void __launch_bounds__(256) k_recon_list(Batch B, int uin) {
-    const int n = min(B.L.counts[LIST_REC], (int)B.L.cap);
-    FOR_LIST(n, e, act) {
-        if (act) {
-            const int2 it = B.L.rec[e];
-            InstState& S = B.st[it.x];
-            const InstDev& d = B.dev[it.x];
-            const long long cc = it.y;
-            const int j = (int)(cc / d.geo.pitch), i = (int)(cc - (long long)j * d.geo.pitch);
-            if (recon_cell(d, S, uin, i, j, cc)) atomicOr(&S.anyFail, 1);
-        }
-    }
-}
 
 // ======================================================================
 // getFluxes_ (getFluxes.f90:16-90) on flagged faces.  Face values are rebuilt
@@ -665,11 +683,66 @@ __device__ __forceinline__ void flux_face(const InstDev& d, const InstState& S, 
         d.CTY[cc] = F[MAGX];
     }
 }
+// getFluxes_ on the face list of a later MOOD pass, 4 lanes per face: lane q
+// takes quadrature point q (both face values and the Riemann solve); the
+// group's first lane sums w_q * F_q in quadrature order, as
+// riemannSolver_getFaceFlux does.
+constexpr int FLUX_GL = 4;
 __global__ void __launch_bounds__(256) k_flux_list(Batch B, int uin) {
     const int n = min(B.L.counts[LIST_FACE], (int)(2 * B.L.cap));
-    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
-        const int2 it = B.L.face[e];
-        flux_face(B.dev[it.x], B.st[it.x], uin, (long long)(it.y >> 1), it.y & 1);
+    FOR_GROUPS(n, FLUX_GL, e, sub, act) {
+        int2 it = make_int2(0, 0);
+        if (act) it = B.L.face[e];
+        const InstDev& d = B.dev[it.x];
+        const InstState& S = B.st[it.x];
+        const Geo& G = d.geo;
+        const long long cc = (long long)(it.y >> 1);
+        const int dir = it.y & 1;
+        double F[NCONS];
+#pragma unroll
+        for (int v = 0; v < NCONS; v++) F[v] = 0.0;
+        int rr = 0;
+        if (act) {
+            const int j = (int)(cc / G.pitch), i = (int)(cc - (long long)j * G.pitch);
+            const long long cn = dir == XDIR ? cc - 1 : cc - G.pitch;
+            const int8_t* sch = d.scheme[S.schemeSel];
+            rr = min((int)sch[cc], (int)sch[cn]);
+            if (sub <= rr) {  // rr == 0: one Riemann solve, on lane 0
+                const int fL = dir == XDIR ? EAST : NORTH, fR = dir == XDIR ? WEST : SOUTH;
+                const int rrL = (d.rrRec[cn] >> (2 * fL)) & 3;
+                const int rrR = (d.rrRec[cc] >> (2 * fR)) & 3;
+                const double* U = role_ptr(d, S.parity, uin);
+                double uL[NCONS], uR[NCONS];
+                face_value(d, U, rrL, dir == XDIR ? i - 1 : i, dir == XDIR ? j : j - 1, fL, sub, uL);
+                face_value(d, U, rrR, i, j, fR, sub, uR);
+                hllc(d.phys, uL, uR, dir, F);
+            }
+        }
+        const int lane0 = (threadIdx.x & 31) & ~(FLUX_GL - 1);
+        double acc[NCONS];
+#pragma unroll
+        for (int v = 0; v < NCONS; v++) acc[v] = 0.0;
+#pragma unroll
+        for (int q = 0; q < FLUX_GL; q++) {
+            double Fq[NCONS];
+#pragma unroll
+            for (int v = 0; v < NCONS; v++) Fq[v] = __shfl_sync(0xffffffffu, F[v], lane0 + q);
+            if (act && sub == 0 && rr > 0 && q <= rr) {
+                const double w = qw_at(d, rr, q);
+#pragma unroll
+                for (int v = 0; v < NCONS; v++) acc[v] = acc[v] + w * Fq[v];
+            }
+        }
+        if (act && sub == 0) {
+            if (rr == 0) {
+#pragma unroll
+                for (int v = 0; v < NCONS; v++) acc[v] = F[v];
+            }
+            double* Fo = dir == XDIR ? d.FX : d.FY;
+#pragma unroll
+            for (int v = 0; v < NCONS; v++) Fo[v * G.plane + cc] = acc[v];
+            (dir == XDIR ? d.CTX : d.CTY)[cc] = dir == XDIR ? acc[MAGY] : acc[MAGX];
+        }
     }
 }
 
@@ -1278,6 +1351,7 @@ dim3 grid_for(K kernel, const Batch& B) {
     return dim3((unsigned)(r < B.maxTiles ? r : B.maxTiles));
 }
 #define TILE_LAUNCH(kern, B, s, ...) kern<<<grid_for(kern, B), kTile, 0, s>>>(B, ##__VA_ARGS__)
+#define LIST_LAUNCH(kern, B, s, ...) kern<<<dim3((unsigned)resident_blocks((const void*)kern)), dim3(256), 0, s>>>(B, ##__VA_ARGS__)
 
 void l_cfl_reduce(const Batch& B, cudaStream_t s) { TILE_LAUNCH(k_cfl_reduce, B, s); }
 void l_step_prepare(const Batch& B, int steps, cudaStream_t s) { k_step_prepare<<<1, 128, 0, s>>>(B, steps); }
@@ -1308,8 +1382,9 @@ void l_cascade_lower(const Batch& B, int /*mode: per instance*/, cudaStream_t s)
     TILE_LAUNCH(k_clear_nextpass, B, s);
     TILE_LAUNCH(k_cascade_lower, B, s);
 }
-void l_recon_check(const Batch& B, int uin, int mask, cudaStream_t s) {
-    TILE_LAUNCH(k_recon_check, B, s, uin, mask);
+void l_recon_check(const Batch& B, int uin, int /*mask*/, cudaStream_t s) {
+    TILE_LAUNCH(k_compact_next, B, s);
+    LIST_LAUNCH(k_recon_group, B, s, uin, (int)LIST_NEXT);
 }
 void l_flux(const Batch& B, int uin, int mode, cudaStream_t s) { TILE_LAUNCH(k_flux, B, s, uin, mode); }
 void l_ct_update_detect(const Batch& B, int uin, int uout, cudaStream_t s) {
@@ -1323,8 +1398,7 @@ void l_compact_rec(const Batch& B, cudaStream_t s) { TILE_LAUNCH(k_compact_rec, 
 void l_compact_post(const Batch& B, cudaStream_t s) { TILE_LAUNCH(k_compact_post, B, s); }
 void l_compact_dirty(const Batch& B, cudaStream_t s) { TILE_LAUNCH(k_compact_dirty, B, s); }
 void l_detect_prep(const Batch& B, int uin, cudaStream_t s) { TILE_LAUNCH(k_detect_prep, B, s, uin); }
-#define LIST_LAUNCH(kern, B, s, ...) kern<<<dim3((unsigned)resident_blocks((const void*)kern)), dim3(256), 0, s>>>(B, ##__VA_ARGS__)
-void l_recon_list(const Batch& B, int uin, cudaStream_t s) { LIST_LAUNCH(k_recon_list, B, s, uin); }
+void l_recon_list(const Batch& B, int uin, cudaStream_t s) { LIST_LAUNCH(k_recon_group, B, s, uin, (int)LIST_REC); }
 void l_flux_list(const Batch& B, int uin, cudaStream_t s) { LIST_LAUNCH(k_flux_list, B, s, uin); }
 void l_ct_list(const Batch& B, int uin, int uout, cudaStream_t s) { LIST_LAUNCH(k_ct_list, B, s, uin, uout); }
 void l_clear_low(const Batch& B, cudaStream_t s) { LIST_LAUNCH(k_clear_low, B, s); }
