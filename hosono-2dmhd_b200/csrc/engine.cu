@@ -161,7 +161,7 @@ Engine::~Engine() {
         if (ev) cudaEventDestroy(ev);
     for (void* p : {(void*)d_dev_, (void*)d_st_, (void*)d_tiles_, (void*)d_ntiles_, (void*)d_flags_, (void*)staging_,
                     (void*)schemeInt_, (void*)lists_.rec, (void*)lists_.face, (void*)lists_.recF, (void*)lists_.low,
-                    (void*)lists_.next, (void*)lists_.counts})
+                    (void*)lists_.next, (void*)lists_.casc, (void*)lists_.sync, (void*)lists_.counts})
         if (p) cudaFree(p);
     if (h_flags_) cudaFreeHost(h_flags_);
     if (h_st_) cudaFreeHost(h_st_);
@@ -185,6 +185,8 @@ int Engine::init(int max_inst, int max_tiles, int fp_mode) {
     CUE(cudaMalloc(&lists_.recF, sizeof(int2) * lists_.cap));
     CUE(cudaMalloc(&lists_.low, sizeof(int2) * lists_.cap));
     CUE(cudaMalloc(&lists_.next, sizeof(int2) * lists_.cap));
+    CUE(cudaMalloc(&lists_.casc, sizeof(int2) * lists_.cap));
+    CUE(cudaMalloc(&lists_.sync, sizeof(int8_t) * 2 * lists_.cap));
     CUE(cudaMalloc(&lists_.counts, sizeof(int) * (LIST_N + 1)));
     CUE(cudaMemsetAsync(lists_.counts, 0, sizeof(int) * (LIST_N + 1), s_));
     CUE(cudaMallocHost(&h_flags_, sizeof(BatchFlags)));
@@ -517,11 +519,11 @@ int Engine::record_stage(Rec& r, int uin, int uout, cudaEvent_t ev0, cudaEvent_t
     TRYE(r.k([&](cudaStream_t s) { K->compact_dirty(B, s); }));
     TRYE(r.k([&](cudaStream_t s) { K->flux_list(B, uin, s); }));
     TRYE(r.k([&](cudaStream_t s) { K->ct_update_detect(B, uin, uout, s); }));
-    TRYE(r.k([&](cudaStream_t s) { K->mood_flags(B, s); }));
+    TRYE(r.k([&](cudaStream_t s) { K->mood_flags(B, 1, s); }));
     if (trace) TRYE(r.host([&] { return trace_snapshot(); }));
     TRYE(r.k([&](cudaStream_t s) { K->clear_low(B, s); }));
     TRYE(r.cond(&hm, 0));
-    TRYE(r.k([&](cudaStream_t s) { K->pass_end(B, hm, s); }));
+    TRYE(r.k([&](cudaStream_t s) { K->pass_end(B, hm, 1, s); }));
     if (trace) TRYE(r.host([&] { return trace_after_pass(); }));
     // later MOOD passes touch the flagged cells only: each step builds a work
     // list (warp ballot + one atomic per warp) and a list kernel consumes it
@@ -536,10 +538,10 @@ int Engine::record_stage(Rec& r, int uin, int uout, cudaEvent_t ev0, cudaEvent_t
         TRYE(b.k([&](cudaStream_t s) { K->compact_post(B, s); }));
         TRYE(b.k([&](cudaStream_t s) { K->flux_list(B, uin, s); }));
         TRYE(b.k([&](cudaStream_t s) { K->ct_list(B, uin, uout, s); }));
-        TRYE(b.k([&](cudaStream_t s) { K->mood_flags(B, s); }));
+        TRYE(b.k([&](cudaStream_t s) { K->mood_flags(B, 0, s); }));
         if (trace) TRYE(b.host([&] { return trace_snapshot(); }));
         TRYE(b.k([&](cudaStream_t s) { K->clear_low(B, s); }));
-        TRYE(b.k([&](cudaStream_t s) { K->pass_end(B, hm, s); }));
+        TRYE(b.k([&](cudaStream_t s) { K->pass_end(B, hm, 0, s); }));
         if (trace) TRYE(b.host([&] { return trace_after_pass(); }));
         return HOSONO_OK;
     }));

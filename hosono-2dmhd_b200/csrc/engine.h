@@ -100,13 +100,16 @@ __host__ __device__ inline double* role_ptr(const InstDev& d, int parity, int ro
 
 // Work lists of the later MOOD passes (compacted by warp ballot): entries are
 // (instance, cell index j*pitch+i); face entries carry 2*cell+dir.
-enum : int { LIST_REC = 0, LIST_FACE = 1, LIST_RECF = 2, LIST_LOW = 3, LIST_NEXT = 4, LIST_N = 5, LIST_OVERFLOW = 5 };
+enum : int { LIST_REC = 0, LIST_FACE = 1, LIST_RECF = 2, LIST_LOW = 3, LIST_NEXT = 4, LIST_CASC = 5, LIST_N = 6,
+             LIST_OVERFLOW = 6 };
 struct Lists {
     int2* rec;    // cells to re-reconstruct (recompute set)
     int2* face;   // faces to re-flux
     int2* recF;   // cells to FLICD + update + detect (recomputeFLICD set)
     int2* low;    // cells detect lowered this pass (to clear `lowered` after use)
     int2* next;   // cells an inner cascade iteration re-reconstructs (nextPass set)
+    int2* casc;   // cells the inner cascade lowered in this MOOD pass (each once)
+    int8_t* sync; // per entry of low then casc: the scheme its translate class takes
     int* counts;  // [LIST_*] entries, [LIST_OVERFLOW] set if a list overflowed
     long long cap;  // entries per list (the face list holds 2*cap)
 };
@@ -143,8 +146,10 @@ struct KernelSet {
     void (*recon_check)(const Batch&, int uin, int mask, cudaStream_t);  // compact nextPass, re-reconstruct
     void (*flux)(const Batch&, int uin, int mode, cudaStream_t);
     void (*ct_update_detect)(const Batch&, int uin, int uout, cudaStream_t);
-    void (*mood_flags)(const Batch&, cudaStream_t);
-    void (*pass_end)(const Batch&, cudaGraphConditionalHandle h, cudaStream_t);
+    // dense: every cell (MOOD pass 1); else from the work lists (later passes)
+    void (*mood_flags)(const Batch&, int dense, cudaStream_t);
+    // flip: the dense flag rebuild wrote the other scheme buffer
+    void (*pass_end)(const Batch&, cudaGraphConditionalHandle h, int flip, cudaStream_t);
     // later MOOD passes on compacted work lists
     void (*compact_rec)(const Batch&, cudaStream_t);
     void (*recon_list)(const Batch&, int uin, cudaStream_t);

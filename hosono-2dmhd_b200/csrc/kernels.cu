@@ -43,6 +43,11 @@ namespace KNS {
 
 constexpr int NTHREADS = TILE_X * TILE_Y;
 
+// detMask bits: the per-stage detect_ALL terms (written by k_detect_prep),
+// and DM_CASC, set while a cell sits on the cascade-lowered list of the
+// current MOOD pass
+enum : int { DM_SHOCK = 1, DM_PLATEAU = 2, DM_SMOOTH = 4, DM_CASC = 8 };
+
 __device__ __forceinline__ int iabs_c(int a) { return a < 0 ? -a : a; }
 
 // The instance and cell a thread works on in tile t.
@@ -122,6 +127,29 @@ __device__ __forceinline__ void warp_count(int* counter, bool v) {
     const unsigned m = __ballot_sync(0xffffffffu, v);
     if (m && (threadIdx.x & 31) == 0) atomicAdd(counter, __popc(m));
 }
+
+// ----------------------------------------------------------------------
+// Work lists of the later MOOD passes.  Appends are warp-aggregated: one
+// atomicAdd per warp reserves the slots, each active lane writes at its rank.
+__device__ __forceinline__ void warp_append(const Lists& L, int which, int2* list, long long cap, bool pred,
+                                            int2 item) {
+    const unsigned m = __ballot_sync(0xffffffffu, pred);
+    if (!m) return;
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(m) - 1;
+    int base = 0;
+    if (lane == leader) base = atomicAdd(L.counts + which, __popc(m));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    const long long pos = (long long)base + __popc(m & ((1u << lane) - 1));
+    if (pred) {
+        if (pos < cap)
+            list[pos] = item;
+        else
+            L.counts[LIST_OVERFLOW] = 1;
+    }
+}
+
+__device__ __forceinline__ int2 entry(int k, long long cc) { return make_int2(k, (int)cc); }
 
 // ======================================================================
 // MOOD pass 1 (every scheme == R): reconstruct_faceValsWithGP + face CAD/PAD
@@ -397,33 +425,17 @@ __device__ __forceinline__ void t_cascade_lower(const Batch& B, const Cell c) {
         if (f) lower_cell(d, S, i, j, cc);
     }
     warp_count(&S.nInner, f);
+    // the first lowering of a cell in this pass puts it on the list whose
+    // translate classes the later-pass flag rebuild brings to one scheme
+    const long long cc = (long long)j * G.pitch + i;
+    const bool first = f && !(d.detMask[cc] & DM_CASC);
+    if (first) d.detMask[cc] |= DM_CASC;
+    warp_append(B.L, LIST_CASC, B.L.casc, B.L.cap, first, entry(c.k, cc));
 }
 __global__ void __launch_bounds__(NTHREADS) k_cascade_lower(Batch B) {
     FOR_TILES(B, t) t_cascade_lower(B, tile_at(B, t));
 }
 
-// ----------------------------------------------------------------------
-// Work lists of the later MOOD passes.  Appends are warp-aggregated: one
-// atomicAdd per warp reserves the slots, each active lane writes at its rank.
-__device__ __forceinline__ void warp_append(const Lists& L, int which, int2* list, long long cap, bool pred,
-                                            int2 item) {
-    const unsigned m = __ballot_sync(0xffffffffu, pred);
-    if (!m) return;
-    const int lane = threadIdx.x & 31;
-    const int leader = __ffs(m) - 1;
-    int base = 0;
-    if (lane == leader) base = atomicAdd(L.counts + which, __popc(m));
-    base = __shfl_sync(0xffffffffu, base, leader);
-    const long long pos = (long long)base + __popc(m & ((1u << lane) - 1));
-    if (pred) {
-        if (pos < cap)
-            list[pos] = item;
-        else
-            L.counts[LIST_OVERFLOW] = 1;
-    }
-}
-
-__device__ __forceinline__ int2 entry(int k, long long cc) { return make_int2(k, (int)cc); }
 
 // Lane groups: list kernels give each item (a cell to re-reconstruct, a face
 // to re-flux) a group of GL lanes that split its independent parts (faces x
@@ -769,7 +781,7 @@ __device__ __forceinline__ double flicd_y(const InstDev& d, long long c) {
 //   bit 0: shock1 && shock2 && shock3 (:115-146), bit 1: plateau (:161),
 //   bit 2: u2 smoothness accepts (:177-213, option 3) --
 // and the per-pass test keeps the reference's order of decisions.
-enum : int { DM_SHOCK = 1, DM_PLATEAU = 2, DM_SMOOTH = 4 };
+
 
 __device__ __forceinline__ bool detect_cell(const InstDev& d, const double* __restrict__ U, long long c,
                                             const double un[NCONS]) {
@@ -1036,21 +1048,135 @@ __device__ __forceinline__ void t_mood_flags(const Batch& B, const Cell c) {
     d.rec[cc] = rec;
     d.recF[cc] = recF;
     schN[cc] = (int8_t)s;
+    d.detMask[cc] &= (uint8_t)~DM_CASC;
 }
 __global__ void __launch_bounds__(NTHREADS) k_mood_flags(Batch B) {
     FOR_TILES(B, t) t_mood_flags(B, tile_at(B, t));
 }
 
+// The same result from the work lists in a later MOOD pass, where few cells
+// change.  The flags read later (recompute on [g-2, g+n+1]^2, recomputeFLICD
+// on [g, g+n]^2) can only be set on cells of this pass's lists -- recompute:
+// the pass's starting list, both cells of each re-fluxed face, the cross of
+// each cascade lowering; recomputeFLICD: its list -- so clear those, then set
+// the cross / diamond of every translate of each cell detect lowered.  The scheme changes only on the translate classes of
+// cells lowered in this pass (by detect or by the inner cascade, which does
+// not sync): each takes min over its class of (scheme - lowered)^+, computed
+// for every listed cell first and written afterwards (two kernels), so no
+// class member is read after it was written.
+__device__ __forceinline__ void sync_cell(const Batch& B, int e, int nLow, int2* it_out, bool* from_low) {
+    *from_low = e < nLow;
+    *it_out = *from_low ? B.L.low[e] : B.L.casc[e - nLow];
+}
+__global__ void __launch_bounds__(256) k_flags_clear(Batch B) {
+    const int nF = min(B.L.counts[LIST_FACE], (int)(2 * B.L.cap));
+    const int nR = min(B.L.counts[LIST_RECF], (int)B.L.cap);
+    const int nP = min(B.L.counts[LIST_REC], (int)B.L.cap);
+    const int nC = min(B.L.counts[LIST_CASC], (int)B.L.cap);
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nF + nR + nP + nC; e += gridDim.x * blockDim.x) {
+        if (e < nF) {  // both cells of a re-fluxed face
+            const int2 it = B.L.face[e];
+            const InstDev& d = B.dev[it.x];
+            const long long cc = (long long)(it.y >> 1);
+            d.rec[cc] = 0;
+            d.rec[(it.y & 1) == XDIR ? cc - 1 : cc - d.geo.pitch] = 0;
+        } else if (e < nF + nR) {
+            const int2 it = B.L.recF[e - nF];
+            B.dev[it.x].recF[it.y] = 0;
+        } else if (e < nF + nR + nP) {  // recompute at the start of the pass
+            const int2 it = B.L.rec[e - nF - nR];
+            B.dev[it.x].rec[it.y] = 0;
+        } else {  // the cross a cascade lowering marked
+            const int2 it = B.L.casc[e - nF - nR - nP];
+            const InstDev& d = B.dev[it.x];
+            const long long cc = it.y, p = d.geo.pitch;
+            d.rec[cc] = 0;
+            d.rec[cc + 1] = 0;
+            d.rec[cc - 1] = 0;
+            d.rec[cc + p] = 0;
+            d.rec[cc - p] = 0;
+        }
+    }
+}
+__global__ void __launch_bounds__(256) k_flags_scatter(Batch B) {
+    const int nL = min(B.L.counts[LIST_LOW], (int)B.L.cap);
+    const int nC = min(B.L.counts[LIST_CASC], (int)B.L.cap);
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nL + nC; e += gridDim.x * blockDim.x) {
+        int2 it;
+        bool fromLow;
+        sync_cell(B, e, nL, &it, &fromLow);
+        const InstDev& d = B.dev[it.x];
+        const InstState& S = B.st[it.x];
+        const Geo& G = d.geo;
+        const int8_t* sch = d.scheme[S.schemeSel];
+        const long long c0 = it.y;
+        const int j0 = (int)(c0 / G.pitch), i0 = (int)(c0 - (long long)j0 * G.pitch);
+        const int reach = G.bc == 1 ? 1 : 0;
+        int s = 127;
+        for (int b = -reach; b <= reach; b++) {
+            const int jo = j0 + b * G.ny;
+            if (jo < 0 || jo >= G.nyt) continue;
+            for (int t = -reach; t <= reach; t++) {
+                const int io = i0 + t * G.nx;
+                if (io < 0 || io >= G.nxt) continue;
+                const long long co = (long long)jo * G.pitch + io;
+                const int so = sch[co] - d.lowered[co];
+                s = min(s, so > 0 ? so : 0);
+                if (!fromLow) continue;
+                for (int dj = -2; dj <= 2; dj++) {
+                    const int jj = jo + dj;
+                    if (jj < 0 || jj >= G.nyt) continue;
+                    for (int di = -2; di <= 2; di++) {
+                        const int dd = iabs_c(di) + iabs_c(dj);
+                        const int ii = io + di;
+                        if (dd > 2 || ii < 0 || ii >= G.nxt) continue;
+                        const long long cn = (long long)jj * G.pitch + ii;
+                        d.recF[cn] = 1;
+                        if (dd <= 1) d.rec[cn] = 1;
+                    }
+                }
+            }
+        }
+        B.L.sync[e] = (int8_t)s;
+    }
+}
+__global__ void __launch_bounds__(256) k_scheme_sync(Batch B) {
+    const int nL = min(B.L.counts[LIST_LOW], (int)B.L.cap);
+    const int nC = min(B.L.counts[LIST_CASC], (int)B.L.cap);
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nL + nC; e += gridDim.x * blockDim.x) {
+        int2 it;
+        bool fromLow;
+        sync_cell(B, e, nL, &it, &fromLow);
+        const InstDev& d = B.dev[it.x];
+        const Geo& G = d.geo;
+        int8_t* sch = d.scheme[B.st[it.x].schemeSel];
+        const long long c0 = it.y;
+        const int j0 = (int)(c0 / G.pitch), i0 = (int)(c0 - (long long)j0 * G.pitch);
+        const int reach = G.bc == 1 ? 1 : 0;
+        const int8_t s = B.L.sync[e];
+        for (int b = -reach; b <= reach; b++) {
+            const int jo = j0 + b * G.ny;
+            if (jo < 0 || jo >= G.nyt) continue;
+            for (int t = -reach; t <= reach; t++) {
+                const int io = i0 + t * G.nx;
+                if (io < 0 || io >= G.nxt) continue;
+                sch[(long long)jo * G.pitch + io] = s;
+            }
+        }
+        if (!fromLow) d.detMask[c0] &= (uint8_t)~DM_CASC;
+    }
+}
+
 // End of a MOOD pass (timeStep.f90:86-128 loop test): an instance whose detect
 // lowered nothing leaves the loop.  Single block, one thread per slot.
-__global__ void k_pass_end(Batch B, cudaGraphConditionalHandle h, int set_handle) {
+__global__ void k_pass_end(Batch B, cudaGraphConditionalHandle h, int set_handle, int flip) {
     __shared__ int any;
     if (threadIdx.x == 0) any = 0;
     __syncthreads();
     for (int k = threadIdx.x; k < B.maxInst; k += blockDim.x) {
         InstState& S = B.st[k];
         if (!(S.stepping && S.stageActive)) continue;
-        S.schemeSel = 1 - S.schemeSel;  // k_mood_flags wrote the other buffer
+        if (flip) S.schemeSel = 1 - S.schemeSel;  // k_mood_flags wrote the other buffer
         S.passes++;
         S.passesTotal++;
         S.innerTotal += S.nInner;
@@ -1390,9 +1516,17 @@ void l_flux(const Batch& B, int uin, int mode, cudaStream_t s) { TILE_LAUNCH(k_f
 void l_ct_update_detect(const Batch& B, int uin, int uout, cudaStream_t s) {
     TILE_LAUNCH(k_ct_update_detect, B, s, uin, uout);
 }
-void l_mood_flags(const Batch& B, cudaStream_t s) { TILE_LAUNCH(k_mood_flags, B, s); }
-void l_pass_end(const Batch& B, cudaGraphConditionalHandle h, cudaStream_t s) {
-    k_pass_end<<<1, 128, 0, s>>>(B, h, h != 0);
+void l_mood_flags(const Batch& B, int dense, cudaStream_t s) {
+    if (dense) {
+        TILE_LAUNCH(k_mood_flags, B, s);
+    } else {
+        LIST_LAUNCH(k_flags_clear, B, s);
+        LIST_LAUNCH(k_flags_scatter, B, s);
+        LIST_LAUNCH(k_scheme_sync, B, s);
+    }
+}
+void l_pass_end(const Batch& B, cudaGraphConditionalHandle h, int flip, cudaStream_t s) {
+    k_pass_end<<<1, 128, 0, s>>>(B, h, h != 0, flip);
 }
 void l_compact_rec(const Batch& B, cudaStream_t s) { TILE_LAUNCH(k_compact_rec, B, s); }
 void l_compact_post(const Batch& B, cudaStream_t s) { TILE_LAUNCH(k_compact_post, B, s); }
