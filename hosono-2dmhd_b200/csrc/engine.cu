@@ -252,9 +252,11 @@ size_t Engine::instance_bytes(const hosono_params& p) const {
 
 int Engine::upload_tables() {
     tiles_.clear();
+    radii_ = 0;
     for (int k = 0; k < maxInst_; k++) {
         if (!slots_[k].live) continue;
         const Geo& G = slots_[k].dev.geo;
+        radii_ |= 1 << G.R;
         for (int y = 0; y < G.nyt; y += TILE_Y)
             for (int x = 0; x < G.nxt; x += TILE_X) tiles_.push_back(make_int4(k, x, y, 0));
     }
@@ -262,6 +264,7 @@ int Engine::upload_tables() {
     const int n = (int)tiles_.size();
     if (n) CUE(cudaMemcpyAsync(d_tiles_, tiles_.data(), sizeof(int4) * n, cudaMemcpyHostToDevice, s_));
     CUE(cudaMemcpyAsync(d_ntiles_, &n, sizeof(int), cudaMemcpyHostToDevice, s_));
+    CUE(cudaMemcpyAsync(&d_flags_->radii, &radii_, sizeof(int), cudaMemcpyHostToDevice, s_));
     CUE(cudaStreamSynchronize(s_));
     return HOSONO_OK;
 }
@@ -670,6 +673,7 @@ int Engine::advance(int slot, double dt) {
 int Engine::run(int max_steps) {
     BatchFlags f{};
     f.anyLive = 1;
+    f.radii = radii_;
     f.stepsLeft = max_steps > 0 ? max_steps : INT_MAX;
     CUE(cudaMemcpyAsync(d_flags_, &f, sizeof f, cudaMemcpyHostToDevice, s_));
     if (use_graphs && !trace) {
@@ -692,6 +696,7 @@ int Engine::run(int max_steps) {
 int Engine::run_profiled_step(double* pass1_ms, int* pass1_launches) {
     BatchFlags f{};
     f.anyLive = 1;
+    f.radii = radii_;
     f.stepsLeft = 1;
     CUE(cudaMemcpyAsync(d_flags_, &f, sizeof f, cudaMemcpyHostToDevice, s_));
     TRYE(build_graphs());

@@ -88,6 +88,7 @@ struct BatchFlags {
     int anyLive;     // some instance still stepping (time loop)
     int error;
     int stepsLeft;   // step budget of the current run launch
+    int radii;       // bit R set when a live instance has GP radius R (per-radius kernels of absent radii exit)
 };
 
 // Roles of the three U buffers: the state lives in U[parity]; A in

@@ -118,6 +118,7 @@ class Engine {
     const KernelSet* K_ = nullptr;
     cudaStream_t s_ = nullptr;
     int maxInst_ = 0, maxTiles_ = 0;
+    int radii_ = 0;  // BatchFlags::radii of the committed tile list
     InstDev* d_dev_ = nullptr;
     InstState* d_st_ = nullptr;
     int4* d_tiles_ = nullptr;

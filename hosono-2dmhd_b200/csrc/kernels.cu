@@ -291,6 +291,7 @@ __global__ void __launch_bounds__(NTHREADS, HOSONO_PASS1_MIN_BLOCKS) k_face_pass
     using Box = P1Box<R>;
     const int tid = threadIdx.y * TILE_X + threadIdx.x;
     double* acc = smem + 2 * Box::DOUBLES + tid;
+    if (!(B.flags->radii & (1 << R))) return;  // no instance of this radius
     const int n = __ldg(B.ntiles);
     int t = pass1_next<R>(B, blockIdx.x, n);
     int buf = 0;
