@@ -42,6 +42,8 @@ WORKLOADS = {
     "ot1536_r2": dict(n=1536, radius=2, ell=12.0, desc="Orszag-Tang 1536x1536, GP-MOOD R=2 (5th->3rd->1st), ell/dx=12"),
     "ot1024_r2": dict(n=1024, radius=2, ell=12.0, desc="Orszag-Tang 1024x1024, GP-MOOD R=2 (5th->3rd->1st), ell/dx=12"),
     "ot128_r1": dict(n=128, radius=1, ell=6.0, desc="Orszag-Tang 128x128, GP-MOOD R=1 (3rd->1st), ell/dx=6"),
+    "sedov2048_r2": dict(n=2048, radius=2, ell=6.0, problem="sedov",
+                         desc="Sedov blast 2048x2048, hydro, outflow, GP-MOOD R=2, CFL 0.6, ell/dx=6"),
 }
 
 
@@ -53,7 +55,10 @@ def load_pkg():
 def par_for(workload, d):
     import parfiles
     w = WORKLOADS[workload]
-    kv = parfiles.orszag_tang(w["n"], w["radius"], ell=w["ell"], tmax=0.5, cfl=0.8)
+    if w.get("problem") == "sedov":
+        kv = parfiles.sedov(w["n"], w["radius"], ell=w["ell"], tmax=0.05, cfl=0.6)
+    else:
+        kv = parfiles.orszag_tang(w["n"], w["radius"], ell=w["ell"], tmax=0.5, cfl=0.8)
     return parfiles.make(d, workload, kv)
 
 
@@ -149,8 +154,9 @@ def oracle_build():
     return "-O3 AVX2/FMA contraction" if host_has_avx2_fma() else "-O3 SSE2, no contraction"
 
 
-def run_cpu_baseline(workload, steps, threads, fast=None):
-    """Time the oracle restatement on the host cores: returns (zone-updates/s, seconds).
+def run_cpu_baseline(workload, steps, threads, fast=None, to_end=False):
+    """Time the oracle restatement on the host cores: returns (zone-updates/s,
+    seconds, steps).  to_end: the whole run from the initial state to t_end.
     fast=None picks the AVX2/FMA build when the host supports it."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
@@ -161,16 +167,21 @@ def run_cpu_baseline(workload, steps, threads, fast=None):
     with tempfile.TemporaryDirectory() as d:
         par = par_for(workload, d)
         o = oracle.Oracle(par, fast=fast)
-        dt = o.cfl()
-        o.advance(dt)  # warm-up step (page faults, thread pool)
-        t0 = time.perf_counter()
-        for _ in range(steps):
+        if to_end:
+            t0 = time.perf_counter()
+            rc, _, steps = o.run()
+            el = time.perf_counter() - t0
+        else:
             dt = o.cfl()
-            o.advance(dt)
-        el = time.perf_counter() - t0
+            o.advance(dt)  # warm-up step (page faults, thread pool)
+            t0 = time.perf_counter()
+            for _ in range(steps):
+                dt = o.cfl()
+                o.advance(dt)
+            el = time.perf_counter() - t0
         o.close()
     rate = w["n"] * w["n"] * steps / el
-    return rate, el
+    return rate, el, steps
 
 
 def bench_reference(args, rank):
@@ -181,9 +192,9 @@ def bench_reference(args, rank):
     w = WORKLOADS[args.workload]
     # bounded sample: at most ~120 s of CPU time whatever --steps says
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    rate1, el1 = run_cpu_baseline(args.workload, 1, threads)
+    rate1, el1, _ = run_cpu_baseline(args.workload, 1, threads)
     steps = max(1, min(args.steps, int(120.0 / max(el1, 1e-3))))
-    rate, el = run_cpu_baseline(args.workload, steps, threads) if steps > 1 else (rate1, el1)
+    rate, el, _ = run_cpu_baseline(args.workload, steps, threads) if steps > 1 else (rate1, el1, 1)
     line = {
         "metric": "fp64_zone_updates_per_s", "value": rate, "unit": "zone-updates/s", "n_gpus": args.gpus,
         "steps": steps, "warmup": 1, "ms_per_step": el / steps * 1e3, "higher_is_better": True,
@@ -239,13 +250,20 @@ def bench_ours(args, rank, world, local):
     barrier()
     # timed region: K steps, each one launch of the step graph (cfl, dt,
     # three MOOD stages, RK3) with CUDA events bracketing the pass-1 kernels
-    if not args.eager:  # the pass-1 events live in the profiled step graph
+    if not args.eager and not args.to_end:  # the pass-1 events live in the profiled step graph
         sol.profile(True)
     sol.profile_read(reset=True)
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    t_sim, n_steps = sol.step(args.steps)
+    if args.to_end:  # the whole run from the initial state to t_end
+        sol.upload(U0, V0)
+        sol.set_time(0.0, run.tmax, 0, run.nstepmax)
+        e0.record(stream)
+        t_sim, n_steps = sol.step(0)
+        args.steps = n_steps
+    else:
+        t_sim, n_steps = sol.step(args.steps)
     e1.record(stream)
     e1.synchronize()
     clk = clocks.stop()
@@ -317,12 +335,14 @@ def bench_ours(args, rank, world, local):
         line["batched"] = bench_batched(m, fp, torch, limit=args.batched_limit, eager=args.eager)
     served_kept = {}
     if world == 1 and args.serve_requests > 0:
-        line["served"], served_kept = bench_served(m, fp, args.serve_requests, args.serve_check)
+        line["served"], served_kept = bench_served(m, fp, args.serve_requests, args.serve_check,
+                                                   args.serve_calibrate, args.serve_sample, args.serve_hashes)
     if not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        rate, el = run_cpu_baseline(args.workload, 1, threads)
+        rate, el, nst = run_cpu_baseline(args.workload, 1, threads, to_end=args.to_end)
+        what = f"the whole run to t_end ({nst} steps)" if args.to_end else "1 full RK3 step after 1 warm-up step"
         line["cpu_baseline"] = {"value": rate, "unit": "zone-updates/s", "cores": threads, "kind": "port",
-                                "sample": f"1 full RK3 step of {args.workload} after 1 warm-up step, CPU oracle "
+                                "sample": f"{what} of {args.workload}, CPU oracle "
                                           f"(C++ restatement, OpenMP, {oracle_build()}), {el:.1f} s"}
         if served_kept:
             line["served"]["accuracy"] = cpu_baseline_served_check(served_kept)
@@ -399,36 +419,72 @@ def bench_batched(m, fp, torch, manifest="blast64_seed0.json", limit=None, eager
             "unit": "zone-updates/s"}
 
 
-def bench_served(m, fp, requests, check):
+def bench_served(m, fp, requests, check, calibrate=0, sample=0, hashes_path=None):
     """The served request stream (workloads/served2000_seed1.json, first
-    `requests` requests): first closed loop (all submitted at once) to measure
-    the batched capacity in requests/s, then open loop with the manifest's
+    `requests` requests).  Capacity: the stream's first `calibrate` requests
+    (all of them when 0) run closed loop (all submitted at once); their
+    zone-updates/s divided by the stream's mean work per request -- measured
+    when every request ran, else predicted from the calibration run's step
+    counts (steps ~ k_problem * N * t_end, k fitted per problem) -- gives
+    requests/s.  Then the whole stream runs open loop with the manifest's
     seeded exponential gaps scaled to 80% of that capacity.  Latency is
-    submit -> final state on the host.  Returns the report and the final U of
-    the `check` requests with the least work (for the accuracy check)."""
+    submit -> final state on the host.  Returns the report and the final U
+    of the `check` requests with the least work (accuracy check); with
+    `sample`, the SHA-256 of the final U of `sample` seeded-random requests is
+    written to `hashes_path` for a check against the oracle elsewhere."""
+    import hashlib
     import importlib
+    import numpy as np
     load_pkg()
     srv = importlib.import_module("hosono_2dmhd_b200.serve")
     path = os.path.join(ROOT, "hosono-2dmhd_b200", "workloads", "served2000_seed1.json")
     with open(path) as f:
         entries = json.load(f)["requests"][:requests]
+    cal = entries[:calibrate] if 0 < calibrate < len(entries) else entries
     with srv.Server(fp_mode=fp) as s:
-        closed, _, cinfos = srv.run_stream(entries, 1.0, s, fp_mode=fp, closed=True)
-    cap = len(entries) / closed["makespan_s"]
+        closed, _, cinfos = srv.run_stream(cal, 1.0, s, fp_mode=fp, closed=True)
+    if cal is entries:
+        mean_work = closed["zone_updates"] / len(entries)
+    else:
+        by_id = {e["id"]: e for e in cal}
+        ks = {}
+        for i in cinfos:
+            e = by_id[i["entry"]]
+            ks.setdefault(e["problem"], []).append(i["nstep"] / (e["n"] * e["tmax"]))
+        k = {p: float(np.median(v)) for p, v in ks.items()}
+        kall = float(np.median([x for v in ks.values() for x in v]))
+        mean_work = float(np.mean([e["n"] ** 3 * e["tmax"] * k.get(e["problem"], kall) for e in entries]))
+    cap = closed["zone_updates_per_s"] / mean_work
     rate = 0.8 * cap
     keep = [i["entry"] for i in sorted(cinfos, key=lambda i: i["zone_updates"])[:check]]
+    sampled = []
+    if sample > 0:
+        rng = np.random.Generator(np.random.PCG64(2))
+        sampled = sorted(int(x) for x in rng.choice([e["id"] for e in entries], size=min(sample, len(entries)),
+                                                    replace=False))
     with srv.Server(fp_mode=fp) as s:
-        rep, kept, infos = srv.run_stream(entries, rate, s, keep=keep, fp_mode=fp)
+        rep, kept, infos = srv.run_stream(entries, rate, s, keep=keep + sampled, fp_mode=fp)
     out = {"workload": f"served2000 (seed 1) requests 0..{len(entries) - 1}: Orszag-Tang / Sedov / MHD blast, "
                        f"N log-uniform in [64,1024], R in {{1,2}}, t_end U[0.1,1] x default",
-           "requests": len(entries), "load": 0.8, "capacity_rps": cap,
+           "requests": len(entries), "load": 0.8, "calibration_requests": len(cal), "capacity_rps": cap,
            "closed_loop_zone_updates_per_s": closed["zone_updates_per_s"], "rate_per_s": rate}
-    for k in ("zone_updates", "zone_updates_per_s", "makespan_s", "latency_p50_s", "latency_p99_s", "latency_max_s",
-              "queue_wait_p50_s", "queue_wait_p99_s", "submit_lag_max_s", "peak_resident", "peak_bytes",
-              "budget_bytes", "gpu_busy_frac", "completed", "failed"):
-        out[k] = rep[k]
+    for k_ in ("zone_updates", "zone_updates_per_s", "makespan_s", "latency_p50_s", "latency_p99_s",
+               "latency_max_s", "queue_wait_p50_s", "queue_wait_p99_s", "submit_lag_max_s", "peak_resident",
+               "peak_bytes", "budget_bytes", "gpu_busy_frac", "completed", "failed"):
+        out[k_] = rep[k_]
     out["unit"] = "zone-updates/s"
-    return out, {e["id"]: (e, kept[e["id"]]) for e in entries if e["id"] in kept}
+    if sampled and hashes_path:
+        recs = {}
+        for i in infos:
+            if i["entry"] in sampled:
+                U = kept[i["entry"]]
+                recs[str(i["entry"])] = {"sha256": hashlib.sha256(np.ascontiguousarray(U).tobytes()).hexdigest(),
+                                         "nstep": i["nstep"], "t": i["t"], "zone_updates": i["zone_updates"]}
+        with open(hashes_path, "w") as f:
+            json.dump({"manifest": "served2000_seed1.json", "sample_seed": 2, "fp": "strict" if fp == 0 else "fast",
+                       "requests": recs}, f, indent=1)
+        out["sampled_hashes"] = {"file": os.path.basename(hashes_path), "requests": sampled}
+    return out, {e["id"]: (e, kept[e["id"]]) for e in entries if e["id"] in keep}
 
 
 def cpu_baseline_served_check(kept):
@@ -471,10 +527,17 @@ def main():
                     help="launch kernels one by one instead of as CUDA graphs (the plain and batched legs; for "
                          "profilers, which do not see inside conditional graph nodes)")
     ap.add_argument("--batched-limit", type=int, default=64, help="instances of the batched workload to run")
+    ap.add_argument("--to-end", action="store_true",
+                    help="time the whole run from the initial state to t_end instead of --steps steps")
     ap.add_argument("--serve-requests", type=int, default=20,
                     help="requests of the served stream to run (0: skip the served measurement)")
     ap.add_argument("--serve-check", type=int, default=3,
                     help="served requests (least work first) checked against the CPU oracle")
+    ap.add_argument("--serve-calibrate", type=int, default=0,
+                    help="first requests run closed loop to measure capacity (0: all of them)")
+    ap.add_argument("--serve-sample", type=int, default=0,
+                    help="seeded-random served requests whose final-state SHA-256 is written to --serve-hashes")
+    ap.add_argument("--serve-hashes", default=None, help="output JSON of the sampled hashes")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
