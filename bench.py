@@ -304,6 +304,27 @@ def bench_ours(args, rank, world, local):
            "steps": e2e_steps, "ms_per_step": e2e_ms / e2e_steps}
     sol.close()
 
+    # the same workload in fast arithmetic (FMA contraction; results within
+    # 1e-12 relative L1 of strict after one step), for comparison only
+    other = None
+    if fp == m.FP_STRICT and not args.to_end and world == 1:
+        params.fp_mode = m.FP_FAST
+        solf = m.Solver(params, pv, qw, st)
+        solf.upload(U0, V0)
+        solf.set_time(0.0, run.tmax, 0, run.nstepmax)
+        solf.step(max(args.warmup, 1))
+        sf = torch.cuda.ExternalStream(solf.stream())
+        g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        g0.record(sf)
+        solf.step(args.steps)
+        g1.record(sf)
+        g1.synchronize()
+        fms = g0.elapsed_time(g1)
+        other = {"fp": "fast", "value": zones * args.steps / (fms / 1e3), "ms_per_step": fms / args.steps,
+                 "unit": "zone-updates/s", "note": "FMA contraction allowed; not bit-identical to the oracle"}
+        solf.close()
+        params.fp_mode = fp
+
     if rank != 0:
         if dist is not None:
             dist.destroy_process_group()
@@ -331,12 +352,15 @@ def bench_ours(args, rank, world, local):
                    "l2": "inputs larger than L2 (U alone 270 MB at 2048^2)", "mood_passes": passes},
         "gpu_launches": launches, "clocks": clk, "roofline": roofline, "e2e": e2e,
     }
+    if other:
+        line["fast_fp"] = other
     if world == 1 and not args.no_batched:
         line["batched"] = bench_batched(m, fp, torch, limit=args.batched_limit, eager=args.eager)
     served_kept = {}
     if world == 1 and args.serve_requests > 0:
         line["served"], served_kept = bench_served(m, fp, args.serve_requests, args.serve_check,
-                                                   args.serve_calibrate, args.serve_sample, args.serve_hashes)
+                                                   args.serve_calibrate, args.serve_sample, args.serve_hashes,
+                                                   args.serve_mean_work, args.serve_records)
     if not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         rate, el, nst = run_cpu_baseline(args.workload, 1, threads, to_end=args.to_end)
@@ -419,7 +443,8 @@ def bench_batched(m, fp, torch, manifest="blast64_seed0.json", limit=None, eager
             "unit": "zone-updates/s"}
 
 
-def bench_served(m, fp, requests, check, calibrate=0, sample=0, hashes_path=None):
+def bench_served(m, fp, requests, check, calibrate=0, sample=0, hashes_path=None, mean_work=None,
+                 records_path=None):
     """The served request stream (workloads/served2000_seed1.json, first
     `requests` requests).  Capacity: the stream's first `calibrate` requests
     (all of them when 0) run closed loop (all submitted at once); their
@@ -443,7 +468,9 @@ def bench_served(m, fp, requests, check, calibrate=0, sample=0, hashes_path=None
     cal = entries[:calibrate] if 0 < calibrate < len(entries) else entries
     with srv.Server(fp_mode=fp) as s:
         closed, _, cinfos = srv.run_stream(cal, 1.0, s, fp_mode=fp, closed=True)
-    if cal is entries:
+    if mean_work:  # known from an earlier run of the same requests (results are deterministic)
+        mean_work = float(mean_work)
+    elif cal is entries:
         mean_work = closed["zone_updates"] / len(entries)
     else:
         by_id = {e["id"]: e for e in cal}
@@ -473,6 +500,12 @@ def bench_served(m, fp, requests, check, calibrate=0, sample=0, hashes_path=None
                "peak_bytes", "budget_bytes", "gpu_busy_frac", "completed", "failed"):
         out[k_] = rep[k_]
     out["unit"] = "zone-updates/s"
+    out["mean_work_used"] = mean_work
+    out["mean_work_measured"] = rep["zone_updates"] / max(rep["completed"], 1)
+    if records_path:
+        with open(records_path, "w") as f:
+            json.dump([{k_: i[k_] for k_ in ("entry", "status", "nstep", "zone_updates", "submit_s", "admit_s",
+                                              "finish_s")} for i in infos], f)
     if sampled and hashes_path:
         recs = {}
         for i in infos:
@@ -538,6 +571,10 @@ def main():
     ap.add_argument("--serve-sample", type=int, default=0,
                     help="seeded-random served requests whose final-state SHA-256 is written to --serve-hashes")
     ap.add_argument("--serve-hashes", default=None, help="output JSON of the sampled hashes")
+    ap.add_argument("--serve-mean-work", type=float, default=None,
+                    help="mean zone-updates per request of the stream when known from an earlier run (the "
+                         "results, and so the work, are deterministic); else predicted from the calibration")
+    ap.add_argument("--serve-records", default=None, help="output JSON of per-request work and timestamps")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

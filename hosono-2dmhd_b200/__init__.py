@@ -139,6 +139,8 @@ SIGNATURES = {
     "hosono_batch_set_graphs": [_vp, _i],
     "hosono_batch_last_error": [_vp, _cp, _i],
     "hosono_batch_capacity": [_vp, _ip, _ip, _ip, _ip],
+    "hosono_gpu_diagnostics": [_vp, _dp, _ip, _ip, _dp, _dp],
+    "hosono_batch_diagnostics": [_vp, _i, _dp, _ip, _ip, _dp, _dp],
     "hosono_serve_clock": [],
     "hosono_serve_create": [ctypes.POINTER(ServeConfig), ctypes.POINTER(_vp)],
     "hosono_serve_destroy": [_vp],
@@ -392,6 +394,21 @@ class Solver:
         s = ctypes.c_void_p()
         self._check(self.lib.hosono_gpu_stream(self.h, ctypes.byref(s)), "stream")
         return s.value or 0
+
+    DIAG_FIELDS = ("dens", "velx", "vely", "velz", "pres", "eint", "gama", "ener", "magp", "divb", "magx",
+                   "magy", "magz")
+
+    def diagnostics(self):
+        """output_writeHdf5's fields on the device: ({name: (ny, nx) array},
+        scheme, ordr, mean |div B|, max |div B|)."""
+        nx, ny = self.params.nx, self.params.ny
+        f = np.empty((13, ny, nx))
+        s = np.empty((ny, nx), dtype=np.int32)
+        o = np.empty((ny, nx), dtype=np.int32)
+        l1, li = ctypes.c_double(), ctypes.c_double()
+        self._check(self.lib.hosono_gpu_diagnostics(self.h, _p(f), _p(s, ctypes.c_int), _p(o, ctypes.c_int),
+                                                    ctypes.byref(l1), ctypes.byref(li)), "diagnostics")
+        return dict(zip(self.DIAG_FIELDS, f)), s, o, l1.value, li.value
 
     def profile(self, on=True):
         self._check(self.lib.hosono_gpu_profile(self.h, 1 if on else 0), "profile")

@@ -159,6 +159,8 @@ Engine::~Engine() {
         if (g) cudaGraphExecDestroy(g);
     for (cudaEvent_t ev : profEv_)
         if (ev) cudaEventDestroy(ev);
+    for (void* p : {(void*)d_instTiles_, (void*)d_actRange_, (void*)d_actInfo_})
+        if (p) cudaFree(p);
     for (void* p : {(void*)d_dev_, (void*)d_st_, (void*)d_tiles_, (void*)d_ntiles_, (void*)d_flags_, (void*)staging_,
                     (void*)schemeInt_, (void*)lists_.rec, (void*)lists_.face, (void*)lists_.recF, (void*)lists_.low,
                     (void*)lists_.next, (void*)lists_.casc, (void*)lists_.sync, (void*)lists_.counts})
@@ -177,6 +179,12 @@ int Engine::init(int max_inst, int max_tiles, int fp_mode) {
     CUE(cudaMalloc(&d_dev_, sizeof(InstDev) * maxInst_));
     CUE(cudaMalloc(&d_st_, sizeof(InstState) * maxInst_));
     CUE(cudaMalloc(&d_tiles_, sizeof(int4) * maxTiles_));
+    CUE(cudaMalloc(&d_instTiles_, sizeof(int2) * maxInst_));
+    CUE(cudaMalloc(&d_actRange_, sizeof(int2) * maxInst_));
+    CUE(cudaMalloc(&d_actInfo_, sizeof(int) * 2));
+    CUE(cudaMemsetAsync(d_instTiles_, 0, sizeof(int2) * maxInst_, s_));
+    CUE(cudaMemsetAsync(d_actInfo_, 0, sizeof(int) * 2, s_));
+    instTiles_.assign(maxInst_, make_int2(0, 0));
     CUE(cudaMalloc(&d_ntiles_, sizeof(int)));
     CUE(cudaMalloc(&d_flags_, sizeof(BatchFlags)));
     lists_.cap = (long long)maxTiles_ * TILE_X * TILE_Y;
@@ -214,6 +222,9 @@ Batch Engine::batch() const {
     B.L = lists_;
     B.maxTiles = maxTiles_;
     B.maxInst = maxInst_;
+    B.instTiles = d_instTiles_;
+    B.actRange = d_actRange_;
+    B.actInfo = d_actInfo_;
     return B;
 }
 
@@ -254,17 +265,20 @@ int Engine::upload_tables() {
     tiles_.clear();
     radii_ = 0;
     for (int k = 0; k < maxInst_; k++) {
+        instTiles_[k] = make_int2((int)tiles_.size(), 0);
         if (!slots_[k].live) continue;
         const Geo& G = slots_[k].dev.geo;
         radii_ |= 1 << G.R;
         for (int y = 0; y < G.nyt; y += TILE_Y)
             for (int x = 0; x < G.nxt; x += TILE_X) tiles_.push_back(make_int4(k, x, y, 0));
+        instTiles_[k].y = (int)tiles_.size() - instTiles_[k].x;
     }
     if ((int)tiles_.size() > maxTiles_) return fail(HOSONO_EINVAL, "tile capacity exceeded");
     const int n = (int)tiles_.size();
     if (n) CUE(cudaMemcpyAsync(d_tiles_, tiles_.data(), sizeof(int4) * n, cudaMemcpyHostToDevice, s_));
     CUE(cudaMemcpyAsync(d_ntiles_, &n, sizeof(int), cudaMemcpyHostToDevice, s_));
     CUE(cudaMemcpyAsync(&d_flags_->radii, &radii_, sizeof(int), cudaMemcpyHostToDevice, s_));
+    CUE(cudaMemcpyAsync(d_instTiles_, instTiles_.data(), sizeof(int2) * maxInst_, cudaMemcpyHostToDevice, s_));
     CUE(cudaStreamSynchronize(s_));
     return HOSONO_OK;
 }
@@ -450,6 +464,45 @@ int Engine::upload(int slot, const double* U, const double* V) {
     return HOSONO_OK;
 }
 
+int Engine::diagnostics(int slot, double* fields, int* scheme, int* ordr, double* divb_l1, double* divb_linf) {
+    if (slot < 0 || slot >= maxInst_ || !slots_[slot].live) return fail(HOSONO_EINVAL, "bad diagnostics slot");
+    InstState st;
+    TRYE(state(slot, &st));
+    const Slot& sl = slots_[slot];
+    const Geo& G = sl.dev.geo;
+    const size_t n = (size_t)G.nx * G.ny;
+    char* buf = nullptr;
+    const size_t bytes = n * (13 * sizeof(double) + 2 * sizeof(int)) + (2 * (size_t)G.ny + 2) * sizeof(double);
+    cudaError_t e = cudaMalloc(&buf, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(HOSONO_ENOMEM, "no device memory for the diagnostics: %s", cudaGetErrorString(e));
+    }
+    double* f = (double*)buf;
+    double* rows = f + 13 * n;
+    double* res = rows + 2 * G.ny;
+    int* si = (int*)(res + 2);
+    int* oi = si + n;
+    launch_diagnostics(G, sl.dev.V, sl.dev.scheme[st.schemeSel], f, si, oi, rows, res, s_);
+    launches += 3;
+    double r[2] = {0, 0};
+    int rc = HOSONO_OK;
+    if (cudaGetLastError() != cudaSuccess) rc = fail(HOSONO_ECUDA, "diagnostics launch failed");
+    if (!rc && fields && cudaMemcpyAsync(fields, f, n * 13 * sizeof(double), cudaMemcpyDeviceToHost, s_))
+        rc = fail(HOSONO_ECUDA, "diagnostics copy failed");
+    if (!rc && scheme && cudaMemcpyAsync(scheme, si, n * sizeof(int), cudaMemcpyDeviceToHost, s_))
+        rc = fail(HOSONO_ECUDA, "diagnostics copy failed");
+    if (!rc && ordr && cudaMemcpyAsync(ordr, oi, n * sizeof(int), cudaMemcpyDeviceToHost, s_))
+        rc = fail(HOSONO_ECUDA, "diagnostics copy failed");
+    if (!rc && cudaMemcpyAsync(r, res, sizeof r, cudaMemcpyDeviceToHost, s_)) rc = fail(HOSONO_ECUDA, "copy failed");
+    if (cudaStreamSynchronize(s_) != cudaSuccess && !rc) rc = fail(HOSONO_ECUDA, "diagnostics failed");
+    cudaFree(buf);
+    if (rc) return rc;
+    if (divb_l1) *divb_l1 = r[0] / (double)n;
+    if (divb_linf) *divb_linf = r[1];
+    return HOSONO_OK;
+}
+
 int Engine::download(int slot, double* U, double* V, int* scheme) {
     if (slot < 0 || slot >= maxInst_ || !slots_[slot].live) return fail(HOSONO_EINVAL, "bad download");
     InstState st;
@@ -502,23 +555,22 @@ int Engine::record_stage(Rec& r, int uin, int uout, cudaEvent_t ev0, cudaEvent_t
     const KernelSet* K = K_;
     const long long cap = (long long)INT_MAX;
     TRYE(r.k([&](cudaStream_t s) { K->stage_init(B, s); }));
-    TRYE(r.k([&](cudaStream_t s) { K->detect_prep(B, uin, s); }));
     if (ev0) TRYE(r.event(ev0));
     TRYE(r.k([&](cudaStream_t s) { K->face_pass1(B, uin, s); }));
     if (ev1) TRYE(r.event(ev1));
     cudaGraphConditionalHandle hc1, hm;
     TRYE(r.cond(&hc1, 0));
     TRYE(r.k([&](cudaStream_t s) { K->cascade_cond(B, hc1, s); }));
-    auto cascade_body = [&](cudaGraphConditionalHandle hc) {
-        return [&, hc](Rec& c) -> int {
-            TRYE(c.k([&](cudaStream_t s) { K->cascade_lower(B, 0, s); }));
-            if (!c.graph()) launches++;  // cascade_lower launches two kernels
-            TRYE(c.k([&](cudaStream_t s) { K->recon_check(B, uin, MASK_NEXTPASS, s); }));
+    auto cascade_body = [&](cudaGraphConditionalHandle hc, int later) {
+        return [&, hc, later](Rec& c) -> int {
+            TRYE(c.k([&](cudaStream_t s) { K->cascade_lower(B, later, s); }));
+            TRYE(c.k([&](cudaStream_t s) { K->recon_check(B, uin, later, s); }));
+            if (!c.graph()) launches += 2;  // both launch two kernels
             TRYE(c.k([&](cudaStream_t s) { K->cascade_cond(B, hc, s); }));
             return HOSONO_OK;
         };
     };
-    TRYE(r.loop(hc1, &BatchFlags::anyFail, cap, cascade_body(hc1)));
+    TRYE(r.loop(hc1, &BatchFlags::anyFail, cap, cascade_body(hc1, 0)));
     TRYE(r.k([&](cudaStream_t s) { K->compact_dirty(B, s); }));
     TRYE(r.k([&](cudaStream_t s) { K->flux_list(B, uin, s); }));
     TRYE(r.k([&](cudaStream_t s) { K->ct_update_detect(B, uin, uout, s); }));
@@ -537,11 +589,12 @@ int Engine::record_stage(Rec& r, int uin, int uout, cudaEvent_t ev0, cudaEvent_t
         cudaGraphConditionalHandle hc2;
         TRYE(b.cond(&hc2, 0));
         TRYE(b.k([&](cudaStream_t s) { K->cascade_cond(B, hc2, s); }));
-        TRYE(b.loop(hc2, &BatchFlags::anyFail, cap, cascade_body(hc2)));
+        TRYE(b.loop(hc2, &BatchFlags::anyFail, cap, cascade_body(hc2, 1)));
         TRYE(b.k([&](cudaStream_t s) { K->compact_post(B, s); }));
         TRYE(b.k([&](cudaStream_t s) { K->flux_list(B, uin, s); }));
         TRYE(b.k([&](cudaStream_t s) { K->ct_list(B, uin, uout, s); }));
         TRYE(b.k([&](cudaStream_t s) { K->mood_flags(B, 0, s); }));
+        if (!b.graph()) launches += 2;  // three kernels
         if (trace) TRYE(b.host([&] { return trace_snapshot(); }));
         TRYE(b.k([&](cudaStream_t s) { K->clear_low(B, s); }));
         TRYE(b.k([&](cudaStream_t s) { K->pass_end(B, hm, 0, s); }));

@@ -125,11 +125,15 @@ struct Batch {
     Lists L;
     int maxTiles;        // capacity of the tile list
     int maxInst;         // capacity (slots)
+    const int2* instTiles;  // per slot: first tile in the tile list, tile count (0: not live)
+    // instances still in their MOOD loop after the last pass_end, in slot
+    // order: (slot, first virtual tile); actInfo = {instances, tiles}.  The
+    // dense kernels of the later passes walk only these tiles.
+    int2* actRange;
+    int* actInfo;
 };
 
 enum : int { CASCADE_FROM_FACES = 0, CASCADE_FROM_CELLS = 1 };
-enum : int { FLUX_DIRTY = 0, FLUX_REC = 1 };
-enum : int { MASK_REC = 0, MASK_NEXTPASS = 1 };
 
 // Launchers of one arithmetic build (kernels.cu compiled strict or fast).
 struct KernelSet {
@@ -143,9 +147,9 @@ struct KernelSet {
     void (*stage_init)(const Batch&, cudaStream_t);
     void (*face_pass1)(const Batch&, int uin, cudaStream_t);
     void (*cascade_cond)(const Batch&, cudaGraphConditionalHandle h, cudaStream_t);
-    void (*cascade_lower)(const Batch&, int mode, cudaStream_t);
-    void (*recon_check)(const Batch&, int uin, int mask, cudaStream_t);  // compact nextPass, re-reconstruct
-    void (*flux)(const Batch&, int uin, int mode, cudaStream_t);
+    // later: a later MOOD pass (walk the active instances' tiles only)
+    void (*cascade_lower)(const Batch&, int later, cudaStream_t);
+    void (*recon_check)(const Batch&, int uin, int later, cudaStream_t);  // compact nextPass, re-reconstruct
     void (*ct_update_detect)(const Batch&, int uin, int uout, cudaStream_t);
     // dense: every cell (MOOD pass 1); else from the work lists (later passes)
     void (*mood_flags)(const Batch&, int dense, cudaStream_t);
@@ -156,7 +160,6 @@ struct KernelSet {
     void (*recon_list)(const Batch&, int uin, cudaStream_t);
     void (*compact_post)(const Batch&, cudaStream_t);   // faces and recomputeFLICD cells
     void (*compact_dirty)(const Batch&, cudaStream_t);  // pass-1 faces next to re-reconstructed cells
-    void (*detect_prep)(const Batch&, int uin, cudaStream_t);  // per-stage part of detect_ALL
     void (*flux_list)(const Batch&, int uin, cudaStream_t);
     void (*ct_list)(const Batch&, int uin, int uout, cudaStream_t);
     void (*clear_low)(const Batch&, cudaStream_t);
@@ -174,5 +177,8 @@ const KernelSet* kernelset_fast();
 void launch_aos_to_soa(const Geo& G, const double* aos, double* soa, int nvar, cudaStream_t s);
 void launch_soa_to_aos(const Geo& G, const double* soa, double* aos, int nvar, cudaStream_t s);
 void launch_scheme_to_int(const Geo& G, const int8_t* scheme, int* out, cudaStream_t s);
+// output_writeHdf5's derived fields and div(B) norms (diagnostics.cu)
+void launch_diagnostics(const Geo& G, const double* V, const int8_t* scheme, double* fields, int* schOut,
+                        int* ordr, double* rows, double* res, cudaStream_t s);
 
 }  // namespace hosono

@@ -41,6 +41,9 @@ class Engine {
     void set_allocator(DeviceAllocator* a) { alloc_ = a; }
     int upload(int slot, const double* U, const double* V);
     int download(int slot, double* U, double* V, int* scheme);
+    // output_writeHdf5's fields of the interior (13 double planes + scheme,
+    // ordr; any may be null) and mean / max |div B|; allocates device scratch
+    int diagnostics(int slot, double* fields, int* scheme, int* ordr, double* divb_l1, double* divb_linf);
     int set_time(int slot, double t, double tmax, int nstep, int nstepmax);
     int state(int slot, InstState* out);
     // cfl_computedt of one instance (dt to the host)
@@ -122,6 +125,10 @@ class Engine {
     InstDev* d_dev_ = nullptr;
     InstState* d_st_ = nullptr;
     int4* d_tiles_ = nullptr;
+    int2* d_instTiles_ = nullptr;
+    int2* d_actRange_ = nullptr;
+    int* d_actInfo_ = nullptr;
+    std::vector<int2> instTiles_;
     int* d_ntiles_ = nullptr;
     BatchFlags* d_flags_ = nullptr;
     Lists lists_{};

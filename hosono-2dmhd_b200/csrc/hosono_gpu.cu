@@ -43,11 +43,11 @@ hosono_stats stats_delta(const InstState& a, const InstState& b) {
 }
 
 // kernels one graph execution launched, from the work counters: per step 4
-// time-loop kernels (cfl path) or 1 (host dt), 3 RK kernels; per stage 12
+// time-loop kernels (cfl path) or 1 (host dt), 3 RK kernels; per stage 11
 // (MOOD pass 1, three of them the per-radius face kernels); per cascade
 // iteration 5; per further MOOD pass 11.
 long long graph_launches(const hosono_stats& s, int steps, bool host_dt) {
-    return (long long)steps * ((host_dt ? 1 : 4) + 3) + 12LL * s.stages + 5LL * s.cascade_iters +
+    return (long long)steps * ((host_dt ? 1 : 4) + 3) + 11LL * s.stages + 5LL * s.cascade_iters +
            11LL * (s.mood_passes - s.stages);
 }
 
@@ -339,6 +339,16 @@ int hosono_batch_set_graphs(hosono_batch* b, int on) {
     if (!b) return HOSONO_EINVAL;
     b->eng.use_graphs = on != 0;
     return HOSONO_OK;
+}
+
+int hosono_gpu_diagnostics(hosono_handle* h, double* fields, int* scheme, int* ordr, double* divb_l1,
+                           double* divb_linf) {
+    return h ? h->eng.diagnostics(h->slot, fields, scheme, ordr, divb_l1, divb_linf) : HOSONO_EINVAL;
+}
+
+int hosono_batch_diagnostics(hosono_batch* b, int slot, double* fields, int* scheme, int* ordr, double* divb_l1,
+                             double* divb_linf) {
+    return b ? b->eng.diagnostics(slot, fields, scheme, ordr, divb_l1, divb_linf) : HOSONO_EINVAL;
 }
 
 int hosono_batch_last_error(hosono_batch* b, char* buf, int len) {

@@ -43,7 +43,7 @@ namespace KNS {
 
 constexpr int NTHREADS = TILE_X * TILE_Y;
 
-// detMask bits: the per-stage detect_ALL terms (written by k_detect_prep),
+// detMask bits: the per-stage detect_ALL terms (written by k_ct_update_detect),
 // and DM_CASC, set while a cell sits on the cascade-lowered list of the
 // current MOOD pass
 enum : int { DM_SHOCK = 1, DM_PLATEAU = 2, DM_SMOOTH = 4, DM_CASC = 8 };
@@ -65,6 +65,30 @@ __device__ __forceinline__ Cell tile_at(const Batch& B, int t) {
 // Kernels walk the tile list grid-stride: the grid is sized to the GPU, the
 // tile count is read from device memory at run time.
 #define FOR_TILES(B, t) for (int t = blockIdx.x, n_ = __ldg((B).ntiles); t < n_; t += gridDim.x)
+
+// Tile of virtual index v in the active instances' tiles (binary search over
+// the ranges pass_end left); uniform over a block.
+__device__ __forceinline__ int active_tile(const Batch& B, int v) {
+    int lo = 0, hi = B.actInfo[0] - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (B.actRange[mid].y <= v)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    const int2 r = B.actRange[lo];
+    return B.instTiles[r.x].x + (v - r.y);
+}
+// Later MOOD passes: only the tiles of instances still in their MOOD loop.
+#define FOR_ACTIVE_TILES(B, t)                                                              \
+    for (int v_ = blockIdx.x, nv_ = (B).actInfo[1], t = 0; v_ < nv_; v_ += gridDim.x)      \
+        for (bool once_ = (t = active_tile((B), v_), true); once_; once_ = false)
+// dense (pass 1) or active tiles (later passes), chosen at compile time
+#define FOR_SOME_TILES(ACT, B, t)                                                                        \
+    for (int v_ = blockIdx.x, nv_ = (ACT) ? (B).actInfo[1] : __ldg((B).ntiles), t = 0; v_ < nv_;         \
+         v_ += gridDim.x)                                                                                 \
+        for (bool once_ = (t = (ACT) ? active_tile((B), v_) : v_, true); once_; once_ = false)
 
 // the one thread per instance that owns cell (0,0) (every instance has a tile at its origin)
 __device__ __forceinline__ bool first_tile_thread(const Cell& c) { return c.i == 0 && c.j == 0; }
@@ -158,7 +182,7 @@ __device__ __forceinline__ int2 entry(int k, long long cc) { return make_int2(k,
 // quadrature point and never stored.  A cell fails when any of its four
 // faces fails; the verdicts are kept per face side in failX / failY and
 // combined by cascade_lower.  Fluxes next to a cell the cascade
-// re-reconstructs are recomputed after it (flux, FLUX_DIRTY).
+// re-reconstructs are recomputed after it (compact_dirty + flux_list).
 //
 // The block stages its tile's stencil box -- x in [x0-4, x0+36), y in
 // [y0-1-R, y0+9+R), all 8 planes -- in shared memory (16-byte vector loads,
@@ -373,8 +397,9 @@ __device__ __forceinline__ void t_clear_nextpass(const Batch& B, const Cell c) {
     const InstDev& d = B.dev[c.k];
     if (c.i < d.geo.nxt && c.j < d.geo.nyt) d.nextPass[(long long)c.j * d.geo.pitch + c.i] = 0;
 }
+template <bool ACT>
 __global__ void __launch_bounds__(NTHREADS) k_clear_nextpass(Batch B) {
-    FOR_TILES(B, t) t_clear_nextpass(B, tile_at(B, t));
+    FOR_SOME_TILES(ACT, B, t) t_clear_nextpass(B, tile_at(B, t));
 }
 
 // gridBlock_lowerOrder (gridBlock.f90:194-235) of cell (i,j) plus the mark of
@@ -433,8 +458,9 @@ __device__ __forceinline__ void t_cascade_lower(const Batch& B, const Cell c) {
     if (first) d.detMask[cc] |= DM_CASC;
     warp_append(B.L, LIST_CASC, B.L.casc, B.L.cap, first, entry(c.k, cc));
 }
+template <bool ACT>
 __global__ void __launch_bounds__(NTHREADS) k_cascade_lower(Batch B) {
-    FOR_TILES(B, t) t_cascade_lower(B, tile_at(B, t));
+    FOR_SOME_TILES(ACT, B, t) t_cascade_lower(B, tile_at(B, t));
 }
 
 
@@ -505,8 +531,9 @@ __device__ __forceinline__ void t_compact_next(const Batch& B, const Cell c) {
     }
     warp_append(B.L, LIST_NEXT, B.L.next, B.L.cap, p, entry(c.k, cc));
 }
+template <bool ACT>
 __global__ void __launch_bounds__(NTHREADS) k_compact_next(Batch B) {
-    FOR_TILES(B, t) t_compact_next(B, tile_at(B, t));
+    FOR_SOME_TILES(ACT, B, t) t_compact_next(B, tile_at(B, t));
 }
 // ... and re-reconstruct them (list `which`: LIST_NEXT in the cascade,
 // LIST_REC at the start of a later MOOD pass)
@@ -540,7 +567,7 @@ __device__ __forceinline__ void t_compact_rec(const Batch& B, const Cell c) {
     warp_append(B.L, LIST_REC, B.L.rec, B.L.cap, p, entry(c.k, cc));
 }
 __global__ void __launch_bounds__(NTHREADS) k_compact_rec(Batch B) {
-    FOR_TILES(B, t) t_compact_rec(B, tile_at(B, t));
+    FOR_ACTIVE_TILES(B, t) t_compact_rec(B, tile_at(B, t));
 }
 
 // After the face cascade of a later MOOD pass: the faces getFluxes_ recomputes
@@ -567,7 +594,7 @@ __device__ __forceinline__ void t_compact_post(const Batch& B, const Cell c) {
     warp_append(B.L, LIST_RECF, B.L.recF, B.L.cap, pf, entry(c.k, cc));
 }
 __global__ void __launch_bounds__(NTHREADS) k_compact_post(Batch B) {
-    FOR_TILES(B, t) t_compact_post(B, tile_at(B, t));
+    FOR_ACTIVE_TILES(B, t) t_compact_post(B, tile_at(B, t));
 }
 
 // Pass 1 after a face cascade: the faces next to a re-reconstructed cell
@@ -604,98 +631,6 @@ __global__ void __launch_bounds__(NTHREADS) k_compact_dirty(Batch B) {
 // getFluxes_ (getFluxes.f90:16-90) on flagged faces.  Face values are rebuilt
 // from U at the radius each side was last reconstructed with (rrRec); the
 // quadrature uses the face's current radius (riemannSolver.f90:23-47).
-__device__ __forceinline__ void face_flux(const InstDev& d, const double* __restrict__ U, int dir, int iL, int jL,
-                                          int fL, int rrL, int iR, int jR, int fR, int rrR, int rr,
-                                          double flux[NCONS]) {
-    double uL[NCONS], uR[NCONS];
-    if (rr == 0) {
-        face_value(d, U, rrL, iL, jL, fL, 0, uL);
-        face_value(d, U, rrR, iR, jR, fR, 0, uR);
-        hllc(d.phys, uL, uR, dir, flux);
-        return;
-    }
-#pragma unroll
-    for (int v = 0; v < NCONS; v++) flux[v] = 0.0;
-#pragma unroll 1
-    for (int q = 0; q <= rr; q++) {
-        face_value(d, U, rrL, iL, jL, fL, q, uL);
-        face_value(d, U, rrR, iR, jR, fR, q, uR);
-        double F[NCONS];
-        hllc(d.phys, uL, uR, dir, F);
-        const double w = qw_at(d, rr, q);
-#pragma unroll
-        for (int v = 0; v < NCONS; v++) flux[v] = flux[v] + w * F[v];
-    }
-}
-
-__device__ __forceinline__ void t_flux(const Batch& B, int uin, int mode, const Cell c) {
-    const InstState& S = B.st[c.k];
-    if (!(S.stepping && S.stageActive)) return;
-    if (mode == FLUX_DIRTY && !S.cascaded) return;
-    const InstDev& d = B.dev[c.k];
-    const Geo& G = d.geo;
-    const int g = G.g;
-    const int i = c.i, j = c.j;
-    if (i < g - 1 || j < g - 1 || i > g + G.nx + 1 || j > g + G.ny + 1) return;
-    const long long cc = (long long)j * G.pitch + i;
-    const long long cw = cc - 1, cs = cc - G.pitch;
-    const bool doX = mode == FLUX_DIRTY ? (d.dirty[cc] | d.dirty[cw]) != 0 : (d.rec[cc] | d.rec[cw]) != 0;
-    const bool doY = mode == FLUX_DIRTY ? (d.dirty[cc] | d.dirty[cs]) != 0 : (d.rec[cc] | d.rec[cs]) != 0;
-    if (!doX && !doY) return;
-    const double* U = role_ptr(d, S.parity, uin);
-    const int8_t* sch = d.scheme[S.schemeSel];
-    if (doX) {
-        const int rr = min((int)sch[cc], (int)sch[cw]);
-        const int rrL = (d.rrRec[cw] >> (2 * EAST)) & 3;
-        const int rrR = (d.rrRec[cc] >> (2 * WEST)) & 3;
-        double F[NCONS];
-        face_flux(d, U, XDIR, i - 1, j, EAST, rrL, i, j, WEST, rrR, rr, F);
-#pragma unroll
-        for (int v = 0; v < NCONS; v++) d.FX[v * G.plane + cc] = F[v];
-        d.CTX[cc] = F[MAGY];
-    }
-    if (doY) {
-        const int rr = min((int)sch[cc], (int)sch[cs]);
-        const int rrL = (d.rrRec[cs] >> (2 * NORTH)) & 3;
-        const int rrR = (d.rrRec[cc] >> (2 * SOUTH)) & 3;
-        double F[NCONS];
-        face_flux(d, U, YDIR, i, j - 1, NORTH, rrL, i, j, SOUTH, rrR, rr, F);
-#pragma unroll
-        for (int v = 0; v < NCONS; v++) d.FY[v * G.plane + cc] = F[v];
-        d.CTY[cc] = F[MAGX];
-    }
-}
-__global__ void __launch_bounds__(NTHREADS) k_flux(Batch B, int uin, int mode) {
-    FOR_TILES(B, t) t_flux(B, uin, mode, tile_at(B, t));
-}
-
-// getFluxes_ on the face list of a later MOOD pass
-__device__ __forceinline__ void flux_face(const InstDev& d, const InstState& S, int uin, long long cc, int dir) {
-    const Geo& G = d.geo;
-    const int j = (int)(cc / G.pitch), i = (int)(cc - (long long)j * G.pitch);
-    const double* U = role_ptr(d, S.parity, uin);
-    const int8_t* sch = d.scheme[S.schemeSel];
-    double F[NCONS];
-    if (dir == XDIR) {
-        const long long cw = cc - 1;
-        const int rr = min((int)sch[cc], (int)sch[cw]);
-        const int rrL = (d.rrRec[cw] >> (2 * EAST)) & 3;
-        const int rrR = (d.rrRec[cc] >> (2 * WEST)) & 3;
-        face_flux(d, U, XDIR, i - 1, j, EAST, rrL, i, j, WEST, rrR, rr, F);
-#pragma unroll
-        for (int v = 0; v < NCONS; v++) d.FX[v * G.plane + cc] = F[v];
-        d.CTX[cc] = F[MAGY];
-    } else {
-        const long long cs = cc - G.pitch;
-        const int rr = min((int)sch[cc], (int)sch[cs]);
-        const int rrL = (d.rrRec[cs] >> (2 * NORTH)) & 3;
-        const int rrR = (d.rrRec[cc] >> (2 * SOUTH)) & 3;
-        face_flux(d, U, YDIR, i, j - 1, NORTH, rrL, i, j, SOUTH, rrR, rr, F);
-#pragma unroll
-        for (int v = 0; v < NCONS; v++) d.FY[v * G.plane + cc] = F[v];
-        d.CTY[cc] = F[MAGX];
-    }
-}
 // getFluxes_ on the face list of a later MOOD pass, 4 lanes per face: lane q
 // takes quadrature point q (both face values and the Riemann solve); the
 // group's first lane sums w_q * F_q in quadrature order, as
@@ -778,7 +713,7 @@ __device__ __forceinline__ double flicd_y(const InstDev& d, long long c) {
 
 // detect_ALL (detect.f90:84-213).  Everything but CAD, PAD and the DMP reads
 // only the stage input U, so it is the same in every MOOD pass of a stage:
-// k_detect_prep evaluates it once per stage into detMask --
+// the pass-1 update kernel evaluates it once per stage into detMask --
 //   bit 0: shock1 && shock2 && shock3 (:115-146), bit 1: plateau (:161),
 //   bit 2: u2 smoothness accepts (:177-213, option 3) --
 // and the per-pass test keeps the reference's order of decisions.
@@ -802,12 +737,13 @@ __device__ __forceinline__ bool detect_cell(const InstDev& d, const double* __re
     return !(m & DM_SMOOTH);
 }
 
-// Per-stage part of detect_ALL on the interior.  The primitive variables of
-// the tile and a one-cell halo are computed once into shared memory.
+// Per-stage part of detect_ALL on the interior, evaluated once per stage by
+// the pass-1 update kernel (it reads only the stage input U).  The primitive
+// variables of the tile and a one-cell halo are computed once into shared
+// memory.  Called by every thread of the block (it synchronises).
 constexpr int DP_SX = TILE_X + 2, DP_SY = TILE_Y + 2;
-__device__ __forceinline__ void t_detect_prep(const Batch& B, int uin, const Cell c, double* sV) {
-    const InstState& S = B.st[c.k];
-    if (!S.stepping) return;
+__device__ __forceinline__ void detect_prep_tile(const Batch& B, const InstState& S, int uin, const Cell c,
+                                                 double* sV) {
     const InstDev& d = B.dev[c.k];
     const Geo& G = d.geo;
     const Phys& P = d.phys;
@@ -837,7 +773,7 @@ __device__ __forceinline__ void t_detect_prep(const Batch& B, int uin, const Cel
     }
     __syncthreads();
     const int g = G.g;
-    if (!(c.i >= g && c.j >= g && c.i < g + G.nx && c.j < g + G.ny)) return;
+    if (!(c.i >= g && c.j >= g && c.i < g + G.nx && c.j < g + G.ny)) return;  // no barrier follows
     const int e = (threadIdx.y + 1) * DP_SX + threadIdx.x + 1;
     const double* svx = sV;
     const double* svy = sV + DP_SX * DP_SY;
@@ -896,11 +832,7 @@ __device__ __forceinline__ void t_detect_prep(const Batch& B, int uin, const Cel
         const bool sy3 = (fmin(fabs(mny), fabs(mxy)) >= 0.5 * fmax(fabs(mny), fabs(mxy)));
         if ((sx1 && sx2 && sy1 && sy2) || (sx1 && sx3 && sy1 && sy3)) m |= DM_SMOOTH;
     }
-    d.detMask[cc] = (uint8_t)m;
-}
-__global__ void __launch_bounds__(NTHREADS) k_detect_prep(Batch B, int uin) {
-    __shared__ double sV[4 * DP_SX * DP_SY];
-    FOR_TILES(B, t) t_detect_prep(B, uin, tile_at(B, t), sV);
+    d.detMask[cc] = (uint8_t)(m | (d.detMask[cc] & DM_CASC));
 }
 
 // FLICD on [g, g+n]^2 where recomputeFLICD; then, on the interior, the
@@ -955,9 +887,10 @@ __device__ __forceinline__ bool ct_cell(const InstDev& d, const InstState& S, in
     return low;
 }
 
-__device__ __forceinline__ void t_ct_update_detect(const Batch& B, int uin, int uout, const Cell c) {
+__device__ __forceinline__ void t_ct_update_detect(const Batch& B, int uin, int uout, const Cell c, double* sV) {
     InstState& S = B.st[c.k];
-    if (!(S.stepping && S.stageActive)) return;
+    if (!(S.stepping && S.stageActive)) return;  // uniform over the block
+    detect_prep_tile(B, S, uin, c, sV);
     const InstDev& d = B.dev[c.k];
     const Geo& G = d.geo;
     const int g = G.g;
@@ -971,7 +904,8 @@ __device__ __forceinline__ void t_ct_update_detect(const Batch& B, int uin, int 
     warp_append(B.L, LIST_LOW, B.L.low, B.L.cap, low, entry(c.k, cc));
 }
 __global__ void __launch_bounds__(NTHREADS) k_ct_update_detect(Batch B, int uin, int uout) {
-    FOR_TILES(B, t) t_ct_update_detect(B, uin, uout, tile_at(B, t));
+    __shared__ double sV[4 * DP_SX * DP_SY];
+    FOR_TILES(B, t) t_ct_update_detect(B, uin, uout, tile_at(B, t), sV);
 }
 
 // the same on the recomputeFLICD list of a later MOOD pass
@@ -1170,8 +1104,10 @@ __global__ void __launch_bounds__(256) k_scheme_sync(Batch B) {
 
 // End of a MOOD pass (timeStep.f90:86-128 loop test): an instance whose detect
 // lowered nothing leaves the loop.  Single block, one thread per slot.
-__global__ void k_pass_end(Batch B, cudaGraphConditionalHandle h, int set_handle, int flip) {
+constexpr int PASS_END_THREADS = 128;
+__global__ void __launch_bounds__(PASS_END_THREADS) k_pass_end(Batch B, cudaGraphConditionalHandle h, int set_handle, int flip) {
     __shared__ int any;
+    __shared__ int sCnt[PASS_END_THREADS], sTil[PASS_END_THREADS];
     if (threadIdx.x == 0) any = 0;
     __syncthreads();
     for (int k = threadIdx.x; k < B.maxInst; k += blockDim.x) {
@@ -1200,6 +1136,38 @@ __global__ void k_pass_end(Batch B, cudaGraphConditionalHandle h, int set_handle
         S.cascaded = 0;
     }
     __syncthreads();
+    // the instances still in their MOOD loop and their tiles, for the dense
+    // kernels of the next pass: per-thread chunks of slots, block scan of
+    // (instances, tiles), then each thread writes its chunk in slot order
+    const int tid = threadIdx.x;
+    const int per = (B.maxInst + PASS_END_THREADS - 1) / PASS_END_THREADS;
+    const int k0 = min(B.maxInst, tid * per), k1 = min(B.maxInst, k0 + per);
+    int cnt = 0, til = 0;
+    for (int k = k0; k < k1; k++)
+        if (B.st[k].stepping && B.st[k].stageActive) {
+            cnt++;
+            til += B.instTiles[k].y;
+        }
+    sCnt[tid] = cnt;
+    sTil[tid] = til;
+    __syncthreads();
+    for (int off = 1; off < PASS_END_THREADS; off <<= 1) {
+        const int a = tid >= off ? sCnt[tid - off] : 0, b = tid >= off ? sTil[tid - off] : 0;
+        __syncthreads();
+        sCnt[tid] += a;
+        sTil[tid] += b;
+        __syncthreads();
+    }
+    int c0 = sCnt[tid] - cnt, t0 = sTil[tid] - til;
+    for (int k = k0; k < k1; k++)
+        if (B.st[k].stepping && B.st[k].stageActive) {
+            B.actRange[c0++] = make_int2(k, t0);
+            t0 += B.instTiles[k].y;
+        }
+    if (tid == PASS_END_THREADS - 1) {
+        B.actInfo[0] = sCnt[tid];
+        B.actInfo[1] = sTil[tid];
+    }
     if (threadIdx.x == 0) {
         B.flags->anyActive = any;
         if (B.L.counts[LIST_OVERFLOW]) B.flags->error = HOSONO_EINVAL;
@@ -1505,15 +1473,22 @@ void l_face_pass1(const Batch& B, int uin, cudaStream_t s) {
 void l_cascade_cond(const Batch& B, cudaGraphConditionalHandle h, cudaStream_t s) {
     k_cascade_cond<<<1, 128, 0, s>>>(B, h, h != 0);
 }
-void l_cascade_lower(const Batch& B, int /*mode: per instance*/, cudaStream_t s) {
-    TILE_LAUNCH(k_clear_nextpass, B, s);
-    TILE_LAUNCH(k_cascade_lower, B, s);
+void l_cascade_lower(const Batch& B, int later, cudaStream_t s) {
+    if (later) {
+        TILE_LAUNCH(k_clear_nextpass<true>, B, s);
+        TILE_LAUNCH(k_cascade_lower<true>, B, s);
+    } else {
+        TILE_LAUNCH(k_clear_nextpass<false>, B, s);
+        TILE_LAUNCH(k_cascade_lower<false>, B, s);
+    }
 }
-void l_recon_check(const Batch& B, int uin, int /*mask*/, cudaStream_t s) {
-    TILE_LAUNCH(k_compact_next, B, s);
+void l_recon_check(const Batch& B, int uin, int later, cudaStream_t s) {
+    if (later)
+        TILE_LAUNCH(k_compact_next<true>, B, s);
+    else
+        TILE_LAUNCH(k_compact_next<false>, B, s);
     LIST_LAUNCH(k_recon_group, B, s, uin, (int)LIST_NEXT);
 }
-void l_flux(const Batch& B, int uin, int mode, cudaStream_t s) { TILE_LAUNCH(k_flux, B, s, uin, mode); }
 void l_ct_update_detect(const Batch& B, int uin, int uout, cudaStream_t s) {
     TILE_LAUNCH(k_ct_update_detect, B, s, uin, uout);
 }
@@ -1527,12 +1502,11 @@ void l_mood_flags(const Batch& B, int dense, cudaStream_t s) {
     }
 }
 void l_pass_end(const Batch& B, cudaGraphConditionalHandle h, int flip, cudaStream_t s) {
-    k_pass_end<<<1, 128, 0, s>>>(B, h, h != 0, flip);
+    k_pass_end<<<1, PASS_END_THREADS, 0, s>>>(B, h, h != 0, flip);
 }
 void l_compact_rec(const Batch& B, cudaStream_t s) { TILE_LAUNCH(k_compact_rec, B, s); }
 void l_compact_post(const Batch& B, cudaStream_t s) { TILE_LAUNCH(k_compact_post, B, s); }
 void l_compact_dirty(const Batch& B, cudaStream_t s) { TILE_LAUNCH(k_compact_dirty, B, s); }
-void l_detect_prep(const Batch& B, int uin, cudaStream_t s) { TILE_LAUNCH(k_detect_prep, B, s, uin); }
 void l_recon_list(const Batch& B, int uin, cudaStream_t s) { LIST_LAUNCH(k_recon_group, B, s, uin, (int)LIST_REC); }
 void l_flux_list(const Batch& B, int uin, cudaStream_t s) { LIST_LAUNCH(k_flux_list, B, s, uin); }
 void l_ct_list(const Batch& B, int uin, int uout, cudaStream_t s) { LIST_LAUNCH(k_ct_list, B, s, uin, uout); }
@@ -1549,8 +1523,8 @@ const KernelSet kset = {
     "strict",
 #endif
     l_cfl_reduce, l_step_prepare, l_step_begin, l_step_end, l_stage_init, l_face_pass1, l_cascade_cond, l_cascade_lower,
-    l_recon_check, l_flux, l_ct_update_detect, l_mood_flags, l_pass_end, l_compact_rec, l_recon_list,
-    l_compact_post, l_compact_dirty, l_detect_prep, l_flux_list, l_ct_list, l_clear_low, l_bc_fill, l_rk_combine2, l_rk_final,
+    l_recon_check, l_ct_update_detect, l_mood_flags, l_pass_end, l_compact_rec, l_recon_list,
+    l_compact_post, l_compact_dirty, l_flux_list, l_ct_list, l_clear_low, l_bc_fill, l_rk_combine2, l_rk_final,
     l_cons2prim_all};
 
 }  // namespace KNS

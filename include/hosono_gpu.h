@@ -241,6 +241,18 @@ int hosono_batch_capacity(hosono_batch* b, int* max_instances, int* max_tiles, i
 int hosono_cfl_noalloc(const double* V_dev, int nx, int ny, int ngc, int pitch, long long plane, double dx, double dy,
                        double cfl, int force_hydro, double* dt_dev, void* stream);
 
+/* The derived fields output_writeHdf5 writes (src/output.f90:230-274),
+ * computed on the device from the resident state for the interior cells, in
+ * the HDF5 datasets' order (nx*ny, x fastest): `fields` holds 13 planes --
+ * dens velx vely velz pres eint gama ener magp divb magx magy magz --, and
+ * `scheme`, `ordr` (= 2*scheme+1) one int plane each; any of them may be
+ * NULL.  divb_l1 = mean |div B| and divb_linf = max |div B| over the interior
+ * (same bits on every call).  Allocates and frees device scratch. */
+int hosono_gpu_diagnostics(hosono_handle* h, double* fields, int* scheme, int* ordr, double* divb_l1,
+                           double* divb_linf);
+int hosono_batch_diagnostics(hosono_batch* b, int slot, double* fields, int* scheme, int* ordr, double* divb_l1,
+                             double* divb_linf);
+
 /* Kernel timing: when on, CUDA events bracket every launch of the MOOD
  * pass-1 kernel; times[0] = summed milliseconds, counts[0] = launches since
  * the last reset.  launches = kernels launched by this handle since reset. */
