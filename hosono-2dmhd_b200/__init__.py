@@ -442,6 +442,7 @@ class Batch:
             raise HosonoError(rc, "hosono_batch_create")
         self.h = h
         self.shapes = {}
+        self.ngcs = {}
         self._keep = {}
 
     @staticmethod
@@ -478,6 +479,7 @@ class Batch:
                                               ctypes.byref(slot)), "add")
         k = slot.value
         self.shapes[k] = (params.ny + 2 * params.ngc, params.nx + 2 * params.ngc)
+        self.ngcs[k] = params.ngc
         return k
 
     def add_par(self, parfile, fp_mode=None):
@@ -510,6 +512,20 @@ class Batch:
         self._check(self.lib.hosono_batch_download(self.h, int(slot), _p(U), _p(V), _p(S, ctypes.c_int)),
                     "download")
         return U, V, S
+
+    def diagnostics(self, slot):
+        """Solver.diagnostics for one instance of the batch."""
+        nyt, nxt = self.shapes[slot]
+        ngc = self.ngcs[slot]
+        nx, ny = nxt - 2 * ngc, nyt - 2 * ngc
+        f = np.empty((13, ny, nx))
+        s = np.empty((ny, nx), dtype=np.int32)
+        o = np.empty((ny, nx), dtype=np.int32)
+        l1, li = ctypes.c_double(), ctypes.c_double()
+        self._check(self.lib.hosono_batch_diagnostics(self.h, int(slot), _p(f), _p(s, ctypes.c_int),
+                                                      _p(o, ctypes.c_int), ctypes.byref(l1), ctypes.byref(li)),
+                    "diagnostics")
+        return dict(zip(Solver.DIAG_FIELDS, f)), s, o, l1.value, li.value
 
     def set_time(self, slot, t, tmax, nstep=0, nstepmax=1 << 30):
         self._check(self.lib.hosono_batch_set_time(self.h, int(slot), float(t), float(tmax), int(nstep),

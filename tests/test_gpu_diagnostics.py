@@ -61,3 +61,28 @@ def test_divb_at_t_end_matches_oracle(tmp_par_dir):
     np.testing.assert_array_equal(f["divb"], ref)
     assert linf == np.abs(ref).max()
     s.close()
+
+
+@pytest.mark.gpu
+def test_batch_diagnostics_equal_plain(tmp_par_dir):
+    m = pkg.load()
+    pars = [parfiles.make(tmp_par_dir, "b0", parfiles.orszag_tang(36, 2)),
+            parfiles.make(tmp_par_dir, "b1", parfiles.blast(40, 1, p_ratio=100.0, theta=0.3))]
+    tiles = sum(m.Batch.tiles_for(m.par_load(p)[0]) for p in pars)
+    b = m.Batch(2, tiles, fp_mode=m.FP_STRICT)
+    slots = [b.add_par(p) for p in pars]
+    for k in slots:
+        b.set_time(k, 0.0, 1e30)
+    b.run(max_steps=3)
+    for k, par in zip(slots, pars):
+        s = m.Solver.from_par(par, fp_mode=m.FP_STRICT)
+        s.set_time(0.0, 1e30)
+        s.step(3)
+        fb, sb, ob, l1b, lib_ = b.diagnostics(k)
+        fs, ss, os_, l1s, lis = s.diagnostics()
+        for name in fs:
+            np.testing.assert_array_equal(fb[name], fs[name], err_msg=name)
+        np.testing.assert_array_equal(sb, ss)
+        assert (l1b, lib_) == (l1s, lis)
+        s.close()
+    b.close()
