@@ -159,7 +159,8 @@ Engine::~Engine() {
         if (g) cudaGraphExecDestroy(g);
     for (cudaEvent_t ev : profEv_)
         if (ev) cudaEventDestroy(ev);
-    for (void* p : {(void*)d_instTiles_, (void*)d_actRange_, (void*)d_actInfo_})
+    for (void* p : {(void*)d_instTiles_, (void*)d_actRange_, (void*)d_actInfo_, (void*)d_casRange_,
+                    (void*)d_casInfo_})
         if (p) cudaFree(p);
     for (void* p : {(void*)d_dev_, (void*)d_st_, (void*)d_tiles_, (void*)d_ntiles_, (void*)d_flags_, (void*)staging_,
                     (void*)schemeInt_, (void*)lists_.rec, (void*)lists_.face, (void*)lists_.recF, (void*)lists_.low,
@@ -182,6 +183,9 @@ int Engine::init(int max_inst, int max_tiles, int fp_mode) {
     CUE(cudaMalloc(&d_instTiles_, sizeof(int2) * maxInst_));
     CUE(cudaMalloc(&d_actRange_, sizeof(int2) * maxInst_));
     CUE(cudaMalloc(&d_actInfo_, sizeof(int) * 2));
+    CUE(cudaMalloc(&d_casRange_, sizeof(int2) * maxInst_));
+    CUE(cudaMalloc(&d_casInfo_, sizeof(int) * 2));
+    CUE(cudaMemsetAsync(d_casInfo_, 0, sizeof(int) * 2, s_));
     CUE(cudaMemsetAsync(d_instTiles_, 0, sizeof(int2) * maxInst_, s_));
     CUE(cudaMemsetAsync(d_actInfo_, 0, sizeof(int) * 2, s_));
     instTiles_.assign(maxInst_, make_int2(0, 0));
@@ -225,6 +229,8 @@ Batch Engine::batch() const {
     B.instTiles = d_instTiles_;
     B.actRange = d_actRange_;
     B.actInfo = d_actInfo_;
+    B.casRange = d_casRange_;
+    B.casInfo = d_casInfo_;
     return B;
 }
 

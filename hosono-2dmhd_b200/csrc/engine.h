@@ -131,6 +131,10 @@ struct Batch {
     // dense kernels of the later passes walk only these tiles.
     int2* actRange;
     int* actInfo;
+    // the same for the instances in the current face-cascade iteration
+    // (built by cascade_cond; the cascade kernels walk only these tiles)
+    int2* casRange;
+    int* casInfo;
 };
 
 enum : int { CASCADE_FROM_FACES = 0, CASCADE_FROM_CELLS = 1 };
@@ -147,7 +151,8 @@ struct KernelSet {
     void (*stage_init)(const Batch&, cudaStream_t);
     void (*face_pass1)(const Batch&, int uin, cudaStream_t);
     void (*cascade_cond)(const Batch&, cudaGraphConditionalHandle h, cudaStream_t);
-    // later: a later MOOD pass (walk the active instances' tiles only)
+    // face cascade: the kernels walk the tiles of the instances in the
+    // current iteration (Batch::casRange); `later` marks a later MOOD pass
     void (*cascade_lower)(const Batch&, int later, cudaStream_t);
     void (*recon_check)(const Batch&, int uin, int later, cudaStream_t);  // compact nextPass, re-reconstruct
     void (*ct_update_detect)(const Batch&, int uin, int uout, cudaStream_t);

@@ -128,6 +128,8 @@ class Engine {
     int2* d_instTiles_ = nullptr;
     int2* d_actRange_ = nullptr;
     int* d_actInfo_ = nullptr;
+    int2* d_casRange_ = nullptr;
+    int* d_casInfo_ = nullptr;
     std::vector<int2> instTiles_;
     int* d_ntiles_ = nullptr;
     BatchFlags* d_flags_ = nullptr;

@@ -68,27 +68,28 @@ __device__ __forceinline__ Cell tile_at(const Batch& B, int t) {
 
 // Tile of virtual index v in the active instances' tiles (binary search over
 // the ranges pass_end left); uniform over a block.
-__device__ __forceinline__ int active_tile(const Batch& B, int v) {
-    int lo = 0, hi = B.actInfo[0] - 1;
+__device__ __forceinline__ int range_tile(const Batch& B, const int2* range, const int* info, int v) {
+    int lo = 0, hi = info[0] - 1;
     while (lo < hi) {
         const int mid = (lo + hi + 1) >> 1;
-        if (B.actRange[mid].y <= v)
+        if (range[mid].y <= v)
             lo = mid;
         else
             hi = mid - 1;
     }
-    const int2 r = B.actRange[lo];
+    const int2 r = range[lo];
     return B.instTiles[r.x].x + (v - r.y);
 }
+__device__ __forceinline__ int active_tile(const Batch& B, int v) { return range_tile(B, B.actRange, B.actInfo, v); }
+// The face cascade: only the tiles of instances in the current iteration.
+#define FOR_CASCADE_TILES(B, t)                                                              \
+    for (int v_ = blockIdx.x, nv_ = (B).casInfo[1], t = 0; v_ < nv_; v_ += gridDim.x)       \
+        for (bool once_ = (t = range_tile((B), (B).casRange, (B).casInfo, v_), true); once_; once_ = false)
 // Later MOOD passes: only the tiles of instances still in their MOOD loop.
 #define FOR_ACTIVE_TILES(B, t)                                                              \
     for (int v_ = blockIdx.x, nv_ = (B).actInfo[1], t = 0; v_ < nv_; v_ += gridDim.x)      \
         for (bool once_ = (t = active_tile((B), v_), true); once_; once_ = false)
-// dense (pass 1) or active tiles (later passes), chosen at compile time
-#define FOR_SOME_TILES(ACT, B, t)                                                                        \
-    for (int v_ = blockIdx.x, nv_ = (ACT) ? (B).actInfo[1] : __ldg((B).ntiles), t = 0; v_ < nv_;         \
-         v_ += gridDim.x)                                                                                 \
-        for (bool once_ = (t = (ACT) ? active_tile((B), v_) : v_, true); once_; once_ = false)
+
 
 // the one thread per instance that owns cell (0,0) (every instance has a tile at its origin)
 __device__ __forceinline__ bool first_tile_thread(const Cell& c) { return c.i == 0 && c.j == 0; }
@@ -360,11 +361,52 @@ __global__ void __launch_bounds__(NTHREADS, HOSONO_PASS1_MIN_BLOCKS) k_face_pass
     }
 }
 
+constexpr int PASS_END_THREADS = 128;
+
+// (slot, first virtual tile) of every instance with pick(slot) true, in slot
+// order, and info = {instances, tiles}: per-thread chunks of slots, a block
+// scan of the counts, then each thread writes its chunk.  One block of
+// PASS_END_THREADS threads.
+template <class Pick>
+__device__ __forceinline__ void build_ranges(const Batch& B, Pick pick, int2* range, int* info) {
+    __shared__ int sCnt[PASS_END_THREADS], sTil[PASS_END_THREADS];
+    const int tid = threadIdx.x;
+    const int per = (B.maxInst + PASS_END_THREADS - 1) / PASS_END_THREADS;
+    const int k0 = min(B.maxInst, tid * per), k1 = min(B.maxInst, k0 + per);
+    int cnt = 0, til = 0;
+    for (int k = k0; k < k1; k++)
+        if (pick(k)) {
+            cnt++;
+            til += B.instTiles[k].y;
+        }
+    sCnt[tid] = cnt;
+    sTil[tid] = til;
+    __syncthreads();
+    for (int off = 1; off < PASS_END_THREADS; off <<= 1) {
+        const int a = tid >= off ? sCnt[tid - off] : 0, b = tid >= off ? sTil[tid - off] : 0;
+        __syncthreads();
+        sCnt[tid] += a;
+        sTil[tid] += b;
+        __syncthreads();
+    }
+    int c0 = sCnt[tid] - cnt, t0 = sTil[tid] - til;
+    for (int k = k0; k < k1; k++)
+        if (pick(k)) {
+            range[c0++] = make_int2(k, t0);
+            t0 += B.instTiles[k].y;
+        }
+    if (tid == PASS_END_THREADS - 1) {
+        info[0] = sCnt[tid];
+        info[1] = sTil[tid];
+    }
+}
+
 // ======================================================================
 // Face cascade (reconstruct.f90:143-171).
 // cascade_cond: per instance, whether it entered (or stays in) the cascade;
 // sets the batch condition.  Single block, one thread per slot.
-__global__ void k_cascade_cond(Batch B, cudaGraphConditionalHandle h, int set_handle) {
+__global__ void __launch_bounds__(PASS_END_THREADS) k_cascade_cond(Batch B, cudaGraphConditionalHandle h,
+                                                                      int set_handle) {
     __shared__ int any;
     if (threadIdx.x == 0) any = 0;
     __syncthreads();
@@ -380,6 +422,7 @@ __global__ void k_cascade_cond(Batch B, cudaGraphConditionalHandle h, int set_ha
         }
     }
     __syncthreads();
+    build_ranges(B, [&](int k) { return B.st[k].nextIter != 0; }, B.casRange, B.casInfo);
     if (threadIdx.x == 0) {
         B.flags->anyFail = any;
         B.L.counts[LIST_NEXT] = 0;  // the next cascade iteration compacts its cells afresh
@@ -397,9 +440,8 @@ __device__ __forceinline__ void t_clear_nextpass(const Batch& B, const Cell c) {
     const InstDev& d = B.dev[c.k];
     if (c.i < d.geo.nxt && c.j < d.geo.nyt) d.nextPass[(long long)c.j * d.geo.pitch + c.i] = 0;
 }
-template <bool ACT>
 __global__ void __launch_bounds__(NTHREADS) k_clear_nextpass(Batch B) {
-    FOR_SOME_TILES(ACT, B, t) t_clear_nextpass(B, tile_at(B, t));
+    FOR_CASCADE_TILES(B, t) t_clear_nextpass(B, tile_at(B, t));
 }
 
 // gridBlock_lowerOrder (gridBlock.f90:194-235) of cell (i,j) plus the mark of
@@ -458,9 +500,8 @@ __device__ __forceinline__ void t_cascade_lower(const Batch& B, const Cell c) {
     if (first) d.detMask[cc] |= DM_CASC;
     warp_append(B.L, LIST_CASC, B.L.casc, B.L.cap, first, entry(c.k, cc));
 }
-template <bool ACT>
 __global__ void __launch_bounds__(NTHREADS) k_cascade_lower(Batch B) {
-    FOR_SOME_TILES(ACT, B, t) t_cascade_lower(B, tile_at(B, t));
+    FOR_CASCADE_TILES(B, t) t_cascade_lower(B, tile_at(B, t));
 }
 
 
@@ -531,9 +572,8 @@ __device__ __forceinline__ void t_compact_next(const Batch& B, const Cell c) {
     }
     warp_append(B.L, LIST_NEXT, B.L.next, B.L.cap, p, entry(c.k, cc));
 }
-template <bool ACT>
 __global__ void __launch_bounds__(NTHREADS) k_compact_next(Batch B) {
-    FOR_SOME_TILES(ACT, B, t) t_compact_next(B, tile_at(B, t));
+    FOR_CASCADE_TILES(B, t) t_compact_next(B, tile_at(B, t));
 }
 // ... and re-reconstruct them (list `which`: LIST_NEXT in the cascade,
 // LIST_REC at the start of a later MOOD pass)
@@ -1104,10 +1144,8 @@ __global__ void __launch_bounds__(256) k_scheme_sync(Batch B) {
 
 // End of a MOOD pass (timeStep.f90:86-128 loop test): an instance whose detect
 // lowered nothing leaves the loop.  Single block, one thread per slot.
-constexpr int PASS_END_THREADS = 128;
 __global__ void __launch_bounds__(PASS_END_THREADS) k_pass_end(Batch B, cudaGraphConditionalHandle h, int set_handle, int flip) {
     __shared__ int any;
-    __shared__ int sCnt[PASS_END_THREADS], sTil[PASS_END_THREADS];
     if (threadIdx.x == 0) any = 0;
     __syncthreads();
     for (int k = threadIdx.x; k < B.maxInst; k += blockDim.x) {
@@ -1137,37 +1175,8 @@ __global__ void __launch_bounds__(PASS_END_THREADS) k_pass_end(Batch B, cudaGrap
     }
     __syncthreads();
     // the instances still in their MOOD loop and their tiles, for the dense
-    // kernels of the next pass: per-thread chunks of slots, block scan of
-    // (instances, tiles), then each thread writes its chunk in slot order
-    const int tid = threadIdx.x;
-    const int per = (B.maxInst + PASS_END_THREADS - 1) / PASS_END_THREADS;
-    const int k0 = min(B.maxInst, tid * per), k1 = min(B.maxInst, k0 + per);
-    int cnt = 0, til = 0;
-    for (int k = k0; k < k1; k++)
-        if (B.st[k].stepping && B.st[k].stageActive) {
-            cnt++;
-            til += B.instTiles[k].y;
-        }
-    sCnt[tid] = cnt;
-    sTil[tid] = til;
-    __syncthreads();
-    for (int off = 1; off < PASS_END_THREADS; off <<= 1) {
-        const int a = tid >= off ? sCnt[tid - off] : 0, b = tid >= off ? sTil[tid - off] : 0;
-        __syncthreads();
-        sCnt[tid] += a;
-        sTil[tid] += b;
-        __syncthreads();
-    }
-    int c0 = sCnt[tid] - cnt, t0 = sTil[tid] - til;
-    for (int k = k0; k < k1; k++)
-        if (B.st[k].stepping && B.st[k].stageActive) {
-            B.actRange[c0++] = make_int2(k, t0);
-            t0 += B.instTiles[k].y;
-        }
-    if (tid == PASS_END_THREADS - 1) {
-        B.actInfo[0] = sCnt[tid];
-        B.actInfo[1] = sTil[tid];
-    }
+    // kernels of the next pass
+    build_ranges(B, [&](int k) { return B.st[k].stepping && B.st[k].stageActive; }, B.actRange, B.actInfo);
     if (threadIdx.x == 0) {
         B.flags->anyActive = any;
         if (B.L.counts[LIST_OVERFLOW]) B.flags->error = HOSONO_EINVAL;
@@ -1471,22 +1480,14 @@ void l_face_pass1(const Batch& B, int uin, cudaStream_t s) {
     launch_pass1<3>(B, uin, s);
 }
 void l_cascade_cond(const Batch& B, cudaGraphConditionalHandle h, cudaStream_t s) {
-    k_cascade_cond<<<1, 128, 0, s>>>(B, h, h != 0);
+    k_cascade_cond<<<1, PASS_END_THREADS, 0, s>>>(B, h, h != 0);
 }
-void l_cascade_lower(const Batch& B, int later, cudaStream_t s) {
-    if (later) {
-        TILE_LAUNCH(k_clear_nextpass<true>, B, s);
-        TILE_LAUNCH(k_cascade_lower<true>, B, s);
-    } else {
-        TILE_LAUNCH(k_clear_nextpass<false>, B, s);
-        TILE_LAUNCH(k_cascade_lower<false>, B, s);
-    }
+void l_cascade_lower(const Batch& B, int /*later*/, cudaStream_t s) {
+    TILE_LAUNCH(k_clear_nextpass, B, s);
+    TILE_LAUNCH(k_cascade_lower, B, s);
 }
-void l_recon_check(const Batch& B, int uin, int later, cudaStream_t s) {
-    if (later)
-        TILE_LAUNCH(k_compact_next<true>, B, s);
-    else
-        TILE_LAUNCH(k_compact_next<false>, B, s);
+void l_recon_check(const Batch& B, int uin, int /*later*/, cudaStream_t s) {
+    TILE_LAUNCH(k_compact_next, B, s);
     LIST_LAUNCH(k_recon_group, B, s, uin, (int)LIST_NEXT);
 }
 void l_ct_update_detect(const Batch& B, int uin, int uout, cudaStream_t s) {
