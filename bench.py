@@ -184,6 +184,22 @@ def run_cpu_baseline(workload, steps, threads, fast=None, to_end=False):
     return rate, el, steps
 
 
+def max_over_ranks(ms, dist, device):
+    """The slowest rank's time (replicas: the job ends when the last one does)."""
+    if dist is None:
+        return ms
+    import torch
+    t = torch.tensor([ms], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replicas_value(world, zones, steps, ms):
+    """Whole-job zone-updates/s of `world` replicas, each `steps` steps of
+    `zones` cells, over the slowest rank's time."""
+    return world * zones * steps / (ms / 1e3)
+
+
 def bench_reference(args, rank):
     """--impl reference: the reference algorithm on the host cores (rank 0 only)."""
     if rank != 0:
@@ -272,11 +288,8 @@ def bench_ours(args, rank, world, local):
     passes = sol.stats()["mood_passes"]
     sol.profile(False)
     barrier()
-    if dist is not None:
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = world * zones * args.steps / (ms / 1e3)
+    ms = max_over_ranks(ms, dist, "cuda")
+    value = replicas_value(world, zones, args.steps, ms)
 
     # end to end through the C ABI with host buffers: every step uploads U,V
     # from pinned memory, takes the step (dt on the device) and downloads U,V
@@ -294,10 +307,7 @@ def bench_ours(args, rank, world, local):
     f1.record(stream)
     f1.synchronize()
     e2e_ms = f0.elapsed_time(f1)
-    if dist is not None:
-        t = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = max_over_ranks(e2e_ms, dist, "cuda")
     barrier()
     e2e = {"value": world * zones * e2e_steps / (e2e_ms / 1e3), "unit": "zone-updates/s",
            "h2d_bytes_per_step": U0.nbytes + V0.nbytes, "d2h_bytes_per_step": U0.nbytes + V0.nbytes,
