@@ -164,7 +164,8 @@ Engine::~Engine() {
         if (p) cudaFree(p);
     for (void* p : {(void*)d_dev_, (void*)d_st_, (void*)d_tiles_, (void*)d_ntiles_, (void*)d_flags_, (void*)staging_,
                     (void*)schemeInt_, (void*)lists_.rec, (void*)lists_.face, (void*)lists_.recF, (void*)lists_.low,
-                    (void*)lists_.next, (void*)lists_.casc, (void*)lists_.sync, (void*)lists_.counts})
+                    (void*)lists_.next, (void*)lists_.casc, (void*)lists_.sync, (void*)lists_.rec2,
+                    (void*)lists_.counts})
         if (p) cudaFree(p);
     if (h_flags_) cudaFreeHost(h_flags_);
     if (h_st_) cudaFreeHost(h_st_);
@@ -193,6 +194,7 @@ int Engine::init(int max_inst, int max_tiles, int fp_mode) {
     CUE(cudaMalloc(&d_flags_, sizeof(BatchFlags)));
     lists_.cap = (long long)maxTiles_ * TILE_X * TILE_Y;
     CUE(cudaMalloc(&lists_.rec, sizeof(int2) * lists_.cap));
+    CUE(cudaMalloc(&lists_.rec2, sizeof(int2) * lists_.cap));
     CUE(cudaMalloc(&lists_.face, sizeof(int2) * 2 * lists_.cap));
     CUE(cudaMalloc(&lists_.recF, sizeof(int2) * lists_.cap));
     CUE(cudaMalloc(&lists_.low, sizeof(int2) * lists_.cap));
@@ -580,7 +582,7 @@ int Engine::record_stage(Rec& r, int uin, int uout, cudaEvent_t ev0, cudaEvent_t
     TRYE(r.k([&](cudaStream_t s) { K->compact_dirty(B, s); }));
     TRYE(r.k([&](cudaStream_t s) { K->flux_list(B, uin, s); }));
     TRYE(r.k([&](cudaStream_t s) { K->ct_update_detect(B, uin, uout, s); }));
-    TRYE(r.k([&](cudaStream_t s) { K->mood_flags(B, 1, s); }));
+    TRYE(r.k([&](cudaStream_t s) { K->mood_flags(B, MOOD_FLAGS_DENSE, s); }));
     if (trace) TRYE(r.host([&] { return trace_snapshot(); }));
     TRYE(r.k([&](cudaStream_t s) { K->clear_low(B, s); }));
     TRYE(r.cond(&hm, 0));
@@ -590,7 +592,6 @@ int Engine::record_stage(Rec& r, int uin, int uout, cudaEvent_t ev0, cudaEvent_t
     // list (warp ballot + one atomic per warp) and a list kernel consumes it
     TRYE(r.loop(hm, &BatchFlags::anyActive, cap, [&](Rec& b) -> int {
         if (trace) TRYE(b.host([&] { return trace_before_pass(); }));
-        TRYE(b.k([&](cudaStream_t s) { K->compact_rec(B, s); }));
         TRYE(b.k([&](cudaStream_t s) { K->recon_list(B, uin, s); }));
         cudaGraphConditionalHandle hc2;
         TRYE(b.cond(&hc2, 0));
@@ -599,10 +600,14 @@ int Engine::record_stage(Rec& r, int uin, int uout, cudaEvent_t ev0, cudaEvent_t
         TRYE(b.k([&](cudaStream_t s) { K->compact_post(B, s); }));
         TRYE(b.k([&](cudaStream_t s) { K->flux_list(B, uin, s); }));
         TRYE(b.k([&](cudaStream_t s) { K->ct_list(B, uin, uout, s); }));
-        TRYE(b.k([&](cudaStream_t s) { K->mood_flags(B, 0, s); }));
+        if (trace) {  // the trace reads `lowered` before it is cleared
+            TRYE(b.k([&](cudaStream_t s) { K->mood_flags(B, MOOD_FLAGS_LISTS, s); }));
+            TRYE(b.host([&] { return trace_snapshot(); }));
+            TRYE(b.k([&](cudaStream_t s) { K->clear_low(B, s); }));
+        } else {
+            TRYE(b.k([&](cudaStream_t s) { K->mood_flags(B, MOOD_FLAGS_LISTS_CLEAR, s); }));
+        }
         if (!b.graph()) launches += 2;  // three kernels
-        if (trace) TRYE(b.host([&] { return trace_snapshot(); }));
-        TRYE(b.k([&](cudaStream_t s) { K->clear_low(B, s); }));
         TRYE(b.k([&](cudaStream_t s) { K->pass_end(B, hm, 0, s); }));
         if (trace) TRYE(b.host([&] { return trace_after_pass(); }));
         return HOSONO_OK;

@@ -89,6 +89,7 @@ struct BatchFlags {
     int error;
     int stepsLeft;   // step budget of the current run launch
     int radii;       // bit R set when a live instance has GP radius R (per-radius kernels of absent radii exit)
+    int recSel;      // which recompute list the current MOOD pass reads (0: Lists::rec, 1: rec2)
 };
 
 // Roles of the three U buffers: the state lives in U[parity]; A in
@@ -101,10 +102,11 @@ __host__ __device__ inline double* role_ptr(const InstDev& d, int parity, int ro
 
 // Work lists of the later MOOD passes (compacted by warp ballot): entries are
 // (instance, cell index j*pitch+i); face entries carry 2*cell+dir.
-enum : int { LIST_REC = 0, LIST_FACE = 1, LIST_RECF = 2, LIST_LOW = 3, LIST_NEXT = 4, LIST_CASC = 5, LIST_N = 6,
-             LIST_OVERFLOW = 6 };
+enum : int { LIST_REC = 0, LIST_FACE = 1, LIST_RECF = 2, LIST_LOW = 3, LIST_NEXT = 4, LIST_CASC = 5, LIST_REC2 = 6,
+             LIST_N = 7, LIST_OVERFLOW = 7 };
 struct Lists {
-    int2* rec;    // cells to re-reconstruct (recompute set)
+    int2* rec;    // cells to re-reconstruct (recompute set), two buffers:
+    int2* rec2;   // the current pass reads one, the flag rebuild fills the other (BatchFlags::recSel)
     int2* face;   // faces to re-flux
     int2* recF;   // cells to FLICD + update + detect (recomputeFLICD set)
     int2* low;    // cells detect lowered this pass (to clear `lowered` after use)
@@ -138,6 +140,7 @@ struct Batch {
 };
 
 enum : int { CASCADE_FROM_FACES = 0, CASCADE_FROM_CELLS = 1 };
+enum : int { MOOD_FLAGS_LISTS = 0, MOOD_FLAGS_DENSE = 1, MOOD_FLAGS_LISTS_CLEAR = 2 };
 
 // Launchers of one arithmetic build (kernels.cu compiled strict or fast).
 struct KernelSet {
@@ -156,12 +159,12 @@ struct KernelSet {
     void (*cascade_lower)(const Batch&, int later, cudaStream_t);
     void (*recon_check)(const Batch&, int uin, int later, cudaStream_t);  // compact nextPass, re-reconstruct
     void (*ct_update_detect)(const Batch&, int uin, int uout, cudaStream_t);
-    // dense: every cell (MOOD pass 1); else from the work lists (later passes)
-    void (*mood_flags)(const Batch&, int dense, cudaStream_t);
+    // MOOD_FLAGS_*: dense on every cell (pass 1), or from the work lists
+    // (later passes), clearing `lowered` too unless a trace reads it first
+    void (*mood_flags)(const Batch&, int mode, cudaStream_t);
     // flip: the dense flag rebuild wrote the other scheme buffer
     void (*pass_end)(const Batch&, cudaGraphConditionalHandle h, int flip, cudaStream_t);
     // later MOOD passes on compacted work lists
-    void (*compact_rec)(const Batch&, cudaStream_t);
     void (*recon_list)(const Batch&, int uin, cudaStream_t);
     void (*compact_post)(const Batch&, cudaStream_t);   // faces and recomputeFLICD cells
     void (*compact_dirty)(const Batch&, cudaStream_t);  // pass-1 faces next to re-reconstructed cells

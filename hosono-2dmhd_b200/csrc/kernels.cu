@@ -176,6 +176,12 @@ __device__ __forceinline__ void warp_append(const Lists& L, int which, int2* lis
 
 __device__ __forceinline__ int2 entry(int k, long long cc) { return make_int2(k, (int)cc); }
 
+// The two recompute lists: the current MOOD pass reads one (next = false),
+// the flag rebuild at its end fills the other (next = true); pass_end swaps.
+__device__ __forceinline__ int rec_sel(const Batch& B, bool next) { return B.flags->recSel ^ (next ? 1 : 0); }
+__device__ __forceinline__ int2* rec_list(const Batch& B, bool next) { return rec_sel(B, next) ? B.L.rec2 : B.L.rec; }
+__device__ __forceinline__ int rec_count(const Batch& B, bool next) { return rec_sel(B, next) ? LIST_REC2 : LIST_REC; }
+
 // ======================================================================
 // MOOD pass 1 (every scheme == R): reconstruct_faceValsWithGP + face CAD/PAD
 // + getFluxes_ fused.  A thread owns the x-face between (i-1,j) and (i,j) and
@@ -369,7 +375,7 @@ constexpr int PASS_END_THREADS = 128;
 // PASS_END_THREADS threads.
 template <class Pick>
 __device__ __forceinline__ void build_ranges(const Batch& B, Pick pick, int2* range, int* info) {
-    __shared__ int sCnt[PASS_END_THREADS], sTil[PASS_END_THREADS];
+    __shared__ int sCnt[PASS_END_THREADS / 32], sTil[PASS_END_THREADS / 32];
     const int tid = threadIdx.x;
     const int per = (B.maxInst + PASS_END_THREADS - 1) / PASS_END_THREADS;
     const int k0 = min(B.maxInst, tid * per), k1 = min(B.maxInst, k0 + per);
@@ -379,26 +385,36 @@ __device__ __forceinline__ void build_ranges(const Batch& B, Pick pick, int2* ra
             cnt++;
             til += B.instTiles[k].y;
         }
-    sCnt[tid] = cnt;
-    sTil[tid] = til;
-    __syncthreads();
-    for (int off = 1; off < PASS_END_THREADS; off <<= 1) {
-        const int a = tid >= off ? sCnt[tid - off] : 0, b = tid >= off ? sTil[tid - off] : 0;
-        __syncthreads();
-        sCnt[tid] += a;
-        sTil[tid] += b;
-        __syncthreads();
+    // inclusive scan: within each warp by shuffles, then over the warp totals
+    const int lane = tid & 31, wid = tid >> 5;
+    int ic = cnt, it = til;
+    for (int off = 1; off < 32; off <<= 1) {
+        const int a = __shfl_up_sync(0xffffffffu, ic, off), b = __shfl_up_sync(0xffffffffu, it, off);
+        if (lane >= off) {
+            ic += a;
+            it += b;
+        }
     }
-    int c0 = sCnt[tid] - cnt, t0 = sTil[tid] - til;
+    if (lane == 31) {
+        sCnt[wid] = ic;
+        sTil[wid] = it;
+    }
+    __syncthreads();
+    for (int w = 0; w < wid; w++) {
+        ic += sCnt[w];
+        it += sTil[w];
+    }
+    int c0 = ic - cnt, t0 = it - til;
     for (int k = k0; k < k1; k++)
         if (pick(k)) {
             range[c0++] = make_int2(k, t0);
             t0 += B.instTiles[k].y;
         }
     if (tid == PASS_END_THREADS - 1) {
-        info[0] = sCnt[tid];
-        info[1] = sTil[tid];
+        info[0] = ic;
+        info[1] = it;
     }
+    __syncthreads();  // sCnt/sTil may be reused by the caller's next call
 }
 
 // ======================================================================
@@ -578,8 +594,8 @@ __global__ void __launch_bounds__(NTHREADS) k_compact_next(Batch B) {
 // ... and re-reconstruct them (list `which`: LIST_NEXT in the cascade,
 // LIST_REC at the start of a later MOOD pass)
 __global__ void __launch_bounds__(256) k_recon_group(Batch B, int uin, int which) {
-    const int2* list = which == LIST_NEXT ? B.L.next : B.L.rec;
-    const int n = min(B.L.counts[which], (int)B.L.cap);
+    const int2* list = which == LIST_NEXT ? B.L.next : rec_list(B, false);
+    const int n = min(B.L.counts[which == LIST_NEXT ? (int)LIST_NEXT : rec_count(B, false)], (int)B.L.cap);
     FOR_GROUPS(n, RECON_GL, e, sub, act) {
         int2 it = make_int2(0, 0);
         if (act) it = list[e];
@@ -590,25 +606,6 @@ __global__ void __launch_bounds__(256) k_recon_group(Batch B, int uin, int which
 }
 
 
-// cells with recompute in the reconstruct range (reconstruct.f90:83)
-__device__ __forceinline__ void t_compact_rec(const Batch& B, const Cell c) {
-    InstState& S = B.st[c.k];
-    if (!(S.stepping && S.stageActive)) return;
-    const InstDev& d = B.dev[c.k];
-    const Geo& G = d.geo;
-    const int g = G.g;
-    if (first_tile_thread(c)) S.cascadeMode = CASCADE_FROM_CELLS;
-    bool p = false;
-    long long cc = 0;
-    if (c.i >= g - 2 && c.j >= g - 2 && c.i <= g + G.nx + 1 && c.j <= g + G.ny + 1) {
-        cc = (long long)c.j * G.pitch + c.i;
-        p = d.rec[cc] != 0;
-    }
-    warp_append(B.L, LIST_REC, B.L.rec, B.L.cap, p, entry(c.k, cc));
-}
-__global__ void __launch_bounds__(NTHREADS) k_compact_rec(Batch B) {
-    FOR_ACTIVE_TILES(B, t) t_compact_rec(B, tile_at(B, t));
-}
 
 // After the face cascade of a later MOOD pass: the faces getFluxes_ recomputes
 // (x-face (i,j) if recompute(i,j) or (i-1,j), y-face if recompute(i,j) or
@@ -982,13 +979,9 @@ __global__ void __launch_bounds__(256) k_clear_low(Batch B) {
 // boundaryConditions_applyMOOD's periodic sync, which (x sweep over all rows,
 // then y sweep over all columns, N >= 2*NGC) makes every cell the OR (flags) /
 // MIN (scheme) over its translates by multiples of N that lie in the array.
-__device__ __forceinline__ void t_mood_flags(const Batch& B, const Cell c) {
-    const InstState& S = B.st[c.k];
-    if (!(S.stepping && S.stageActive)) return;
-    const InstDev& d = B.dev[c.k];
+// one cell of the dense rebuild; returns its new recompute flag
+__device__ __forceinline__ bool mood_flags_cell(const InstDev& d, const InstState& S, int i, int j) {
     const Geo& G = d.geo;
-    const int i = c.i, j = c.j;
-    if (i >= G.nxt || j >= G.nyt) return;
     const int8_t* sch = d.scheme[S.schemeSel];
     int8_t* schN = d.scheme[1 - S.schemeSel];
     const int reach = G.bc == 1 ? 1 : 0;
@@ -1024,6 +1017,21 @@ __device__ __forceinline__ void t_mood_flags(const Batch& B, const Cell c) {
     d.recF[cc] = recF;
     schN[cc] = (int8_t)s;
     d.detMask[cc] &= (uint8_t)~DM_CASC;
+    return rec;
+}
+__device__ __forceinline__ void t_mood_flags(const Batch& B, const Cell c) {
+    const InstState& S = B.st[c.k];
+    if (!(S.stepping && S.stageActive)) return;
+    const InstDev& d = B.dev[c.k];
+    const Geo& G = d.geo;
+    const int i = c.i, j = c.j;
+    const bool inArr = i < G.nxt && j < G.nyt;
+    const int g = G.g;
+    const bool inRec = inArr && i >= g - 2 && j >= g - 2 && i <= g + G.nx + 1 && j <= g + G.ny + 1;
+    const bool newRec = inArr && mood_flags_cell(d, S, i, j);
+    // the next pass's recompute list (reconstruct range, reconstruct.f90:83)
+    warp_append(B.L, rec_count(B, true), rec_list(B, true), B.L.cap, newRec && inRec,
+                entry(c.k, (long long)j * G.pitch + i));
 }
 __global__ void __launch_bounds__(NTHREADS) k_mood_flags(Batch B) {
     FOR_TILES(B, t) t_mood_flags(B, tile_at(B, t));
@@ -1039,6 +1047,23 @@ __global__ void __launch_bounds__(NTHREADS) k_mood_flags(Batch B) {
 // not sync): each takes min over its class of (scheme - lowered)^+, computed
 // for every listed cell first and written afterwards (two kernels), so no
 // class member is read after it was written.
+// recompute := 1; the first setter of a cell in the reconstruct range puts
+// it on the next pass's list (the byte is set through its 32-bit word so
+// that exactly one thread sees it change)
+__device__ __forceinline__ void set_rec(const Batch& B, const InstDev& d, long long cn, int ii, int jj, int k) {
+    const unsigned sh = 8u * (unsigned)(cn & 3);
+    unsigned* w = reinterpret_cast<unsigned*>(d.rec + (cn - (cn & 3)));
+    const unsigned old = atomicOr(w, 1u << sh);
+    const Geo& G = d.geo;
+    const int g = G.g;
+    if (((old >> sh) & 0xffu) == 0 && ii >= g - 2 && jj >= g - 2 && ii <= g + G.nx + 1 && jj <= g + G.ny + 1) {
+        const int pos = atomicAdd(B.L.counts + rec_count(B, true), 1);
+        if (pos < B.L.cap)
+            rec_list(B, true)[pos] = entry(k, cn);
+        else
+            B.L.counts[LIST_OVERFLOW] = 1;
+    }
+}
 __device__ __forceinline__ void sync_cell(const Batch& B, int e, int nLow, int2* it_out, bool* from_low) {
     *from_low = e < nLow;
     *it_out = *from_low ? B.L.low[e] : B.L.casc[e - nLow];
@@ -1046,7 +1071,8 @@ __device__ __forceinline__ void sync_cell(const Batch& B, int e, int nLow, int2*
 __global__ void __launch_bounds__(256) k_flags_clear(Batch B) {
     const int nF = min(B.L.counts[LIST_FACE], (int)(2 * B.L.cap));
     const int nR = min(B.L.counts[LIST_RECF], (int)B.L.cap);
-    const int nP = min(B.L.counts[LIST_REC], (int)B.L.cap);
+    const int nP = min(B.L.counts[rec_count(B, false)], (int)B.L.cap);
+    const int2* recCur = rec_list(B, false);
     const int nC = min(B.L.counts[LIST_CASC], (int)B.L.cap);
     for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nF + nR + nP + nC; e += gridDim.x * blockDim.x) {
         if (e < nF) {  // both cells of a re-fluxed face
@@ -1059,7 +1085,7 @@ __global__ void __launch_bounds__(256) k_flags_clear(Batch B) {
             const int2 it = B.L.recF[e - nF];
             B.dev[it.x].recF[it.y] = 0;
         } else if (e < nF + nR + nP) {  // recompute at the start of the pass
-            const int2 it = B.L.rec[e - nF - nR];
+            const int2 it = recCur[e - nF - nR];
             B.dev[it.x].rec[it.y] = 0;
         } else {  // the cross a cascade lowering marked
             const int2 it = B.L.casc[e - nF - nR - nP];
@@ -1107,7 +1133,7 @@ __global__ void __launch_bounds__(256) k_flags_scatter(Batch B) {
                         if (dd > 2 || ii < 0 || ii >= G.nxt) continue;
                         const long long cn = (long long)jj * G.pitch + ii;
                         d.recF[cn] = 1;
-                        if (dd <= 1) d.rec[cn] = 1;
+                        if (dd <= 1) set_rec(B, d, cn, ii, jj, it.x);
                     }
                 }
             }
@@ -1115,7 +1141,7 @@ __global__ void __launch_bounds__(256) k_flags_scatter(Batch B) {
         B.L.sync[e] = (int8_t)s;
     }
 }
-__global__ void __launch_bounds__(256) k_scheme_sync(Batch B) {
+__global__ void __launch_bounds__(256) k_scheme_sync(Batch B, int clear_low) {
     const int nL = min(B.L.counts[LIST_LOW], (int)B.L.cap);
     const int nC = min(B.L.counts[LIST_CASC], (int)B.L.cap);
     for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nL + nC; e += gridDim.x * blockDim.x) {
@@ -1139,6 +1165,7 @@ __global__ void __launch_bounds__(256) k_scheme_sync(Batch B) {
             }
         }
         if (!fromLow) d.detMask[c0] &= (uint8_t)~DM_CASC;
+        if (fromLow && clear_low) d.lowered[c0] = 0;  // k_flags_scatter has read it
     }
 }
 
@@ -1168,6 +1195,7 @@ __global__ void __launch_bounds__(PASS_END_THREADS) k_pass_end(Batch B, cudaGrap
             S.error = HOSONO_EMOODCAP;
         } else {
             any = 1;
+            S.cascadeMode = CASCADE_FROM_CELLS;  // later passes' cascades start from re-reconstructions
         }
         S.nInner = 0;
         S.nDetect = 0;
@@ -1180,7 +1208,12 @@ __global__ void __launch_bounds__(PASS_END_THREADS) k_pass_end(Batch B, cudaGrap
     if (threadIdx.x == 0) {
         B.flags->anyActive = any;
         if (B.L.counts[LIST_OVERFLOW]) B.flags->error = HOSONO_EINVAL;
-        for (int w = 0; w < LIST_N; w++) B.L.counts[w] = 0;  // the next pass builds its lists afresh
+        // the next pass reads the recompute list the flag rebuild just filled
+        // and builds every other list afresh
+        const int cur = B.flags->recSel ^ 1;
+        B.flags->recSel = cur;
+        for (int w = 0; w < LIST_N; w++)
+            if (w != (cur ? LIST_REC2 : LIST_REC)) B.L.counts[w] = 0;
         if (set_handle) cudaGraphSetConditional(h, any ? 1u : 0u);
     }
 }
@@ -1213,6 +1246,10 @@ __device__ __forceinline__ void t_stage_init(const Batch& B, const Cell c) {
     d.innerCount[cc] = 0;
 }
 __global__ void __launch_bounds__(NTHREADS) k_stage_init(Batch B) {
+    if (blockIdx.x == 0 && threadIdx.x == 0 && threadIdx.y == 0) {  // the recompute lists start empty
+        B.L.counts[LIST_REC] = 0;
+        B.L.counts[LIST_REC2] = 0;
+    }
     FOR_TILES(B, t) t_stage_init(B, tile_at(B, t));
 }
 
@@ -1493,19 +1530,18 @@ void l_recon_check(const Batch& B, int uin, int /*later*/, cudaStream_t s) {
 void l_ct_update_detect(const Batch& B, int uin, int uout, cudaStream_t s) {
     TILE_LAUNCH(k_ct_update_detect, B, s, uin, uout);
 }
-void l_mood_flags(const Batch& B, int dense, cudaStream_t s) {
-    if (dense) {
+void l_mood_flags(const Batch& B, int mode, cudaStream_t s) {
+    if (mode == MOOD_FLAGS_DENSE) {
         TILE_LAUNCH(k_mood_flags, B, s);
     } else {
         LIST_LAUNCH(k_flags_clear, B, s);
         LIST_LAUNCH(k_flags_scatter, B, s);
-        LIST_LAUNCH(k_scheme_sync, B, s);
+        LIST_LAUNCH(k_scheme_sync, B, s, mode == MOOD_FLAGS_LISTS_CLEAR ? 1 : 0);
     }
 }
 void l_pass_end(const Batch& B, cudaGraphConditionalHandle h, int flip, cudaStream_t s) {
     k_pass_end<<<1, PASS_END_THREADS, 0, s>>>(B, h, h != 0, flip);
 }
-void l_compact_rec(const Batch& B, cudaStream_t s) { TILE_LAUNCH(k_compact_rec, B, s); }
 void l_compact_post(const Batch& B, cudaStream_t s) { TILE_LAUNCH(k_compact_post, B, s); }
 void l_compact_dirty(const Batch& B, cudaStream_t s) { TILE_LAUNCH(k_compact_dirty, B, s); }
 void l_recon_list(const Batch& B, int uin, cudaStream_t s) { LIST_LAUNCH(k_recon_group, B, s, uin, (int)LIST_REC); }
@@ -1524,7 +1560,7 @@ const KernelSet kset = {
     "strict",
 #endif
     l_cfl_reduce, l_step_prepare, l_step_begin, l_step_end, l_stage_init, l_face_pass1, l_cascade_cond, l_cascade_lower,
-    l_recon_check, l_ct_update_detect, l_mood_flags, l_pass_end, l_compact_rec, l_recon_list,
+    l_recon_check, l_ct_update_detect, l_mood_flags, l_pass_end, l_recon_list,
     l_compact_post, l_compact_dirty, l_flux_list, l_ct_list, l_clear_low, l_bc_fill, l_rk_combine2, l_rk_final,
     l_cons2prim_all};
 
