@@ -85,6 +85,10 @@ class ServeTotals(ctypes.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class ICDesc(ctypes.Structure):
+    _fields_ = [("type", ctypes.c_int), ("pad", ctypes.c_int), ("c", ctypes.c_double * 16)]
+
+
 REQ_QUEUED, REQ_RUNNING, REQ_DONE = 0, 1, 2
 
 # Every symbol the C ABI exports (include/hosono_gpu.h), with its signature.
@@ -139,6 +143,11 @@ SIGNATURES = {
     "hosono_batch_set_graphs": [_vp, _i],
     "hosono_batch_last_error": [_vp, _cp, _i],
     "hosono_batch_capacity": [_vp, _ip, _ip, _ip, _ip],
+    "hosono_ic_describe": [_cp, ctypes.POINTER(Params), ctypes.POINTER(ICDesc), _dp, _dp, _cp, _i],
+    "hosono_gpu_ic": [_vp, ctypes.POINTER(ICDesc), _dp, _dp],
+    "hosono_batch_ic": [_vp, _i, ctypes.POINTER(ICDesc), _dp, _dp],
+    "hosono_serve_submit_ic": [_vp, ctypes.POINTER(Params), _dp, _dp, _ip, ctypes.POINTER(ICDesc), _dp, _dp, _d, _i,
+                               _dp, _dp, _ip, ctypes.POINTER(ctypes.c_longlong)],
     "hosono_gpu_diagnostics": [_vp, _dp, _ip, _ip, _dp, _dp],
     "hosono_batch_diagnostics": [_vp, _i, _dp, _ip, _ip, _dp, _dp],
     "hosono_serve_clock": [],
@@ -248,6 +257,21 @@ def ic_set(parfile, params):
     return U, V
 
 
+def ic_describe(parfile, params):
+    """initialCondition_set for the device: (ICDesc, xtab, ytab) -- a few
+    constants and per-column / per-row tables, O(nx+ny)."""
+    lib = load_library()
+    nxt, nyt = params.nx + 2 * params.ngc, params.ny + 2 * params.ngc
+    d = ICDesc()
+    xt = np.zeros(3 * nxt)
+    yt = np.zeros(2 * nyt)
+    err = ctypes.create_string_buffer(512)
+    rc = lib.hosono_ic_describe(os.fsencode(parfile), ctypes.byref(params), ctypes.byref(d), _p(xt), _p(yt), err, 512)
+    if rc:
+        raise HosonoError(rc, err.value.decode())
+    return d, xt, yt
+
+
 class Solver:
     """One block advanced on the GPU (gridBlock_t + gridState_t resident in HBM)."""
 
@@ -320,6 +344,11 @@ class Solver:
         self._check(self.lib.hosono_gpu_download(self.h, _p(U), _p(V), _p(S, ctypes.c_int) if with_scheme else None),
                     "download")
         return U, V, S
+
+    def upload_ic(self, desc, xtab, ytab):
+        """Build the initial state on the device (see ic_describe)."""
+        self._check(self.lib.hosono_gpu_ic(self.h, ctypes.byref(desc), _p(np.ascontiguousarray(xtab)),
+                                           _p(np.ascontiguousarray(ytab))), "ic")
 
     def cfl_computedt(self):
         dt = ctypes.c_double()

@@ -58,7 +58,7 @@ def jobs(verbose=False):
     out.append((os.path.join(BUILD, "kernels_fast.o"), [k] + hdrs,
                 [nv, "-c", k, "-DHOSONO_FAST=1", "--fmad=true", "-Xptxas", "-v" if verbose else "-O3"] + ccbin
                 + NVCC_COMMON + ["-o", os.path.join(BUILD, "kernels_fast.o")]))
-    for name in ("hosono_gpu.cu", "engine.cu", "layout.cu", "noalloc.cu", "server.cu", "diagnostics.cu"):
+    for name in ("hosono_gpu.cu", "engine.cu", "layout.cu", "noalloc.cu", "server.cu", "diagnostics.cu", "ic.cu"):
         src = os.path.join(CSRC, name)
         obj = os.path.join(BUILD, name.replace(".cu", ".o"))
         out.append((obj, [src] + hdrs, [nv, "-c", src, "--fmad=false"] + ccbin + NVCC_COMMON + ["-o", obj]))

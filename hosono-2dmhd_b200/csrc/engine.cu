@@ -472,6 +472,25 @@ int Engine::upload(int slot, const double* U, const double* V) {
     return HOSONO_OK;
 }
 
+int Engine::ic(int slot, const hosono_ic_desc& d, const double* xtab, const double* ytab) {
+    if (slot < 0 || slot >= maxInst_ || !slots_[slot].live || !xtab || !ytab) return fail(HOSONO_EINVAL, "bad ic");
+    if (d.type != HOSONO_IC_EXPLOSION && d.type != HOSONO_IC_SEDOV && d.type != HOSONO_IC_ORSZAG_TANG)
+        return fail(HOSONO_EINVAL, "unknown initial-condition type %d", d.type);
+    InstState st;
+    TRYE(state(slot, &st));
+    const Slot& sl = slots_[slot];
+    const Geo& G = sl.dev.geo;
+    // the tables go through the staging buffer (cells*10 doubles >= 3*nxt + 2*nyt)
+    CUE(cudaMemcpyAsync(staging_, xtab, sizeof(double) * 3 * G.nxt, cudaMemcpyHostToDevice, s_));
+    CUE(cudaMemcpyAsync(staging_ + 3 * G.nxt, ytab, sizeof(double) * 2 * G.nyt, cudaMemcpyHostToDevice, s_));
+    launch_ic(G, sl.dev.phys.force_hydro, sl.dev.phys.gamma, d, staging_, staging_ + 3 * G.nxt, sl.dev.U[st.parity],
+              sl.dev.V, s_);
+    launches++;
+    CUE(cudaGetLastError());
+    CUE(cudaStreamSynchronize(s_));
+    return HOSONO_OK;
+}
+
 int Engine::diagnostics(int slot, double* fields, int* scheme, int* ordr, double* divb_l1, double* divb_linf) {
     if (slot < 0 || slot >= maxInst_ || !slots_[slot].live) return fail(HOSONO_EINVAL, "bad diagnostics slot");
     InstState st;

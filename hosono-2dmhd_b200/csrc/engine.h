@@ -13,6 +13,7 @@
 #include <cuda_runtime.h>
 #include <cstdint>
 
+#include "hosono_gpu.h"
 #include "physics.cuh"
 
 namespace hosono {
@@ -185,6 +186,9 @@ const KernelSet* kernelset_fast();
 void launch_aos_to_soa(const Geo& G, const double* aos, double* soa, int nvar, cudaStream_t s);
 void launch_soa_to_aos(const Geo& G, const double* soa, double* aos, int nvar, cudaStream_t s);
 void launch_scheme_to_int(const Geo& G, const int8_t* scheme, int* out, cudaStream_t s);
+// initialCondition_set on the device (ic.cu)
+void launch_ic(const Geo& G, int force_hydro, double gamma, const hosono_ic_desc& ic, const double* xtab,
+               const double* ytab, double* U, double* V, cudaStream_t s);
 // output_writeHdf5's derived fields and div(B) norms (diagnostics.cu)
 void launch_diagnostics(const Geo& G, const double* V, const int8_t* scheme, double* fields, int* schOut,
                         int* ordr, double* rows, double* res, cudaStream_t s);

@@ -41,6 +41,8 @@ class Engine {
     void set_allocator(DeviceAllocator* a) { alloc_ = a; }
     int upload(int slot, const double* U, const double* V);
     int download(int slot, double* U, double* V, int* scheme);
+    // the initial state built on the device (hosono_ic_describe's output)
+    int ic(int slot, const hosono_ic_desc& d, const double* xtab, const double* ytab);
     // output_writeHdf5's fields of the interior (13 double planes + scheme,
     // ordr; any may be null) and mean / max |div B|; allocates device scratch
     int diagnostics(int slot, double* fields, int* scheme, int* ordr, double* divb_l1, double* divb_linf);

@@ -341,6 +341,14 @@ int hosono_batch_set_graphs(hosono_batch* b, int on) {
     return HOSONO_OK;
 }
 
+int hosono_gpu_ic(hosono_handle* h, const hosono_ic_desc* ic, const double* xtab, const double* ytab) {
+    return h && ic ? h->eng.ic(h->slot, *ic, xtab, ytab) : HOSONO_EINVAL;
+}
+
+int hosono_batch_ic(hosono_batch* b, int slot, const hosono_ic_desc* ic, const double* xtab, const double* ytab) {
+    return b && ic ? b->eng.ic(slot, *ic, xtab, ytab) : HOSONO_EINVAL;
+}
+
 int hosono_gpu_diagnostics(hosono_handle* h, double* fields, int* scheme, int* ordr, double* divb_l1,
                            double* divb_linf) {
     return h ? h->eng.diagnostics(h->slot, fields, scheme, ordr, divb_l1, divb_linf) : HOSONO_EINVAL;

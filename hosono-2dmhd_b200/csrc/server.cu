@@ -50,6 +50,9 @@ double clock_s() {
 struct Request {
     hosono_params p{};
     std::vector<double> pv, qw, U, V;
+    bool devIC = false;  // initial state built on the device from ic + tables
+    hosono_ic_desc ic{};
+    std::vector<double> xtab, ytab;
     double tmax = 0;
     int nstepmax = 0;
     double* outU = nullptr;
@@ -286,10 +289,14 @@ class Scheduler {
         if (added.empty()) return HOSONO_OK;
         int rc = eng->commit_tables();
         for (Request* r : added) {
-            if (!rc) rc = eng->upload(r->info.slot, r->U.data(), r->V.empty() ? nullptr : r->V.data());
+            if (!rc)
+                rc = r->devIC ? eng->ic(r->info.slot, r->ic, r->xtab.data(), r->ytab.data())
+                              : eng->upload(r->info.slot, r->U.data(), r->V.empty() ? nullptr : r->V.data());
             if (!rc) rc = eng->set_time(r->info.slot, 0.0, r->tmax, 0, r->nstepmax);
             r->U = std::vector<double>();
             r->V = std::vector<double>();
+            r->xtab = std::vector<double>();
+            r->ytab = std::vector<double>();
         }
         return rc;
     }
@@ -470,10 +477,32 @@ int hosono_serve_destroy(hosono_server* S) {
     return HOSONO_OK;
 }
 
+static int submit_common(hosono_server* S, const hosono_params* p, const double* pv, const double* qw,
+                         const int* stenc, const double* U, const double* V, const hosono_ic_desc* ic,
+                         const double* xtab, const double* ytab, double tmax, int nstepmax, double* U_out,
+                         double* V_out, int* scheme_out, long long* id);
+
 int hosono_serve_submit(hosono_server* S, const hosono_params* p, const double* pv, const double* qw, const int* stenc,
                         const double* U, const double* V, double tmax, int nstepmax, double* U_out, double* V_out,
                         int* scheme_out, long long* id) {
-    if (!S || !p || !pv || !qw || !U || !id) return HOSONO_EINVAL;
+    if (!U) return HOSONO_EINVAL;
+    return submit_common(S, p, pv, qw, stenc, U, V, nullptr, nullptr, nullptr, tmax, nstepmax, U_out, V_out,
+                         scheme_out, id);
+}
+
+int hosono_serve_submit_ic(hosono_server* S, const hosono_params* p, const double* pv, const double* qw,
+                           const int* stenc, const hosono_ic_desc* ic, const double* xtab, const double* ytab,
+                           double tmax, int nstepmax, double* U_out, double* V_out, int* scheme_out, long long* id) {
+    if (!ic || !xtab || !ytab) return HOSONO_EINVAL;
+    return submit_common(S, p, pv, qw, stenc, nullptr, nullptr, ic, xtab, ytab, tmax, nstepmax, U_out, V_out,
+                         scheme_out, id);
+}
+
+static int submit_common(hosono_server* S, const hosono_params* p, const double* pv, const double* qw,
+                         const int* stenc, const double* U, const double* V, const hosono_ic_desc* ic,
+                         const double* xtab, const double* ytab, double tmax, int nstepmax, double* U_out,
+                         double* V_out, int* scheme_out, long long* id) {
+    if (!S || !p || !pv || !qw || !id) return HOSONO_EINVAL;
     if (!params_ok(*p) || !stencil_ok(p->max_radius, stenc) || std::isnan(tmax) || nstepmax < 0) {
         std::lock_guard<std::mutex> lk(S->mu);
         return S->fail(HOSONO_EINVAL, "invalid solve parameters");
@@ -486,8 +515,16 @@ int hosono_serve_submit(hosono_server* S, const hosono_params* p, const double* 
     try {
         r->pv.assign(pv, pv + nsMax * nqMax * 4 * R);
         r->qw.assign(qw, qw + nqMax * R);
-        r->U.assign(U, U + cells * NCONS);
-        if (V) r->V.assign(V, V + cells * NPRIM);
+        if (ic) {
+            r->devIC = true;
+            r->ic = *ic;
+            const size_t nxt = (size_t)(p->nx + 2 * p->ngc), nyt = (size_t)(p->ny + 2 * p->ngc);
+            r->xtab.assign(xtab, xtab + 3 * nxt);
+            r->ytab.assign(ytab, ytab + 2 * nyt);
+        } else {
+            r->U.assign(U, U + cells * NCONS);
+            if (V) r->V.assign(V, V + cells * NPRIM);
+        }
     } catch (...) {
         return HOSONO_ENOMEM;
     }

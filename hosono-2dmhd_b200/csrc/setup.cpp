@@ -305,3 +305,64 @@ extern "C" int hosono_ic_set(const char* parfile, const hosono_params* p, double
     }
     return HOSONO_OK;
 }
+
+extern "C" int hosono_ic_describe(const char* parfile, const hosono_params* p, hosono_ic_desc* ic, double* xtab,
+                                  double* ytab, char* err, int errlen) {
+    if (!p || !ic || !xtab || !ytab) return HOSONO_EINVAL;
+    ParFile f(parfile);
+    if (!f.ok) {
+        put_err(err, errlen, "cannot open parameter file");
+        return HOSONO_EPAR;
+    }
+    const int g = p->ngc, nxt = p->nx + 2 * g, nyt = p->ny + 2 * g;
+    const double gam = p->gamma;
+    try {
+        const double xb = get_real(f, "grid_xBeg"), yb = get_real(f, "grid_yBeg");
+        // the expressions of hosono_ic_set, tabulated per column / row
+        for (int i = 0; i < nxt; i++) {
+            const double xx = ((i + 1) - g - 0.5) * p->dx + xb;
+            xtab[i] = xx;
+            xtab[nxt + i] = std::sin(kPi * xx * 2.0);
+            xtab[2 * nxt + i] = std::sin(kPi * xx * 4.0);
+        }
+        for (int j = 0; j < nyt; j++) {
+            const double yy = ((j + 1) - g - 0.5) * p->dy + yb;
+            ytab[j] = yy;
+            ytab[nyt + j] = std::sin(kPi * yy * 2.0);
+        }
+        hosono_ic_desc d{};
+        const std::string type = get_str(f, "IC_type");
+        if (type == "explosion2d") {
+            d.type = HOSONO_IC_EXPLOSION;
+            const char* keys[13] = {"IC_shockCenter_x", "IC_shockCenter_y", "IC_shockRad", "IC_densIns", "IC_densOut",
+                                    "IC_velxIns", "IC_velyIns", "IC_velzIns", "IC_velxOut", "IC_velyOut",
+                                    "IC_velzOut", "IC_presIns", "IC_presOut"};
+            for (int k = 0; k < 13; k++) d.c[k] = get_real(f, keys[k]);
+            d.c[13] = get_real_or(f, "IC_magx", 0.0);
+            d.c[14] = get_real_or(f, "IC_magy", 0.0);
+            d.c[15] = get_real_or(f, "IC_magz", 0.0);
+        } else if (type == "sedov2d") {
+            d.type = HOSONO_IC_SEDOV;
+            d.c[0] = get_real(f, "IC_shockCenter_x");
+            d.c[1] = get_real(f, "IC_shockCenter_y");
+            const double rad = 3.5 * std::fmin(p->dx, p->dy);
+            const int nn = 2;
+            d.c[2] = rad;
+            d.c[3] = 3 * (gam - 1) * 1.0 / ((nn + 1) * kPi * (rad * rad));
+        } else if (type == "OrszagTang2d") {
+            d.type = HOSONO_IC_ORSZAG_TANG;
+            d.c[0] = get_real(f, "IC_U0");
+            d.c[1] = get_real(f, "IC_dens");
+            d.c[2] = get_real_or(f, "IC_B0", 1 / gam);
+            d.c[3] = get_real_or(f, "IC_pres", 1 / gam);
+        } else {
+            put_err(err, errlen, "Unrecognized choice of initial condition: " + type);
+            return HOSONO_EPAR;
+        }
+        *ic = d;
+    } catch (const Missing& m) {
+        put_err(err, errlen, "The parameter '" + m.key + "' was not found inside of '" + f.path + "'");
+        return HOSONO_EPAR;
+    }
+    return HOSONO_OK;
+}

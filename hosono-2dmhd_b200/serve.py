@@ -24,8 +24,8 @@ import time
 
 import numpy as np
 
-from . import (ETIMEOUT, FP_STRICT, HosonoError, RequestInfo, ServeConfig, ServeTotals, _p, ic_set, load_library,
-               par_gp, par_load)
+from . import (ETIMEOUT, FP_STRICT, HosonoError, RequestInfo, ServeConfig, ServeTotals, _p, ic_describe, ic_set,
+               load_library, par_gp, par_load)
 from . import problems
 
 
@@ -95,6 +95,26 @@ class Server:
             self._outputs[rid.value] = (Uo, Vo, So)
         return rid.value
 
+    def submit_ic(self, params, pv, qw, stenc, desc, xtab, ytab, tmax, nstepmax=0, want_state=True):
+        """Queue one solve whose initial state the server builds on the device
+        from ic_describe's output (O(nx+ny) host data); returns its id."""
+        nxt, nyt = params.nx + 2 * params.ngc, params.ny + 2 * params.ngc
+        pv = np.ascontiguousarray(pv, dtype=np.float64)
+        qw = np.ascontiguousarray(qw, dtype=np.float64)
+        st = np.ascontiguousarray(stenc, dtype=np.int32)
+        xt = np.ascontiguousarray(xtab, dtype=np.float64)
+        yt = np.ascontiguousarray(ytab, dtype=np.float64)
+        assert xt.size == 3 * nxt and yt.size == 2 * nyt
+        Uo = np.empty((nyt, nxt, 8)) if want_state else None
+        rid = ctypes.c_longlong()
+        self._check(self.lib.hosono_serve_submit_ic(
+            self.h, ctypes.byref(params), _p(pv), _p(qw), _p(st, ctypes.c_int), ctypes.byref(desc), _p(xt), _p(yt),
+            float(tmax), int(nstepmax), _p(Uo) if Uo is not None else None, None, None, ctypes.byref(rid)),
+            "submit_ic")
+        with self._lock:
+            self._outputs[rid.value] = (Uo, None, None)
+        return rid.value
+
     def wait(self, rid, timeout=None):
         """Block until the solve is done; returns (info dict, U, V, scheme)."""
         info = RequestInfo()
@@ -142,14 +162,18 @@ class Server:
         return s.as_dict()
 
 
-def prepare(entry, workdir):
+def prepare(entry, workdir, device_ic=False):
     """Host set-up of one manifest entry, as the reference's mhd_driver init:
-    (params, pv, qw, stenc, U, V, tmax)."""
+    (params, pv, qw, stenc, U, V, tmax); with device_ic, U and V are replaced
+    by the (ICDesc, xtab, ytab) the server builds them from on the device."""
     kv = problems.from_entry(entry)
     par = problems.make(workdir, f"req{entry['id']}", kv)
     p, run = par_load(par)
     pv, qw, st = par_gp(par, p.max_radius)
-    U, V = ic_set(par, p)
+    if device_ic:
+        U, V = None, ic_describe(par, p)
+    else:
+        U, V = ic_set(par, p)
     os.remove(par)
     return p, pv, qw, st, U, V, run.tmax
 
@@ -163,7 +187,7 @@ def percentile(xs, q):
     return xs[lo] + (xs[hi] - xs[lo]) * (k - lo)
 
 
-def run_stream(entries, rate, server, keep=(), prefetch=6, fp_mode=FP_STRICT, closed=False):
+def run_stream(entries, rate, server, keep=(), prefetch=6, fp_mode=FP_STRICT, closed=False, device_ic=False):
     """Submit `entries` with arrival gaps entry['gap'] / rate seconds (open
     loop), or all at once (closed=True); wait for every solve.  Returns the
     report dict and {id in keep: final U}."""
@@ -175,7 +199,7 @@ def run_stream(entries, rate, server, keep=(), prefetch=6, fp_mode=FP_STRICT, cl
     def producer():
         try:
             for e in entries:
-                p, pv, qw, st, U, V, tmax = prepare(e, work)
+                p, pv, qw, st, U, V, tmax = prepare(e, work, device_ic)
                 p.fp_mode = fp_mode
                 ready.put((e, p, pv, qw, st, U, V, tmax))
         except Exception as exc:  # surfaced by the submitter
@@ -200,7 +224,10 @@ def run_stream(entries, rate, server, keep=(), prefetch=6, fp_mode=FP_STRICT, cl
                 if wait <= 0:
                     break
                 time.sleep(min(wait, 0.05))
-        rid = server.submit(p, pv, qw, st, U, V, tmax, want_state=e["id"] in keep)
+        if device_ic:
+            rid = server.submit_ic(p, pv, qw, st, *V, tmax, want_state=e["id"] in keep)
+        else:
+            rid = server.submit(p, pv, qw, st, U, V, tmax, want_state=e["id"] in keep)
         ids.append((e, rid, due))
     th.join()
     kept = {}

@@ -119,6 +119,24 @@ int hosono_par_gp(const char* parfile, double* pv, double* qw, int* stenc, char*
  * (default 0). */
 int hosono_ic_set(const char* parfile, const hosono_params* p, double* U, double* V, char* err, int errlen);
 
+/* initialCondition_set for the device: a problem's initial state as a few
+ * constants and per-row / per-column tables (the only libm terms, sines of
+ * the Orszag-Tang state, are evaluated here on the host), from which
+ * hosono_gpu_ic / hosono_batch_ic / hosono_serve_submit_ic build U and V on
+ * the GPU with the same bits as hosono_ic_set (src/initialCondition.f90:
+ * 86-226, then the boundary fill).  O(nx+ny) host work and transfer instead
+ * of O(nx*ny).  xtab: 3*(nx+2*ngc) doubles, ytab: 2*(ny+2*ngc) doubles. */
+#define HOSONO_IC_EXPLOSION 1   /* explosion2d (plus IC_magx/y/z) */
+#define HOSONO_IC_SEDOV 2       /* sedov2d */
+#define HOSONO_IC_ORSZAG_TANG 3 /* OrszagTang2d (plus IC_B0, IC_pres) */
+typedef struct hosono_ic_desc {
+    int type;    /* HOSONO_IC_* */
+    int pad;
+    double c[16]; /* the problem's constants (centre, radius, inside/outside states, ...) */
+} hosono_ic_desc;
+int hosono_ic_describe(const char* parfile, const hosono_params* p, hosono_ic_desc* ic, double* xtab, double* ytab,
+                       char* err, int errlen);
+
 /* ---------------------------------------------------------------- solver */
 
 /* Allocate a device instance (gridBlock_t + gridState_t of grid.f90:88-89
@@ -132,6 +150,8 @@ int hosono_gpu_destroy(hosono_handle* h);
  * on upload (then V = cons2prim(U) on every cell).  Any download pointer
  * may be NULL. */
 int hosono_gpu_upload(hosono_handle* h, const double* U, const double* V);
+/* the initial state built on the device from hosono_ic_describe's output */
+int hosono_gpu_ic(hosono_handle* h, const hosono_ic_desc* ic, const double* xtab, const double* ytab);
 int hosono_gpu_download(hosono_handle* h, double* U, double* V, int* scheme);
 
 /* cfl_computedt (src/cfl.f90:14-52) on the resident state. */
@@ -209,6 +229,7 @@ int hosono_batch_add(hosono_batch* b, const hosono_params* p, const double* pv, 
                      int* slot);
 int hosono_batch_remove(hosono_batch* b, int slot);
 int hosono_batch_upload(hosono_batch* b, int slot, const double* U, const double* V);
+int hosono_batch_ic(hosono_batch* b, int slot, const hosono_ic_desc* ic, const double* xtab, const double* ytab);
 int hosono_batch_download(hosono_batch* b, int slot, double* U, double* V, int* scheme);
 int hosono_batch_set_time(hosono_batch* b, int slot, double t, double tmax, int nstep, int nstepmax);
 /* every live, unfinished instance steps until its tmax/nstepmax, or at most
@@ -332,6 +353,11 @@ int hosono_serve_destroy(hosono_server* s);
 int hosono_serve_submit(hosono_server* s, const hosono_params* p, const double* pv, const double* qw, const int* stenc,
                         const double* U, const double* V, double tmax, int nstepmax, double* U_out, double* V_out,
                         int* scheme_out, long long* id);
+/* the same with the initial state described by hosono_ic_describe (tables
+ * copied): the server builds it on the device at admission */
+int hosono_serve_submit_ic(hosono_server* s, const hosono_params* p, const double* pv, const double* qw,
+                           const int* stenc, const hosono_ic_desc* ic, const double* xtab, const double* ytab,
+                           double tmax, int nstepmax, double* U_out, double* V_out, int* scheme_out, long long* id);
 /* block until the solve is done (HOSONO_ETIMEOUT after timeout_s; < 0: no limit) */
 int hosono_serve_wait(hosono_server* s, long long id, double timeout_s, hosono_request_info* info);
 /* ids of solves finished since the last poll (up to cap) */
