@@ -118,3 +118,28 @@ def test_oversized_solve_refused_and_shutdown_cancels(tmp_par_dir):
     s.close()
     th.join(30)
     assert out and out[0][0]["status"] == m.ECANCELED
+
+
+@pytest.mark.gpu
+def test_failed_solve_is_isolated(tmp_par_dir):
+    """A solve with a negative CFL number gets a negative first dt, which
+    validTimeStep rejects: it leaves with HOSONO_ENANDT at step 0 while the
+    solves resident beside it finish unchanged.  (NaN wave speeds would not
+    do: the CFL maximum, like the oracle's, is an fmax that drops NaN.)"""
+    m = pkg.load()
+    srv = _serve()
+    good = [ENTRIES[0], ENTRIES[3]]
+    prepared = [srv.prepare(e, tmp_par_dir) for e in good]
+    p, pv, qw, st, U0, V0, tmax = srv.prepare(dict(ENTRIES[2], id=9), tmp_par_dir)
+    p = type(p).from_buffer_copy(p)
+    p.cfl = -abs(p.cfl)
+    with srv.Server() as s:
+        ids = [s.submit(*prep) for prep in prepared]
+        bid = s.submit(p, pv, qw, st, U0, V0, tmax)
+        infos = [s.wait(i) for i in ids]
+        binfo = s.wait(bid)[0]
+    assert binfo["status"] == m.ENANDT and binfo["nstep"] == 0
+    for e, (info, U, _, _) in zip(good, infos):
+        assert info["status"] == 0
+        Uo, _, _ = _oracle_final(e, tmp_par_dir)
+        np.testing.assert_array_equal(U, Uo)
