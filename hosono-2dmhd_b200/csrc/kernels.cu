@@ -231,15 +231,19 @@ __device__ __forceinline__ void gp_face_s(const double* __restrict__ sU, int sx,
 // one face (both sides, every quadrature point); returns the side verdict bits
 // (the Gauss sum of the fluxes accumulates in this thread's column of
 // shared memory, acc[v * NTHREADS], which keeps it out of the registers the
-// Riemann solver needs)
-template <int R, int DIR>
+// Riemann solver needs).  dir is a run-time value: the kernel holds one copy
+// of this code (and of the Riemann solver) for both face directions, which
+// halves its instruction footprint.
+template <int R>
 __device__ __forceinline__ uint8_t pass1_face(const InstDev& d, const double* __restrict__ sU, int sx, int sy,
-                                              bool needL, bool needR, bool doFlux, long long c, double* acc) {
+                                              int dir, bool needL, bool needR, bool doFlux, long long c,
+                                              double* acc) {
     const Geo& G = d.geo;
     const Phys& P = d.phys;
     constexpr int NQ = R + 1;
-    constexpr int FL = DIR == XDIR ? EAST : NORTH, FR = DIR == XDIR ? WEST : SOUTH;
-    const int lx = DIR == XDIR ? sx - 1 : sx, ly = DIR == XDIR ? sy : sy - 1;
+    const bool x = dir == XDIR;
+    const int FL = x ? EAST : NORTH, FR = x ? WEST : SOUTH;
+    const int lx = x ? sx - 1 : sx, ly = x ? sy : sy - 1;
     uint8_t bits = 0;
 #pragma unroll
     for (int v = 0; v < NCONS; v++) acc[v * NTHREADS] = 0.0;
@@ -256,17 +260,17 @@ __device__ __forceinline__ uint8_t pass1_face(const InstDev& d, const double* __
         }
         if (doFlux) {
             double F[NCONS];
-            hllc(P, uL, uR, DIR, F);
+            hllc(P, uL, uR, dir, F);
             const double w = qw_at(d, R, q);
 #pragma unroll
             for (int v = 0; v < NCONS; v++) acc[v * NTHREADS] = acc[v * NTHREADS] + w * F[v];
         }
     }
     if (doFlux) {
-        double* Fo = DIR == XDIR ? d.FX : d.FY;
+        double* Fo = x ? d.FX : d.FY;
 #pragma unroll
         for (int v = 0; v < NCONS; v++) Fo[v * G.plane + c] = acc[v * NTHREADS];
-        (DIR == XDIR ? d.CTX : d.CTY)[c] = acc[(DIR == XDIR ? MAGY : MAGX) * NTHREADS];
+        (x ? d.CTX : d.CTY)[c] = acc[(x ? MAGY : MAGX) * NTHREADS];
     }
     return bits;
 }
@@ -350,15 +354,15 @@ __global__ void __launch_bounds__(NTHREADS, HOSONO_PASS1_MIN_BLOCKS) k_face_pass
         const long long cc = (long long)j * G.pitch + i;
         const bool inF = i >= flo && i <= fxhi && j >= flo && j <= fyhi;
         bool bad = false;
-        if (i >= clo && i <= cxhi + 1 && j >= clo && j <= cyhi) {  // x-face
-            const uint8_t bits = pass1_face<R, XDIR>(d, sU, sx, sy, i - 1 >= clo, i <= cxhi, inF, cc, acc);
-            d.failX[cc] = bits;
-            bad |= bits != 0;
-        }
-        if (i >= clo && i <= cxhi && j >= clo && j <= cyhi + 1) {  // y-face
-            const uint8_t bits = pass1_face<R, YDIR>(d, sU, sx, sy, j - 1 >= clo, j <= cyhi, inF, cc, acc);
-            d.failY[cc] = bits;
-            bad |= bits != 0;
+#pragma unroll 1
+        for (int dir = XDIR; dir <= YDIR; dir++) {  // the x-face, then the y-face of this cell
+            const bool x = dir == XDIR;
+            if (i >= clo && i <= cxhi + (x ? 1 : 0) && j >= clo && j <= cyhi + (x ? 0 : 1)) {
+                const int a = x ? i : j, ahi = x ? cxhi : cyhi;
+                const uint8_t bits = pass1_face<R>(d, sU, sx, sy, dir, a - 1 >= clo, a <= ahi, inF, cc, acc);
+                (x ? d.failX : d.failY)[cc] = bits;
+                bad |= bits != 0;
+            }
         }
         warp_flag(&S.anyFail, bad);
         __syncthreads();  // every read of this box is done before it is refilled

@@ -225,26 +225,33 @@ __device__ __forceinline__ void side_flux(const Phys& s, const double* U, const 
     if (!s.force_hydro) Bp = 0.5 * (U[MAGX] * U[MAGX] + U[MAGY] * U[MAGY] + U[MAGZ] * U[MAGZ]);
     const double E = U[ENER];
     const double Ptot = V.p + Bp;
-    const int mN = dir == XDIR ? MOMX : MOMY, mT1 = dir == XDIR ? MOMY : MOMX, mT2 = MOMZ;
-    const int bN = dir == XDIR ? MAGX : MAGY, bT1 = dir == XDIR ? MAGY : MAGX, bT2 = MAGZ;
+    // normal (N) and tangential (T1, T2 = z) components; the array slots are
+    // chosen by selects, so a run-time dir keeps F and U in registers
+    const bool x = dir == XDIR;
     const double vN = side_vel(V, dir), vT1 = side_vel(V, 1 - dir), vT2 = V.vz;
     const double BN = side_mag(V, dir), BT1 = side_mag(V, 1 - dir), BT2 = V.bz;
-    F[DENS] = U[mN];
-    F[mN] = dv.div(U[mN] * U[mN], V.rrho) + Ptot;
-    F[mT1] = U[mN] * vT1;
-    F[mT2] = U[mN] * vT2;
-    F[ENER] = (E + Ptot) * vN;
-    F[bN] = 0.0;
-    F[bT1] = 0.0;
-    F[bT2] = 0.0;
+    const double mN = x ? U[MOMX] : U[MOMY];
+    double fN = dv.div(mN * mN, V.rrho) + Ptot;
+    double fT1 = mN * vT1;
+    double fT2 = mN * vT2;
+    double fE = (E + Ptot) * vN;
+    double gT1 = 0.0, gT2 = 0.0;  // induction fluxes; the normal one is 0
     if (!s.force_hydro) {
-        F[mN] = F[mN] - BN * BN;
-        F[mT1] = F[mT1] - BT1 * BN;
-        F[mT2] = F[mT2] - BT2 * BN;
-        F[bT1] = vN * BT1 - vT1 * BN;
-        F[bT2] = vN * BT2 - vT2 * BN;
-        F[ENER] = F[ENER] - BN * (V.vx * V.bx + V.vy * V.by + V.vz * V.bz);
+        fN = fN - BN * BN;
+        fT1 = fT1 - BT1 * BN;
+        fT2 = fT2 - BT2 * BN;
+        gT1 = vN * BT1 - vT1 * BN;
+        gT2 = vN * BT2 - vT2 * BN;
+        fE = fE - BN * (V.vx * V.bx + V.vy * V.by + V.vz * V.bz);
     }
+    F[DENS] = mN;
+    F[MOMX] = x ? fN : fT1;
+    F[MOMY] = x ? fT1 : fN;
+    F[MOMZ] = fT2;
+    F[ENER] = fE;
+    F[MAGX] = x ? 0.0 : gT1;
+    F[MAGY] = x ? gT1 : 0.0;
+    F[MAGZ] = gT2;
 }
 
 // src/riemannSolver.f90:68-221 (HLLC for MHD, Li 2005).  Every value keeps
@@ -258,8 +265,9 @@ __device__ __forceinline__ void hllc_t(const Phys& s, const double* uL, const do
     Side<D> L, R;
     side_prim(s, uL, L, dv);
     side_prim(s, uR, R, dv);
-    const int mN = dir == XDIR ? MOMX : MOMY, mT1 = dir == XDIR ? MOMY : MOMX, mT2 = MOMZ;
-    const int bN = dir == XDIR ? MAGX : MAGY, bT1 = dir == XDIR ? MAGY : MAGX, bT2 = MAGZ;
+    // array slots of the normal / first tangential components are chosen by
+    // selects, so a run-time dir keeps every array in registers
+    const bool x = dir == XDIR;
     const double velNL = side_vel(L, dir), velNR = side_vel(R, dir);
     const double magNL = side_mag(L, dir), magNR = side_mag(R, dir);
     // eigenvalues 1 and 7 of L, R and the arithmetic average (riemannSolver.f90:84-96)
@@ -277,7 +285,8 @@ __device__ __forceinline__ void hllc_t(const Phys& s, const double* uL, const do
     const double pTotL = L.p + 0.5 * dot3(L.bx, L.by, L.bz, L.bx, L.by, L.bz);
     const double pTotR = R.p + 0.5 * dot3(R.bx, R.by, R.bz, R.bx, R.by, R.bz);
     const double dL = sL - velNL, dR = sR - velNR;
-    const double sStr = (uR[mN] * dR - uL[mN] * dL + pTotL - pTotR - magNL * magNL + magNR * magNR) /
+    const double mNL = x ? uL[MOMX] : uL[MOMY], mNR = x ? uR[MOMX] : uR[MOMY];
+    const double sStr = (mNR * dR - mNL * dL + pTotL - pTotR - magNL * magNL + magNR * magNR) /
                         (rhoR * dR - rhoL * dL);
     // final choice (riemannSolver.f90:189-219): fL if 0 < sL; left star state
     // if sL <= 0 < sStr; right star state if sStr <= 0 <= sR; fR otherwise.
@@ -310,7 +319,8 @@ __device__ __forceinline__ void hllc_t(const Phys& s, const double* uL, const do
     const double velHy = dv.div(uHLL[MOMY], rH);
     const double velHz = dv.div(uHLL[MOMZ], rH);
     const double magDotVelHLL = dot3(uHLL[MAGX], uHLL[MAGY], uHLL[MAGZ], velHx, velHy, velHz);
-    const double magNHLL = uHLL[bN];
+    const double magNHLL = x ? uHLL[MAGX] : uHLL[MAGY];
+    const double magT1HLL = x ? uHLL[MAGY] : uHLL[MAGX];
     const double pStr = rhoL * dL * (sStr - velNL) + pTotL - magNL * magNL + magNHLL * magNHLL;
     const bool left = side == 1;
     const Side<D>& K = left ? L : R;
@@ -326,12 +336,15 @@ __device__ __forceinline__ void hllc_t(const Phys& s, const double* uL, const do
     const typename D::R rK = dv.recip(sK - sStr);
     double uStr[NCONS];
     uStr[DENS] = dv.div(K.rho * dK, rK);
-    uStr[mN] = uStr[DENS] * sStr;
-    uStr[mT1] = uStr[DENS] * vT1K - dv.div(magNHLL * uHLL[bT1] - magNK * bT1K, rK);
-    uStr[mT2] = uStr[DENS] * vT2K - dv.div(magNHLL * uHLL[bT2] - magNK * bT2K, rK);
-    uStr[bN] = magNHLL;
-    uStr[bT1] = uHLL[bT1];
-    uStr[bT2] = uHLL[bT2];
+    const double sN = uStr[DENS] * sStr;
+    const double sT1 = uStr[DENS] * vT1K - dv.div(magNHLL * magT1HLL - magNK * bT1K, rK);
+    const double sT2 = uStr[DENS] * vT2K - dv.div(magNHLL * uHLL[MAGZ] - magNK * bT2K, rK);
+    uStr[MOMX] = x ? sN : sT1;
+    uStr[MOMY] = x ? sT1 : sN;
+    uStr[MOMZ] = sT2;
+    uStr[MAGX] = x ? magNHLL : magT1HLL;
+    uStr[MAGY] = x ? magT1HLL : magNHLL;
+    uStr[MAGZ] = uHLL[MAGZ];
     uStr[ENER] = eK * dK + pStr * sStr - pTotK * velNK - magNHLL * magDotVelHLL + magNK * magDotVelK;
     uStr[ENER] = dv.div(uStr[ENER], rK);
 #pragma unroll
