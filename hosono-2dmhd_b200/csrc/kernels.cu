@@ -944,7 +944,10 @@ __device__ __forceinline__ void t_ct_update_detect(const Batch& B, int uin, int 
     warp_count(&S.nDetect, low);
     warp_append(B.L, LIST_LOW, B.L.low, B.L.cap, low, entry(c.k, cc));
 }
-__global__ void __launch_bounds__(NTHREADS) k_ct_update_detect(Batch B, int uin, int uout) {
+// four resident blocks (a 64-register budget): the tile's loads wait at two
+// barriers, so more warps in flight keep HBM busier (80 registers and three
+// blocks were 2 % slower per step on Orszag-Tang 2048^2)
+__global__ void __launch_bounds__(NTHREADS, 4) k_ct_update_detect(Batch B, int uin, int uout) {
     __shared__ double sV[4 * DP_SX * DP_SY];
     FOR_TILES(B, t) t_ct_update_detect(B, uin, uout, tile_at(B, t), sV);
 }
