@@ -73,50 +73,11 @@ __device__ __forceinline__ double cons2pres(const Phys& s, const double* U) {
     return (s.gamma - 1.0) * (U[ENER] - Bp - 0.5 * msq / U[DENS]);
 }
 
-// src/convert.f90:28-92
-__device__ __forceinline__ void cons2flux(const Phys& s, const double* U, const double* V, int dir, double* F) {
-    double Bp = 0.0;
-    if (!s.force_hydro) Bp = 0.5 * (U[MAGX] * U[MAGX] + U[MAGY] * U[MAGY] + U[MAGZ] * U[MAGZ]);
-    const double E = U[ENER];
-    const double Ptot = V[PRES] + Bp;
-    const int mN = dir == XDIR ? MOMX : MOMY, mT1 = dir == XDIR ? MOMY : MOMX, mT2 = MOMZ;
-    const int vN = mN, vT1 = mT1, vT2 = mT2;  // velocity indices equal momentum indices
-    const int bN = dir == XDIR ? MAGX : MAGY, bT1 = dir == XDIR ? MAGY : MAGX, bT2 = MAGZ;
-#pragma unroll
-    for (int v = 0; v < NCONS; v++) F[v] = 0.0;
-    F[DENS] = U[mN];
-    F[mN] = U[mN] * U[mN] / U[DENS] + Ptot;
-    F[mT1] = U[mN] * V[vT1];
-    F[mT2] = U[mN] * V[vT2];
-    F[ENER] = (E + Ptot) * V[vN];
-    if (!s.force_hydro) {
-        F[mN] = F[mN] - V[bN] * V[bN];
-        F[mT1] = F[mT1] - V[bT1] * V[bN];
-        F[mT2] = F[mT2] - V[bT2] * V[bN];
-        F[bT1] = V[vN] * V[bT1] - V[vT1] * V[bN];
-        F[bT2] = V[vN] * V[bT2] - V[vT2] * V[bN];
-        F[ENER] = F[ENER] - V[bN] * (V[VELX] * V[MAGX] + V[VELY] * V[MAGY] + V[VELZ] * V[MAGZ]);
-    }
-}
-
 // src/eigen.f90:305-321 (Ryu & Jones 1995, eqs. 2.18-2.19)
 __device__ __forceinline__ double c_fs(double gam, double rho, double p, double BB, double B_N, double pm) {
     double c = (gam * p + BB) / rho;
     c = 0.5 * (c + pm * sqrt(c * c - 4.0 * gam * p * (B_N * B_N) / (rho * rho)));
     return sqrt(fmax(1.0e-14, c));
-}
-
-// src/eigen.f90:257-303, eigenvalues 1 and 7 (the only ones HLLC uses)
-__device__ __forceinline__ void fast_speeds(const Phys& s, const double* V, int dir, double& lam1, double& lam7) {
-    const double rho = fmax(V[DENS], s.small_density);
-    const double velN = V[VELX + dir];
-    const double B_N = V[MAGX + dir];
-    const double p = fmax(V[PRES], s.small_pressure);
-    const double gam = V[GAMM];
-    const double BB = V[MAGX] * V[MAGX] + V[MAGY] * V[MAGY] + V[MAGZ] * V[MAGZ];
-    const double cf = c_fs(gam, rho, p, BB, B_N, +1.0);
-    lam1 = velN - cf;
-    lam7 = velN + cf;
 }
 
 __device__ __forceinline__ double dot3(double a0, double a1, double a2, double b0, double b1, double b2) {
