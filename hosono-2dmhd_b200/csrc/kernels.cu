@@ -202,10 +202,15 @@ struct P1Box {
     static constexpr int PLANE = SX * SY;
     static constexpr int DOUBLES = NCONS * PLANE;
     static constexpr int OX = 4, OY = 1 + R;       // shared coordinates of the tile origin
+    // the instance's radius-R prediction vectors pv(k, q, face) (the rr = R
+    // block of its (nsMax, nqMax, 4, R) table, nsMax = NS, nqMax = NQ)
+    static constexpr int NS = 1 + 2 * R * (R + 1), NQ = R + 1;
+    static constexpr int PVN = NS * NQ * 4;
 };
 
 // GP prediction from the shared box: sum_k pv(k,q,f,RR) * U(:, stencil_k)
-// around shared coordinates (sx, sy), stencil order k=1..ns
+// around shared coordinates (sx, sy), stencil order k=1..ns; pvq points at
+// the prediction vector in shared memory (one broadcast load per k)
 template <int RR, int R>
 __device__ __forceinline__ void gp_face_s(const double* __restrict__ sU, int sx, int sy,
                                           const double* __restrict__ pvq, double out[NCONS]) {
@@ -219,7 +224,7 @@ __device__ __forceinline__ void gp_face_s(const double* __restrict__ sU, int sx,
 #pragma unroll
         for (int b = -RR; b <= RR; b++) {
             if (iabs_c(a) + iabs_c(b) <= RR) {
-                const double p = __ldg(pvq + k);
+                const double p = pvq[k];
 #pragma unroll
                 for (int v = 0; v < NCONS; v++) out[v] = out[v] + p * base[v * PL + b * SX + a];
                 k++;
@@ -235,9 +240,9 @@ __device__ __forceinline__ void gp_face_s(const double* __restrict__ sU, int sx,
 // of this code (and of the Riemann solver) for both face directions, which
 // halves its instruction footprint.
 template <int R>
-__device__ __forceinline__ uint8_t pass1_face(const InstDev& d, const double* __restrict__ sU, int sx, int sy,
-                                              int dir, bool needL, bool needR, bool doFlux, long long c,
-                                              double* acc) {
+__device__ __forceinline__ uint8_t pass1_face(const InstDev& d, const double* __restrict__ sU,
+                                              const double* __restrict__ sPv, int sx, int sy, int dir, bool needL,
+                                              bool needR, bool doFlux, long long c, double* acc) {
     const Geo& G = d.geo;
     const Phys& P = d.phys;
     constexpr int NQ = R + 1;
@@ -251,11 +256,11 @@ __device__ __forceinline__ uint8_t pass1_face(const InstDev& d, const double* __
     for (int q = 0; q < NQ; q++) {
         double uL[NCONS], uR[NCONS];
         if (needL) {
-            gp_face_s<R, R>(sU, lx, ly, pv_ptr(d, R, FL, q), uL);
+            gp_face_s<R, R>(sU, lx, ly, sPv + P1Box<R>::NS * (q + P1Box<R>::NQ * FL), uL);
             if (!admissible(uL[DENS], cons2pres(P, uL))) bits |= 1;
         }
         if (needR) {
-            gp_face_s<R, R>(sU, sx, sy, pv_ptr(d, R, FR, q), uR);
+            gp_face_s<R, R>(sU, sx, sy, sPv + P1Box<R>::NS * (q + P1Box<R>::NQ * FR), uR);
             if (!admissible(uR[DENS], cons2pres(P, uR))) bits |= 2;
         }
         if (doFlux) {
@@ -281,6 +286,11 @@ __device__ __forceinline__ void cp_async16(void* dst, const void* src, int src_b
     const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(src), "r"(src_bytes) : "memory");
 }
+// 8-byte asynchronous copy global -> shared (cp.async.ca: 4, 8 or 16 bytes)
+__device__ __forceinline__ void cp_async8(void* dst, const void* src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
@@ -295,9 +305,10 @@ __device__ __forceinline__ int pass1_next(const Batch& B, int t, int n) {
     return n;
 }
 
-// stage tile t's stencil box (zeros outside the array) into dst
+// stage tile t's stencil box (zeros outside the array) into dst and its
+// instance's radius-R prediction vectors into dstPv (one commit group)
 template <int R>
-__device__ __forceinline__ void pass1_stage(const Batch& B, int uin, int t, double* dst, int tid) {
+__device__ __forceinline__ void pass1_stage(const Batch& B, int uin, int t, double* dst, double* dstPv, int tid) {
     using Box = P1Box<R>;
     const int4 tl = B.tiles[t];
     const InstDev& d = B.dev[tl.x];
@@ -313,34 +324,38 @@ __device__ __forceinline__ void pass1_stage(const Batch& B, int uin, int t, doub
         const double* src = in ? U + v * G.plane + (long long)gy * G.pitch + gx : U;
         cp_async16(dst + v * Box::PLANE + yy * Box::SX + xx, src, in ? 16 : 0);
     }
+    const double* pv = d.pv + (long long)Box::PVN * (R - 1);  // geo.R == R: nsMax = NS, nqMax = NQ
+    for (int e = tid; e < Box::PVN; e += NTHREADS) cp_async8(dstPv + e, pv + e);
     cp_async_commit();
 }
 
 // One launch per radius: blocks skip tiles of instances with another GP
-// radius.  Shared memory: two stencil boxes (the next tile's box is copied in
-// asynchronously while the current one is computed) and the per-thread flux
-// accumulators.
+// radius.  Shared memory: two stencil boxes with their prediction vectors
+// (the next tile's are copied in asynchronously while the current one is
+// computed) and the per-thread flux accumulators.
 template <int R>
 __global__ void __launch_bounds__(NTHREADS, HOSONO_PASS1_MIN_BLOCKS) k_face_pass1(Batch B, int uin) {
     extern __shared__ double smem[];
     using Box = P1Box<R>;
     const int tid = threadIdx.y * TILE_X + threadIdx.x;
     double* acc = smem + 2 * Box::DOUBLES + tid;
+    double* pvBuf = smem + 2 * Box::DOUBLES + NCONS * NTHREADS;  // two PVN-double buffers
     if (!(B.flags->radii & (1 << R))) return;  // no instance of this radius
     const int n = __ldg(B.ntiles);
     int t = pass1_next<R>(B, blockIdx.x, n);
     int buf = 0;
-    if (t < n) pass1_stage<R>(B, uin, t, smem, tid);
+    if (t < n) pass1_stage<R>(B, uin, t, smem, pvBuf, tid);
     while (t < n) {
         const int tn = pass1_next<R>(B, t + gridDim.x, n);
         if (tn < n) {
-            pass1_stage<R>(B, uin, tn, smem + (buf ^ 1) * Box::DOUBLES, tid);
+            pass1_stage<R>(B, uin, tn, smem + (buf ^ 1) * Box::DOUBLES, pvBuf + (buf ^ 1) * Box::PVN, tid);
             cp_async_wait<1>();
         } else {
             cp_async_wait<0>();
         }
         __syncthreads();  // tile t's box is in place for every thread
         const double* sU = smem + buf * Box::DOUBLES;
+        const double* sPv = pvBuf + buf * Box::PVN;
         const Cell c = tile_at(B, t);
         InstState& S = B.st[c.k];
         const InstDev& d = B.dev[c.k];
@@ -359,7 +374,8 @@ __global__ void __launch_bounds__(NTHREADS, HOSONO_PASS1_MIN_BLOCKS) k_face_pass
             const bool x = dir == XDIR;
             if (i >= clo && i <= cxhi + (x ? 1 : 0) && j >= clo && j <= cyhi + (x ? 0 : 1)) {
                 const int a = x ? i : j, ahi = x ? cxhi : cyhi;
-                const uint8_t bits = pass1_face<R>(d, sU, sx, sy, dir, a - 1 >= clo, a <= ahi, inF, cc, acc);
+                const uint8_t bits =
+                    pass1_face<R>(d, sU, sPv, sx, sy, dir, a - 1 >= clo, a <= ahi, inF, cc, acc);
                 (x ? d.failX : d.failY)[cc] = bits;
                 bad |= bits != 0;
             }
@@ -1510,7 +1526,7 @@ void l_step_end(const Batch& B, cudaGraphConditionalHandle h, cudaStream_t s) {
 void l_stage_init(const Batch& B, cudaStream_t s) { TILE_LAUNCH(k_stage_init, B, s); }
 template <int R>
 void launch_pass1(const Batch& B, int uin, cudaStream_t s) {
-    constexpr int smem = (2 * P1Box<R>::DOUBLES + NCONS * NTHREADS) * (int)sizeof(double);
+    constexpr int smem = (2 * P1Box<R>::DOUBLES + NCONS * NTHREADS + 2 * P1Box<R>::PVN) * (int)sizeof(double);
     static const bool attr =  // once per process (thread-safe static initialisation)
         cudaFuncSetAttribute((const void*)k_face_pass1<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) ==
         cudaSuccess;
