@@ -2,7 +2,7 @@
 src/output.f90:230-274) against the same expressions evaluated in numpy on
 the state V (host copy): every field bit for bit, and the div(B) norms; at
 t_end of Orszag-Tang 128^2 R=1 the GPU's divB equals the one of the oracle's
-final state (the north star asks for within 2x)."""
+final state (the accuracy gate only asks for within 2x)."""
 import numpy as np
 import pytest
 
