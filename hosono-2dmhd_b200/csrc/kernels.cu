@@ -960,10 +960,11 @@ __device__ __forceinline__ void t_ct_update_detect(const Batch& B, int uin, int 
     warp_count(&S.nDetect, low);
     warp_append(B.L, LIST_LOW, B.L.low, B.L.cap, low, entry(c.k, cc));
 }
-// four resident blocks (a 64-register budget): the tile's loads wait at two
-// barriers, so more warps in flight keep HBM busier (80 registers and three
-// blocks were 2 % slower per step on Orszag-Tang 2048^2)
-__global__ void __launch_bounds__(NTHREADS, 4) k_ct_update_detect(Batch B, int uin, int uout) {
+// six resident blocks (a 40-register budget, a few hundred bytes of spills):
+// the tile's loads wait at two barriers, so more warps in flight keep HBM
+// busier.  Per step on Orszag-Tang 2048^2: 3 blocks (80 registers) 11.66 ms,
+// 4 blocks 11.23 ms, 5 blocks 11.14 ms, 6 blocks 11.08 ms.
+__global__ void __launch_bounds__(NTHREADS, 6) k_ct_update_detect(Batch B, int uin, int uout) {
     __shared__ double sV[4 * DP_SX * DP_SY];
     FOR_TILES(B, t) t_ct_update_detect(B, uin, uout, tile_at(B, t), sV);
 }
