@@ -1057,7 +1057,9 @@ __device__ __forceinline__ void t_mood_flags(const Batch& B, const Cell c) {
     warp_append(B.L, rec_count(B, true), rec_list(B, true), B.L.cap, newRec && inRec,
                 entry(c.k, (long long)j * G.pitch + i));
 }
-__global__ void __launch_bounds__(NTHREADS) k_mood_flags(Batch B) {
+// eight resident blocks (32 registers): a latency-bound byte-gather over the
+// lowered flags, faster with more warps in flight
+__global__ void __launch_bounds__(NTHREADS, 8) k_mood_flags(Batch B) {
     FOR_TILES(B, t) t_mood_flags(B, tile_at(B, t));
 }
 
@@ -1344,7 +1346,8 @@ __device__ __forceinline__ void t_rk_final(const Batch& B, const Cell c) {
 #pragma unroll
     for (int v = 0; v < NPRIM; v++) d.V[v * G.plane + cc] = V[v];
 }
-__global__ void __launch_bounds__(NTHREADS) k_rk_final(Batch B) {
+// six resident blocks (40 registers) for more loads in flight
+__global__ void __launch_bounds__(NTHREADS, 6) k_rk_final(Batch B) {
     FOR_TILES(B, t) t_rk_final(B, tile_at(B, t));
 }
 
