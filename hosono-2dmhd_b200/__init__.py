@@ -102,6 +102,8 @@ SIGNATURES = {
     "hosono_gp_build": [_i, _cp, _cp, _i, _cp, _cp, _i, _cp, _dp, _dp, _ip],
     "hosono_par_load": [_cp, ctypes.POINTER(Params), ctypes.POINTER(RunInfo), _cp, _i],
     "hosono_par_gp": [_cp, _dp, _dp, _ip, _cp, _i],
+    "hosono_gp_cache_info": [ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong), _ip],
+    "hosono_gp_cache_clear": [],
     "hosono_ic_set": [_cp, ctypes.POINTER(Params), _dp, _dp, _cp, _i],
     "hosono_gpu_create": [ctypes.POINTER(Params), _dp, _dp, _ip, ctypes.POINTER(_vp)],
     "hosono_gpu_destroy": [_vp],
@@ -229,6 +231,18 @@ def par_load(parfile):
     if rc:
         raise HosonoError(rc, err.value.decode())
     return p, r
+
+
+def gp_cache_info():
+    """Hits, misses and entries of the library's GP table cache."""
+    lib = load_library()
+    h, m, n = ctypes.c_longlong(), ctypes.c_longlong(), ctypes.c_int()
+    lib.hosono_gp_cache_info(ctypes.byref(h), ctypes.byref(m), ctypes.byref(n))
+    return dict(hits=h.value, misses=m.value, entries=n.value)
+
+
+def gp_cache_clear():
+    load_library().hosono_gp_cache_clear()
 
 
 def par_gp(parfile, radius):

@@ -1,7 +1,8 @@
 // gp_setup.cpp -- GP prediction vectors on the host, in quad precision
 // (GP_init, src/GP.f90:37-200, with the SPD solve of
-// src/linAlgQuadPrecision.f90:107-365).  Built once per (radius, ell/Delta,
-// dx, dy) and uploaded; the per-cell work never touches quad precision.
+// src/linAlgQuadPrecision.f90:107-365).  Built once per (radius, dx, dy,
+// ell) -- later requests with the same values are served from a cache -- and
+// uploaded; the per-cell work never touches quad precision.
 //
 // Every quad operation is one correctly rounded libquadmath/soft-float
 // operation in the order the Fortran statement evaluates it, and the final
@@ -14,6 +15,8 @@
 
 #include <cmath>
 #include <cstdlib>
+#include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -130,7 +133,59 @@ void quadrature(int rr, std::vector<quad>& x, double* w) {
     }
 }
 
+// Process-wide cache of built tables.  The tables are a deterministic
+// function of (R, dx, dy, ell) as the quad values computed from the inputs,
+// so the key is those values' bits: a hit returns exactly the bits a fresh
+// build would (and two inputs that give the same spacing, such as [0,1] and
+// [-0.5,0.5] at equal N, share an entry).  Bounded, oldest entry evicted.
+struct GpKey {
+    int R;
+    unsigned char bits[3 * sizeof(quad)];
+    bool operator==(const GpKey& o) const { return R == o.R && std::memcmp(bits, o.bits, sizeof bits) == 0; }
+};
+struct GpEntry {
+    GpKey key;
+    std::vector<double> pv, qw;
+    std::vector<int> stenc;
+};
+struct GpCache {
+    static constexpr size_t CAP = 256;
+    std::mutex mu;
+    std::vector<GpEntry> entries;  // oldest first
+    long long hits = 0, misses = 0;
+};
+GpCache& gp_cache() {
+    static GpCache c;
+    return c;
+}
+GpKey gp_key(int R, quad dx, quad dy, quad ell) {
+    GpKey k;
+    std::memset(&k, 0, sizeof k);
+    k.R = R;
+    std::memcpy(k.bits, &dx, sizeof(quad));
+    std::memcpy(k.bits + sizeof(quad), &dy, sizeof(quad));
+    std::memcpy(k.bits + 2 * sizeof(quad), &ell, sizeof(quad));
+    return k;
+}
+
 }  // namespace
+
+extern "C" int hosono_gp_cache_info(long long* hits, long long* misses, int* entries) {
+    GpCache& c = gp_cache();
+    std::lock_guard<std::mutex> lk(c.mu);
+    if (hits) *hits = c.hits;
+    if (misses) *misses = c.misses;
+    if (entries) *entries = (int)c.entries.size();
+    return HOSONO_OK;
+}
+
+extern "C" int hosono_gp_cache_clear(void) {
+    GpCache& c = gp_cache();
+    std::lock_guard<std::mutex> lk(c.mu);
+    c.entries.clear();
+    c.hits = c.misses = 0;
+    return HOSONO_OK;
+}
 
 extern "C" int hosono_gp_build(int R, const char* x_beg, const char* x_end, int nx, const char* y_beg,
                                const char* y_end, int ny, const char* ell_over_delta, double* pv, double* qw,
@@ -141,6 +196,20 @@ extern "C" int hosono_gp_build(int R, const char* x_beg, const char* x_end, int 
     const quad ell = quad_from_text(ell_over_delta) * (dx < dy ? dx : dy);
     if (!(dx > 0) || !(dy > 0) || !(ell > 0)) return HOSONO_EINVAL;
     const int nsMax = 1 + 2 * R * (R + 1), nqMax = R + 1;
+    const size_t npv = (size_t)nsMax * nqMax * 4 * R, nqw = (size_t)nqMax * R, nst = (size_t)2 * nsMax * R;
+    const GpKey key = gp_key(R, dx, dy, ell);
+    GpCache& cache = gp_cache();
+    {
+        std::lock_guard<std::mutex> lk(cache.mu);
+        for (const GpEntry& e : cache.entries)
+            if (e.key == key) {
+                std::memcpy(pv, e.pv.data(), npv * sizeof(double));
+                std::memcpy(qw, e.qw.data(), nqw * sizeof(double));
+                std::memcpy(stenc, e.stenc.data(), nst * sizeof(int));
+                cache.hits++;
+                return HOSONO_OK;
+            }
+    }
     const SqExpKernel K(dx, dy, ell);
     for (size_t t = 0; t < (size_t)nsMax * nqMax * 4 * R; t++) pv[t] = 0.0;
     for (size_t t = 0; t < (size_t)nqMax * R; t++) qw[t] = 0.0;
@@ -189,6 +258,17 @@ extern "C" int hosono_gp_build(int R, const char* x_beg, const char* x_end, int 
             for (int q = 0; q < nq; q++)
                 for (int k = 0; k < ns; k++)
                     pv[k + nsMax * (q + nqMax * (f + 4 * (rr - 1)))] = (double)W[k * np + f * nq + q];
+    }
+    {
+        std::lock_guard<std::mutex> lk(cache.mu);
+        cache.misses++;
+        bool present = false;  // another thread may have built the same tables meanwhile
+        for (const GpEntry& e : cache.entries) present = present || e.key == key;
+        if (!present) {
+            if (cache.entries.size() >= GpCache::CAP) cache.entries.erase(cache.entries.begin());
+            cache.entries.push_back(GpEntry{key, std::vector<double>(pv, pv + npv), std::vector<double>(qw, qw + nqw),
+                                            std::vector<int>(stenc, stenc + nst)});
+        }
     }
     return HOSONO_OK;
 }

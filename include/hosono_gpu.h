@@ -89,6 +89,12 @@ typedef struct hosono_stats {
 int hosono_gp_build(int max_radius, const char* x_beg, const char* x_end, int nx,
                     const char* y_beg, const char* y_end, int ny, const char* ell_over_delta,
                     double* pv, double* qw, int* stenc);
+/* hosono_gp_build keeps the tables of the last 256 distinct (R, dx, dy, ell)
+ * (the quad values it computes from its inputs) and returns them again for
+ * the same values: the same bits as a fresh build, without the quad-precision
+ * solve.  No counterpart in the reference (GP_init runs once per process). */
+int hosono_gp_cache_info(long long* hits, long long* misses, int* entries);
+int hosono_gp_cache_clear(void);
 
 /* Run settings of a .par file that are not part of hosono_params. */
 typedef struct hosono_run_info {
