@@ -130,6 +130,17 @@ PASS1_PROFILE = {"workload": "ot1536_r2", "n": 1536, "radius": 2, "dram_bytes": 
                  "fp64_pipe_active_frac": 0.485}
 
 
+# Algorithmic FP64 operations of one pass-1 launch per interior cell: the
+# operation-counting build of the oracle (oracle/flopcount.h, `make -C oracle
+# count`) counts every double add, multiply, divide and square root of the
+# MOOD pass-1 reconstruction and fluxes (GP face states, face CAD/PAD, the
+# Riemann solves and their Gauss sums) over the three stages of one step;
+# per launch is a third of that.  Orszag-Tang R=2, ell/dx=12, counted at
+# 2048^2 on steps 1 and 13 (15858.3 and 15858.2 flops per zone-update).
+PASS1_FLOPS = {("ot", 2, 12.0): 15858.2 / 3}
+FP64_LANES_PER_SM = 64  # FP64 FMA lanes per B200 SM (two flops per lane per clock)
+
+
 def pass1_bytes(n, radius):
     """Algorithmic HBM bytes of one MOOD pass-1 kernel launch (n x n interior):
     read U once over the interior plus NGC guard rings (8 doubles/cell), write
@@ -354,6 +365,19 @@ def bench_ours(args, rank, world, local):
                 "fp64_pipe_active_frac": PASS1_PROFILE["fp64_pipe_active_frac"],
                 "note": "FP64 CUDA-core kernel bound by the FP64 pipe and latency (fp64_pipe_active_frac from "
                         "ncu); the HBM line is shown as the contract requires"}
+    fpc = PASS1_FLOPS.get((w.get("problem", "ot"), w["radius"], w["ell"]))
+    if fpc is not None and p1_avg > 0:
+        sms = torch.cuda.get_device_properties(local).multi_processor_count
+        mhz = (clk or {}).get("sm_max_mhz") or 1965.0
+        peak = sms * FP64_LANES_PER_SM * 2 * mhz * 1e6 / 1e12
+        tf = fpc * w["n"] * w["n"] / (p1_avg / 1e3) / 1e12
+        roofline["fp64"] = {"achieved": tf, "peak": peak, "unit": "TFLOP/s", "frac": tf / peak,
+                            "frac_of_unfused_rate": tf / (peak / 2), "flops_per_cell": fpc,
+                            "peak_kind": f"nominal: {sms} SMs x {FP64_LANES_PER_SM} FP64 lanes x 2 (FMA) x "
+                                         f"{mhz:.0f} MHz",
+                            "note": "strict arithmetic cannot contract to FMA, so one flop per lane per clock "
+                                    "(frac_of_unfused_rate) is its ceiling; flops counted by the oracle's "
+                                    "operation-counting build"}
     line = {
         "metric": "fp64_zone_updates_per_s", "value": value, "unit": "zone-updates/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,

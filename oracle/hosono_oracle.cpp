@@ -31,6 +31,11 @@
 #include <sstream>
 #include <algorithm>
 
+// phase markers for the operation-counting build (flopcount.h); no-ops here
+#ifndef FC_PHASE
+#define FC_PHASE(p) ((void)0)
+#endif
+
 namespace {
 
 // ---------------------------------------------------------------- constants
@@ -888,8 +893,10 @@ void forward_euler(orc_handle* h, double dt, const std::vector<double>& U, std::
             tr.inner.assign(b.ncell(), 0);
             tr.detect.assign(b.ncell(), 0);
         }
+        FC_PHASE(pass == 0 ? 1 : 2);
         reconstruct(h, U, h->trace ? &tr.inner : nullptr, &tr.nInner);
         getFluxes(h);
+        FC_PHASE(3);
         flicd(h);
 #pragma omp parallel for collapse(2) schedule(static)
         for (int j = b.strt[1]; j <= b.stop[1]; j++) {
@@ -911,6 +918,7 @@ void forward_euler(orc_handle* h, double dt, const std::vector<double>& U, std::
         if (h->trace) h->traces.push_back(std::move(tr));
         pass++;
     }
+    FC_PHASE(0);
 }
 
 // src/timeStep.f90:132-171

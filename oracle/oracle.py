@@ -24,14 +24,18 @@ def build():
     subprocess.run(["make", "-s", "-C", HERE], check=True)
 
 
-def _lib(fast=False):
-    key = "fast" if fast else "strict"
+def _lib(fast=False, count=False):
+    key = "count" if count else "fast" if fast else "strict"
     if key in _libs:
         return _libs[key]
-    name = "libhosono_oracle_fast.so" if fast else "libhosono_oracle.so"
+    name = dict(count="libhosono_oracle_count.so", fast="libhosono_oracle_fast.so",
+                strict="libhosono_oracle.so")[key]
     path = os.path.join(BUILD, name)
     if not os.path.exists(path):
-        build()
+        if count:
+            subprocess.run(["make", "-s", "-C", HERE, "count"], check=True)
+        else:
+            build()
     lib = ctypes.CDLL(path)
     d, i, p = ctypes.c_double, ctypes.c_int, ctypes.c_void_p
     dp = ctypes.POINTER(ctypes.c_double)
@@ -64,8 +68,36 @@ def _lib(fast=False):
                                  ctypes.c_char_p, dp, dp, ip]
     lib.orc_set_threads.argtypes = [i]
     lib.orc_get_threads.restype = i
+    if count:
+        lib.orc_count_get.argtypes = [i, ctypes.POINTER(ctypes.c_ulonglong)]
+        lib.orc_count_reset.argtypes = []
     _libs[key] = lib
     return lib
+
+
+COUNT_CLASSES = ("add", "mul", "div", "sqrt", "cmp", "other")
+
+
+def count_reset():
+    """Zero the operation counters of the counting build (flopcount.h)."""
+    _lib(count=True).orc_count_reset()
+
+
+COUNT_PHASES = ("rest", "pass1", "later_passes", "update_detect")
+
+
+def count_get():
+    """Operations the counting build executed since count_reset(), by phase
+    of the time step (COUNT_PHASES) and class; 'flops' = add + mul + div +
+    sqrt."""
+    out = {}
+    for k, name in enumerate(COUNT_PHASES):
+        c = (ctypes.c_ulonglong * 6)()
+        _lib(count=True).orc_count_get(k, c)
+        d = dict(zip(COUNT_CLASSES, (int(v) for v in c)))
+        d["flops"] = d["add"] + d["mul"] + d["div"] + d["sqrt"]
+        out[name] = d
+    return out
 
 
 def _dp(a):
@@ -76,8 +108,8 @@ def _ip(a):
     return a.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
 
 
-def set_threads(n, fast=False):
-    _lib(fast).orc_set_threads(int(n))
+def set_threads(n, fast=False, count=False):
+    _lib(fast, count).orc_set_threads(int(n))
 
 
 def get_threads(fast=False):
@@ -102,8 +134,8 @@ def gp_build(R, x_beg, x_end, nx, y_beg, y_end, ny, ell_over_delta):
 class Oracle:
     """One solver instance built from a .par file."""
 
-    def __init__(self, parfile, fast=False):
-        self.lib = _lib(fast)
+    def __init__(self, parfile, fast=False, count=False):
+        self.lib = _lib(fast, count)
         err = ctypes.create_string_buffer(512)
         self.h = self.lib.orc_create_from_par(os.fsencode(parfile), err, 512)
         if not self.h:
