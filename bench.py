@@ -135,9 +135,12 @@ PASS1_PROFILE = {"workload": "ot1536_r2", "n": 1536, "radius": 2, "dram_bytes": 
 # count`) counts every double add, multiply, divide and square root of the
 # MOOD pass-1 reconstruction and fluxes (GP face states, face CAD/PAD, the
 # Riemann solves and their Gauss sums) over the three stages of one step;
-# per launch is a third of that.  Orszag-Tang R=2, ell/dx=12, counted at
-# 2048^2 on steps 1 and 13 (15858.3 and 15858.2 flops per zone-update).
-PASS1_FLOPS = {("ot", 2, 12.0): 15858.2 / 3}
+# per launch is a third of that.  Counted on each workload's own grid (the
+# halo work of a small grid included): Orszag-Tang R=2, ell/dx=12 at 2048^2
+# on steps 1 and 13 (15858.3 and 15858.2 flops per zone-update); Sedov R=2
+# (hydro) at 2048^2, steps 1-3 (14269.5); Orszag-Tang R=1 at 128^2, steps 1-3
+# (7855.4 to 7855.8).
+PASS1_FLOPS = {("ot", 2, 12.0): 15858.2 / 3, ("sedov", 2, 6.0): 14269.5 / 3, ("ot", 1, 6.0): 7855.8 / 3}
 FP64_LANES_PER_SM = 64  # FP64 FMA lanes per B200 SM (two flops per lane per clock)
 
 
