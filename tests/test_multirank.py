@@ -52,3 +52,11 @@ def test_reference_arm_under_torchrun():
     assert len(lines) == 1
     d = json.loads(lines[0])
     assert d["impl"] == "reference" and d["n_gpus"] == 2 and d["value"] > 0
+    # the same metric, unit and workload as the GPU arm, and the reference-arm keys
+    assert d["metric"] == "fp64_zone_updates_per_s" and d["unit"] == "zone-updates/s"
+    assert d["higher_is_better"] is True and d["config"]["workload"] == "ot128_r1"
+    cb = d["cpu_baseline"]
+    assert cb["value"] == d["value"] and cb["kind"] in ("port", "reference") and cb["cores"] >= 1 and cb["sample"]
+    e = d["e2e"]
+    assert e["value"] == d["value"] and e["unit"] == d["unit"]
+    assert e["h2d_bytes_per_step"] == 0 and e["d2h_bytes_per_step"] == 0
