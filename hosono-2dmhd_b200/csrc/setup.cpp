@@ -115,11 +115,30 @@ void host_bc(const hosono_params* p, double* A, int nv) {
 
 }  // namespace
 
+// keys simulation_init, GP_init and grid_init read, in the reference's read
+// order (checked up front, so one call names every missing key)
+const char* const kRequiredKeys[] = {
+    "sim_smallB",       "sim_smallPressure", "sim_smallDensity",   "sim_smallEnergy",    "sim_gamma",
+    "sim_riemannSolver", "sim_cfl",          "sim_tmax",           "sim_nstepmax",       "sim_BC",
+    "sim_dataFileBaseName", "sim_outputFreqTime", "sim_outputFreqStep", "sim_outputHdf5", "sim_outputAscii",
+    "sim_forceHydro",   "GP_maxRadius",      "GP_ellOverDelta",    "grid_Nx",            "grid_Ny",
+    "grid_xBeg",        "grid_xEnd",         "grid_yBeg",          "grid_yEnd"};
+
 extern "C" int hosono_par_load(const char* parfile, hosono_params* p, hosono_run_info* run, char* err, int errlen) {
     if (!p) return HOSONO_EINVAL;
     ParFile f(parfile);
     if (!f.ok) {
         put_err(err, errlen, std::string("cannot open parameter file ") + (parfile ? parfile : "(null)"));
+        return HOSONO_EPAR;
+    }
+    std::vector<std::string> missing;
+    for (const char* k : kRequiredKeys)
+        if (!f.raw(k)) missing.emplace_back(k);
+    if (!missing.empty()) {  // the reference's message for the first, then the rest
+        std::string m = "The parameter '" + missing[0] + "' was not found inside of '" + f.path + "'";
+        for (size_t k = 1; k < missing.size(); k++) m += (k == 1 ? " (also missing: " : ", ") + missing[k];
+        if (missing.size() > 1) m += ")";
+        put_err(err, errlen, m);
         return HOSONO_EPAR;
     }
     try {

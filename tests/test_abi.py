@@ -69,6 +69,22 @@ def test_par_missing_key_is_reported(tmp_par_dir):
     assert e.value.code == m.EPAR and "sim_cfl" in str(e.value)
 
 
+def test_par_every_missing_key_is_reported(tmp_par_dir):
+    """The required keys are checked up front: the reference's message names
+    the first missing key (in its read order), and the rest follow."""
+    m = pkg.load()
+    kv = parfiles.orszag_tang(16, 1)
+    for k in ("grid_yEnd", "sim_gamma", "GP_ellOverDelta"):
+        del kv[k]
+    par = parfiles.make(tmp_par_dir, "missing3", kv)
+    with pytest.raises(m.HosonoError) as e:
+        m.par_load(par)
+    msg = str(e.value)
+    assert e.value.code == m.EPAR
+    assert "The parameter 'sim_gamma' was not found" in msg
+    assert "also missing: GP_ellOverDelta, grid_yEnd" in msg
+
+
 def test_par_first_match_and_comments(tmp_par_dir):
     """readParamFile.f90:150-175: comment lines skipped, text after '#'
     dropped, first matching key wins, leading blanks make a different key."""
