@@ -123,9 +123,9 @@ def peaks():
         return FALLBACK_HBM_GBS, "fallback"
 
 
-# DRAM bytes of one k_face_pass1<2> launch measured with ncu on ot1536_r2
-# (profiles/k_face_pass1_ot1536_r2.md), and the FP64-pipe activity there;
-# the bench scales the bytes to its workload by the algorithmic bytes.
+# DRAM bytes of one k_face_pass1<2> launch measured with ncu on ot1536_r2,
+# and the FP64-pipe activity there; the bench scales the bytes to its
+# workload by the algorithmic bytes.
 PASS1_PROFILE = {"workload": "ot1536_r2", "n": 1536, "radius": 2, "dram_bytes": 162735872 + 314940160,
                  "fp64_pipe_active_frac": 0.485}
 

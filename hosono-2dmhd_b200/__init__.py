@@ -59,7 +59,11 @@ class Stats(ctypes.Structure):
 
 class ServeConfig(ctypes.Structure):
     _fields_ = [("memory_budget", ctypes.c_longlong), ("max_resident", ctypes.c_int), ("fp_mode", ctypes.c_int),
-                ("chunk_ms", ctypes.c_double), ("max_chunk_steps", ctypes.c_int), ("pad", ctypes.c_int)]
+                ("chunk_ms", ctypes.c_double), ("max_chunk_steps", ctypes.c_int), ("policy", ctypes.c_int),
+                ("aging_s", ctypes.c_double), ("fill_tiles", ctypes.c_int), ("pad", ctypes.c_int)]
+
+
+SERVE_FIFO, SERVE_SHORTEST = 0, 1
 
 
 class RequestInfo(ctypes.Structure):
@@ -83,6 +87,24 @@ class ServeTotals(ctypes.Structure):
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class LaunchInfo(ctypes.Structure):
+    _fields_ = [("tiles", ctypes.c_int), ("sms", ctypes.c_int), ("pass1_grid", ctypes.c_int),
+                ("tile_grid_max", ctypes.c_int)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class Tuning(ctypes.Structure):
+    _fields_ = [("pass1_staging", ctypes.c_int), ("pad", ctypes.c_int * 7)]
+
+    def as_dict(self):
+        return {"pass1_staging": self.pass1_staging}
+
+
+STAGE_CP_ASYNC, STAGE_TMA = 0, 1
 
 
 class ICDesc(ctypes.Structure):
@@ -119,14 +141,32 @@ SIGNATURES = {
     "hosono_gpu_trace_count": [_vp],
     "hosono_gpu_trace_get": [_vp, _i, _ip, _vp, _vp],
     "hosono_gpu_trace_clear": [_vp],
+    "hosono_gpu_module_set": [_vp, _ip, _ip, _ip],
+    "hosono_gpu_module_get": [_vp, _dp, _dp, _dp, _dp, _ip, _ip, _ip],
+    "hosono_gpu_reconstruct": [_vp],
+    "hosono_gpu_getfluxes": [_vp],
+    "hosono_gpu_flicd": [_vp],
+    "hosono_gpu_update": [_vp, _d],
+    "hosono_gpu_detect": [_vp, _ip],
+    "hosono_gpu_bc": [_vp, _i],
+    "hosono_gpu_bc_mood": [_vp],
+    "hosono_gpu_mood_pass_stats": [_vp, _ip, ctypes.POINTER(ctypes.c_longlong)],
+    "hosono_gpu_riemann": [_vp, _i, _vp, _vp, _i, _vp],
     "hosono_gpu_state_layout": [_vp, ctypes.POINTER(_vp), _ip, ctypes.POINTER(ctypes.c_longlong)],
     "hosono_gpu_build_info": [_ip, _ip],
     "hosono_gpu_set_device": [_i],
     "hosono_gpu_stream": [_vp, ctypes.POINTER(_vp)],
+    "hosono_gpu_launch_info": [_vp, ctypes.POINTER(LaunchInfo)],
+    "hosono_gpu_set_tuning": [_vp, ctypes.POINTER(Tuning)],
+    "hosono_gpu_get_tuning": [_vp, ctypes.POINTER(Tuning)],
+    "hosono_batch_set_tuning": [_vp, ctypes.POINTER(Tuning)],
+    "hosono_batch_get_tuning": [_vp, ctypes.POINTER(Tuning)],
     "hosono_gpu_profile": [_vp, _i],
     "hosono_gpu_profile_read": [_vp, _dp, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong), _i],
     "hosono_cfl_noalloc": [_vp, _i, _i, _i, _i, ctypes.c_longlong, _d, _d, _d, _i, _vp, _vp],
     "hosono_gpu_set_time": [_vp, _d, _d, _i, _i],
+    "hosono_gpu_set_mood_cap": [_vp, _i],
+    "hosono_batch_set_mood_cap": [_vp, _i, _i],
     "hosono_gpu_step": [_vp, _i, _dp, _ip],
     "hosono_gpu_set_graphs": [_vp, _i],
     "hosono_batch_create": [_i, _i, _i, ctypes.POINTER(_vp)],
@@ -158,6 +198,7 @@ SIGNATURES = {
     "hosono_serve_submit": [_vp, ctypes.POINTER(Params), _dp, _dp, _ip, _dp, _dp, _d, _i, _dp, _dp, _ip,
                             ctypes.POINTER(ctypes.c_longlong)],
     "hosono_serve_wait": [_vp, ctypes.c_longlong, _d, ctypes.POINTER(RequestInfo)],
+    "hosono_serve_release": [_vp, ctypes.c_longlong],
     "hosono_serve_poll": [_vp, ctypes.POINTER(ctypes.c_longlong), _i, _ip],
     "hosono_serve_info": [_vp, ctypes.c_longlong, ctypes.POINTER(RequestInfo)],
     "hosono_serve_snapshot": [_vp, ctypes.c_longlong, _dp, _dp, _ip, _dp, _ip],
@@ -167,6 +208,11 @@ SIGNATURES = {
 }
 RESTYPES = {"hosono_batch_instance_bytes": ctypes.c_longlong, "hosono_serve_clock": ctypes.c_double}
 NOALLOC_MAX_ROWS = 16384  # HOSONO_NOALLOC_MAX_ROWS
+
+
+def mood_cap_default(radius):
+    """HOSONO_MOOD_CAP_DEFAULT(R): MOOD passes per stage before EMOODCAP."""
+    return 16 * (radius + 1)
 
 
 def set_device(device):
@@ -386,6 +432,11 @@ class Solver:
         self._check(self.lib.hosono_gpu_set_time(self.h, float(t), float(tmax), int(nstep), int(nstepmax)),
                     "set_time")
 
+    def set_mood_cap(self, cap):
+        """MOOD passes a stage may take before the solve stops with EMOODCAP
+        (cap <= 0: the proven bound R*nx*ny + 1)."""
+        self._check(self.lib.hosono_gpu_set_mood_cap(self.h, int(cap)), "set_mood_cap")
+
     def step(self, max_steps=1):
         """Continue the time loop (cfl + validTimeStep + advance on the device) by
         up to max_steps steps; returns (t, nstep)."""
@@ -437,6 +488,92 @@ class Solver:
         s = ctypes.c_void_p()
         self._check(self.lib.hosono_gpu_stream(self.h, ctypes.byref(s)), "stream")
         return s.value or 0
+
+    # ---- the reference's stage modules one at a time (module state of the
+    # handle; host arrays in the reference's layout, numpy-shaped [j, i, ...])
+    def module_set(self, scheme=None, recompute=None, recompute_flicd=None):
+        keep = []
+
+        def arg(a):
+            if a is None:
+                return None
+            a = np.ascontiguousarray(a, dtype=np.int32).reshape(-1)
+            assert a.size == self.nxt * self.nyt
+            keep.append(a)
+            return _p(a, ctypes.c_int)
+        self._check(self.lib.hosono_gpu_module_set(self.h, arg(scheme), arg(recompute), arg(recompute_flicd)),
+                    "module_set")
+
+    def module_get(self):
+        """dict of faceVals [j, i, face, q, var], fluxRaw / flux [j, i, dir, var],
+        Unew [j, i, var], scheme / recompute / recompute_flicd [j, i]."""
+        nq = self.params.max_radius + 1
+        sh = (self.nyt, self.nxt)
+        fv = np.zeros((*sh, 4, nq, 8))
+        fr = np.zeros((*sh, 2, 8))
+        fl = np.zeros((*sh, 2, 8))
+        un = np.zeros((*sh, 8))
+        sc, rc, rf = (np.zeros(sh, dtype=np.int32) for _ in range(3))
+        self._check(self.lib.hosono_gpu_module_get(self.h, _p(fv), _p(fr), _p(fl), _p(un), _p(sc, ctypes.c_int),
+                                                   _p(rc, ctypes.c_int), _p(rf, ctypes.c_int)), "module_get")
+        return dict(faceVals=fv, fluxRaw=fr, flux=fl, Unew=un, scheme=sc, recompute=rc, recompute_flicd=rf)
+
+    def reconstruct(self):
+        """reconstruct_faceValsWithGP(blk, state%U)"""
+        self._check(self.lib.hosono_gpu_reconstruct(self.h), "reconstruct")
+
+    def getfluxes(self):
+        self._check(self.lib.hosono_gpu_getfluxes(self.h), "getfluxes")
+
+    def flicd(self):
+        self._check(self.lib.hosono_gpu_flicd(self.h), "flicd")
+
+    def update(self, dt):
+        self._check(self.lib.hosono_gpu_update(self.h, float(dt)), "update")
+
+    def detect(self):
+        """detect_ALL; returns exit_mood_loop."""
+        e = ctypes.c_int()
+        self._check(self.lib.hosono_gpu_detect(self.h, ctypes.byref(e)), "detect")
+        return bool(e.value)
+
+    def bc(self, which):
+        """boundaryConditions_applyBlk on U (0), V (1) or Unew (2)."""
+        self._check(self.lib.hosono_gpu_bc(self.h, int(which)), "bc")
+
+    def bc_mood(self):
+        self._check(self.lib.hosono_gpu_bc_mood(self.h), "bc_mood")
+
+    def mood_pass_stats(self):
+        n = ctypes.c_int()
+        t = ctypes.c_longlong()
+        self._check(self.lib.hosono_gpu_mood_pass_stats(self.h, ctypes.byref(n), ctypes.byref(t)),
+                    "mood_pass_stats")
+        return n.value, t.value
+
+    def riemann(self, n, uL_dev, uR_dev, direction, flux_dev):
+        """riemannSolver_fromConsHllcMHD on n faces of device arrays (8, n)."""
+        self._check(self.lib.hosono_gpu_riemann(self.h, int(n), ctypes.c_void_p(uL_dev), ctypes.c_void_p(uR_dev),
+                                                int(direction), ctypes.c_void_p(flux_dev)), "riemann")
+
+    def set_tuning(self, **kw):
+        """Launch choices (results are the same bits for every choice)."""
+        t = Tuning()
+        self._check(self.lib.hosono_gpu_get_tuning(self.h, ctypes.byref(t)), "get_tuning")
+        for k, v in kw.items():
+            setattr(t, k, int(v))
+        self._check(self.lib.hosono_gpu_set_tuning(self.h, ctypes.byref(t)), "set_tuning")
+
+    def tuning(self):
+        t = Tuning()
+        self._check(self.lib.hosono_gpu_get_tuning(self.h, ctypes.byref(t)), "get_tuning")
+        return t.as_dict()
+
+    def launch_info(self):
+        """Launch geometry: tiles, SMs, pass-1 grid, largest other tile-kernel grid."""
+        li = LaunchInfo()
+        self._check(self.lib.hosono_gpu_launch_info(self.h, ctypes.byref(li)), "launch_info")
+        return li.as_dict()
 
     DIAG_FIELDS = ("dens", "velx", "vely", "velz", "pres", "eint", "gama", "ener", "magp", "divb", "magx",
                    "magy", "magz")
@@ -573,6 +710,16 @@ class Batch:
     def set_time(self, slot, t, tmax, nstep=0, nstepmax=1 << 30):
         self._check(self.lib.hosono_batch_set_time(self.h, int(slot), float(t), float(tmax), int(nstep),
                                                    int(nstepmax)), "set_time")
+
+    def set_tuning(self, **kw):
+        t = Tuning()
+        self._check(self.lib.hosono_batch_get_tuning(self.h, ctypes.byref(t)), "get_tuning")
+        for k, v in kw.items():
+            setattr(t, k, int(v))
+        self._check(self.lib.hosono_batch_set_tuning(self.h, ctypes.byref(t)), "set_tuning")
+
+    def set_mood_cap(self, slot, cap):
+        self._check(self.lib.hosono_batch_set_mood_cap(self.h, int(slot), int(cap)), "set_mood_cap")
 
     def run(self, max_steps=0):
         self._check(self.lib.hosono_batch_run(self.h, int(max_steps)), "run")

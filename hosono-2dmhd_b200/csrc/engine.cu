@@ -1,6 +1,6 @@
 // engine.cu -- host side of the batched engine: instance slots, device
 // tables, and the time-step structure (timeStep.f90:22-171 with the driver
-// loop of mhd_driver.f90:198-217) recorded either as eager launches driven by
+// loop of mhd_driver.f90:76-95) recorded either as eager launches driven by
 // host loops, or as one CUDA graph whose loops are conditional WHILE nodes:
 //
 //   run:   WHILE(any instance stepping) {
@@ -21,6 +21,7 @@
 #include <climits>
 #include <cstdarg>
 #include <cstddef>
+#include <cstdint>
 #include <cstdio>
 #include <cstring>
 #include <utility>
@@ -153,14 +154,16 @@ class Engine::Rec {
 // ----------------------------------------------------------------------
 Engine::~Engine() {
     if (s_) cudaStreamSynchronize(s_);
-    for (auto& sl : slots_)
+    for (auto& sl : slots_) {
         for (void* p : sl.allocs) dfree(p);
+        if (sl.modAlloc) cudaFree(sl.modAlloc);
+    }
     for (cudaGraphExec_t g : {gAdvance_, gRun_, gProf_})
         if (g) cudaGraphExecDestroy(g);
     for (cudaEvent_t ev : profEv_)
         if (ev) cudaEventDestroy(ev);
     for (void* p : {(void*)d_instTiles_, (void*)d_actRange_, (void*)d_actInfo_, (void*)d_casRange_,
-                    (void*)d_casInfo_})
+                    (void*)d_casInfo_, (void*)d_hold_})
         if (p) cudaFree(p);
     for (void* p : {(void*)d_dev_, (void*)d_st_, (void*)d_tiles_, (void*)d_ntiles_, (void*)d_flags_, (void*)staging_,
                     (void*)schemeInt_, (void*)lists_.rec, (void*)lists_.face, (void*)lists_.recF, (void*)lists_.low,
@@ -186,6 +189,8 @@ int Engine::init(int max_inst, int max_tiles, int fp_mode) {
     CUE(cudaMalloc(&d_actInfo_, sizeof(int) * 2));
     CUE(cudaMalloc(&d_casRange_, sizeof(int2) * maxInst_));
     CUE(cudaMalloc(&d_casInfo_, sizeof(int) * 2));
+    CUE(cudaMalloc(&d_hold_, sizeof(int) * maxInst_));
+    CUE(cudaMemsetAsync(d_hold_, 0, sizeof(int) * maxInst_, s_));
     CUE(cudaMemsetAsync(d_casInfo_, 0, sizeof(int) * 2, s_));
     CUE(cudaMemsetAsync(d_instTiles_, 0, sizeof(int2) * maxInst_, s_));
     CUE(cudaMemsetAsync(d_actInfo_, 0, sizeof(int) * 2, s_));
@@ -218,8 +223,66 @@ int Engine::init(int max_inst, int max_tiles, int fp_mode) {
     return HOSONO_OK;
 }
 
+namespace {
+// cuTensorMapEncodeTiled through the runtime's driver entry point (the
+// library links no libcuda of its own)
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiledFn encode_tiled() {
+    static const EncodeTiledFn fn = [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess) {
+            cudaGetLastError();
+            return (EncodeTiledFn) nullptr;
+        }
+        return (EncodeTiledFn)p;
+    }();
+    return fn;
+}
+}  // namespace
+
+// TMA descriptors of the three U buffers: a 3D tensor (x: pitch doubles,
+// y: nyt rows, var: 8 planes) read in boxes of the pass-1 stencil box
+int Engine::encode_tmaps(InstDev& dev) {
+    const EncodeTiledFn enc = encode_tiled();
+    if (!enc) return fail(HOSONO_ECUDA, "cuTensorMapEncodeTiled is not available from the driver");
+    const Geo& G = dev.geo;
+    const cuuint64_t dims[3] = {(cuuint64_t)G.pitch, (cuuint64_t)G.nyt, (cuuint64_t)NCONS};
+    const cuuint64_t strides[2] = {(cuuint64_t)G.pitch * sizeof(double), (cuuint64_t)G.plane * sizeof(double)};
+    const cuuint32_t box[3] = {(cuuint32_t)P1_SX, (cuuint32_t)p1_sy(G.R), (cuuint32_t)NCONS};
+    const cuuint32_t es[3] = {1, 1, 1};
+    for (int r = 0; r < 3; r++) {
+        const CUresult e = enc(&dev.tmU[r], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, dev.U[r], dims, strides, box, es,
+                               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                               CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (e != CUDA_SUCCESS) return fail(HOSONO_ECUDA, "cuTensorMapEncodeTiled failed (%d)", (int)e);
+    }
+    return HOSONO_OK;
+}
+
+void Engine::drop_graphs() {
+    if (s_) cudaStreamSynchronize(s_);
+    for (cudaGraphExec_t* g : {&gAdvance_, &gRun_, &gProf_})
+        if (*g) {
+            cudaGraphExecDestroy(*g);
+            *g = nullptr;
+        }
+}
+
+int Engine::set_tuning(const hosono_tuning& t) {
+    if (t.pass1_staging != HOSONO_STAGE_CP_ASYNC && t.pass1_staging != HOSONO_STAGE_TMA)
+        return fail(HOSONO_EINVAL, "pass1_staging %d", t.pass1_staging);
+    tune_ = t;
+    drop_graphs();  // the graphs hold the launch choices in their kernel parameters
+    return HOSONO_OK;
+}
+
 Batch Engine::batch() const {
     Batch B;
+    B.p1Tma = tune_.pass1_staging == HOSONO_STAGE_TMA ? 1 : 0;
     B.dev = d_dev_;
     B.st = d_st_;
     B.tiles = d_tiles_;
@@ -233,6 +296,7 @@ Batch Engine::batch() const {
     B.actInfo = d_actInfo_;
     B.casRange = d_casRange_;
     B.casInfo = d_casInfo_;
+    B.hold = d_hold_;
     return B;
 }
 
@@ -400,6 +464,10 @@ int Engine::add(const hosono_params& p, const double* pv, const double* qw, int*
     double* dqw = q + npv;
     sl.dev.pv = dpv;
     sl.dev.qw = dqw;
+    if (int rc = encode_tmaps(sl.dev)) {
+        for (void* a : sl.allocs) dfree(a);
+        return rc;
+    }
     uint8_t* b = byt;
     sl.dev.scheme[0] = (int8_t*)b;
     sl.dev.scheme[1] = (int8_t*)(b + plane);
@@ -420,8 +488,9 @@ int Engine::add(const hosono_params& p, const double* pv, const double* qw, int*
     st.live = 1;
     st.tmax = HUGE_VAL;
     st.nstepmax = INT_MAX;
-    st.passCap = (int)std::min<long long>((long long)R * p.nx * p.ny + 2, INT_MAX);
+    st.passCap = HOSONO_MOOD_CAP_DEFAULT(R);
     CUE(cudaMemcpyAsync(d_st_ + k, &st, sizeof(InstState), cudaMemcpyHostToDevice, s_));
+    CUE(cudaMemsetAsync(d_hold_ + k, 0, sizeof(int), s_));
     sl.live = true;
     sl.ntiles = tiles_of(p);
     slots_[k] = sl;
@@ -442,6 +511,7 @@ int Engine::remove(int slot, bool commit) {
     if (commit) TRYE(upload_tables());
     CUE(cudaStreamSynchronize(s_));  // no kernel of this stream still reads the memory
     for (void* p : slots_[slot].allocs) dfree(p);
+    if (slots_[slot].modAlloc) cudaFree(slots_[slot].modAlloc);
     slots_[slot] = Slot{};
     return HOSONO_OK;
 }
@@ -557,6 +627,23 @@ int Engine::download(int slot, double* U, double* V, int* scheme) {
     }
     CUE(cudaGetLastError());
     return HOSONO_OK;
+}
+
+int Engine::set_holds(const int* holds) {
+    CUE(cudaMemcpyAsync(d_hold_, holds, sizeof(int) * maxInst_, cudaMemcpyHostToDevice, s_));
+    CUE(cudaStreamSynchronize(s_));
+    return HOSONO_OK;
+}
+
+int Engine::set_mood_cap(int slot, int cap) {
+    if (slot < 0 || slot >= maxInst_ || !slots_[slot].live) return fail(HOSONO_EINVAL, "bad slot %d", slot);
+    const hosono_params& p = slots_[slot].p;
+    // every pass that does not end the loop lowers at least one cell by one
+    // order, and a cell can be lowered at most R times: R*nx*ny + 1 passes
+    // always suffice (guard cells only follow their interior images)
+    const long long proven = (long long)p.max_radius * p.nx * p.ny + 1;
+    const long long c = cap > 0 ? std::min<long long>(cap, proven) : proven;
+    return write_field(slot, &InstState::passCap, (int)std::min<long long>(c, INT_MAX));
 }
 
 int Engine::set_time(int slot, double t, double tmax, int nstep, int nstepmax) {
@@ -793,6 +880,254 @@ int Engine::run_profiled_step(double* pass1_ms, int* pass1_launches) {
     *pass1_ms = ms;
     *pass1_launches = 3;
     return check_errors();
+}
+
+// ----------------------------------------------------------------------
+// Per-module form: reconstruct_faceValsWithGP, getFluxes_, FLICD, the
+// update, detect_ALL and the boundary routines one at a time on one
+// instance (modules.cuh), for a host that keeps its own MOOD loop.
+int Engine::mod_ensure(int slot) {
+    if (slot < 0 || slot >= maxInst_ || !slots_[slot].live) return fail(HOSONO_EINVAL, "bad slot %d", slot);
+    Slot& sl = slots_[slot];
+    if (sl.modAlloc) return HOSONO_OK;
+    const Geo& G = sl.dev.geo;
+    const size_t plane = (size_t)G.plane;
+    const size_t nfv = (size_t)NCONS * G.nqMax * 4, nfl = 2 * NCONS, nbyte = 8;
+    const size_t bytes = sizeof(double) * plane * (nfv + nfl) + plane * nbyte + 256;
+    char* p = nullptr;
+    cudaError_t e = cudaMalloc(&p, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(HOSONO_ENOMEM, "no device memory for the module buffers (%zu bytes): %s", bytes,
+                    cudaGetErrorString(e));
+    }
+    CUE(cudaMemsetAsync(p, 0, bytes, s_));  // faceVals and flux start at zero (gridBlock.f90:160-169)
+    ModBuf& M = sl.mod;
+    M.fv = (double*)p;
+    M.flux = M.fv + plane * nfv;
+    uint8_t* b = (uint8_t*)(M.flux + plane * nfl);
+    uint8_t** planes[] = {&M.recon, &M.adm, &M.next, &M.check, &M.lower, &M.tRec, &M.tRecF, (uint8_t**)&M.tSch};
+    for (uint8_t** pp : planes) {
+        *pp = b;
+        b += plane;
+    }
+    M.flag = (int*)(((uintptr_t)b + 15) & ~(uintptr_t)15);
+    sl.modAlloc = p;
+    CUE(cudaStreamSynchronize(s_));
+    return HOSONO_OK;
+}
+
+namespace {
+// Fortran (i, j) order with guards <-> a device plane (rows `pitch` elements apart)
+template <typename T>
+cudaError_t plane_copy_down(const Geo& G, const T* d, T* h, cudaStream_t s) {
+    return cudaMemcpy2DAsync(h, sizeof(T) * G.nxt, d, sizeof(T) * G.pitch, sizeof(T) * G.nxt, G.nyt,
+                             cudaMemcpyDeviceToHost, s);
+}
+template <typename T>
+cudaError_t plane_copy_up(const Geo& G, T* d, const T* h, cudaStream_t s) {
+    return cudaMemcpy2DAsync(d, sizeof(T) * G.pitch, h, sizeof(T) * G.nxt, sizeof(T) * G.nxt, G.nyt,
+                             cudaMemcpyHostToDevice, s);
+}
+}  // namespace
+
+int Engine::mod_set(int slot, const int* scheme, const int* rec, const int* recF) {
+    TRYE(mod_ensure(slot));
+    InstState st;
+    TRYE(state(slot, &st));
+    const InstDev& d = slots_[slot].dev;
+    const Geo& G = d.geo;
+    const size_t n = (size_t)G.nxt * G.nyt;
+    std::vector<int8_t> sb(scheme ? n : 0);
+    std::vector<uint8_t> rb(rec ? n : 0), fb(recF ? n : 0);
+    for (size_t c = 0; c < n; c++) {
+        if (scheme) {
+            if (scheme[c] < 0 || scheme[c] > G.R) return fail(HOSONO_EINVAL, "scheme %d outside [0, R]", scheme[c]);
+            sb[c] = (int8_t)scheme[c];
+        }
+        if (rec) rb[c] = rec[c] ? 1 : 0;
+        if (recF) fb[c] = recF[c] ? 1 : 0;
+    }
+    if (scheme) CUE(plane_copy_up(G, d.scheme[st.schemeSel], sb.data(), s_));
+    if (rec) CUE(plane_copy_up(G, d.rec, rb.data(), s_));
+    if (recF) CUE(plane_copy_up(G, d.recF, fb.data(), s_));
+    CUE(cudaStreamSynchronize(s_));
+    return HOSONO_OK;
+}
+
+int Engine::mod_get(int slot, double* faceVals, double* fluxRaw, double* flux, double* Unew, int* scheme, int* rec,
+                    int* recF) {
+    TRYE(mod_ensure(slot));
+    InstState st;
+    TRYE(state(slot, &st));
+    const InstDev& d = slots_[slot].dev;
+    const ModBuf& M = slots_[slot].mod;
+    const Geo& G = d.geo;
+    const size_t n = (size_t)G.nxt * G.nyt;
+    std::vector<double> tmp(n);
+    // one device plane into every k-th double of a host array starting at `first`
+    auto scatter = [&](const double* dplane, double* host, size_t first, size_t k) -> int {
+        CUE(plane_copy_down(G, dplane, tmp.data(), s_));
+        CUE(cudaStreamSynchronize(s_));
+        for (size_t c = 0; c < n; c++) host[first + k * c] = tmp[c];
+        return HOSONO_OK;
+    };
+    if (faceVals) {  // (8, nqMax, 4, nxt, nyt)
+        const size_t per = (size_t)NCONS * G.nqMax * 4;
+        for (int f = 0; f < 4; f++)
+            for (int q = 0; q < G.nqMax; q++)
+                for (int v = 0; v < NCONS; v++)
+                    TRYE(scatter(M.fv + ((size_t)(f * G.nqMax + q) * NCONS + v) * G.plane, faceVals,
+                                 v + (size_t)NCONS * (q + (size_t)G.nqMax * f), per));
+    }
+    for (int dir = 0; dir < 2; dir++)
+        for (int v = 0; v < NCONS; v++) {  // (8, 2, nxt, nyt)
+            if (fluxRaw) TRYE(scatter((dir == XDIR ? d.FX : d.FY) + (size_t)v * G.plane, fluxRaw, v + NCONS * dir, 2 * NCONS));
+            if (flux) TRYE(scatter(M.flux + (size_t)(dir * NCONS + v) * G.plane, flux, v + NCONS * dir, 2 * NCONS));
+        }
+    if (Unew) {
+        const double* A = role_ptr(d, st.parity, ROLE_A);
+        for (int v = 0; v < NCONS; v++) TRYE(scatter(A + (size_t)v * G.plane, Unew, v, NCONS));
+    }
+    std::vector<uint8_t> b(n);
+    auto bytes_to_int = [&](const void* dplane, int* out, bool is_signed) -> int {
+        CUE(plane_copy_down(G, (const uint8_t*)dplane, b.data(), s_));
+        CUE(cudaStreamSynchronize(s_));
+        for (size_t c = 0; c < n; c++) out[c] = is_signed ? (int)(int8_t)b[c] : (int)b[c];
+        return HOSONO_OK;
+    };
+    if (scheme) TRYE(bytes_to_int(d.scheme[st.schemeSel], scheme, true));
+    if (rec) TRYE(bytes_to_int(d.rec, rec, false));
+    if (recF) TRYE(bytes_to_int(d.recF, recF, false));
+    return HOSONO_OK;
+}
+
+int Engine::mod_reconstruct(int slot) {
+    TRYE(mod_ensure(slot));
+    const Slot& sl = slots_[slot];
+    const Geo& G = sl.dev.geo;
+    const ModBuf& M = sl.mod;
+    const Batch B = batch();
+    const size_t plane = (size_t)G.plane;
+    CUE(cudaMemcpyAsync(M.recon, sl.dev.rec, plane, cudaMemcpyDeviceToDevice, s_));  // reconstructCell = recompute
+    // every inner pass that goes on lowers at least one cell of the range by
+    // one order, so (R + 1) * cells passes bound the loop
+    const long long cap = (long long)(G.R + 1) * G.nxt * G.nyt + 1;
+    for (long long it = 0;; it++) {
+        if (it > cap) return fail(HOSONO_EMOODCAP, "reconstruct: inner cascade exceeded %lld passes", cap);
+        CUE(cudaMemsetAsync(M.adm, 1, plane, s_));
+        CUE(cudaMemsetAsync(M.next, 0, plane, s_));
+        CUE(cudaMemsetAsync(M.flag, 0, sizeof(int), s_));
+        K_->mod->recon(B, slot, G, M, s_);
+        K_->mod->recon_lower(B, slot, G, M, s_);
+        launches += 2;
+        CUE(cudaGetLastError());
+        int lowered = 0;
+        CUE(cudaMemcpyAsync(&lowered, M.flag, sizeof(int), cudaMemcpyDeviceToHost, s_));
+        CUE(cudaStreamSynchronize(s_));
+        if (!lowered) break;
+        CUE(cudaMemcpyAsync(M.recon, M.next, plane, cudaMemcpyDeviceToDevice, s_));
+    }
+    return HOSONO_OK;
+}
+
+int Engine::mod_getfluxes(int slot) {
+    TRYE(mod_ensure(slot));
+    K_->mod->getfluxes(batch(), slot, slots_[slot].dev.geo, slots_[slot].mod, s_);
+    launches++;
+    CUE(cudaGetLastError());
+    CUE(cudaStreamSynchronize(s_));
+    return HOSONO_OK;
+}
+
+int Engine::mod_flicd(int slot) {
+    TRYE(mod_ensure(slot));
+    const Geo& G = slots_[slot].dev.geo;
+    const ModBuf& M = slots_[slot].mod;
+    K_->mod->flicd(batch(), slot, G, M, s_);
+    launches++;
+    CUE(cudaGetLastError());
+    // FLICDdivB.f90:67-68: the normal-B fluxes are zero over the whole array
+    CUE(cudaMemsetAsync(M.flux + (size_t)(XDIR * NCONS + MAGX) * G.plane, 0, sizeof(double) * G.plane, s_));
+    CUE(cudaMemsetAsync(M.flux + (size_t)(YDIR * NCONS + MAGY) * G.plane, 0, sizeof(double) * G.plane, s_));
+    CUE(cudaStreamSynchronize(s_));
+    return HOSONO_OK;
+}
+
+int Engine::mod_update(int slot, double dt) {
+    TRYE(mod_ensure(slot));
+    K_->mod->update(batch(), slot, slots_[slot].dev.geo, slots_[slot].mod, dt, s_);
+    launches++;
+    CUE(cudaGetLastError());
+    CUE(cudaStreamSynchronize(s_));
+    return HOSONO_OK;
+}
+
+int Engine::mod_detect(int slot, int* exit_mood_loop) {
+    TRYE(mod_ensure(slot));
+    const Slot& sl = slots_[slot];
+    const Geo& G = sl.dev.geo;
+    const ModBuf& M = sl.mod;
+    const size_t plane = (size_t)G.plane;
+    // checkCell = recomputeFLICD; both flag planes start the pass cleared (detect.f90:65-68)
+    CUE(cudaMemcpyAsync(M.check, sl.dev.recF, plane, cudaMemcpyDeviceToDevice, s_));
+    CUE(cudaMemsetAsync(sl.dev.rec, 0, plane, s_));
+    CUE(cudaMemsetAsync(sl.dev.recF, 0, plane, s_));
+    CUE(cudaMemsetAsync(M.lower, 0, plane, s_));
+    CUE(cudaMemsetAsync(M.flag, 0, sizeof(int), s_));
+    const Batch B = batch();
+    K_->mod->detect(B, slot, G, M, s_);
+    K_->mod->detect_lower(B, slot, G, M, s_);
+    launches += 2;
+    CUE(cudaGetLastError());
+    int lowered = 0;
+    CUE(cudaMemcpyAsync(&lowered, M.flag, sizeof(int), cudaMemcpyDeviceToHost, s_));
+    CUE(cudaStreamSynchronize(s_));
+    if (exit_mood_loop) *exit_mood_loop = lowered ? 0 : 1;
+    return HOSONO_OK;
+}
+
+int Engine::mod_bc(int slot, int which) {
+    if (which < 0 || which > 2) return fail(HOSONO_EINVAL, "boundary target %d: 0 = U, 1 = V, 2 = Unew", which);
+    TRYE(mod_ensure(slot));
+    InstState st;
+    TRYE(state(slot, &st));
+    const InstDev& d = slots_[slot].dev;
+    double* A = which == 0 ? d.U[st.parity] : which == 1 ? d.V : role_ptr(d, st.parity, ROLE_A);
+    K_->mod->bc(batch(), slot, d.geo, A, which == 1 ? NPRIM : NCONS, s_);
+    launches++;
+    CUE(cudaGetLastError());
+    CUE(cudaStreamSynchronize(s_));
+    return HOSONO_OK;
+}
+
+int Engine::mod_bc_mood(int slot) {
+    TRYE(mod_ensure(slot));
+    InstState st;
+    TRYE(state(slot, &st));
+    const InstDev& d = slots_[slot].dev;
+    if (d.geo.bc != HOSONO_BC_PERIODIC) return HOSONO_OK;  // outflow: nothing to do (boundaryConditions.f90:39-48)
+    const ModBuf& M = slots_[slot].mod;
+    const size_t plane = (size_t)d.geo.plane;
+    K_->mod->bc_mood(batch(), slot, d.geo, M, s_);
+    launches++;
+    CUE(cudaGetLastError());
+    CUE(cudaMemcpyAsync(d.scheme[st.schemeSel], M.tSch, plane, cudaMemcpyDeviceToDevice, s_));
+    CUE(cudaMemcpyAsync(d.rec, M.tRec, plane, cudaMemcpyDeviceToDevice, s_));
+    CUE(cudaMemcpyAsync(d.recF, M.tRecF, plane, cudaMemcpyDeviceToDevice, s_));
+    CUE(cudaStreamSynchronize(s_));
+    return HOSONO_OK;
+}
+
+int Engine::riemann(int slot, int n, const double* uL, const double* uR, int dir, double* F) {
+    if (slot < 0 || slot >= maxInst_ || !slots_[slot].live) return fail(HOSONO_EINVAL, "bad slot %d", slot);
+    if (n < 0 || (dir != XDIR && dir != YDIR) || (n > 0 && (!uL || !uR || !F)))
+        return fail(HOSONO_EINVAL, "riemann: bad arguments");
+    K_->mod->riemann(slots_[slot].dev.phys, n, uL, uR, dir, F, s_);
+    launches++;
+    CUE(cudaGetLastError());
+    CUE(cudaStreamSynchronize(s_));
+    return HOSONO_OK;
 }
 
 // ----------------------------------------------------------------------

@@ -10,6 +10,7 @@
 // added or removed between launches without rebuilding a CUDA graph.
 #pragma once
 
+#include <cuda.h>  // CUtensorMap (TMA descriptors; encoded through the runtime's driver entry point)
 #include <cuda_runtime.h>
 #include <cstdint>
 
@@ -19,6 +20,11 @@
 namespace hosono {
 
 constexpr int TILE_X = 32, TILE_Y = 8;
+// the MOOD pass-1 stencil box of a tile: x in [x0-4, x0+36), y in
+// [y0-1-R, y0+9+R), all 8 conserved variables (kernels.cu P1Box; the TMA
+// descriptors are encoded for this box shape)
+constexpr int P1_SX = TILE_X + 8;
+constexpr int p1_sy(int R) { return TILE_Y + 2 * R + 1; }
 
 // Index bookkeeping of gridBlock_t (src/gridBlock.f90:36-45), 0-based:
 // cells i in [0, nxt), interior [g, g+nx); planes are pitch*nyt doubles.
@@ -56,6 +62,9 @@ struct InstDev {
     uint8_t* lowered;   // lowered by detect in this pass
     uint8_t* innerCount;  // per-cell inner lowerings of this pass (trace)
     uint8_t* detMask;     // per-stage detect_ALL terms (shock, plateau, u2 smooth)
+    // TMA descriptors of U[0..2] as (x: pitch, y: nyt, var: 8) boxes of the
+    // pass-1 stencil box shape (zero fill outside the array)
+    CUtensorMap tmU[3];
 };
 
 // Per-instance mutable scalars (device memory).
@@ -76,7 +85,7 @@ struct InstState {
     int nInner, nDetect;  // lowerings in the current pass
     int lastInner, lastDetect;  // lowerings of the last finished pass
     int passes;      // MOOD passes in the current stage
-    int passCap;     // pass limit (a stage lowers >= 1 cell per pass: R*nx*ny+1 suffices)
+    int passCap;     // pass limit of a stage (HOSONO_MOOD_CAP_DEFAULT, or set by the caller)
     int maxPasses, stages, cascadeIters, passesTotal;
     long long innerTotal, detectTotal;
     unsigned long long cflbits[2];
@@ -126,9 +135,11 @@ struct Batch {
     const int* ntiles;   // device counter
     BatchFlags* flags;
     Lists L;
+    int p1Tma;           // pass 1 stages its stencil box with TMA (1) or cp.async (0)
     int maxTiles;        // capacity of the tile list
     int maxInst;         // capacity (slots)
     const int2* instTiles;  // per slot: first tile in the tile list, tile count (0: not live)
+    const int* hold;        // per slot: nonzero = sits out the run launches (state untouched)
     // instances still in their MOOD loop after the last pass_end, in slot
     // order: (slot, first virtual tile); actInfo = {instances, tiles}.  The
     // dense kernels of the later passes walk only these tiles.
@@ -142,6 +153,36 @@ struct Batch {
 
 enum : int { CASCADE_FROM_FACES = 0, CASCADE_FROM_CELLS = 1 };
 enum : int { MOOD_FLAGS_LISTS = 0, MOOD_FLAGS_DENSE = 1, MOOD_FLAGS_LISTS_CLEAR = 2 };
+
+// Buffers of the per-module entry points (the reference's block arrays the
+// fused path does not keep), allocated on a handle's first module call.
+struct ModBuf {
+    double* fv;       // faceVals: plane ((f*nqMax + q)*8 + v), f = NORTH..WEST
+    double* flux;     // flux (gridBlock%flux): plane (dir*8 + v)
+    uint8_t* recon;   // reconstructCell of the inner cascade
+    uint8_t* adm;     // cellIsAdmissible
+    uint8_t* next;    // reconstructNextPass
+    uint8_t* check;   // detect_ALL's checkCell (recomputeFLICD on entry)
+    uint8_t* lower;   // detect_ALL's lowerCell
+    uint8_t* tRec;    // applyMOOD gathers (copied back afterwards)
+    uint8_t* tRecF;
+    int8_t* tSch;
+    int* flag;        // cells lowered by the last lowering kernel
+};
+
+// Launchers of the per-module kernels (modules.cuh) for one instance.
+struct ModuleOps {
+    void (*recon)(const Batch&, int slot, const Geo&, const ModBuf&, cudaStream_t);
+    void (*recon_lower)(const Batch&, int slot, const Geo&, const ModBuf&, cudaStream_t);
+    void (*getfluxes)(const Batch&, int slot, const Geo&, const ModBuf&, cudaStream_t);
+    void (*flicd)(const Batch&, int slot, const Geo&, const ModBuf&, cudaStream_t);
+    void (*update)(const Batch&, int slot, const Geo&, const ModBuf&, double dt, cudaStream_t);
+    void (*detect)(const Batch&, int slot, const Geo&, const ModBuf&, cudaStream_t);
+    void (*detect_lower)(const Batch&, int slot, const Geo&, const ModBuf&, cudaStream_t);
+    void (*bc_mood)(const Batch&, int slot, const Geo&, const ModBuf&, cudaStream_t);
+    void (*bc)(const Batch&, int slot, const Geo&, double* A, int nv, cudaStream_t);
+    void (*riemann)(const Phys&, int n, const double* uL, const double* uR, int dir, double* F, cudaStream_t);
+};
 
 // Launchers of one arithmetic build (kernels.cu compiled strict or fast).
 struct KernelSet {
@@ -177,6 +218,10 @@ struct KernelSet {
     void (*rk_combine2)(const Batch&, cudaStream_t);
     void (*rk_final)(const Batch&, cudaStream_t);
     void (*cons2prim_all)(const Batch&, cudaStream_t);
+    // grids the launchers use: the pass-1 kernel of radius R, and the
+    // largest grid of the other per-tile kernels (each capped at maxTiles)
+    void (*launch_info)(int R, int maxTiles, int* pass1_grid, int* tile_grid_max);
+    const ModuleOps* mod;
 };
 
 const KernelSet* kernelset_strict();

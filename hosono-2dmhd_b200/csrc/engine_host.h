@@ -47,6 +47,12 @@ class Engine {
     // ordr; any may be null) and mean / max |div B|; allocates device scratch
     int diagnostics(int slot, double* fields, int* scheme, int* ordr, double* divb_l1, double* divb_linf);
     int set_time(int slot, double t, double tmax, int nstep, int nstepmax);
+    // per slot (maxInst entries): nonzero holds the instance out of the
+    // following run() launches, its state untouched (serving priority)
+    int set_holds(const int* holds);
+    // MOOD passes a stage may take before the instance stops with
+    // HOSONO_EMOODCAP (cap <= 0: the proven bound R*nx*ny + 1)
+    int set_mood_cap(int slot, int cap);
     int state(int slot, InstState* out);
     // cfl_computedt of one instance (dt to the host)
     int cfl(int slot, double* dt);
@@ -58,6 +64,23 @@ class Engine {
     int run_profiled_step(double* pass1_ms, int* pass1_launches);
 
     int tiles_of(const hosono_params& p) const;
+    // ---- per-module form (the reference's stage modules one at a time on
+    // one instance; modules.cuh).  Host arrays in the reference's Fortran
+    // order; NULL pointers are skipped.
+    int mod_set(int slot, const int* scheme, const int* rec, const int* recF);
+    int mod_get(int slot, double* faceVals, double* fluxRaw, double* flux, double* Unew, int* scheme, int* rec,
+                int* recF);
+    int mod_reconstruct(int slot);
+    int mod_getfluxes(int slot);
+    int mod_flicd(int slot);
+    int mod_update(int slot, double dt);
+    int mod_detect(int slot, int* exit_mood_loop);
+    int mod_bc(int slot, int which);
+    int mod_bc_mood(int slot);
+    int riemann(int slot, int n, const double* uL, const double* uR, int dir, double* F);
+
+    // launch geometry of the kernels for radius R over this engine's tile capacity
+    void launch_info(int R, int* pass1_grid, int* tile_grid_max) const { K_->launch_info(R, maxTiles_, pass1_grid, tile_grid_max); }
     int live_count() const;
     size_t instance_bytes(const hosono_params& p) const;
     const hosono_params& params(int slot) const { return slots_[slot].p; }
@@ -77,6 +100,9 @@ class Engine {
     bool instance_errors_fatal = true;
     // per-slot states as of the end of the last run() (pinned host copy)
     const InstState* host_states() const { return h_st_; }
+    // launch choices (hosono_tuning); changing them rebuilds the step graphs
+    int set_tuning(const hosono_tuning& t);
+    const hosono_tuning& tuning() const { return tune_; }
     bool use_graphs = true;
     bool trace = false;
     std::vector<TraceRec> traces;
@@ -94,7 +120,13 @@ class Engine {
         InstDev dev{};
         std::vector<void*> allocs;
         int ntiles = 0;
+        ModBuf mod{};         // per-module buffers, allocated on first use
+        void* modAlloc = nullptr;
     };
+    int mod_ensure(int slot);
+    int encode_tmaps(InstDev& dev);
+    void drop_graphs();
+    hosono_tuning tune_{};
     class Rec;
     friend class Rec;
 
@@ -132,6 +164,7 @@ class Engine {
     int* d_actInfo_ = nullptr;
     int2* d_casRange_ = nullptr;
     int* d_casInfo_ = nullptr;
+    int* d_hold_ = nullptr;
     std::vector<int2> instTiles_;
     int* d_ntiles_ = nullptr;
     BatchFlags* d_flags_ = nullptr;

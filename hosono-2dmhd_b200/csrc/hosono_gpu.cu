@@ -110,6 +110,11 @@ int hosono_gpu_set_time(hosono_handle* h, double t, double tmax, int nstep, int 
     return h->eng.set_time(h->slot, t, tmax, nstep, nstepmax);
 }
 
+int hosono_gpu_set_mood_cap(hosono_handle* h, int cap) {
+    if (!h) return HOSONO_EINVAL;
+    return h->eng.set_mood_cap(h->slot, cap);
+}
+
 int hosono_gpu_step(hosono_handle* h, int max_steps, double* t_out, int* nstep_out) {
     if (!h) return HOSONO_EINVAL;
     InstState a, b;
@@ -194,6 +199,34 @@ int hosono_gpu_trace_clear(hosono_handle* h) {
     return rc;
 }
 
+int hosono_gpu_module_set(hosono_handle* h, const int* scheme, const int* recompute, const int* recompute_flicd) {
+    return h ? h->eng.mod_set(h->slot, scheme, recompute, recompute_flicd) : HOSONO_EINVAL;
+}
+int hosono_gpu_module_get(hosono_handle* h, double* faceVals, double* fluxRaw, double* flux, double* Unew,
+                          int* scheme, int* recompute, int* recompute_flicd) {
+    return h ? h->eng.mod_get(h->slot, faceVals, fluxRaw, flux, Unew, scheme, recompute, recompute_flicd)
+             : HOSONO_EINVAL;
+}
+int hosono_gpu_reconstruct(hosono_handle* h) { return h ? h->eng.mod_reconstruct(h->slot) : HOSONO_EINVAL; }
+int hosono_gpu_getfluxes(hosono_handle* h) { return h ? h->eng.mod_getfluxes(h->slot) : HOSONO_EINVAL; }
+int hosono_gpu_flicd(hosono_handle* h) { return h ? h->eng.mod_flicd(h->slot) : HOSONO_EINVAL; }
+int hosono_gpu_update(hosono_handle* h, double dt) { return h ? h->eng.mod_update(h->slot, dt) : HOSONO_EINVAL; }
+int hosono_gpu_detect(hosono_handle* h, int* exit_mood_loop) {
+    return h ? h->eng.mod_detect(h->slot, exit_mood_loop) : HOSONO_EINVAL;
+}
+int hosono_gpu_bc(hosono_handle* h, int which) { return h ? h->eng.mod_bc(h->slot, which) : HOSONO_EINVAL; }
+int hosono_gpu_bc_mood(hosono_handle* h) { return h ? h->eng.mod_bc_mood(h->slot) : HOSONO_EINVAL; }
+int hosono_gpu_mood_pass_stats(hosono_handle* h, int* npasses, long long* ntroubled) {
+    if (!h) return HOSONO_EINVAL;
+    if (npasses) *npasses = h->stats.mood_passes;
+    if (ntroubled) *ntroubled = h->stats.detect_lowered + h->stats.inner_lowered;
+    return HOSONO_OK;
+}
+int hosono_gpu_riemann(hosono_handle* h, int n, const double* uL_dev, const double* uR_dev, int dir,
+                       double* flux_dev) {
+    return h ? h->eng.riemann(h->slot, n, uL_dev, uR_dev, dir, flux_dev) : HOSONO_EINVAL;
+}
+
 int hosono_gpu_state_layout(hosono_handle* h, double** U_dev, int* pitch, long long* plane) {
     if (!h) return HOSONO_EINVAL;
     InstState st;
@@ -217,6 +250,37 @@ int hosono_gpu_set_device(int device) { return cudaSetDevice(device) == cudaSucc
 int hosono_gpu_stream(hosono_handle* h, void** stream) {
     if (!h || !stream) return HOSONO_EINVAL;
     *stream = (void*)h->eng.stream();
+    return HOSONO_OK;
+}
+
+int hosono_gpu_set_tuning(hosono_handle* h, const hosono_tuning* t) {
+    return h && t ? h->eng.set_tuning(*t) : HOSONO_EINVAL;
+}
+int hosono_gpu_get_tuning(hosono_handle* h, hosono_tuning* t) {
+    if (!h || !t) return HOSONO_EINVAL;
+    *t = h->eng.tuning();
+    return HOSONO_OK;
+}
+int hosono_batch_set_tuning(hosono_batch* b, const hosono_tuning* t) {
+    return b && t ? b->eng.set_tuning(*t) : HOSONO_EINVAL;
+}
+int hosono_batch_get_tuning(hosono_batch* b, hosono_tuning* t) {
+    if (!b || !t) return HOSONO_EINVAL;
+    *t = b->eng.tuning();
+    return HOSONO_OK;
+}
+
+int hosono_gpu_launch_info(hosono_handle* h, hosono_launch_info* info) {
+    if (!h || !info) return HOSONO_EINVAL;
+    int dev = 0, sms = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) !=
+                                                  cudaSuccess) {
+        cudaGetLastError();
+        return HOSONO_ECUDA;
+    }
+    info->tiles = h->eng.used_tiles();
+    info->sms = sms;
+    h->eng.launch_info(h->eng.params(h->slot).max_radius, &info->pass1_grid, &info->tile_grid_max);
     return HOSONO_OK;
 }
 
@@ -298,6 +362,10 @@ int hosono_batch_download(hosono_batch* b, int slot, double* U, double* V, int* 
 
 int hosono_batch_set_time(hosono_batch* b, int slot, double t, double tmax, int nstep, int nstepmax) {
     return b ? b->eng.set_time(slot, t, tmax, nstep, nstepmax) : HOSONO_EINVAL;
+}
+
+int hosono_batch_set_mood_cap(hosono_batch* b, int slot, int cap) {
+    return b ? b->eng.set_mood_cap(slot, cap) : HOSONO_EINVAL;
 }
 
 int hosono_batch_run(hosono_batch* b, int max_steps) { return b ? b->eng.run(max_steps) : HOSONO_EINVAL; }

@@ -14,10 +14,11 @@
 //
 // Index ranges (0-based) of the reference loops:
 //   reconstruct   [strt-2, stop+2] -> [g-2, g+n+1]   (reconstruct.f90:81-82)
-//   getFluxes     [strt-1, stop+2] -> [g-1, g+n+1]   (getFluxes.f90:204-205)
-//   FLICD         [strt,   stop+1] -> [g,   g+n]     (FLICDdivB.f90:301-302)
+//   getFluxes     [strt-1, stop+2] -> [g-1, g+n+1]   (getFluxes.f90:27-28)
+//   FLICD         [strt,   stop+1] -> [g,   g+n]     (FLICDdivB.f90:34-35)
 //   update/detect [strt,   stop]   -> [g,   g+n-1]   (timeStep.f90:108-109, detect.f90:81-82)
 
+#include <algorithm>
 #include <mutex>
 
 #include "engine.h"
@@ -197,8 +198,8 @@ __device__ __forceinline__ int rec_count(const Batch& B, bool next) { return rec
 // known at compile time.
 template <int R>
 struct P1Box {
-    static constexpr int SX = TILE_X + 8;          // [x0-4, x0+36)
-    static constexpr int SY = TILE_Y + 2 * R + 1;  // [y0-1-R, y0+8+R)
+    static constexpr int SX = P1_SX;     // [x0-4, x0+36)
+    static constexpr int SY = p1_sy(R);  // [y0-1-R, y0+8+R)
     static constexpr int PLANE = SX * SY;
     static constexpr int DOUBLES = NCONS * PLANE;
     static constexpr int OX = 4, OY = 1 + R;       // shared coordinates of the tile origin
@@ -239,7 +240,7 @@ __device__ __forceinline__ void gp_face_s(const double* __restrict__ sU, int sx,
 // Riemann solver needs).  dir is a run-time value: the kernel holds one copy
 // of this code (and of the Riemann solver) for both face directions, which
 // halves its instruction footprint.
-template <int R>
+template <int R, int FH>
 __device__ __forceinline__ uint8_t pass1_face(const InstDev& d, const double* __restrict__ sU,
                                               const double* __restrict__ sPv, int sx, int sy, int dir, bool needL,
                                               bool needR, bool doFlux, long long c, double* acc) {
@@ -257,15 +258,15 @@ __device__ __forceinline__ uint8_t pass1_face(const InstDev& d, const double* __
         double uL[NCONS], uR[NCONS];
         if (needL) {
             gp_face_s<R, R>(sU, lx, ly, sPv + P1Box<R>::NS * (q + P1Box<R>::NQ * FL), uL);
-            if (!admissible(uL[DENS], cons2pres(P, uL))) bits |= 1;
+            if (!admissible(uL[DENS], cons2pres<FH>(P, uL))) bits |= 1;
         }
         if (needR) {
             gp_face_s<R, R>(sU, sx, sy, sPv + P1Box<R>::NS * (q + P1Box<R>::NQ * FR), uR);
-            if (!admissible(uR[DENS], cons2pres(P, uR))) bits |= 2;
+            if (!admissible(uR[DENS], cons2pres<FH>(P, uR))) bits |= 2;
         }
         if (doFlux) {
             double F[NCONS];
-            hllc(P, uL, uR, dir, F);
+            hllc<FH>(P, uL, uR, dir, F);
             const double w = qw_at(d, R, q);
 #pragma unroll
             for (int v = 0; v < NCONS; v++) acc[v * NTHREADS] = acc[v * NTHREADS] + w * F[v];
@@ -278,6 +279,34 @@ __device__ __forceinline__ uint8_t pass1_face(const InstDev& d, const double* __
         (x ? d.CTX : d.CTY)[c] = acc[(x ? MAGY : MAGX) * NTHREADS];
     }
     return bits;
+}
+
+// the x- and y-faces of one cell of the staged tile (sim_forceHydro fixed at
+// compile time); returns whether any face state failed CAD/PAD
+template <int R, int FH>
+__device__ __forceinline__ bool pass1_tile(const InstDev& d, const double* __restrict__ sU,
+                                           const double* __restrict__ sPv, const Cell& c, double* acc) {
+    using Box = P1Box<R>;
+    const Geo& G = d.geo;
+    const int i = c.i, j = c.j;
+    const int g = G.g;
+    const int clo = g - 2, cxhi = g + G.nx + 1, cyhi = g + G.ny + 1;  // reconstruct range
+    const int flo = g - 1, fxhi = g + G.nx + 1, fyhi = g + G.ny + 1;  // flux range
+    const int sx = threadIdx.x + Box::OX, sy = threadIdx.y + Box::OY;
+    const long long cc = (long long)j * G.pitch + i;
+    const bool inF = i >= flo && i <= fxhi && j >= flo && j <= fyhi;
+    bool bad = false;
+#pragma unroll 1
+    for (int dir = XDIR; dir <= YDIR; dir++) {  // the x-face, then the y-face of this cell
+        const bool x = dir == XDIR;
+        if (i >= clo && i <= cxhi + (x ? 1 : 0) && j >= clo && j <= cyhi + (x ? 0 : 1)) {
+            const int a = x ? i : j, ahi = x ? cxhi : cyhi;
+            const uint8_t bits = pass1_face<R, FH>(d, sU, sPv, sx, sy, dir, a - 1 >= clo, a <= ahi, inF, cc, acc);
+            (x ? d.failX : d.failY)[cc] = bits;
+            bad |= bits != 0;
+        }
+    }
+    return bad;
 }
 
 // 16-byte asynchronous copy global -> shared (cp.async); src_bytes = 0
@@ -294,6 +323,57 @@ __device__ __forceinline__ void cp_async8(void* dst, const void* src) {
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+// ---- TMA staging (cp.async.bulk.tensor with an mbarrier; 1-GPU memory
+// only, no multicast).  One thread issues the copies of a box; every thread
+// waits on the box's mbarrier.  Waits are bounded: after about two seconds a
+// wait gives up and the kernel reports HOSONO_ETIMEOUT instead of hanging.
+constexpr long long kWaitCycles = 4000000000LL;
+__device__ __forceinline__ unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(uint64_t* bar) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_addr(bar)) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+}
+// true once the barrier's phase `parity` has completed; false after kWaitCycles
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity) {
+    const unsigned a = smem_addr(bar);
+    const long long t0 = clock64();
+    for (;;) {
+        unsigned done;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(done)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (done) return true;
+        if (clock64() - t0 > kWaitCycles) return false;
+    }
+}
+// a (x, y, var) box of the tensor map into shared memory; x * 8 bytes is a
+// multiple of 16 (x = x0 - 4 with x0 a multiple of 32) and may be negative
+// (zero fill), as may y
+__device__ __forceinline__ void tma_box3(void* dst, const CUtensorMap* tm, int x, int y, int z, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+        "[%5];\n" ::"r"(smem_addr(dst)),
+        "l"(tm), "r"(x), "r"(y), "r"(z), "r"(smem_addr(bar))
+        : "memory");
+}
+// contiguous bytes (a multiple of 16, both addresses 16-byte aligned)
+__device__ __forceinline__ void bulk_copy(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+            smem_addr(dst)),
+        "l"(src), "r"(bytes), "r"(smem_addr(bar))
+        : "memory");
+}
 
 // next tile at or after t (stride gridDim.x) that this launch works on
 template <int R>
@@ -329,29 +409,75 @@ __device__ __forceinline__ void pass1_stage(const Batch& B, int uin, int t, doub
     cp_async_commit();
 }
 
+// the same staging by TMA: one (x, y, var) box of the stage input's tensor
+// map and one bulk copy of the prediction vectors, both completing on `bar`
+template <int R>
+__device__ __forceinline__ void pass1_stage_tma(const Batch& B, int uin, int t, double* dst, double* dstPv,
+                                                uint64_t* bar) {
+    using Box = P1Box<R>;
+    const int4 tl = B.tiles[t];
+    const InstDev& d = B.dev[tl.x];
+    const int par = B.st[tl.x].parity;
+    const int u = uin == ROLE_STATE ? par : uin == ROLE_A ? 1 - par : 2;  // role_ptr's buffer index
+    mbar_expect_tx(bar, (unsigned)((Box::DOUBLES + Box::PVN) * sizeof(double)));
+    tma_box3(dst, &d.tmU[u], tl.y - Box::OX, tl.z - Box::OY, 0, bar);
+    bulk_copy(dstPv, d.pv + (long long)Box::PVN * (R - 1), (unsigned)(Box::PVN * sizeof(double)), bar);
+}
+
 // One launch per radius: blocks skip tiles of instances with another GP
 // radius.  Shared memory: two stencil boxes with their prediction vectors
 // (the next tile's are copied in asynchronously while the current one is
-// computed) and the per-thread flux accumulators.
-template <int R>
+// computed), the per-thread flux accumulators and, with TMA staging, the two
+// boxes' mbarriers.  TMA = false stages with per-thread cp.async copies.
+template <int R, bool TMA>
 __global__ void __launch_bounds__(NTHREADS, HOSONO_PASS1_MIN_BLOCKS) k_face_pass1(Batch B, int uin) {
-    extern __shared__ double smem[];
+    extern __shared__ __align__(128) double smem[];
     using Box = P1Box<R>;
     const int tid = threadIdx.y * TILE_X + threadIdx.x;
     double* acc = smem + 2 * Box::DOUBLES + tid;
     double* pvBuf = smem + 2 * Box::DOUBLES + NCONS * NTHREADS;  // two PVN-double buffers
+    uint64_t* bars = reinterpret_cast<uint64_t*>(pvBuf + 2 * Box::PVN);
     if (!(B.flags->radii & (1 << R))) return;  // no instance of this radius
+    if (TMA) {
+        if (tid == 0) {
+            mbar_init(bars);
+            mbar_init(bars + 1);
+            mbar_fence_init();
+        }
+        __syncthreads();
+    }
+    unsigned phase = 0;  // bit b: parity of buffer b's next completion
     const int n = __ldg(B.ntiles);
     int t = pass1_next<R>(B, blockIdx.x, n);
     int buf = 0;
-    if (t < n) pass1_stage<R>(B, uin, t, smem, pvBuf, tid);
+    if (t < n) {
+        if (!TMA)
+            pass1_stage<R>(B, uin, t, smem, pvBuf, tid);
+        else if (tid == 0)
+            pass1_stage_tma<R>(B, uin, t, smem, pvBuf, bars);
+    }
     while (t < n) {
         const int tn = pass1_next<R>(B, t + gridDim.x, n);
-        if (tn < n) {
-            pass1_stage<R>(B, uin, tn, smem + (buf ^ 1) * Box::DOUBLES, pvBuf + (buf ^ 1) * Box::PVN, tid);
-            cp_async_wait<1>();
+        if (!TMA) {
+            if (tn < n) {
+                pass1_stage<R>(B, uin, tn, smem + (buf ^ 1) * Box::DOUBLES, pvBuf + (buf ^ 1) * Box::PVN, tid);
+                cp_async_wait<1>();
+            } else {
+                cp_async_wait<0>();
+            }
         } else {
-            cp_async_wait<0>();
+            if (tn < n && tid == 0)
+                pass1_stage_tma<R>(B, uin, tn, smem + (buf ^ 1) * Box::DOUBLES, pvBuf + (buf ^ 1) * Box::PVN,
+                                   bars + (buf ^ 1));
+            const bool ok = mbar_wait(bars + buf, (phase >> buf) & 1u);
+            phase ^= 1u << buf;
+            if (!__syncthreads_and(ok)) {
+                // a copy that never lands: report it, let the copies in flight
+                // finish (bounded), and leave without reading the box
+                if (tid == 0) atomicExch(&B.flags->error, HOSONO_ETIMEOUT);
+                if (tn < n) mbar_wait(bars + (buf ^ 1), (phase >> (buf ^ 1)) & 1u);
+                return;
+            }
         }
         __syncthreads();  // tile t's box is in place for every thread
         const double* sU = smem + buf * Box::DOUBLES;
@@ -359,27 +485,9 @@ __global__ void __launch_bounds__(NTHREADS, HOSONO_PASS1_MIN_BLOCKS) k_face_pass
         const Cell c = tile_at(B, t);
         InstState& S = B.st[c.k];
         const InstDev& d = B.dev[c.k];
-        const Geo& G = d.geo;
         if (first_tile_thread(c)) S.cascadeMode = CASCADE_FROM_FACES;
-        const int i = c.i, j = c.j;
-        const int g = G.g;
-        const int clo = g - 2, cxhi = g + G.nx + 1, cyhi = g + G.ny + 1;  // reconstruct range
-        const int flo = g - 1, fxhi = g + G.nx + 1, fyhi = g + G.ny + 1;  // flux range
-        const int sx = threadIdx.x + Box::OX, sy = threadIdx.y + Box::OY;
-        const long long cc = (long long)j * G.pitch + i;
-        const bool inF = i >= flo && i <= fxhi && j >= flo && j <= fyhi;
-        bool bad = false;
-#pragma unroll 1
-        for (int dir = XDIR; dir <= YDIR; dir++) {  // the x-face, then the y-face of this cell
-            const bool x = dir == XDIR;
-            if (i >= clo && i <= cxhi + (x ? 1 : 0) && j >= clo && j <= cyhi + (x ? 0 : 1)) {
-                const int a = x ? i : j, ahi = x ? cxhi : cyhi;
-                const uint8_t bits =
-                    pass1_face<R>(d, sU, sPv, sx, sy, dir, a - 1 >= clo, a <= ahi, inF, cc, acc);
-                (x ? d.failX : d.failY)[cc] = bits;
-                bad |= bits != 0;
-            }
-        }
+        // one instance per tile: the branch is uniform over the block
+        const bool bad = d.phys.force_hydro ? pass1_tile<R, 1>(d, sU, sPv, c, acc) : pass1_tile<R, 0>(d, sU, sPv, c, acc);
         warp_flag(&S.anyFail, bad);
         __syncthreads();  // every read of this box is done before it is refilled
         buf ^= 1;
@@ -629,7 +737,7 @@ __global__ void __launch_bounds__(256) k_recon_group(Batch B, int uin, int which
 
 // After the face cascade of a later MOOD pass: the faces getFluxes_ recomputes
 // (x-face (i,j) if recompute(i,j) or (i-1,j), y-face if recompute(i,j) or
-// (i,j-1), on [g-1, g+n+1]^2, getFluxes.f90:204-250) and the cells FLICD,
+// (i,j-1), on [g-1, g+n+1]^2, getFluxes.f90:27-89) and the cells FLICD,
 // the update and detect visit (recomputeFLICD on [g, g+n]^2).
 __device__ __forceinline__ void t_compact_post(const Batch& B, const Cell c) {
     const InstState& S = B.st[c.k];
@@ -1280,7 +1388,7 @@ __global__ void __launch_bounds__(NTHREADS) k_stage_init(Batch B) {
 }
 
 // ======================================================================
-// boundary conditions (boundaryConditions.f90:291-360) as a gather
+// boundary conditions (boundaryConditions.f90:79-187) as a gather
 __device__ __forceinline__ int bc_src(int i, int n, int g, int bc) {
     if (i < g) return bc == 1 ? i + n : g;
     if (i >= g + n) return bc == 1 ? i - n : g + n - 1;
@@ -1427,7 +1535,7 @@ __global__ void __launch_bounds__(NTHREADS) k_cfl_reduce(Batch B) {
 }
 
 // Step begin: dt = cfl * min(dx/xmax, dy/ymax) (cfl.f90:50) and validTimeStep
-// (mhd_driver.f90:239-266: clamp to tmax first, then reject negative, NaN or
+// (mhd_driver.f90:117-144: clamp to tmax first, then reject negative, NaN or
 // infinite dt).  With use_host_dt the host already stored dt.
 __global__ void k_step_begin(Batch B, int use_host_dt) {
     for (int k = threadIdx.x; k < B.maxInst; k += blockDim.x) {
@@ -1454,14 +1562,14 @@ __global__ void k_step_begin(Batch B, int use_host_dt) {
 __global__ void k_step_prepare(Batch B, int /*unused*/) {
     for (int k = threadIdx.x; k < B.maxInst; k += blockDim.x) {
         InstState& S = B.st[k];
-        S.stepping = (S.live && !S.done) ? 1 : 0;
+        S.stepping = (S.live && !S.done && !B.hold[k]) ? 1 : 0;
         S.cflbits[0] = 0;
         S.cflbits[1] = 0;
     }
 }
 
 // Step end: the new state is buffer A (parity flips), t += dt, nstep += 1,
-// and the time-loop test of mhd_driver.f90:198; next step's participants and
+// and the time-loop test of mhd_driver.f90:76; next step's participants and
 // the batch condition.
 __global__ void k_step_end(Batch B, cudaGraphConditionalHandle h, int set_handle) {
     __shared__ int any;
@@ -1478,7 +1586,7 @@ __global__ void k_step_end(Batch B, cudaGraphConditionalHandle h, int set_handle
         S.stepping = 0;  // at rest between launches; step_prepare picks the next participants
         S.cflbits[0] = 0;
         S.cflbits[1] = 0;
-        if (S.live && !S.done) any = 1;
+        if (S.live && !S.done && !B.hold[k]) any = 1;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -1528,15 +1636,27 @@ void l_step_end(const Batch& B, cudaGraphConditionalHandle h, cudaStream_t s) {
     k_step_end<<<1, 128, 0, s>>>(B, h, h != 0);
 }
 void l_stage_init(const Batch& B, cudaStream_t s) { TILE_LAUNCH(k_stage_init, B, s); }
+// dynamic shared memory of the pass-1 kernel of radius R: two boxes, the
+// accumulators, two prediction-vector buffers and two mbarriers
+template <int R>
+constexpr int pass1_smem() {
+    return (2 * P1Box<R>::DOUBLES + NCONS * NTHREADS + 2 * P1Box<R>::PVN) * (int)sizeof(double) + 2 * 8;
+}
+template <int R, bool TMA>
+int pass1_grid(int maxTiles) {
+    static const bool attr =  // once per process (thread-safe static initialisation)
+        cudaFuncSetAttribute((const void*)k_face_pass1<R, TMA>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             pass1_smem<R>()) == cudaSuccess;
+    (void)attr;
+    const int r = resident_blocks((const void*)k_face_pass1<R, TMA>, pass1_smem<R>());
+    return r < maxTiles ? r : maxTiles;
+}
 template <int R>
 void launch_pass1(const Batch& B, int uin, cudaStream_t s) {
-    constexpr int smem = (2 * P1Box<R>::DOUBLES + NCONS * NTHREADS + 2 * P1Box<R>::PVN) * (int)sizeof(double);
-    static const bool attr =  // once per process (thread-safe static initialisation)
-        cudaFuncSetAttribute((const void*)k_face_pass1<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) ==
-        cudaSuccess;
-    (void)attr;
-    const int r = resident_blocks((const void*)k_face_pass1<R>, smem);
-    k_face_pass1<R><<<dim3((unsigned)(r < B.maxTiles ? r : B.maxTiles)), kTile, smem, s>>>(B, uin);
+    if (B.p1Tma)
+        k_face_pass1<R, true><<<dim3((unsigned)pass1_grid<R, true>(B.maxTiles)), kTile, pass1_smem<R>(), s>>>(B, uin);
+    else
+        k_face_pass1<R, false><<<dim3((unsigned)pass1_grid<R, false>(B.maxTiles)), kTile, pass1_smem<R>(), s>>>(B, uin);
 }
 void l_face_pass1(const Batch& B, int uin, cudaStream_t s) {
     launch_pass1<2>(B, uin, s);
@@ -1579,6 +1699,22 @@ void l_bc_fill(const Batch& B, int role, cudaStream_t s) { TILE_LAUNCH(k_bc_fill
 void l_rk_combine2(const Batch& B, cudaStream_t s) { TILE_LAUNCH(k_rk_combine2, B, s); }
 void l_rk_final(const Batch& B, cudaStream_t s) { TILE_LAUNCH(k_rk_final, B, s); }
 void l_cons2prim_all(const Batch& B, cudaStream_t s) { TILE_LAUNCH(k_cons2prim_all, B, s); }
+void l_launch_info(int R, int maxTiles, int* pass1, int* tile_grid_max) {
+    *pass1 = R == 1 ? pass1_grid<1, false>(maxTiles) : R == 2 ? pass1_grid<2, false>(maxTiles) : pass1_grid<3, false>(maxTiles);
+    const void* tile_kernels[] = {(const void*)k_cfl_reduce,     (const void*)k_stage_init,   (const void*)k_clear_nextpass,
+                                  (const void*)k_cascade_lower,  (const void*)k_compact_next, (const void*)k_compact_post,
+                                  (const void*)k_compact_dirty,  (const void*)k_ct_update_detect, (const void*)k_mood_flags,
+                                  (const void*)k_bc_fill,        (const void*)k_rk_combine2,  (const void*)k_rk_final,
+                                  (const void*)k_cons2prim_all};
+    int mx = 0;
+    for (const void* k : tile_kernels) {
+        const int r = resident_blocks(k);
+        mx = std::max(mx, r < maxTiles ? r : maxTiles);
+    }
+    *tile_grid_max = mx;
+}
+
+#include "modules.cuh"
 
 const KernelSet kset = {
 #if HOSONO_FAST
@@ -1589,7 +1725,7 @@ const KernelSet kset = {
     l_cfl_reduce, l_step_prepare, l_step_begin, l_step_end, l_stage_init, l_face_pass1, l_cascade_cond, l_cascade_lower,
     l_recon_check, l_ct_update_detect, l_mood_flags, l_pass_end, l_recon_list,
     l_compact_post, l_compact_dirty, l_flux_list, l_ct_list, l_clear_low, l_bc_fill, l_rk_combine2, l_rk_final,
-    l_cons2prim_all};
+    l_cons2prim_all, l_launch_info, &mops};
 
 }  // namespace KNS
 

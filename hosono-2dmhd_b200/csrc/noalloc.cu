@@ -18,10 +18,17 @@
 //     last call's contents; each call writes every slot it later reads, so no
 //     clearing is needed -- but calls whose kernels overlap on the GPU (two
 //     streams, two threads) race on it and must be serialised by the caller;
-//   * the first call on each device resolves the array's device address with
-//     cudaGetSymbolAddress (the host-side symbol is only a stand-in and must
-//     never be handed to a kernel); make that first call before any stream
-//     capture begins.
+//   * the array's device address comes from cudaGetSymbolAddress with the
+//     device current (the host-side symbol is only a stand-in and must never
+//     be handed to a kernel).  A call on a stream that is not capturing looks
+//     it up afresh, so the address stays right after a cudaDeviceReset or a
+//     context re-creation reloads the module; a call on a capturing stream
+//     uses the address the last such call found.  So the first call on each
+//     device must come before any stream capture begins (a capturing first
+//     call returns HOSONO_EINVAL);
+//   * errors: the kernels are launched with cudaLaunchKernel and only its own
+//     return codes are reported, so an earlier, unrelated error pending on the
+//     calling thread is neither returned nor cleared.
 
 #include "hosono_gpu.h"
 #include "physics.cuh"
@@ -110,13 +117,23 @@ __global__ void __launch_bounds__(kThreads) k_cfl_final(const double* __restrict
     if (threadIdx.x == 0) *dt = cfl * fmin(dx / xm, dy / ym);
 }
 
-// device address of the scratch array on the current device (set-up once per device)
-int scratch_for_current_device(double** out) {
+// device address of the scratch array on the current device: looked up
+// afresh outside a stream capture (a device reset reloads the module at a new
+// address), taken from the last lookup inside one
+int scratch_for_current_device(cudaStream_t s, double** out) {
     int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess) return HOSONO_ECUDA;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        cudaGetLastError();  // this call's own failure
+        return HOSONO_ECUDA;
+    }
     if (dev < 0 || dev >= kMaxDevices) return HOSONO_EINVAL;
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &cap) != cudaSuccess) {
+        cudaGetLastError();  // e.g. the legacy stream while another stream captures
+        cap = cudaStreamCaptureStatusActive;
+    }
     std::lock_guard<std::mutex> lock(g_mutex);
-    if (!g_scratch[dev]) {
+    if (cap == cudaStreamCaptureStatusNone) {
         void* p = nullptr;
         if (cudaGetSymbolAddress(&p, g_cfl_row_max) != cudaSuccess || !p) {
             cudaGetLastError();
@@ -124,6 +141,7 @@ int scratch_for_current_device(double** out) {
         }
         g_scratch[dev] = static_cast<double*>(p);
     }
+    if (!g_scratch[dev]) return HOSONO_EINVAL;  // first call on this device inside a capture
     *out = g_scratch[dev];
     return HOSONO_OK;
 }
@@ -136,11 +154,21 @@ extern "C" int hosono_cfl_noalloc(const double* V_dev, int nx, int ny, int ngc, 
         plane < (long long)pitch * (ny + 2 * ngc) || !(dx > 0) || !(dy > 0))
         return HOSONO_EINVAL;
     if (ny > HOSONO_NOALLOC_MAX_ROWS) return HOSONO_EINVAL;  // scratch holds one slot pair per row
-    double* rows = nullptr;
-    const int rc = scratch_for_current_device(&rows);
-    if (rc) return rc;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    k_cfl_rows<<<ny, kThreads, 0, s>>>(V_dev, nx, ngc, pitch, plane, force_hydro ? 1 : 0, rows);
-    k_cfl_final<<<1, kThreads, 0, s>>>(rows, ny, dx, dy, cfl, dt_dev);
-    return cudaGetLastError() == cudaSuccess ? HOSONO_OK : HOSONO_ECUDA;
+    double* rows = nullptr;
+    const int rc = scratch_for_current_device(s, &rows);
+    if (rc) return rc;
+    int fh = force_hydro ? 1 : 0;
+    void* rowArgs[] = {(void*)&V_dev, (void*)&nx, (void*)&ngc, (void*)&pitch, (void*)&plane, (void*)&fh, (void*)&rows};
+    cudaError_t e = cudaLaunchKernel((const void*)k_cfl_rows, dim3((unsigned)ny), dim3(kThreads), rowArgs, 0, s);
+    if (e == cudaSuccess) {
+        const double* rowsIn = rows;
+        void* finArgs[] = {(void*)&rowsIn, (void*)&ny, (void*)&dx, (void*)&dy, (void*)&cfl, (void*)&dt_dev};
+        e = cudaLaunchKernel((const void*)k_cfl_final, dim3(1), dim3(kThreads), finArgs, 0, s);
+    }
+    if (e != cudaSuccess) {
+        cudaGetLastError();  // the launch's own error, reported by the return value
+        return HOSONO_ECUDA;
+    }
+    return HOSONO_OK;
 }

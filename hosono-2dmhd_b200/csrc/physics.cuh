@@ -25,6 +25,16 @@ struct Phys {
     int force_hydro;
 };
 
+// sim_forceHydro as a run-time flag (FH = -1) or as a compile-time constant
+// (FH = 0: MHD, 1: hydro), for kernels instantiated per mode.  The
+// expressions are the same either way; with a constant the compiler drops
+// the other mode's branch and keeps the magnetic field of an MHD state in
+// the registers of the conserved variables.
+template <int FH>
+__device__ __forceinline__ bool hydro(const Phys& s) {
+    return FH < 0 ? s.force_hydro != 0 : FH != 0;
+}
+
 // src/eos.f90:9-26 (pressure floor)
 __device__ __forceinline__ double eos_pres(const Phys& s, double dens, double eint) {
     double pres = (s.gamma - 1.0) * dens * eint;
@@ -63,9 +73,10 @@ __device__ __forceinline__ void cons2prim(const Phys& s, const double* U, double
 }
 
 // src/convert.f90:236-254 (not floored; SUM starts from zero)
+template <int FH = -1>
 __device__ __forceinline__ double cons2pres(const Phys& s, const double* U) {
     double Bp;
-    if (s.force_hydro)
+    if (hydro<FH>(s))
         Bp = 0.0;
     else
         Bp = 0.5 * ((0.0 + U[MAGX] * U[MAGX]) + U[MAGY] * U[MAGY] + U[MAGZ] * U[MAGZ]);
@@ -141,10 +152,10 @@ struct Side {
     double rho, vx, vy, vz, p, bx, by, bz;
     typename D::R rrho;  // the density as a shared denominator
 };
-template <class D>
+template <int FH, class D>
 __device__ __forceinline__ void side_prim(const Phys& s, const double* U, Side<D>& V, D& dv) {
     double Bp;
-    if (s.force_hydro)
+    if (hydro<FH>(s))
         Bp = 0.0;
     else
         Bp = 0.5 * (U[MAGX] * U[MAGX] + U[MAGY] * U[MAGY] + U[MAGZ] * U[MAGZ]);
@@ -156,9 +167,9 @@ __device__ __forceinline__ void side_prim(const Phys& s, const double* U, Side<D
     V.vz = dv.div(U[MOMZ], V.rrho);
     const double eint = dv.div(U[ENER] - Bp, V.rrho) - 0.5 * (V.vx * V.vx + V.vy * V.vy + V.vz * V.vz);
     V.p = eos_pres(s, density, eint);
-    V.bx = s.force_hydro ? 0.0 : U[MAGX];
-    V.by = s.force_hydro ? 0.0 : U[MAGY];
-    V.bz = s.force_hydro ? 0.0 : U[MAGZ];
+    V.bx = hydro<FH>(s) ? 0.0 : U[MAGX];
+    V.by = hydro<FH>(s) ? 0.0 : U[MAGY];
+    V.bz = hydro<FH>(s) ? 0.0 : U[MAGZ];
 }
 template <class D>
 __device__ __forceinline__ double side_vel(const Side<D>& V, int c) {
@@ -179,11 +190,11 @@ __device__ __forceinline__ double side_cf(const Phys& s, double rho0, double p0,
 }
 
 // cons2flux (convert.f90:28-92) of one side
-template <class D>
+template <int FH, class D>
 __device__ __forceinline__ void side_flux(const Phys& s, const double* U, const Side<D>& V, int dir, double* F,
                                           D& dv) {
     double Bp = 0.0;
-    if (!s.force_hydro) Bp = 0.5 * (U[MAGX] * U[MAGX] + U[MAGY] * U[MAGY] + U[MAGZ] * U[MAGZ]);
+    if (!hydro<FH>(s)) Bp = 0.5 * (U[MAGX] * U[MAGX] + U[MAGY] * U[MAGY] + U[MAGZ] * U[MAGZ]);
     const double E = U[ENER];
     const double Ptot = V.p + Bp;
     // normal (N) and tangential (T1, T2 = z) components; the array slots are
@@ -197,7 +208,7 @@ __device__ __forceinline__ void side_flux(const Phys& s, const double* U, const 
     double fT2 = mN * vT2;
     double fE = (E + Ptot) * vN;
     double gT1 = 0.0, gT2 = 0.0;  // induction fluxes; the normal one is 0
-    if (!s.force_hydro) {
+    if (!hydro<FH>(s)) {
         fN = fN - BN * BN;
         fT1 = fT1 - BT1 * BN;
         fT2 = fT2 - BT2 * BN;
@@ -220,12 +231,12 @@ __device__ __forceinline__ void side_flux(const Phys& s, const double* U, const 
 // computed: a supersonic face (flux = fL or fR) evaluates one physical flux
 // and no HLL or star state, and the star state is evaluated once, on the
 // operands of the chosen side.
-template <class D>
+template <int FH, class D>
 __device__ __forceinline__ void hllc_t(const Phys& s, const double* uL, const double* uR, int dir, double* flux,
                                        D& dv) {
     Side<D> L, R;
-    side_prim(s, uL, L, dv);
-    side_prim(s, uR, R, dv);
+    side_prim<FH>(s, uL, L, dv);
+    side_prim<FH>(s, uR, R, dv);
     // array slots of the normal / first tangential components are chosen by
     // selects, so a run-time dir keeps every array in registers
     const bool x = dir == XDIR;
@@ -262,14 +273,14 @@ __device__ __forceinline__ void hllc_t(const Phys& s, const double* uL, const do
         side = 3;
     if (side == 0 || side == 3) {
         if (side == 0)
-            side_flux(s, uL, L, dir, flux, dv);
+            side_flux<FH>(s, uL, L, dir, flux, dv);
         else
-            side_flux(s, uR, R, dir, flux, dv);
+            side_flux<FH>(s, uR, R, dir, flux, dv);
         return;
     }
     double fL[NCONS], fR[NCONS];
-    side_flux(s, uL, L, dir, fL, dv);
-    side_flux(s, uR, R, dir, fR, dv);
+    side_flux<FH>(s, uL, L, dir, fL, dv);
+    side_flux<FH>(s, uR, R, dir, fR, dv);
     double uHLL[NCONS];
     const typename D::R rS = dv.recip(sR - sL);
 #pragma unroll
@@ -313,17 +324,19 @@ __device__ __forceinline__ void hllc_t(const Phys& s, const double* uL, const do
 }
 
 // the Riemann solver with IEEE division throughout (the rare fallback)
+template <int FH>
 static __device__ __noinline__ void hllc_ieee(const Phys& s, const double* uL, const double* uR, int dir, double* flux) {
     IeeeDiv dv;
-    hllc_t(s, uL, uR, dir, flux, dv);
+    hllc_t<FH>(s, uL, uR, dir, flux, dv);
 }
 
 // HLLC with shared reciprocals; any operand outside their proven range sends
 // the whole solve through IEEE division instead (same result bits either way)
+template <int FH = -1>
 __device__ __forceinline__ void hllc(const Phys& s, const double* uL, const double* uR, int dir, double* flux) {
     SharedRecipDiv dv;
-    hllc_t(s, uL, uR, dir, flux, dv);
-    if (!dv.ok) hllc_ieee(s, uL, uR, dir, flux);
+    hllc_t<FH>(s, uL, uR, dir, flux, dv);
+    if (!dv.ok) hllc_ieee<FH>(s, uL, uR, dir, flux);
 }
 
 // src/detect.f90:250-265 (CAD) and :238-248 (PAD): both finite (not NaN,

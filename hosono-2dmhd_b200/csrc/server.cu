@@ -1,17 +1,23 @@
 // server.cu -- the serving layer of include/hosono_gpu.h (no counterpart in
-// the reference): a FIFO of solves, admission by a device-memory budget, and
-// continuous batching of every resident solve over one Engine.
+// the reference): a queue of solves, admission by a device-memory budget, and
+// continuous batching of the resident solves over one Engine, under one of
+// two policies (FIFO; or shortest estimated work first with an aging bound,
+// HOSONO_SERVE_SHORTEST).
 //
 // Threads: callers submit, wait, poll and ask for snapshots under one mutex;
 // a scheduler thread owns the Engine, the CUDA stream and the budget arena,
 // and is the only thread that makes CUDA calls.  Its loop:
-//   admit    -- while the queue head fits (slot, tiles, a free arena range):
-//               Engine::add on arena memory, one tile-list upload for all,
-//               then upload each initial state and set its time limits;
+//   admit    -- while the next solve (the queue head, or under SHORTEST the
+//               oldest past the aging bound, else the least estimated work)
+//               fits (slot, tiles, a free arena range): Engine::add on arena
+//               memory, one tile-list upload for all, then upload each
+//               initial state and set its time limits;
 //   snapshot -- copy out resident solves that callers asked for;
 //   launch   -- one batched run of up to `steps` time steps (one graph
 //               launch); `steps` follows the measured time per step so that
-//               a launch takes about chunk_ms;
+//               a launch takes about chunk_ms.  Under SHORTEST the residents
+//               with the most estimated remaining work sit the launch out
+//               (Engine::set_holds) once the others fill fill_tiles tiles;
 //   retire   -- solves whose InstState says done: copy the final state to
 //               the caller's buffers, free the slot and the arena range.
 // Each solve keeps its own t, dt, MOOD loop and limits inside the batch, so
@@ -60,6 +66,8 @@ struct Request {
     int* outScheme = nullptr;
     int tiles = 0;
     int baseNstep = 0;
+    double work = 0;         // estimated work: interior cells x tmax / min(dx, dy)
+    double lastStep_s = 0;   // server clock when it last took part in a launch (or was admitted)
     hosono_request_info info{};
 };
 
@@ -244,19 +252,45 @@ class Scheduler {
         return S->resident.empty();
     }
 
+    // the queued solve to admit next: the head (FIFO); or the oldest solve
+    // past the aging bound, else the one with the least estimated work that
+    // was not passed over in this admission round (SHORTEST).  `aged` tells
+    // the caller not to pass over it.  Caller holds S->mu.
+    Request* pick_locked(const std::vector<Request*>& passed, bool* aged) {
+        *aged = true;
+        if (S->cfg.policy != HOSONO_SERVE_SHORTEST) return S->queue.front();
+        const double now = clock_s();
+        for (Request* r : S->queue)  // queue order is arrival order
+            if (now - r->info.submit_s >= S->cfg.aging_s) return r;
+        *aged = false;
+        Request* best = nullptr;
+        for (Request* r : S->queue)
+            if (std::find(passed.begin(), passed.end(), r) == passed.end() && (!best || r->work < best->work)) best = r;
+        return best;
+    }
+
     int admit() {
-        std::vector<Request*> added;
+        std::vector<Request*> added, passed;
         for (;;) {
             Request* r = nullptr;
+            bool aged = true;
             {
                 std::lock_guard<std::mutex> lk(S->mu);
                 if (S->queue.empty() || S->stop) break;
-                r = S->queue.front();
+                r = pick_locked(passed, &aged);
+                if (!r) break;  // every queued solve was passed over this round
             }
-            if (eng->live_count() >= eng->max_inst() || eng->used_tiles() + r->tiles > eng->max_tiles()) {
+            if (eng->live_count() >= eng->max_inst()) {
                 std::lock_guard<std::mutex> lk(S->mu);
                 S->st.head_blocked++;
                 break;
+            }
+            if (eng->used_tiles() + r->tiles > eng->max_tiles()) {
+                std::lock_guard<std::mutex> lk(S->mu);
+                S->st.head_blocked++;
+                if (aged) break;
+                passed.push_back(r);
+                continue;
             }
             const size_t before = mem.arena.used();
             int slot = -1;
@@ -264,10 +298,12 @@ class Scheduler {
             if (rc == HOSONO_ENOMEM && eng->live_count() > 0) {  // wait for a retirement
                 std::lock_guard<std::mutex> lk(S->mu);
                 S->st.head_blocked++;
-                break;
+                if (aged) break;
+                passed.push_back(r);
+                continue;
             }
             std::lock_guard<std::mutex> lk(S->mu);
-            S->queue.pop_front();
+            S->queue.erase(std::find(S->queue.begin(), S->queue.end(), r));
             if (rc == HOSONO_ECUDA) return rc;
             if (rc) {  // cannot ever be admitted
                 finish_locked(S, r, rc);
@@ -277,6 +313,7 @@ class Scheduler {
             r->info.state = HOSONO_REQ_RUNNING;
             r->info.slot = slot;
             r->info.admit_s = clock_s();
+            r->lastStep_s = r->info.admit_s;
             r->info.device_bytes = (long long)(mem.arena.used() - before);
             S->resident.push_back(r);
             S->st.resident = (long long)S->resident.size();
@@ -331,12 +368,49 @@ class Scheduler {
         }
     }
 
+    // SHORTEST: which residents step in the next launch.  A solve that has
+    // not stepped yet (no dt known) or has sat out aging_s seconds steps;
+    // then the least estimated remaining work first until fill_tiles tiles
+    // step.  The others hold (state untouched).
+    int choose_holds() {
+        const InstState* hs = eng->host_states();
+        const double now = clock_s();
+        std::vector<std::pair<double, Request*>> rest;
+        std::vector<int> hold(eng->max_inst(), 1);
+        int tiles = 0;
+        {
+            std::lock_guard<std::mutex> lk(S->mu);
+            for (Request* r : S->resident) {
+                const InstState& st = hs[r->info.slot];
+                if (r->info.nstep == 0 || !(st.dt > 0) || now - r->lastStep_s >= S->cfg.aging_s) {
+                    hold[r->info.slot] = 0;
+                    tiles += r->tiles;
+                } else {
+                    const double left = std::max(0.0, r->tmax - st.t) / st.dt;
+                    rest.emplace_back((double)r->p.nx * r->p.ny * std::min(left, (double)(r->nstepmax - st.nstep)), r);
+                }
+            }
+        }
+        std::sort(rest.begin(), rest.end(),
+                  [](const std::pair<double, Request*>& a, const std::pair<double, Request*>& b) {
+                      return a.first < b.first;
+                  });
+        for (const auto& w : rest) {
+            if (tiles >= S->cfg.fill_tiles) break;
+            hold[w.second->info.slot] = 0;
+            tiles += w.second->tiles;
+        }
+        return eng->set_holds(hold.data());
+    }
+
     int launch() {
         int steps = 1;
         if (msPerStep > 0) {
             const double want = S->cfg.chunk_ms / msPerStep;
             steps = (int)std::max(1.0, std::min((double)S->cfg.max_chunk_steps, std::floor(want)));
         }
+        if (S->cfg.policy == HOSONO_SERVE_SHORTEST)
+            if (int rc = choose_holds()) return rc;
         {
             std::lock_guard<std::mutex> lk(S->mu);
             for (Request* r : S->resident) r->baseNstep = r->info.nstep;
@@ -347,12 +421,14 @@ class Scheduler {
         if (rc) return rc;
         const InstState* hs = eng->host_states();
         int taken = 0;
+        const double now = clock_s();
         std::lock_guard<std::mutex> lk(S->mu);
         for (Request* r : S->resident) {
             const InstState& s = hs[r->info.slot];
             r->info.nstep = s.nstep;
             r->info.t = s.t;
             taken = std::max(taken, s.nstep - r->baseNstep);
+            if (s.nstep > r->baseNstep) r->lastStep_s = now;
         }
         if (taken > 0) msPerStep = el / taken;
         S->st.chunks++;
@@ -431,6 +507,17 @@ int hosono_serve_create(const hosono_serve_config* cfg, hosono_server** out) {
     if (!(c.chunk_ms > 0)) c.chunk_ms = 25.0;
     if (c.max_chunk_steps <= 0) c.max_chunk_steps = 64;
     if (c.fp_mode != HOSONO_FP_STRICT && c.fp_mode != HOSONO_FP_FAST) return HOSONO_EINVAL;
+    if (c.policy != HOSONO_SERVE_FIFO && c.policy != HOSONO_SERVE_SHORTEST) return HOSONO_EINVAL;
+    if (!(c.aging_s > 0)) c.aging_s = 20.0;
+    if (c.fill_tiles <= 0) {
+        int dev = 0, sms = 148;
+        if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) !=
+                                                      cudaSuccess) {
+            cudaGetLastError();
+            sms = 148;
+        }
+        c.fill_tiles = 8 * sms;
+    }
     hosono_server* S = new (std::nothrow) hosono_server();
     if (!S) return HOSONO_ENOMEM;
     S->cfg = c;
@@ -535,6 +622,7 @@ static int submit_common(hosono_server* S, const hosono_params* p, const double*
     r->outV = V_out;
     r->outScheme = scheme_out;
     r->tiles = hosono_batch_tiles_for(p);
+    r->work = (double)p->nx * p->ny * (std::isfinite(tmax) ? std::max(tmax, 0.0) : 1e30) / std::min(p->dx, p->dy);
     const long long bytes = hosono_batch_instance_bytes(p);
     std::lock_guard<std::mutex> lk(S->mu);
     if (S->fatal) return S->fail(S->fatal, "server stopped after an error; " + S->msg);
@@ -570,6 +658,16 @@ int hosono_serve_wait(hosono_server* S, long long id, double timeout_s, hosono_r
     S->inflight--;
     S->done.notify_all();
     return ok ? HOSONO_OK : HOSONO_ETIMEOUT;
+}
+
+int hosono_serve_release(hosono_server* S, long long id) {
+    if (!S) return HOSONO_EINVAL;
+    std::lock_guard<std::mutex> lk(S->mu);
+    auto it = S->reqs.find(id);
+    if (it == S->reqs.end()) return S->fail(HOSONO_EINVAL, "unknown solve id");
+    if (it->second->info.state != HOSONO_REQ_DONE) return S->fail(HOSONO_EINVAL, "solve is not done");
+    S->reqs.erase(it);
+    return HOSONO_OK;
 }
 
 int hosono_serve_poll(hosono_server* S, long long* ids, int cap, int* n) {

@@ -94,7 +94,7 @@ void put_err(char* err, int len, const std::string& m) {
     if (err && len > 0) std::snprintf(err, (size_t)len, "%s", m.c_str());
 }
 
-// boundaryConditions_apply (src/boundaryConditions.f90:252-360) on a Fortran-order host array
+// boundaryConditions_apply (src/boundaryConditions.f90:79-187) on a Fortran-order host array
 void host_bc(const hosono_params* p, double* A, int nv) {
     const int g = p->ngc, nxt = p->nx + 2 * g, nyt = p->ny + 2 * g;
     auto src = [&](int i, int n) {
@@ -116,13 +116,15 @@ void host_bc(const hosono_params* p, double* A, int nv) {
 }  // namespace
 
 // keys simulation_init, GP_init and grid_init read, in the reference's read
-// order (checked up front, so one call names every missing key)
+// order (checked up front, so one call names every missing key): the sim_*
+// keys, then GP_init's grid_xBeg .. grid_Ny, GP_ellOverDelta, GP_maxRadius
+// (GP.f90:58-69); grid_init reads no key GP_init has not read before it
 const char* const kRequiredKeys[] = {
     "sim_smallB",       "sim_smallPressure", "sim_smallDensity",   "sim_smallEnergy",    "sim_gamma",
     "sim_riemannSolver", "sim_cfl",          "sim_tmax",           "sim_nstepmax",       "sim_BC",
     "sim_dataFileBaseName", "sim_outputFreqTime", "sim_outputFreqStep", "sim_outputHdf5", "sim_outputAscii",
-    "sim_forceHydro",   "GP_maxRadius",      "GP_ellOverDelta",    "grid_Nx",            "grid_Ny",
-    "grid_xBeg",        "grid_xEnd",         "grid_yBeg",          "grid_yEnd"};
+    "sim_forceHydro",   "grid_xBeg",         "grid_xEnd",          "grid_yBeg",          "grid_yEnd",
+    "grid_Nx",          "grid_Ny",           "GP_ellOverDelta",    "GP_maxRadius"};
 
 extern "C" int hosono_par_load(const char* parfile, hosono_params* p, hosono_run_info* run, char* err, int errlen) {
     if (!p) return HOSONO_EINVAL;

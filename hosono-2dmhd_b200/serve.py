@@ -24,8 +24,8 @@ import time
 
 import numpy as np
 
-from . import (ETIMEOUT, FP_STRICT, HosonoError, RequestInfo, ServeConfig, ServeTotals, _p, ic_describe, ic_set,
-               load_library, par_gp, par_load)
+from . import (ECANCELED, ETIMEOUT, FP_STRICT, SERVE_FIFO, SERVE_SHORTEST, HosonoError, RequestInfo, ServeConfig, ServeTotals,
+               _p, ic_describe, ic_set, load_library, par_gp, par_load)
 from . import problems
 
 
@@ -35,12 +35,16 @@ def clock():
 
 
 class Server:
-    """hosono_serve_*: FIFO admission by device-memory budget, continuous batching."""
+    """hosono_serve_*: admission by device-memory budget, continuous batching;
+    policy SERVE_FIFO (the queue in order, every resident steps every launch)
+    or SERVE_SHORTEST (least estimated work first, long residents sit out
+    launches once the short ones fill `fill_tiles` tiles, an aging bound)."""
 
-    def __init__(self, memory_budget=0, max_resident=0, fp_mode=FP_STRICT, chunk_ms=0.0, max_chunk_steps=0):
+    def __init__(self, memory_budget=0, max_resident=0, fp_mode=FP_STRICT, chunk_ms=0.0, max_chunk_steps=0,
+                 policy=SERVE_FIFO, aging_s=0.0, fill_tiles=0):
         self.lib = load_library()
         cfg = ServeConfig(int(memory_budget), int(max_resident), int(fp_mode), float(chunk_ms),
-                          int(max_chunk_steps), 0)
+                          int(max_chunk_steps), int(policy), float(aging_s), int(fill_tiles), 0)
         h = ctypes.c_void_p()
         rc = self.lib.hosono_serve_create(ctypes.byref(cfg), ctypes.byref(h))
         if rc:
@@ -115,17 +119,24 @@ class Server:
             self._outputs[rid.value] = (Uo, None, None)
         return rid.value
 
-    def wait(self, rid, timeout=None):
-        """Block until the solve is done; returns (info dict, U, V, scheme)."""
+    def wait(self, rid, timeout=None, release=True):
+        """Block until the solve is done; returns (info dict, U, V, scheme).
+        With release (the default) the server then forgets the solve."""
         info = RequestInfo()
         rc = self.lib.hosono_serve_wait(self.h, int(rid), -1.0 if timeout is None else float(timeout),
                                         ctypes.byref(info))
         if rc == ETIMEOUT:
             raise TimeoutError(f"solve {rid} not done after {timeout} s")
         self._check(rc, "wait")
+        if release and info.status != ECANCELED:  # a canceled solve: the server is shutting down
+            self.release(rid)
         with self._lock:
             out = self._outputs.pop(int(rid), (None, None, None))
         return (info.as_dict(),) + tuple(out)
+
+    def release(self, rid):
+        """Forget a finished solve (its id becomes unknown to the server)."""
+        self._check(self.lib.hosono_serve_release(self.h, int(rid)), "release")
 
     def info(self, rid):
         info = RequestInfo()

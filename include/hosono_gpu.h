@@ -166,13 +166,25 @@ int hosono_gpu_cfl(hosono_handle* h, double* dt);
 /* timeStep_advanceSolution (src/timeStep.f90:22-43) on the resident state. */
 int hosono_gpu_advance(hosono_handle* h, double dt);
 
-/* The mhd_driver time loop (src/mhd_driver.f90:198-217 with validTimeStep
- * :239-266) on the resident state, without output: steps until t >= tmax,
+/* The mhd_driver time loop (src/mhd_driver.f90:76-95 with validTimeStep
+ * :117-144) on the resident state, without output: steps until t >= tmax,
  * nstep >= nstepmax or max_steps steps (max_steps <= 0: no extra limit). */
 int hosono_gpu_run(hosono_handle* h, double tmax, int nstepmax, int max_steps, double* t_out, int* nstep_out);
 
 /* Set the instance's time-loop position (t, nstep) and limits (tmax, nstepmax). */
 int hosono_gpu_set_time(hosono_handle* h, double t, double tmax, int nstep, int nstepmax);
+
+/* MOOD pass cap.  The reference's forward-Euler MOOD loop
+ * (src/timeStep.f90:86-128) has no limit; every pass that does not end it
+ * lowers at least one cell by one order, so it ends after at most
+ * R*nx*ny + 1 passes -- 8.4 M at 2048^2, R=2, which on a device that never
+ * converged would spin for hours.  A stage that reaches `cap` passes without
+ * converging stops its instance with HOSONO_EMOODCAP instead (the state
+ * stays at the start of that step; other instances of a batch go on).
+ * Default HOSONO_MOOD_CAP_DEFAULT(R) passes per stage; cap <= 0 restores the
+ * proven bound R*nx*ny + 1.  No counterpart in the reference. */
+#define HOSONO_MOOD_CAP_DEFAULT(R) (16 * ((R) + 1))
+int hosono_gpu_set_mood_cap(hosono_handle* h, int cap);
 
 /* Continue the driver's time loop from the current t/nstep: up to max_steps
  * steps of cfl_computedt + validTimeStep + timeStep_advanceSolution, each one
@@ -202,6 +214,57 @@ int hosono_gpu_trace_get(hosono_handle* h, int k, int* meta, unsigned char* inne
                          unsigned char* detect_mask);
 int hosono_gpu_trace_clear(hosono_handle* h);
 
+/* ------------------------------------------------------- stage modules
+ * The reference's stage modules one at a time on the handle's block, for a
+ * host that keeps its own forward-Euler MOOD loop (src/timeStep.f90:76-128)
+ * and for unit parity of each module.  They work on the handle's module
+ * state, the arrays of gridBlock_t (src/gridBlock.f90:51-88): scheme,
+ * recompute, recomputeFLICD, faceVals, flux and fluxRaw, with U = the
+ * resident state and Unew = the handle's stage buffer.  faceVals and flux
+ * (8*nqMax*4 + 16 doubles a cell: 3.8 GB at 2048^2, R=2) are allocated on
+ * the handle's first module call and freed with it; the fused time step
+ * (hosono_gpu_advance / _step) never reads them, and it overwrites the flags,
+ * fluxRaw and Unew.  Each call returns when its kernels are done.
+ *
+ * Host arrays in the reference's Fortran order with guard cells:
+ *   scheme, recompute, recomputeFLICD: (nxTot, nyTot) int (logicals 0/1)
+ *   faceVals (8, nqMax, 4, nxTot, nyTot), faces north, south, east, west
+ *   fluxRaw, flux (8, 2, nxTot, nyTot); Unew (8, nxTot, nyTot)
+ * Any pointer may be NULL (that array is left alone / not copied). */
+int hosono_gpu_module_set(hosono_handle* h, const int* scheme, const int* recompute, const int* recompute_flicd);
+int hosono_gpu_module_get(hosono_handle* h, double* faceVals, double* fluxRaw, double* flux, double* Unew,
+                          int* scheme, int* recompute, int* recompute_flicd);
+/* reconstruct_faceValsWithGP(blk, state%U) (src/reconstruct.f90:18-175):
+ * faceVals of the recompute cells of [strt-2, stop+2]^2 at the EDP1 radius,
+ * with the inner CAD/PAD cascade (failing cells lowered until every face
+ * state is admissible) */
+int hosono_gpu_reconstruct(hosono_handle* h);
+/* getFluxes_(blk) (src/getFluxes.f90:16-90, riemannSolver_getFaceFlux
+ * src/riemannSolver.f90:23-47): fluxRaw and flux of the faces next to a
+ * recompute cell, on [strt-1, stop+2]^2 */
+int hosono_gpu_getfluxes(hosono_handle* h);
+/* FLICDdivB_fluxCorrections(blk) (src/FLICDdivB.f90:13-70) */
+int hosono_gpu_flicd(hosono_handle* h);
+/* the unsplit update of timeStep_forwardEuler (src/timeStep.f90:105-118):
+ * Unew = U - dt/dx (F(i+1)-F(i)) - dt/dy (G(j+1)-G(j)) where recomputeFLICD */
+int hosono_gpu_update(hosono_handle* h, double dt);
+/* detect_ALL(blk, U, Unew, exit_mood_loop) (src/detect.f90:18-236) */
+int hosono_gpu_detect(hosono_handle* h, int* exit_mood_loop);
+/* boundaryConditions_applyBlk (src/boundaryConditions.f90:53-77) on the
+ * resident U (which = 0), V (1) or Unew (2) */
+int hosono_gpu_bc(hosono_handle* h, int which);
+/* boundaryConditions_applyMOOD(blk) (src/boundaryConditions.f90:16-51) */
+int hosono_gpu_bc_mood(hosono_handle* h);
+/* MOOD activity of the last hosono_gpu_advance / _step: passes summed over
+ * its stages, and troubled cells (lowerings by detect_ALL plus by the
+ * reconstruct cascade) */
+int hosono_gpu_mood_pass_stats(hosono_handle* h, int* npasses, long long* ntroubled);
+/* riemannSolver_fromConsHllcMHD (src/riemannSolver.f90:68-221) on n faces
+ * of caller-owned device arrays uL, uR, flux, each (8, n) (the 8 conserved
+ * variables of a face together), direction 0 (x) or 1 (y), with the
+ * handle's gamma, floors and sim_forceHydro; returns when flux is written */
+int hosono_gpu_riemann(hosono_handle* h, int n, const double* uL_dev, const double* uR_dev, int dir, double* flux_dev);
+
 /* Device-resident access for callers that manage their own buffers
  * (benchmarks, batching): device pointer of the first U plane; planes are
  * pitch*nyTot doubles apart, rows pitch doubles apart. */
@@ -216,6 +279,31 @@ int hosono_gpu_set_device(int device);
 
 /* The cudaStream_t every kernel of this handle runs on (for events). */
 int hosono_gpu_stream(hosono_handle* h, void** stream);
+
+/* Launch choices of the time-step kernels (no counterpart in the reference,
+ * whose loops are OpenMP regions).  Results do not depend on them: every
+ * choice gives the same bits.  Setting them rebuilds the handle's step
+ * graphs on the next step. */
+#define HOSONO_STAGE_CP_ASYNC 0  /* pass-1 stencil box staged by per-thread cp.async copies */
+#define HOSONO_STAGE_TMA 1       /* ... by one TMA tensor copy (cp.async.bulk.tensor) per box */
+typedef struct hosono_tuning {
+    int pass1_staging;  /* HOSONO_STAGE_* */
+    int pad[7];         /* zero */
+} hosono_tuning;
+int hosono_gpu_set_tuning(hosono_handle* h, const hosono_tuning* t);
+int hosono_gpu_get_tuning(hosono_handle* h, hosono_tuning* t);
+
+/* Launch geometry of the handle's kernels: every per-tile kernel walks the
+ * tile list grid-stride with a grid sized to the GPU, so a grid smaller than
+ * `tiles` makes each block take several tiles in turn.  No counterpart in
+ * the reference (its loops are OpenMP regions). */
+typedef struct hosono_launch_info {
+    int tiles;          /* 32x8 cell tiles of the instance, guard cells included */
+    int sms;            /* multiprocessors of the device                          */
+    int pass1_grid;     /* blocks of the MOOD pass-1 kernel (radius R)            */
+    int tile_grid_max;  /* the largest grid of the other per-tile kernels          */
+} hosono_launch_info;
+int hosono_gpu_launch_info(hosono_handle* h, hosono_launch_info* info);
 
 /* ---------------------------------------------------------------- batches
  * Many independent blocks (any sizes, radii, boundary conditions, problems)
@@ -238,6 +326,10 @@ int hosono_batch_upload(hosono_batch* b, int slot, const double* U, const double
 int hosono_batch_ic(hosono_batch* b, int slot, const hosono_ic_desc* ic, const double* xtab, const double* ytab);
 int hosono_batch_download(hosono_batch* b, int slot, double* U, double* V, int* scheme);
 int hosono_batch_set_time(hosono_batch* b, int slot, double t, double tmax, int nstep, int nstepmax);
+int hosono_batch_set_tuning(hosono_batch* b, const hosono_tuning* t);
+int hosono_batch_get_tuning(hosono_batch* b, hosono_tuning* t);
+/* hosono_gpu_set_mood_cap for one instance of the batch */
+int hosono_batch_set_mood_cap(hosono_batch* b, int slot, int cap);
 /* every live, unfinished instance steps until its tmax/nstepmax, or at most
  * max_steps steps (max_steps <= 0: no limit) */
 int hosono_batch_run(hosono_batch* b, int max_steps);
@@ -258,12 +350,18 @@ int hosono_batch_capacity(hosono_batch* b, int* max_instances, int* max_tiles, i
  * of a caller-owned device V (10 SoA planes, rows `pitch` doubles apart,
  * planes `plane` doubles apart, ngc guard cells; the layout of the handle's
  * own V) and writes it to the caller-owned device double *dt_dev, on
- * `stream` (NULL = default stream).  Result equal to hosono_gpu_cfl's.
+ * `stream` (NULL = default stream).  Result equal to hosono_gpu_cfl's on an
+ * HOSONO_FP_STRICT handle (this entry point is built without FMA contraction;
+ * a HOSONO_FP_FAST handle's dt may differ in the last bits).
  * Scratch: a file-scope device array of 2*HOSONO_NOALLOC_MAX_ROWS doubles
  * (256 KiB) per GPU, held until process exit; ny > HOSONO_NOALLOC_MAX_ROWS
  * returns HOSONO_EINVAL.  All calls on a device share that array, so calls
- * whose kernels overlap on the GPU race.  The first call on a device looks
- * up the array's address; make it before any stream capture. */
+ * whose kernels overlap on the GPU race.  Every call outside a stream capture
+ * looks up the array's address afresh (so it survives a cudaDeviceReset);
+ * calls inside a capture reuse the last address found, so make the first
+ * call on each device before any stream capture (a first call inside one
+ * returns HOSONO_EINVAL).  Only this call's own launch errors are returned;
+ * an earlier error pending on the thread is left as it was. */
 #define HOSONO_NOALLOC_MAX_ROWS 16384
 int hosono_cfl_noalloc(const double* V_dev, int nx, int ny, int ngc, int pitch, long long plane, double dx, double dy,
                        double cfl, int force_hydro, double* dt_dev, void* stream);
@@ -290,8 +388,9 @@ int hosono_gpu_profile_read(hosono_handle* h, double* pass1_ms, long long* pass1
 /* ---------------------------------------------------------------- serving
  * No counterpart in the reference, which runs one solve per process.  A
  * server owns one batch on the current GPU and a scheduler thread.  Solves
- * are submitted at any time from any thread and wait in a FIFO queue.  The
- * head of the queue is admitted when an instance slot, tile capacity and a
+ * are submitted at any time from any thread and wait in a queue.  A queued
+ * solve is admitted (in the order of the server's policy, HOSONO_SERVE_*)
+ * when an instance slot, tile capacity and a
  * free range of the server's device-memory budget are available: the budget
  * is one device allocation made at start-up, so admission and retirement
  * never call cudaMalloc.  An admitted solve advances with every other
@@ -302,12 +401,26 @@ int hosono_gpu_profile_read(hosono_handle* h, double* pass1_ms, long long* pass1
  * scheduler admits, retires and serves snapshots. */
 typedef struct hosono_server hosono_server;
 
+/* Scheduling policies.  FIFO: the queue head is admitted first and every
+ * resident solve takes every time step of every launch.  SHORTEST: queued
+ * solves are admitted shortest estimated work first (interior cells x
+ * tmax / min(dx, dy); a solve that does not fit is passed over), and each
+ * launch steps the resident solves with the least estimated remaining work
+ * (cells x (tmax - t) / dt) until they cover fill_tiles tiles, while the
+ * others sit out that launch with their state untouched; any solve that has
+ * waited (queued or sitting out) for aging_s seconds goes first.  A solve's
+ * result is the same bits under either policy. */
+#define HOSONO_SERVE_FIFO 0
+#define HOSONO_SERVE_SHORTEST 1
 typedef struct hosono_serve_config {
     long long memory_budget; /* device bytes for resident solves; <= 0: 55% of free memory  */
     int max_resident;        /* instance slots; <= 0: 1024                                  */
     int fp_mode;             /* HOSONO_FP_*                                                 */
     double chunk_ms;         /* target GPU time of one batched launch; <= 0: 25 ms          */
     int max_chunk_steps;     /* time steps per batched launch at most; <= 0: 64             */
+    int policy;              /* HOSONO_SERVE_*                                              */
+    double aging_s;          /* SHORTEST: wait after which a solve goes first; <= 0: 20 s    */
+    int fill_tiles;          /* SHORTEST: tiles a launch steps at least; <= 0: 8 per SM     */
     int pad;
 } hosono_serve_config;
 
@@ -366,6 +479,11 @@ int hosono_serve_submit_ic(hosono_server* s, const hosono_params* p, const doubl
                            double tmax, int nstepmax, double* U_out, double* V_out, int* scheme_out, long long* id);
 /* block until the solve is done (HOSONO_ETIMEOUT after timeout_s; < 0: no limit) */
 int hosono_serve_wait(hosono_server* s, long long id, double timeout_s, hosono_request_info* info);
+/* Forget a finished solve: its id becomes unknown to wait/info.  The server
+ * keeps the record of every solve (its info) until this call or the
+ * server's end, one entry per submitted solve; a long-running server's
+ * callers release each solve once they have read its result. */
+int hosono_serve_release(hosono_server* s, long long id);
 /* ids of solves finished since the last poll (up to cap) */
 int hosono_serve_poll(hosono_server* s, long long* ids, int cap, int* n);
 int hosono_serve_info(hosono_server* s, long long id, hosono_request_info* info);

@@ -110,6 +110,7 @@ struct orc_handle {
     GPTab gp;
     Block blk;
     std::vector<double> U, V;  // (8|10, nx, ny)
+    std::vector<double> Unew;  // stage output of the per-module entry points
     double ellOverDelta = 0;
     bool trace = false;
     int stageCounter = 0;
@@ -817,7 +818,7 @@ bool detect_all(orc_handle* h, const std::vector<double>& U, std::vector<double>
     return exit_mood_loop;
 }
 
-// src/boundaryConditions.f90:291-325 (outflow), :327-360 (periodic)
+// src/boundaryConditions.f90:79-116 (dispatch), :118-152 (outflow), :154-187 (periodic)
 void bc_apply(const Block& b, int bc, std::vector<double>& A, int nv) {
     const int nx = b.nTot[0], ny = b.nTot[1];
     auto at = [&](int i, int j) { return &A[(size_t)nv * ((size_t)(i - 1) + (size_t)nx * (j - 1))]; };
@@ -873,10 +874,30 @@ void bc_apply_mood(Block& b, int bc) {
     }
 }
 
+// the unsplit finite-volume update where recomputeFLICD (src/timeStep.f90:105-118)
+void update(orc_handle* h, double dt, const std::vector<double>& U, std::vector<double>& Unew) {
+    Block& b = h->blk;
+    const double dx = b.dl[0], dy = b.dl[1];
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int j = b.strt[1]; j <= b.stop[1]; j++) {
+        for (int i = b.strt[0]; i <= b.stop[0]; i++) {
+            if (b.recomputeFLICD[b.c(i, j)]) {
+                const double* u = Uc(b, U, i, j);
+                double* un = Uc(b, Unew, i, j);
+                const double* fxp = b.fl(XDIR, i + 1, j);
+                const double* fx = b.fl(XDIR, i, j);
+                const double* fyp = b.fl(YDIR, i, j + 1);
+                const double* fy = b.fl(YDIR, i, j);
+                for (int v = 0; v < NCONS; v++)
+                    un[v] = u[v] - (dt / dx) * (fxp[v] - fx[v]) - (dt / dy) * (fyp[v] - fy[v]);
+            }
+        }
+    }
+}
+
 // src/timeStep.f90:45-130
 void forward_euler(orc_handle* h, double dt, const std::vector<double>& U, std::vector<double>& Unew) {
     Block& b = h->blk;
-    const double dx = b.dl[0], dy = b.dl[1];
     std::fill(b.scheme.begin(), b.scheme.end(), h->gp.R);
     std::fill(b.recompute.begin(), b.recompute.end(), 1);
     std::fill(b.recomputeFLICD.begin(), b.recomputeFLICD.end(), 1);
@@ -898,21 +919,7 @@ void forward_euler(orc_handle* h, double dt, const std::vector<double>& U, std::
         getFluxes(h);
         FC_PHASE(3);
         flicd(h);
-#pragma omp parallel for collapse(2) schedule(static)
-        for (int j = b.strt[1]; j <= b.stop[1]; j++) {
-            for (int i = b.strt[0]; i <= b.stop[0]; i++) {
-                if (b.recomputeFLICD[b.c(i, j)]) {
-                    const double* u = Uc(b, U, i, j);
-                    double* un = Uc(b, Unew, i, j);
-                    const double* fxp = b.fl(XDIR, i + 1, j);
-                    const double* fx = b.fl(XDIR, i, j);
-                    const double* fyp = b.fl(YDIR, i, j + 1);
-                    const double* fy = b.fl(YDIR, i, j);
-                    for (int v = 0; v < NCONS; v++)
-                        un[v] = u[v] - (dt / dx) * (fxp[v] - fx[v]) - (dt / dy) * (fyp[v] - fy[v]);
-                }
-            }
-        }
+        update(h, dt, U, Unew);
         exit_mood_loop = detect_all(h, U, Unew, h->trace ? &tr.detect : nullptr, &tr.nDetect);
         bc_apply_mood(b, h->sim.bc);
         if (h->trace) h->traces.push_back(std::move(tr));
@@ -1176,7 +1183,7 @@ int orc_advance(orc_handle* h, double dt) {
     return 0;
 }
 
-// src/mhd_driver.f90:186-217 with validTimeStep :239-266 (status instead of stop)
+// src/mhd_driver.f90:64-95 with validTimeStep :117-144 (status instead of stop)
 int orc_run(orc_handle* h, int max_steps, double* t_out, int* nstep_out) {
     int nStep = 0;
     double t = 0.0;
@@ -1203,6 +1210,67 @@ int orc_reconstruct_all(orc_handle* h, int radius, double* faceVals) {
     std::fill(b.recompute.begin(), b.recompute.end(), 1);
     reconstruct(h, h->U, nullptr, nullptr);
     if (faceVals) std::memcpy(faceVals, b.faceVals.data(), sizeof(double) * b.faceVals.size());
+    return 0;
+}
+
+// ---------------------------------------------------------------- modules
+// The stage modules one at a time on the handle's block and state, in the
+// reference's arrays (the per-module form of the CUDA library is checked
+// against these).  Unew is the handle's stage output (zero until written).
+static std::vector<double>& unew_of(orc_handle* h) {
+    if (h->Unew.size() != h->U.size()) h->Unew.assign(h->U.size(), 0.0);
+    return h->Unew;
+}
+int orc_mod_set(orc_handle* h, const int* scheme, const int* recompute, const int* recomputeFLICD) {
+    Block& b = h->blk;
+    const size_t n = b.ncell();
+    for (size_t c = 0; c < n; c++) {
+        if (scheme) b.scheme[c] = scheme[c];
+        if (recompute) b.recompute[c] = recompute[c] ? 1 : 0;
+        if (recomputeFLICD) b.recomputeFLICD[c] = recomputeFLICD[c] ? 1 : 0;
+    }
+    return 0;
+}
+int orc_mod_get(orc_handle* h, double* faceVals, double* fluxRaw, double* flux, double* Unew, int* scheme,
+                int* recompute, int* recomputeFLICD) {
+    Block& b = h->blk;
+    if (faceVals) std::memcpy(faceVals, b.faceVals.data(), sizeof(double) * b.faceVals.size());
+    if (fluxRaw) std::memcpy(fluxRaw, b.fluxRaw.data(), sizeof(double) * b.fluxRaw.size());
+    if (flux) std::memcpy(flux, b.flux.data(), sizeof(double) * b.flux.size());
+    if (Unew) std::memcpy(Unew, unew_of(h).data(), sizeof(double) * h->U.size());
+    const size_t n = b.ncell();
+    for (size_t c = 0; c < n; c++) {
+        if (scheme) scheme[c] = b.scheme[c];
+        if (recompute) recompute[c] = b.recompute[c];
+        if (recomputeFLICD) recomputeFLICD[c] = b.recomputeFLICD[c];
+    }
+    return 0;
+}
+int orc_mod_reconstruct(orc_handle* h) {
+    reconstruct(h, h->U, nullptr, nullptr);
+    return 0;
+}
+int orc_mod_getfluxes(orc_handle* h) {
+    getFluxes(h);
+    return 0;
+}
+int orc_mod_flicd(orc_handle* h) {
+    flicd(h);
+    return 0;
+}
+int orc_mod_update(orc_handle* h, double dt) {
+    update(h, dt, h->U, unew_of(h));
+    return 0;
+}
+int orc_mod_detect(orc_handle* h) { return detect_all(h, h->U, unew_of(h), nullptr, nullptr) ? 1 : 0; }
+int orc_mod_bc(orc_handle* h, int which) {
+    if (which == 0) bc_apply(h->blk, h->sim.bc, h->U, NCONS);
+    else if (which == 1) bc_apply(h->blk, h->sim.bc, h->V, NPRIM);
+    else bc_apply(h->blk, h->sim.bc, unew_of(h), NCONS);
+    return 0;
+}
+int orc_mod_bc_mood(orc_handle* h) {
+    bc_apply_mood(h->blk, h->sim.bc);
     return 0;
 }
 

@@ -23,7 +23,7 @@ extern "C" {
 typedef struct orc_handle orc_handle;
 
 /* Build an instance from a .par file (simulation_init + GP_init + grid_init
- * + initialCondition_set of mhd_driver.f90:162-180).  Returns NULL on error
+ * + initialCondition_set of mhd_driver.f90:40-58).  Returns NULL on error
  * and writes a message into err. */
 orc_handle* orc_create_from_par(const char* parfile, char* err, int errlen);
 void orc_destroy(orc_handle* h);
@@ -45,7 +45,7 @@ int orc_get_scheme(const orc_handle* h, int* scheme);
 double orc_cfl(const orc_handle* h);
 /* timeStep_advanceSolution (timeStep.f90:22-43) */
 int orc_advance(orc_handle* h, double dt);
-/* mhd_driver main loop (mhd_driver.f90:186-217) without output; stops after
+/* mhd_driver main loop (mhd_driver.f90:64-95) without output; stops after
  * max_steps steps (<=0: no extra limit).  Returns 0 or a nonzero status. */
 int orc_run(orc_handle* h, int max_steps, double* t_out, int* nstep_out);
 
@@ -53,6 +53,29 @@ int orc_run(orc_handle* h, int max_steps, double* t_out, int* nstep_out);
  * test/test_reconstruct_faceValsWithGP.f90:31-34).  faceVals in Fortran
  * order (8, nqMax, 4, nxTot, nyTot). */
 int orc_reconstruct_all(orc_handle* h, int radius, double* faceVals);
+
+/* The stage modules one at a time on the instance's block, for unit parity
+ * of the CUDA library's per-module entry points.  Arrays in the reference's
+ * Fortran order: scheme/recompute/recomputeFLICD (nxTot, nyTot) (logicals as
+ * 0/1 ints), faceVals (8, nqMax, 4, nxTot, nyTot), fluxRaw/flux (8, 2, nxTot,
+ * nyTot), Unew like U.  NULL arguments are skipped.
+ *   orc_mod_reconstruct  reconstruct_faceValsWithGP(blk, U)  reconstruct.f90:18-175
+ *   orc_mod_getfluxes    getFluxes_(blk)                     getFluxes.f90:16-90
+ *   orc_mod_flicd        FLICDdivB_fluxCorrections(blk)      FLICDdivB.f90:13-70
+ *   orc_mod_update       Unew where recomputeFLICD           timeStep.f90:105-118
+ *   orc_mod_detect       detect_ALL(blk, U, Unew, exit)      detect.f90:18-236; returns exit_mood_loop
+ *   orc_mod_bc           boundaryConditions_applyBlk on U (0), V (1), Unew (2)
+ *   orc_mod_bc_mood      boundaryConditions_applyMOOD(blk)   boundaryConditions.f90:16-51 */
+int orc_mod_set(orc_handle* h, const int* scheme, const int* recompute, const int* recomputeFLICD);
+int orc_mod_get(orc_handle* h, double* faceVals, double* fluxRaw, double* flux, double* Unew, int* scheme,
+                int* recompute, int* recomputeFLICD);
+int orc_mod_reconstruct(orc_handle* h);
+int orc_mod_getfluxes(orc_handle* h);
+int orc_mod_flicd(orc_handle* h);
+int orc_mod_update(orc_handle* h, double dt);
+int orc_mod_detect(orc_handle* h);
+int orc_mod_bc(orc_handle* h, int which);
+int orc_mod_bc_mood(orc_handle* h);
 
 /* MOOD trace: one record per MOOD pass of every forward-Euler stage. */
 int orc_trace_enable(orc_handle* h, int on);

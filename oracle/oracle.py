@@ -31,11 +31,8 @@ def _lib(fast=False, count=False):
     name = dict(count="libhosono_oracle_count.so", fast="libhosono_oracle_fast.so",
                 strict="libhosono_oracle.so")[key]
     path = os.path.join(BUILD, name)
-    if not os.path.exists(path):
-        if count:
-            subprocess.run(["make", "-s", "-C", HERE, "count"], check=True)
-        else:
-            build()
+    # make rebuilds a library whose sources changed (a no-op otherwise)
+    subprocess.run(["make", "-s", "-C", HERE] + (["count"] if count else []), check=True)
     lib = ctypes.CDLL(path)
     d, i, p = ctypes.c_double, ctypes.c_int, ctypes.c_void_p
     dp = ctypes.POINTER(ctypes.c_double)
@@ -66,6 +63,12 @@ def _lib(fast=False, count=False):
     lib.orc_c_fs.argtypes = [d, d, d, d, d, d]
     lib.orc_gp_build.argtypes = [i, ctypes.c_char_p, ctypes.c_char_p, i, ctypes.c_char_p, ctypes.c_char_p, i,
                                  ctypes.c_char_p, dp, dp, ip]
+    lib.orc_mod_set.argtypes = [p, ip, ip, ip]
+    lib.orc_mod_get.argtypes = [p, dp, dp, dp, dp, ip, ip, ip]
+    for n in ("orc_mod_reconstruct", "orc_mod_getfluxes", "orc_mod_flicd", "orc_mod_detect", "orc_mod_bc_mood"):
+        getattr(lib, n).argtypes = [p]
+    lib.orc_mod_update.argtypes = [p, d]
+    lib.orc_mod_bc.argtypes = [p, i]
     lib.orc_set_threads.argtypes = [i]
     lib.orc_get_threads.restype = i
     if count:
@@ -234,6 +237,55 @@ class Oracle:
                 rec["detect"] = det.reshape(self.nyTot, self.nxTot)
             out.append(rec)
         return out
+
+    # ---- the stage modules one at a time (reference arrays, Fortran order)
+    def mod_set(self, scheme=None, recompute=None, recompute_flicd=None):
+        """Set blk%scheme / recompute / recomputeFLICD, each (nyTot, nxTot) or None."""
+        def arg(a):
+            if a is None:
+                return None, None
+            a = np.ascontiguousarray(a, dtype=np.int32).reshape(-1)
+            assert a.size == self.ncell
+            return a, _ip(a)
+        keep = [arg(a) for a in (scheme, recompute, recompute_flicd)]
+        self.lib.orc_mod_set(self.h, *(k[1] for k in keep))
+
+    def mod_get(self):
+        """dict of faceVals [j, i, face, q, var], fluxRaw / flux [j, i, dir, var],
+        Unew [j, i, var], scheme / recompute / recompute_flicd [j, i]."""
+        nq = self.nqMax
+        fv = np.zeros(self.ncell * 8 * nq * 4)
+        fr = np.zeros(self.ncell * 16)
+        fl = np.zeros(self.ncell * 16)
+        un = np.zeros(self.ncell * 8)
+        sc, rc, rf = (np.zeros(self.ncell, dtype=np.int32) for _ in range(3))
+        self.lib.orc_mod_get(self.h, _dp(fv), _dp(fr), _dp(fl), _dp(un), _ip(sc), _ip(rc), _ip(rf))
+        sh = (self.nyTot, self.nxTot)
+        return dict(faceVals=fv.reshape(*sh, 4, nq, 8), fluxRaw=fr.reshape(*sh, 2, 8), flux=fl.reshape(*sh, 2, 8),
+                    Unew=un.reshape(*sh, 8), scheme=sc.reshape(sh), recompute=rc.reshape(sh),
+                    recompute_flicd=rf.reshape(sh))
+
+    def mod_reconstruct(self):
+        self.lib.orc_mod_reconstruct(self.h)
+
+    def mod_getfluxes(self):
+        self.lib.orc_mod_getfluxes(self.h)
+
+    def mod_flicd(self):
+        self.lib.orc_mod_flicd(self.h)
+
+    def mod_update(self, dt):
+        self.lib.orc_mod_update(self.h, float(dt))
+
+    def mod_detect(self):
+        """detect_ALL; returns exit_mood_loop."""
+        return bool(self.lib.orc_mod_detect(self.h))
+
+    def mod_bc(self, which):
+        self.lib.orc_mod_bc(self.h, int(which))
+
+    def mod_bc_mood(self):
+        self.lib.orc_mod_bc_mood(self.h)
 
     # pointwise physics
     def cons2prim(self, u):

@@ -1,7 +1,11 @@
 """Extract the reference's known-answer values into committed fixtures.
 
-Run in a container where the reference project is mounted (its path is the
-first argument, default /root/reference).  Writes:
+Run where the reference project is checked out; its path is the required
+first argument:
+
+    python tests/golden/make_golden.py PATH_TO_REFERENCE
+
+Writes:
 
 * gp_facevals_r3_kat.json -- the momentum-x face values and cell averages
   printed by test/test_reconstruct_faceValsWithGP.f90 (output captured in
@@ -21,7 +25,9 @@ import os
 import re
 import sys
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+if len(sys.argv) < 2:
+    sys.exit("usage: make_golden.py PATH_TO_REFERENCE (the hosono-2DMHD project root)")
+REF = sys.argv[1]
 HERE = os.path.dirname(os.path.abspath(__file__))
 FLOAT = re.compile(r"[-+]?\d\.\d+E[-+]\d+")
 

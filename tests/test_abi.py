@@ -74,7 +74,7 @@ def test_par_every_missing_key_is_reported(tmp_par_dir):
     the first missing key (in its read order), and the rest follow."""
     m = pkg.load()
     kv = parfiles.orszag_tang(16, 1)
-    for k in ("grid_yEnd", "sim_gamma", "GP_ellOverDelta"):
+    for k in ("grid_yEnd", "sim_gamma", "GP_ellOverDelta", "GP_maxRadius", "grid_xBeg"):
         del kv[k]
     par = parfiles.make(tmp_par_dir, "missing3", kv)
     with pytest.raises(m.HosonoError) as e:
@@ -82,7 +82,9 @@ def test_par_every_missing_key_is_reported(tmp_par_dir):
     msg = str(e.value)
     assert e.value.code == m.EPAR
     assert "The parameter 'sim_gamma' was not found" in msg
-    assert "also missing: GP_ellOverDelta, grid_yEnd" in msg
+    # GP_init reads grid_xBeg .. grid_Ny, then GP_ellOverDelta, then
+    # GP_maxRadius (GP.f90:58-69)
+    assert "also missing: grid_xBeg, grid_yEnd, GP_ellOverDelta, GP_maxRadius" in msg
 
 
 def test_par_first_match_and_comments(tmp_par_dir):

@@ -1,6 +1,8 @@
 """Batched engine: independent instances of different problems, sizes, radii
 and boundary conditions advanced together must each equal their own oracle
 run bit for bit (strict arithmetic), each with its own dt."""
+import os
+
 import numpy as np
 import pytest
 
@@ -80,3 +82,52 @@ def test_batch_runs_each_instance_to_its_own_tmax(tmp_par_dir):
     o.run()
     np.testing.assert_array_equal(b.download(k)[0], o.U())
     b.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("graphs", [True, False])
+def test_mood_cap_stops_only_its_instance(graphs, tmp_par_dir):
+    """A stage that reaches its MOOD pass cap stops its instance with
+    HOSONO_EMOODCAP, its state left at the start of the step, while the other
+    instances of the batch run on bit-identical to their oracle runs."""
+    m = pkg.load()
+    kvs = [parfiles.blast(40, 2, p_ratio=1000.0, theta=0.3), parfiles.orszag_tang(32, 2),
+           parfiles.blast(32, 1, p_ratio=50.0, theta=0.9)]
+    pars = [parfiles.make(tmp_par_dir, f"cap{i}", kv) for i, kv in enumerate(kvs)]
+    # precondition: the capped solve's first stage needs more than one MOOD pass
+    o0 = oracle.Oracle(pars[0])
+    o0.trace(True)
+    o0.advance(o0.cfl())
+    assert max(t["mood_pass"] for t in o0.traces(masks=False) if t["stage"] == 0) >= 1
+    o0.close()
+    tiles = sum(m.Batch.tiles_for(m.par_load(p)[0]) for p in pars)
+    b = m.Batch(len(pars), tiles, fp_mode=m.FP_STRICT)
+    b.set_graphs(graphs)
+    slots = [b.add_par(p) for p in pars]
+    for k in slots:
+        b.set_time(k, 0.0, 1e30)
+    U0 = b.download(slots[0])[0]
+    b.set_mood_cap(slots[0], 1)
+    with pytest.raises(m.HosonoError) as e:
+        b.run(max_steps=2)
+    assert e.value.code == m.EMOODCAP
+    st = b.status(slots[0])
+    assert st["done"] and st["error"] == m.EMOODCAP and st["nstep"] == 0
+    np.testing.assert_array_equal(b.download(slots[0])[0], U0)
+    for k, p in zip(slots[1:], pars[1:]):
+        o = oracle.Oracle(p)
+        for _ in range(2):
+            o.advance(o.cfl())
+        st = b.status(k)
+        assert st["error"] == 0 and st["nstep"] == 2
+        U, V, S = b.download(k)
+        np.testing.assert_array_equal(U, o.U())
+        np.testing.assert_array_equal(S, o.scheme())
+    b.close()
+
+
+def test_mood_cap_default_matches_header():
+    m = pkg.load()
+    src = open(os.path.join(pkg.ROOT, "include", "hosono_gpu.h")).read()
+    assert "#define HOSONO_MOOD_CAP_DEFAULT(R) (16 * ((R) + 1))" in src
+    assert [m.mood_cap_default(r) for r in (1, 2, 3)] == [32, 48, 64]

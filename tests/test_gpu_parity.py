@@ -119,3 +119,27 @@ def test_orszag_tang_128_r1_to_t_end(tmp_par_dir):
     np.testing.assert_array_equal(U, o.U())
     np.testing.assert_array_equal(V, o.V())
     s.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", ["ot32_r1", "ot24_r3_refic", "sedov33x40_r1", "blast40_r2"])
+def test_tma_staging_bitwise(case, tmp_par_dir):
+    """Pass 1 with its stencil box staged by TMA (one cp.async.bulk.tensor per
+    box, zero fill beyond the array) gives the oracle's bits, as the
+    per-thread cp.async staging does."""
+    m = pkg.load()
+    par = parfiles.make(tmp_par_dir, case + "_tma", CASES[case]())
+    o = oracle.Oracle(par)
+    s = m.Solver.from_par(par, fp_mode=m.FP_STRICT)
+    s.set_tuning(pass1_staging=m.STAGE_TMA)
+    assert s.tuning()["pass1_staging"] == m.STAGE_TMA
+    s.set_time(0.0, o.tmax, 0, 1 << 30)
+    for chunk in (1, 3):
+        for _ in range(chunk):
+            o.advance(o.cfl())
+        s.step(chunk)
+        U, V, S = s.download()
+        np.testing.assert_array_equal(U, o.U())
+        np.testing.assert_array_equal(V, o.V())
+        np.testing.assert_array_equal(S, o.scheme())
+    s.close()

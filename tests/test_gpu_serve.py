@@ -143,3 +143,42 @@ def test_failed_solve_is_isolated(tmp_par_dir):
         assert info["status"] == 0
         Uo, _, _ = _oracle_final(e, tmp_par_dir)
         np.testing.assert_array_equal(U, Uo)
+
+
+@pytest.mark.gpu
+def test_shortest_first_policy_gives_the_same_results(tmp_par_dir):
+    """SERVE_SHORTEST admits the least estimated work first and lets the
+    residents with the most remaining work sit launches out (fill_tiles set
+    low so that they do): every solve still ends bit-identical to its oracle
+    run, and the short ones finish before the long ones that arrived with
+    them."""
+    m = pkg.load()
+    srv = _serve()
+    keep = [e["id"] for e in ENTRIES]
+    with srv.Server(policy=m.SERVE_SHORTEST, fill_tiles=1, chunk_ms=2.0) as s:
+        rep, kept, infos = srv.run_stream(ENTRIES, rate=1.0, server=s, keep=keep, closed=True)
+    assert rep["completed"] == len(ENTRIES) and rep["failed"] == 0
+    for e in ENTRIES:
+        U, t, n = _oracle_final(e, tmp_par_dir)
+        np.testing.assert_array_equal(kept[e["id"]], U)
+        info = next(i for i in infos if i["entry"] == e["id"])
+        assert info["t"] == t and info["nstep"] == n
+    work = {i["entry"]: i["zone_updates"] for i in infos}
+    fin = {i["entry"]: i["finish_s"] for i in infos}
+    small, big = min(work, key=work.get), max(work, key=work.get)
+    assert fin[small] < fin[big]
+
+
+@pytest.mark.gpu
+def test_released_solve_is_forgotten(tmp_par_dir):
+    m = pkg.load()
+    srv = _serve()
+    p, pv, qw, st, U0, V0, tmax = srv.prepare(ENTRIES[0], tmp_par_dir)
+    with srv.Server() as s:
+        rid = s.submit(p, pv, qw, st, U0, V0, tmax)
+        info = s.wait(rid, release=False)[0]
+        assert info["status"] == 0 and s.info(rid)["state"] == m.REQ_DONE
+        s.release(rid)
+        with pytest.raises(m.HosonoError) as e:
+            s.info(rid)
+        assert e.value.code == m.EINVAL
