@@ -123,11 +123,26 @@ def peaks():
         return FALLBACK_HBM_GBS, "fallback"
 
 
-# DRAM bytes of one k_face_pass1<2> launch measured with ncu on ot1536_r2,
-# and the FP64-pipe activity there; the bench scales the bytes to its
-# workload by the algorithmic bytes.
-PASS1_PROFILE = {"workload": "ot1536_r2", "n": 1536, "radius": 2, "dram_bytes": 162735872 + 314940160,
-                 "fp64_pipe_active_frac": 0.485}
+# The ncu capture of one k_face_pass1<2> launch (DRAM bytes, FP64-pipe
+# activity) lives in the committed profile summary; its "bench-keys:" line
+# holds the numbers this bench scales to its workload by algorithmic bytes.
+PASS1_PROFILE_FILE = os.path.join(ROOT, "profiles", "k_face_pass1_ot1536_r2.md")
+
+
+def pass1_profile():
+    """{workload, n, radius, dram_bytes, fp64_pipe_active_frac} from the
+    profile summary's bench-keys line, or None when it has none."""
+    try:
+        with open(PASS1_PROFILE_FILE) as f:
+            line = next((ln for ln in f if ln.startswith("bench-keys:")), None)
+    except OSError:
+        return None
+    if not line:
+        return None
+    kv = dict(tok.split("=", 1) for tok in line.split(":", 1)[1].split())
+    return {"workload": kv["workload"], "n": int(kv["n"]), "radius": int(kv["radius"]),
+            "dram_bytes": float(kv["dram_bytes"]), "fp64_pipe_active_frac": float(kv["fp64_pipe_active_frac"]),
+            "source": os.path.relpath(PASS1_PROFILE_FILE, ROOT)}
 
 
 # Algorithmic FP64 operations of one pass-1 launch per interior cell: the
@@ -264,6 +279,7 @@ def bench_ours(args, rank, world, local):
         sol.set_graphs(False)
     sol.upload(U0, V0)
     sol.set_time(0.0, run.tmax, 0, run.nstepmax)
+    tune = sol.autotune(trials=5, force=True) if not args.no_tune else None
     stream = torch.cuda.ExternalStream(sol.stream())
     zones = w["n"] * w["n"]
 
@@ -305,27 +321,32 @@ def bench_ours(args, rank, world, local):
     ms = max_over_ranks(ms, dist, "cuda")
     value = replicas_value(world, zones, args.steps, ms)
 
-    # end to end through the C ABI with host buffers: every step uploads U,V
-    # from pinned memory, takes the step (dt on the device) and downloads U,V
+    # end to end through the reference-facing calls with host buffers, as a
+    # Fortran driver that keeps grid_state%U on the host makes them each step:
+    # dt = cfl_computedt (hosono_gpu_cfl, dt to the host), then
+    # timeStep_advanceSolution on the host array (hosono_gpu_advance_host:
+    # U from pinned memory to the device -- V = cons2prim(U) is rebuilt there,
+    # bit-identical to the host's -- the step, U back to the host)
     Uh = torch.from_numpy(np.ascontiguousarray(U0)).pin_memory().numpy()
-    Vh = torch.from_numpy(np.ascontiguousarray(V0)).pin_memory().numpy()
+    sol.upload(Uh, None)
     e2e_steps = max(1, min(args.steps, 5))
     barrier()
     f0 = torch.cuda.Event(enable_timing=True)
     f1 = torch.cuda.Event(enable_timing=True)
     f0.record(stream)
     for _ in range(e2e_steps):
-        sol.upload(Uh, Vh)
-        sol.step(1)
-        sol.download(Uh, Vh, with_scheme=False)
+        dt = sol.cfl_computedt()
+        sol.advance_host(dt, Uh, None)
     f1.record(stream)
     f1.synchronize()
     e2e_ms = f0.elapsed_time(f1)
     e2e_ms = max_over_ranks(e2e_ms, dist, "cuda")
     barrier()
     e2e = {"value": world * zones * e2e_steps / (e2e_ms / 1e3), "unit": "zone-updates/s",
-           "h2d_bytes_per_step": U0.nbytes + V0.nbytes, "d2h_bytes_per_step": U0.nbytes + V0.nbytes,
-           "steps": e2e_steps, "ms_per_step": e2e_ms / e2e_steps}
+           "h2d_bytes_per_step": U0.nbytes, "d2h_bytes_per_step": U0.nbytes + 8,
+           "steps": e2e_steps, "ms_per_step": e2e_ms / e2e_steps,
+           "calls": "per step: hosono_gpu_cfl (dt to the host), hosono_gpu_advance_host(dt, U, NULL): U host->device, "
+                    "step, U device->host (V rebuilt on the device)"}
     sol.close()
 
     # the same workload in fast arithmetic (FMA contraction; results within
@@ -357,15 +378,16 @@ def bench_ours(args, rank, world, local):
     p1_avg = p1_ms / max(p1_n, 1)
     bytes1 = pass1_bytes(w["n"], w["radius"])
     achieved = bytes1 / (p1_avg / 1e3) / 1e9 if p1_avg > 0 else None
+    prof = pass1_profile()
     traffic = None
-    if w["radius"] == PASS1_PROFILE["radius"]:
-        traffic = PASS1_PROFILE["dram_bytes"] * bytes1 / pass1_bytes(PASS1_PROFILE["n"], PASS1_PROFILE["radius"])
+    if prof and w["radius"] == prof["radius"]:
+        traffic = prof["dram_bytes"] * bytes1 / pass1_bytes(prof["n"], prof["radius"])
     roofline = {"bound": "hbm", "kernel": "k_face_pass1", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                 "frac": achieved / hbm if achieved else None, "traffic": traffic, "peak_kind": hbm_kind,
                 "kernel_ms": p1_avg, "kernel_launches": p1_n,
-                "traffic_source": f"ncu dram bytes of one launch on {PASS1_PROFILE['workload']}, scaled by "
-                                  "algorithmic bytes",
-                "fp64_pipe_active_frac": PASS1_PROFILE["fp64_pipe_active_frac"],
+                "traffic_source": (f"ncu dram bytes of one launch on {prof['workload']} ({prof['source']}), scaled "
+                                   "by algorithmic bytes") if prof else None,
+                "fp64_pipe_active_frac": prof["fp64_pipe_active_frac"] if prof else None,
                 "note": "FP64 CUDA-core kernel bound by the FP64 pipe and latency (fp64_pipe_active_frac from "
                         "ncu); the HBM line is shown as the contract requires"}
     fpc = PASS1_FLOPS.get((w.get("problem", "ot"), w["radius"], w["ell"]))
@@ -389,6 +411,8 @@ def bench_ours(args, rank, world, local):
                    "l2": "inputs larger than L2 (U alone 270 MB at 2048^2)", "mood_passes": passes},
         "gpu_launches": launches, "clocks": clk, "roofline": roofline, "e2e": e2e,
     }
+    if tune:
+        line["tuning"] = tune
     if other:
         line["fast_fp"] = other
     if world == 1 and not args.no_batched:
@@ -436,6 +460,7 @@ def bench_batched(m, fp, torch, manifest="blast64_seed0.json", limit=None, eager
         if eager:
             b.set_graphs(False)
         slots = [b.add_par(p) for p in pars]
+        tune_b = b.autotune(trials=3, force=True)
         b.run(max_steps=1)
         n0 = {k: b.status(k)["nstep"] for k in slots}
         stream = torch.cuda.ExternalStream(b.stream())
@@ -460,6 +485,7 @@ def bench_batched(m, fp, torch, manifest="blast64_seed0.json", limit=None, eager
         zu_p = 0
         for p, e in zip(pars, entries):
             s = m.Solver.from_par(p, fp_mode=fp)
+            s.autotune(trials=3)  # per size class: timed once, then taken from the cache
             s.set_time(0.0, e["tmax"], 0, 1 << 30)
             s.step(1)
             st_ = torch.cuda.ExternalStream(s.stream())
@@ -477,23 +503,25 @@ def bench_batched(m, fp, torch, manifest="blast64_seed0.json", limit=None, eager
             "instances": len(entries), "zone_updates": zu_b, "steps_min": min(steps), "steps_max": max(steps),
             "batched_value": rate_b, "batched_s": ms_b / 1e3, "batched_wall_s": wall_b,
             "plain_value": rate_p, "plain_s": ms_p / 1e3, "ratio_batched_over_plain": rate_b / rate_p,
-            "unit": "zone-updates/s"}
+            "unit": "zone-updates/s", "tuning": tune_b}
 
 
 def bench_served(m, fp, requests, check, calibrate=0, sample=0, hashes_path=None, mean_work=None,
                  records_path=None):
     """The served request stream (workloads/served2000_seed1.json, first
-    `requests` requests).  Capacity: the stream's first `calibrate` requests
-    (all of them when 0) run closed loop (all submitted at once); their
-    zone-updates/s divided by the stream's mean work per request -- measured
-    when every request ran, else predicted from the calibration run's step
-    counts (steps ~ k_problem * N * t_end, k fitted per problem) -- gives
-    requests/s.  Then the whole stream runs open loop with the manifest's
-    seeded exponential gaps scaled to 80% of that capacity.  Latency is
-    submit -> final state on the host.  Returns the report and the final U
-    of the `check` requests with the least work (accuracy check); with
-    `sample`, the SHA-256 of the final U of `sample` seeded-random requests is
-    written to `hashes_path` for a check against the oracle elsewhere."""
+    `requests` requests) under both scheduling policies.  Capacity: the
+    stream's first `calibrate` requests (all of them when 0) run closed loop
+    (all submitted at once, FIFO); their zone-updates/s divided by the
+    stream's mean work per request -- measured when every request ran, else
+    predicted from the calibration run's step counts (steps ~ k_problem * N *
+    t_end, k fitted per problem) -- gives requests/s.  Then the whole stream
+    runs open loop, once per policy (FIFO; shortest estimated work first with
+    an aging bound), with the manifest's seeded exponential gaps scaled to
+    80% of that capacity.  Latency is submit -> final state on the host.  The
+    `check` requests with the least predicted work keep their final U, which
+    must be the same bits under both policies; they are returned for the
+    accuracy check against the CPU oracle.  With `sample`, the SHA-256 of the
+    final U of `sample` seeded-random requests is written to `hashes_path`."""
     import hashlib
     import importlib
     import numpy as np
@@ -505,56 +533,67 @@ def bench_served(m, fp, requests, check, calibrate=0, sample=0, hashes_path=None
     cal = entries[:calibrate] if 0 < calibrate < len(entries) else entries
     with srv.Server(fp_mode=fp) as s:
         closed, _, cinfos = srv.run_stream(cal, 1.0, s, fp_mode=fp, closed=True)
+    by_id = {e["id"]: e for e in cal}
+    ks = {}
+    for i in cinfos:
+        e = by_id[i["entry"]]
+        ks.setdefault(e["problem"], []).append(i["nstep"] / (e["n"] * e["tmax"]))
+    k = {p_: float(np.median(v)) for p_, v in ks.items()}
+    kall = float(np.median([x for v in ks.values() for x in v]))
+
+    def predicted(e):  # zone-updates of one request
+        return e["n"] ** 3 * e["tmax"] * k.get(e["problem"], kall)
     if mean_work:  # known from an earlier run of the same requests (results are deterministic)
         mean_work = float(mean_work)
     elif cal is entries:
         mean_work = closed["zone_updates"] / len(entries)
     else:
-        by_id = {e["id"]: e for e in cal}
-        ks = {}
-        for i in cinfos:
-            e = by_id[i["entry"]]
-            ks.setdefault(e["problem"], []).append(i["nstep"] / (e["n"] * e["tmax"]))
-        k = {p: float(np.median(v)) for p, v in ks.items()}
-        kall = float(np.median([x for v in ks.values() for x in v]))
-        mean_work = float(np.mean([e["n"] ** 3 * e["tmax"] * k.get(e["problem"], kall) for e in entries]))
+        mean_work = float(np.mean([predicted(e) for e in entries]))
     cap = closed["zone_updates_per_s"] / mean_work
     rate = 0.8 * cap
-    keep = [i["entry"] for i in sorted(cinfos, key=lambda i: i["zone_updates"])[:check]]
+    keep = [e["id"] for e in sorted(entries, key=predicted)[:check]]
     sampled = []
     if sample > 0:
         rng = np.random.Generator(np.random.PCG64(2))
         sampled = sorted(int(x) for x in rng.choice([e["id"] for e in entries], size=min(sample, len(entries)),
                                                     replace=False))
-    with srv.Server(fp_mode=fp) as s:
-        rep, kept, infos = srv.run_stream(entries, rate, s, keep=keep + sampled, fp_mode=fp)
     out = {"workload": f"served2000 (seed 1) requests 0..{len(entries) - 1}: Orszag-Tang / Sedov / MHD blast, "
                        f"N log-uniform in [64,1024], R in {{1,2}}, t_end U[0.1,1] x default",
            "requests": len(entries), "load": 0.8, "calibration_requests": len(cal), "capacity_rps": cap,
-           "closed_loop_zone_updates_per_s": closed["zone_updates_per_s"], "rate_per_s": rate}
-    for k_ in ("zone_updates", "zone_updates_per_s", "makespan_s", "latency_p50_s", "latency_p99_s",
-               "latency_max_s", "queue_wait_p50_s", "queue_wait_p99_s", "submit_lag_max_s", "peak_resident",
-               "peak_bytes", "budget_bytes", "gpu_busy_frac", "completed", "failed"):
-        out[k_] = rep[k_]
-    out["unit"] = "zone-updates/s"
-    out["mean_work_used"] = mean_work
-    out["mean_work_measured"] = rep["zone_updates"] / max(rep["completed"], 1)
+           "closed_loop_zone_updates_per_s": closed["zone_updates_per_s"], "rate_per_s": rate,
+           "unit": "zone-updates/s", "mean_work_used": mean_work}
+    keys = ("zone_updates", "zone_updates_per_s", "makespan_s", "latency_p50_s", "latency_p99_s", "latency_max_s",
+            "queue_wait_p50_s", "queue_wait_p99_s", "submit_lag_max_s", "peak_resident", "peak_bytes",
+            "budget_bytes", "gpu_busy_frac", "completed", "failed")
+    kept_by = {}
+    for name, pol in (("fifo", srv.SERVE_FIFO), ("shortest", srv.SERVE_SHORTEST)):
+        with srv.Server(fp_mode=fp, policy=pol) as s:
+            rep, kept, infos = srv.run_stream(entries, rate, s, keep=keep + sampled, fp_mode=fp)
+        out[name] = {k_: rep[k_] for k_ in keys}
+        out[name]["mean_work_measured"] = rep["zone_updates"] / max(rep["completed"], 1)
+        kept_by[name] = kept
+        if name == "fifo":
+            for k_ in keys:  # the default policy's figures at the top level
+                out[k_] = rep[k_]
+            fifo_infos = infos
+    out["policies_identical"] = all(np.array_equal(kept_by["fifo"][i], kept_by["shortest"][i])
+                                    for i in keep + sampled)
     if records_path:
         with open(records_path, "w") as f:
             json.dump([{k_: i[k_] for k_ in ("entry", "status", "nstep", "zone_updates", "submit_s", "admit_s",
-                                              "finish_s")} for i in infos], f)
+                                              "finish_s")} for i in fifo_infos], f)
     if sampled and hashes_path:
         recs = {}
-        for i in infos:
+        for i in fifo_infos:
             if i["entry"] in sampled:
-                U = kept[i["entry"]]
+                U = kept_by["fifo"][i["entry"]]
                 recs[str(i["entry"])] = {"sha256": hashlib.sha256(np.ascontiguousarray(U).tobytes()).hexdigest(),
                                          "nstep": i["nstep"], "t": i["t"], "zone_updates": i["zone_updates"]}
         with open(hashes_path, "w") as f:
             json.dump({"manifest": "served2000_seed1.json", "sample_seed": 2, "fp": "strict" if fp == 0 else "fast",
                        "requests": recs}, f, indent=1)
         out["sampled_hashes"] = {"file": os.path.basename(hashes_path), "requests": sampled}
-    return out, {e["id"]: (e, kept[e["id"]]) for e in entries if e["id"] in keep}
+    return out, {e["id"]: (e, kept_by["fifo"][e["id"]]) for e in entries if e["id"] in keep}
 
 
 def cpu_baseline_served_check(kept):
@@ -592,6 +631,7 @@ def main():
     ap.add_argument("--workload", default="ot2048_r2", choices=sorted(WORKLOADS))
     ap.add_argument("--fp", default="strict", choices=["strict", "fast"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-tune", action="store_true", help="keep the default launch choices (no autotuning)")
     ap.add_argument("--no-batched", action="store_true", help="skip the 64-instance batched-vs-plain measurement")
     ap.add_argument("--eager", action="store_true",
                     help="launch kernels one by one instead of as CUDA graphs (the plain and batched legs; for "
@@ -599,11 +639,11 @@ def main():
     ap.add_argument("--batched-limit", type=int, default=64, help="instances of the batched workload to run")
     ap.add_argument("--to-end", action="store_true",
                     help="time the whole run from the initial state to t_end instead of --steps steps")
-    ap.add_argument("--serve-requests", type=int, default=20,
+    ap.add_argument("--serve-requests", type=int, default=100,
                     help="requests of the served stream to run (0: skip the served measurement)")
-    ap.add_argument("--serve-check", type=int, default=3,
-                    help="served requests (least work first) checked against the CPU oracle")
-    ap.add_argument("--serve-calibrate", type=int, default=0,
+    ap.add_argument("--serve-check", type=int, default=20,
+                    help="served requests (least predicted work first) checked against the CPU oracle")
+    ap.add_argument("--serve-calibrate", type=int, default=30,
                     help="first requests run closed loop to measure capacity (0: all of them)")
     ap.add_argument("--serve-sample", type=int, default=0,
                     help="seeded-random served requests whose final-state SHA-256 is written to --serve-hashes")

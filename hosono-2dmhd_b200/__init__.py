@@ -98,13 +98,28 @@ class LaunchInfo(ctypes.Structure):
 
 
 class Tuning(ctypes.Structure):
-    _fields_ = [("pass1_staging", ctypes.c_int), ("pad", ctypes.c_int * 7)]
+    _fields_ = [("pass1_staging", ctypes.c_int), ("pass1_schedule", ctypes.c_int),
+                ("pass1_blocks_per_sm", ctypes.c_int), ("pad", ctypes.c_int * 5)]
 
     def as_dict(self):
-        return {"pass1_staging": self.pass1_staging}
+        return {"pass1_staging": self.pass1_staging, "pass1_schedule": self.pass1_schedule,
+                "pass1_blocks_per_sm": self.pass1_blocks_per_sm}
 
 
 STAGE_CP_ASYNC, STAGE_TMA = 0, 1
+SCHED_STATIC, SCHED_DYNAMIC = 0, 1
+TUNE_MAX = 8
+
+
+class TuneReport(ctypes.Structure):
+    _fields_ = [("candidates", ctypes.c_int), ("cached", ctypes.c_int), ("size_class", ctypes.c_int),
+                ("instances", ctypes.c_int), ("tried", Tuning * TUNE_MAX), ("ms", ctypes.c_double * TUNE_MAX),
+                ("best", Tuning)]
+
+    def as_dict(self):
+        return {"cached": bool(self.cached), "size_class": self.size_class, "instances": self.instances,
+                "best": self.best.as_dict(),
+                "table": [dict(self.tried[k].as_dict(), pass1_ms=self.ms[k]) for k in range(self.candidates)]}
 
 
 class ICDesc(ctypes.Structure):
@@ -158,6 +173,8 @@ SIGNATURES = {
     "hosono_gpu_stream": [_vp, ctypes.POINTER(_vp)],
     "hosono_gpu_launch_info": [_vp, ctypes.POINTER(LaunchInfo)],
     "hosono_gpu_set_tuning": [_vp, ctypes.POINTER(Tuning)],
+    "hosono_gpu_autotune": [_vp, _i, _i, ctypes.POINTER(TuneReport)],
+    "hosono_batch_autotune": [_vp, _i, _i, ctypes.POINTER(TuneReport)],
     "hosono_gpu_get_tuning": [_vp, ctypes.POINTER(Tuning)],
     "hosono_batch_set_tuning": [_vp, ctypes.POINTER(Tuning)],
     "hosono_batch_get_tuning": [_vp, ctypes.POINTER(Tuning)],
@@ -569,6 +586,13 @@ class Solver:
         self._check(self.lib.hosono_gpu_get_tuning(self.h, ctypes.byref(t)), "get_tuning")
         return t.as_dict()
 
+    def autotune(self, trials=5, force=False):
+        """Time the candidate launch choices on this solve and apply the fastest."""
+        r = TuneReport()
+        self._check(self.lib.hosono_gpu_autotune(self.h, int(trials), 1 if force else 0, ctypes.byref(r)),
+                    "autotune")
+        return r.as_dict()
+
     def launch_info(self):
         """Launch geometry: tiles, SMs, pass-1 grid, largest other tile-kernel grid."""
         li = LaunchInfo()
@@ -717,6 +741,13 @@ class Batch:
         for k, v in kw.items():
             setattr(t, k, int(v))
         self._check(self.lib.hosono_batch_set_tuning(self.h, ctypes.byref(t)), "set_tuning")
+
+    def autotune(self, trials=5, force=False):
+        """Time the candidate launch choices on the batch's instances; apply the fastest."""
+        r = TuneReport()
+        self._check(self.lib.hosono_batch_autotune(self.h, int(trials), 1 if force else 0, ctypes.byref(r)),
+                    "autotune")
+        return r.as_dict()
 
     def set_mood_cap(self, slot, cap):
         self._check(self.lib.hosono_batch_set_mood_cap(self.h, int(slot), int(cap)), "set_mood_cap")

@@ -24,6 +24,9 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
+#include <map>
+#include <mutex>
+#include <tuple>
 #include <utility>
 
 namespace hosono {
@@ -275,14 +278,118 @@ void Engine::drop_graphs() {
 int Engine::set_tuning(const hosono_tuning& t) {
     if (t.pass1_staging != HOSONO_STAGE_CP_ASYNC && t.pass1_staging != HOSONO_STAGE_TMA)
         return fail(HOSONO_EINVAL, "pass1_staging %d", t.pass1_staging);
+    if (t.pass1_schedule != HOSONO_SCHED_STATIC && t.pass1_schedule != HOSONO_SCHED_DYNAMIC)
+        return fail(HOSONO_EINVAL, "pass1_schedule %d", t.pass1_schedule);
+    if (t.pass1_blocks_per_sm != 0 && (t.pass1_blocks_per_sm < 2 || t.pass1_blocks_per_sm > 4))
+        return fail(HOSONO_EINVAL, "pass1_blocks_per_sm %d (0 or 2..4)", t.pass1_blocks_per_sm);
+    if (t.pass1_blocks_per_sm > 2 && t.pass1_staging == HOSONO_STAGE_TMA)
+        return fail(HOSONO_EINVAL, "TMA staging runs at two pass-1 blocks per SM");
     tune_ = t;
     drop_graphs();  // the graphs hold the launch choices in their kernel parameters
     return HOSONO_OK;
 }
 
+namespace {
+// the autotuner's process-wide cache: (fp mode, radii, size class, instance class) -> tuning
+std::mutex g_tune_mu;
+std::map<std::tuple<int, int, int, int>, hosono_tuning> g_tune_cache;
+}  // namespace
+
+int Engine::autotune(int trials, bool force, hosono_tune_report* rep) {
+    if (trials < 1 || trials > 1000) return fail(HOSONO_EINVAL, "autotune: trials %d outside [1, 1000]", trials);
+    hosono_tune_report r{};
+    long long cells = 0;
+    int inst = 0;
+    for (const Slot& sl : slots_)
+        if (sl.live) {
+            cells += (long long)sl.p.nx * sl.p.ny;
+            inst++;
+        }
+    if (!inst) return fail(HOSONO_EINVAL, "autotune: no instance to time");
+    int sc = 0, ic = 0;
+    while ((2LL << sc) <= cells) sc++;
+    while ((2 << ic) <= inst) ic++;
+    r.size_class = sc;
+    r.instances = inst;
+    const auto key = std::make_tuple(K_ == kernelset_fast() ? 1 : 0, radii_, sc, ic);
+    if (!force) {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        auto it = g_tune_cache.find(key);
+        if (it != g_tune_cache.end()) {
+            r.cached = 1;
+            r.best = it->second;
+            if (rep) *rep = r;
+            return set_tuning(r.best);
+        }
+    }
+    CUE(cudaStreamSynchronize(s_));
+    const hosono_tuning saved = tune_;
+    // candidates: two blocks per SM with cp.async or TMA staging, three and
+    // four blocks per SM with cp.async; each with the static and the dynamic
+    // tile schedule
+    std::vector<hosono_tuning> cands;
+    const int forms[4][2] = {{2, HOSONO_STAGE_CP_ASYNC}, {2, HOSONO_STAGE_TMA}, {3, HOSONO_STAGE_CP_ASYNC},
+                             {4, HOSONO_STAGE_CP_ASYNC}};
+    for (const auto& f : forms)
+        for (int sched : {HOSONO_SCHED_STATIC, HOSONO_SCHED_DYNAMIC}) {
+            hosono_tuning t{};
+            t.pass1_blocks_per_sm = f[0];
+            t.pass1_staging = f[1];
+            t.pass1_schedule = sched;
+            cands.push_back(t);
+        }
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    CUE(cudaEventCreate(&e0));
+    CUE(cudaEventCreate(&e1));
+    int rc = HOSONO_OK;
+    K_->tune_mark(batch(), 1, s_);
+    for (size_t c = 0; c < cands.size() && c < HOSONO_TUNE_MAX && !rc; c++) {
+        {
+            const hosono_tuning t = cands[c];
+            tune_ = t;
+            const Batch B = batch();
+            float ms = 0.f;
+            for (int k = 0; k <= trials; k++) {
+                if (k == 1) cudaEventRecord(e0, s_);
+                cudaMemsetAsync(d_flags_->p1Next, 0, sizeof d_flags_->p1Next, s_);
+                K_->face_pass1(B, ROLE_STATE, s_);
+            }
+            cudaEventRecord(e1, s_);
+            if (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess ||
+                cudaGetLastError() != cudaSuccess)
+                rc = fail(HOSONO_ECUDA, "autotune: timing launch failed");
+            r.tried[r.candidates] = t;
+            r.ms[r.candidates] = ms / trials;
+            r.candidates++;
+        }
+    }
+    K_->tune_mark(batch(), 0, s_);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    tune_ = saved;
+    if (rc) return rc;
+    CUE(cudaStreamSynchronize(s_));
+    if (h_flags_) {  // a bounded wait of the TMA variant that gave up is an error, not a result
+        CUE(cudaMemcpy(h_flags_, d_flags_, sizeof(BatchFlags), cudaMemcpyDeviceToHost));
+        if (h_flags_->error) return fail(h_flags_->error, "autotune: a timing launch reported an error");
+    }
+    int best = 0;
+    for (int k = 1; k < r.candidates; k++)
+        if (r.ms[k] < r.ms[best]) best = k;
+    r.best = r.tried[best];
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        g_tune_cache[key] = r.best;
+    }
+    if (rep) *rep = r;
+    return set_tuning(r.best);
+}
+
 Batch Engine::batch() const {
     Batch B;
     B.p1Tma = tune_.pass1_staging == HOSONO_STAGE_TMA ? 1 : 0;
+    B.p1Dyn = tune_.pass1_schedule == HOSONO_SCHED_DYNAMIC ? 1 : 0;
+    B.p1Blocks = tune_.pass1_blocks_per_sm == 0 ? 2 : tune_.pass1_blocks_per_sm;
     B.dev = d_dev_;
     B.st = d_st_;
     B.tiles = d_tiles_;

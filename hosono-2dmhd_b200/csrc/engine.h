@@ -100,6 +100,7 @@ struct BatchFlags {
     int stepsLeft;   // step budget of the current run launch
     int radii;       // bit R set when a live instance has GP radius R (per-radius kernels of absent radii exit)
     int recSel;      // which recompute list the current MOOD pass reads (0: Lists::rec, 1: rec2)
+    int p1Next[4];   // pass 1 with the dynamic schedule: next tile index per radius (zeroed by stage_init)
 };
 
 // Roles of the three U buffers: the state lives in U[parity]; A in
@@ -136,6 +137,8 @@ struct Batch {
     BatchFlags* flags;
     Lists L;
     int p1Tma;           // pass 1 stages its stencil box with TMA (1) or cp.async (0)
+    int p1Dyn;           // pass-1 blocks take tiles from a shared counter (1) or grid-stride (0)
+    int p1Blocks;        // resident pass-1 blocks per SM the variant aims at (2, 3 or 4)
     int maxTiles;        // capacity of the tile list
     int maxInst;         // capacity (slots)
     const int2* instTiles;  // per slot: first tile in the tile list, tile count (0: not live)
@@ -218,6 +221,9 @@ struct KernelSet {
     void (*rk_combine2)(const Batch&, cudaStream_t);
     void (*rk_final)(const Batch&, cudaStream_t);
     void (*cons2prim_all)(const Batch&, cudaStream_t);
+    // autotuner: mark the live, unfinished, not held instances as stepping
+    // (on) or at rest (off) so that pass 1 can be timed outside a step
+    void (*tune_mark)(const Batch&, int on, cudaStream_t);
     // grids the launchers use: the pass-1 kernel of radius R, and the
     // largest grid of the other per-tile kernels (each capped at maxTiles)
     void (*launch_info)(int R, int maxTiles, int* pass1_grid, int* tile_grid_max);

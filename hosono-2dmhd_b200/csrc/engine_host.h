@@ -102,6 +102,8 @@ class Engine {
     const InstState* host_states() const { return h_st_; }
     // launch choices (hosono_tuning); changing them rebuilds the step graphs
     int set_tuning(const hosono_tuning& t);
+    // time the candidate tunings on the live instances, apply the fastest
+    int autotune(int trials, bool force, hosono_tune_report* rep);
     const hosono_tuning& tuning() const { return tune_; }
     bool use_graphs = true;
     bool trace = false;

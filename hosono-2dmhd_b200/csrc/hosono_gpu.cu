@@ -270,6 +270,13 @@ int hosono_batch_get_tuning(hosono_batch* b, hosono_tuning* t) {
     return HOSONO_OK;
 }
 
+int hosono_gpu_autotune(hosono_handle* h, int trials, int force, hosono_tune_report* report) {
+    return h ? h->eng.autotune(trials, force != 0, report) : HOSONO_EINVAL;
+}
+int hosono_batch_autotune(hosono_batch* b, int trials, int force, hosono_tune_report* report) {
+    return b ? b->eng.autotune(trials, force != 0, report) : HOSONO_EINVAL;
+}
+
 int hosono_gpu_launch_info(hosono_handle* h, hosono_launch_info* info) {
     if (!h || !info) return HOSONO_EINVAL;
     int dev = 0, sms = 0;

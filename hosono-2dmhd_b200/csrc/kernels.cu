@@ -34,10 +34,6 @@
 #define KNS kstrict
 #endif
 
-// resident 256-thread blocks per SM the pass-1 register budget aims at
-#ifndef HOSONO_PASS1_MIN_BLOCKS
-#define HOSONO_PASS1_MIN_BLOCKS 2
-#endif
 
 namespace hosono {
 namespace KNS {
@@ -385,6 +381,18 @@ __device__ __forceinline__ int pass1_next(const Batch& B, int t, int n) {
     return n;
 }
 
+// the dynamic schedule: the next tile of this radius from the launch-wide
+// counter (one atomic per tile taken; n when none is left)
+template <int R>
+__device__ __forceinline__ int pass1_take(const Batch& B, int n) {
+    for (;;) {
+        const int t = atomicAdd(&B.flags->p1Next[R], 1);
+        if (t >= n) return n;
+        const int k = B.tiles[t].x;
+        if (B.st[k].stepping && B.dev[k].geo.R == R) return t;
+    }
+}
+
 // stage tile t's stencil box (zeros outside the array) into dst and its
 // instance's radius-R prediction vectors into dstPv (one commit group)
 template <int R>
@@ -429,14 +437,30 @@ __device__ __forceinline__ void pass1_stage_tma(const Batch& B, int uin, int t, 
 // (the next tile's are copied in asynchronously while the current one is
 // computed), the per-thread flux accumulators and, with TMA staging, the two
 // boxes' mbarriers.  TMA = false stages with per-thread cp.async copies.
-template <int R, bool TMA>
-__global__ void __launch_bounds__(NTHREADS, HOSONO_PASS1_MIN_BLOCKS) k_face_pass1(Batch B, int uin) {
+//
+// MINB is the number of resident blocks per SM the register budget aims at
+// (launch bounds: 128 registers at 2, 80 at 3, 64 at 4).  Two blocks keep
+// two boxes (the next one loads while the current one is computed); three
+// or four keep one box each, which fits their shared memory, and rely on the
+// other resident blocks to hide the load.
+template <int R>
+struct P1Smem {  // dynamic shared memory layout (doubles): boxes, accumulators, prediction vectors, mbarriers
+    static constexpr int box(int nbuf) { return nbuf * P1Box<R>::DOUBLES; }
+    static constexpr int bytes(int nbuf) {
+        return (nbuf * P1Box<R>::DOUBLES + NCONS * NTHREADS + nbuf * P1Box<R>::PVN) * (int)sizeof(double) + 2 * 8;
+    }
+};
+template <int R, bool TMA, bool DYN, int MINB>
+__global__ void __launch_bounds__(NTHREADS, MINB) k_face_pass1(Batch B, int uin) {
+    constexpr int NBUF = MINB <= 2 ? 2 : 1;
+    static_assert(NBUF == 2 || !TMA, "TMA staging is double-buffered");
     extern __shared__ __align__(128) double smem[];
+    __shared__ int sTile;  // the dynamic schedule's tile, as thread 0 took it
     using Box = P1Box<R>;
     const int tid = threadIdx.y * TILE_X + threadIdx.x;
-    double* acc = smem + 2 * Box::DOUBLES + tid;
-    double* pvBuf = smem + 2 * Box::DOUBLES + NCONS * NTHREADS;  // two PVN-double buffers
-    uint64_t* bars = reinterpret_cast<uint64_t*>(pvBuf + 2 * Box::PVN);
+    double* acc = smem + P1Smem<R>::box(NBUF) + tid;
+    double* pvBuf = smem + P1Smem<R>::box(NBUF) + NCONS * NTHREADS;  // NBUF prediction-vector buffers
+    uint64_t* bars = reinterpret_cast<uint64_t*>(pvBuf + NBUF * Box::PVN);
     if (!(B.flags->radii & (1 << R))) return;  // no instance of this radius
     if (TMA) {
         if (tid == 0) {
@@ -448,8 +472,34 @@ __global__ void __launch_bounds__(NTHREADS, HOSONO_PASS1_MIN_BLOCKS) k_face_pass
     }
     unsigned phase = 0;  // bit b: parity of buffer b's next completion
     const int n = __ldg(B.ntiles);
-    int t = pass1_next<R>(B, blockIdx.x, n);
+    // the block's next tile: grid-stride (every thread computes it), or
+    // taken from the counter by thread 0 and broadcast
+    auto next_tile = [&](int after) -> int {
+        if (!DYN) return pass1_next<R>(B, after, n);
+        __syncthreads();  // every thread has read the previous sTile
+        if (tid == 0) sTile = pass1_take<R>(B, n);
+        __syncthreads();
+        return sTile;
+    };
+    int t = next_tile(blockIdx.x);
     int buf = 0;
+    if constexpr (NBUF == 1) {  // one box: load, compute, next
+        while (t < n) {
+            pass1_stage<R>(B, uin, t, smem, pvBuf, tid);
+            cp_async_wait<0>();
+            __syncthreads();  // tile t's box is in place for every thread
+            const Cell c = tile_at(B, t);
+            InstState& S = B.st[c.k];
+            const InstDev& d = B.dev[c.k];
+            if (first_tile_thread(c)) S.cascadeMode = CASCADE_FROM_FACES;
+            const bool bad = d.phys.force_hydro ? pass1_tile<R, 1>(d, smem, pvBuf, c, acc)
+                                                : pass1_tile<R, 0>(d, smem, pvBuf, c, acc);
+            warp_flag(&S.anyFail, bad);
+            __syncthreads();  // every read of this box is done before it is refilled
+            t = next_tile(t + gridDim.x);
+        }
+        return;
+    }
     if (t < n) {
         if (!TMA)
             pass1_stage<R>(B, uin, t, smem, pvBuf, tid);
@@ -457,7 +507,7 @@ __global__ void __launch_bounds__(NTHREADS, HOSONO_PASS1_MIN_BLOCKS) k_face_pass
             pass1_stage_tma<R>(B, uin, t, smem, pvBuf, bars);
     }
     while (t < n) {
-        const int tn = pass1_next<R>(B, t + gridDim.x, n);
+        const int tn = next_tile(t + gridDim.x);
         if (!TMA) {
             if (tn < n) {
                 pass1_stage<R>(B, uin, tn, smem + (buf ^ 1) * Box::DOUBLES, pvBuf + (buf ^ 1) * Box::PVN, tid);
@@ -1383,6 +1433,7 @@ __global__ void __launch_bounds__(NTHREADS) k_stage_init(Batch B) {
     if (blockIdx.x == 0 && threadIdx.x == 0 && threadIdx.y == 0) {  // the recompute lists start empty
         B.L.counts[LIST_REC] = 0;
         B.L.counts[LIST_REC2] = 0;
+        for (int r = 0; r < 4; r++) B.flags->p1Next[r] = 0;  // pass 1's dynamic schedule starts over
     }
     FOR_TILES(B, t) t_stage_init(B, tile_at(B, t));
 }
@@ -1596,6 +1647,17 @@ __global__ void k_step_end(Batch B, cudaGraphConditionalHandle h, int set_handle
     }
 }
 
+// The autotuner times pass 1 between steps: the instances that would step
+// are marked stepping, and put back at rest afterwards (the face-cascade
+// flag pass 1 raised is cleared too; every stage starts from stage_init).
+__global__ void k_tune_mark(Batch B, int on) {
+    for (int k = threadIdx.x; k < B.maxInst; k += blockDim.x) {
+        InstState& S = B.st[k];
+        S.stepping = (on && S.live && !S.done && !B.hold[k]) ? 1 : 0;
+        S.anyFail = 0;
+    }
+}
+
 // ======================================================================
 const dim3 kTile(TILE_X, TILE_Y);
 
@@ -1636,27 +1698,49 @@ void l_step_end(const Batch& B, cudaGraphConditionalHandle h, cudaStream_t s) {
     k_step_end<<<1, 128, 0, s>>>(B, h, h != 0);
 }
 void l_stage_init(const Batch& B, cudaStream_t s) { TILE_LAUNCH(k_stage_init, B, s); }
-// dynamic shared memory of the pass-1 kernel of radius R: two boxes, the
-// accumulators, two prediction-vector buffers and two mbarriers
-template <int R>
+// dynamic shared memory of a pass-1 kernel variant
+template <int R, int MINB>
 constexpr int pass1_smem() {
-    return (2 * P1Box<R>::DOUBLES + NCONS * NTHREADS + 2 * P1Box<R>::PVN) * (int)sizeof(double) + 2 * 8;
+    return P1Smem<R>::bytes(MINB <= 2 ? 2 : 1);
 }
-template <int R, bool TMA>
+template <int R, bool TMA, bool DYN, int MINB>
 int pass1_grid(int maxTiles) {
     static const bool attr =  // once per process (thread-safe static initialisation)
-        cudaFuncSetAttribute((const void*)k_face_pass1<R, TMA>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             pass1_smem<R>()) == cudaSuccess;
+        cudaFuncSetAttribute((const void*)k_face_pass1<R, TMA, DYN, MINB>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, pass1_smem<R, MINB>()) == cudaSuccess;
     (void)attr;
-    const int r = resident_blocks((const void*)k_face_pass1<R, TMA>, pass1_smem<R>());
+    const int r = resident_blocks((const void*)k_face_pass1<R, TMA, DYN, MINB>, pass1_smem<R, MINB>());
     return r < maxTiles ? r : maxTiles;
 }
+template <int R, bool TMA, bool DYN, int MINB>
+void launch_pass1_v(const Batch& B, int uin, cudaStream_t s) {
+    k_face_pass1<R, TMA, DYN, MINB>
+        <<<dim3((unsigned)pass1_grid<R, TMA, DYN, MINB>(B.maxTiles)), kTile, pass1_smem<R, MINB>(), s>>>(B, uin);
+}
+// the variant the tuning asks for: TMA staging only with two blocks per SM
 template <int R>
 void launch_pass1(const Batch& B, int uin, cudaStream_t s) {
-    if (B.p1Tma)
-        k_face_pass1<R, true><<<dim3((unsigned)pass1_grid<R, true>(B.maxTiles)), kTile, pass1_smem<R>(), s>>>(B, uin);
-    else
-        k_face_pass1<R, false><<<dim3((unsigned)pass1_grid<R, false>(B.maxTiles)), kTile, pass1_smem<R>(), s>>>(B, uin);
+    if (B.p1Blocks == 3) {
+        if (B.p1Dyn)
+            launch_pass1_v<R, false, true, 3>(B, uin, s);
+        else
+            launch_pass1_v<R, false, false, 3>(B, uin, s);
+    } else if (B.p1Blocks == 4) {
+        if (B.p1Dyn)
+            launch_pass1_v<R, false, true, 4>(B, uin, s);
+        else
+            launch_pass1_v<R, false, false, 4>(B, uin, s);
+    } else if (B.p1Tma) {
+        if (B.p1Dyn)
+            launch_pass1_v<R, true, true, 2>(B, uin, s);
+        else
+            launch_pass1_v<R, true, false, 2>(B, uin, s);
+    } else {
+        if (B.p1Dyn)
+            launch_pass1_v<R, false, true, 2>(B, uin, s);
+        else
+            launch_pass1_v<R, false, false, 2>(B, uin, s);
+    }
 }
 void l_face_pass1(const Batch& B, int uin, cudaStream_t s) {
     launch_pass1<2>(B, uin, s);
@@ -1699,8 +1783,10 @@ void l_bc_fill(const Batch& B, int role, cudaStream_t s) { TILE_LAUNCH(k_bc_fill
 void l_rk_combine2(const Batch& B, cudaStream_t s) { TILE_LAUNCH(k_rk_combine2, B, s); }
 void l_rk_final(const Batch& B, cudaStream_t s) { TILE_LAUNCH(k_rk_final, B, s); }
 void l_cons2prim_all(const Batch& B, cudaStream_t s) { TILE_LAUNCH(k_cons2prim_all, B, s); }
+void l_tune_mark(const Batch& B, int on, cudaStream_t s) { k_tune_mark<<<1, 128, 0, s>>>(B, on); }
 void l_launch_info(int R, int maxTiles, int* pass1, int* tile_grid_max) {
-    *pass1 = R == 1 ? pass1_grid<1, false>(maxTiles) : R == 2 ? pass1_grid<2, false>(maxTiles) : pass1_grid<3, false>(maxTiles);
+    *pass1 = R == 1 ? pass1_grid<1, false, false, 2>(maxTiles)
+                    : R == 2 ? pass1_grid<2, false, false, 2>(maxTiles) : pass1_grid<3, false, false, 2>(maxTiles);
     const void* tile_kernels[] = {(const void*)k_cfl_reduce,     (const void*)k_stage_init,   (const void*)k_clear_nextpass,
                                   (const void*)k_cascade_lower,  (const void*)k_compact_next, (const void*)k_compact_post,
                                   (const void*)k_compact_dirty,  (const void*)k_ct_update_detect, (const void*)k_mood_flags,
@@ -1725,7 +1811,7 @@ const KernelSet kset = {
     l_cfl_reduce, l_step_prepare, l_step_begin, l_step_end, l_stage_init, l_face_pass1, l_cascade_cond, l_cascade_lower,
     l_recon_check, l_ct_update_detect, l_mood_flags, l_pass_end, l_recon_list,
     l_compact_post, l_compact_dirty, l_flux_list, l_ct_list, l_clear_low, l_bc_fill, l_rk_combine2, l_rk_final,
-    l_cons2prim_all, l_launch_info, &mops};
+    l_cons2prim_all, l_tune_mark, l_launch_info, &mops};
 
 }  // namespace KNS
 

@@ -286,12 +286,37 @@ int hosono_gpu_stream(hosono_handle* h, void** stream);
  * graphs on the next step. */
 #define HOSONO_STAGE_CP_ASYNC 0  /* pass-1 stencil box staged by per-thread cp.async copies */
 #define HOSONO_STAGE_TMA 1       /* ... by one TMA tensor copy (cp.async.bulk.tensor) per box */
+#define HOSONO_SCHED_STATIC 0    /* pass-1 blocks walk the tile list grid-stride */
+#define HOSONO_SCHED_DYNAMIC 1   /* ... take their next tile from a launch-wide counter */
 typedef struct hosono_tuning {
-    int pass1_staging;  /* HOSONO_STAGE_* */
-    int pad[7];         /* zero */
+    int pass1_staging;        /* HOSONO_STAGE_* */
+    int pass1_schedule;       /* HOSONO_SCHED_* */
+    int pass1_blocks_per_sm;  /* resident pass-1 blocks per SM the register budget aims at: 2 (0 = 2;
+                                 128 registers, two stencil boxes per block), 3 or 4 (80 / 64 registers,
+                                 one box; cp.async staging only) */
+    int pad[5];               /* zero */
 } hosono_tuning;
 int hosono_gpu_set_tuning(hosono_handle* h, const hosono_tuning* t);
 int hosono_gpu_get_tuning(hosono_handle* h, hosono_tuning* t);
+
+/* Autotuner.  Times every candidate hosono_tuning on the instances the
+ * handle or batch holds now -- `trials` launches of the MOOD pass-1 kernels
+ * (83 % of a time step; they only write scratch that every stage rewrites,
+ * so the solution is untouched) per candidate, after one untimed launch --
+ * and applies the fastest.  The choice is kept in a process-wide cache keyed
+ * by (arithmetic mode, GP radii present, size class = floor(log2(interior
+ * cells)), floor(log2(instances))); a later call with the same key applies
+ * the cached choice without timing unless `force` is set. */
+#define HOSONO_TUNE_MAX 8
+typedef struct hosono_tune_report {
+    int candidates;                    /* entries of tried/ms filled                  */
+    int cached;                        /* 1: taken from the cache, nothing was timed  */
+    int size_class, instances;         /* the cache key's size class; instances held  */
+    hosono_tuning tried[HOSONO_TUNE_MAX];
+    double ms[HOSONO_TUNE_MAX];        /* mean ms of one pass-1 launch (all radii)    */
+    hosono_tuning best;
+} hosono_tune_report;
+int hosono_gpu_autotune(hosono_handle* h, int trials, int force, hosono_tune_report* report);
 
 /* Launch geometry of the handle's kernels: every per-tile kernel walks the
  * tile list grid-stride with a grid sized to the GPU, so a grid smaller than
@@ -328,6 +353,7 @@ int hosono_batch_download(hosono_batch* b, int slot, double* U, double* V, int* 
 int hosono_batch_set_time(hosono_batch* b, int slot, double t, double tmax, int nstep, int nstepmax);
 int hosono_batch_set_tuning(hosono_batch* b, const hosono_tuning* t);
 int hosono_batch_get_tuning(hosono_batch* b, hosono_tuning* t);
+int hosono_batch_autotune(hosono_batch* b, int trials, int force, hosono_tune_report* report);
 /* hosono_gpu_set_mood_cap for one instance of the batch */
 int hosono_batch_set_mood_cap(hosono_batch* b, int slot, int cap);
 /* every live, unfinished instance steps until its tmax/nstepmax, or at most

@@ -143,3 +143,29 @@ def test_tma_staging_bitwise(case, tmp_par_dir):
         np.testing.assert_array_equal(V, o.V())
         np.testing.assert_array_equal(S, o.scheme())
     s.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", ["ot32_r2", "sedov32_r2", "blast40_r2"])
+def test_advance_host_drop_in(case, tmp_par_dir):
+    """hosono_gpu_advance_host, the form a driver that keeps grid_state on
+    the host binds: the host U (and V, or none: then V = cons2prim(U) on the
+    device) goes in, the advanced U and V come back in place; three steps of
+    cfl_computedt + advance_host equal the oracle bit for bit."""
+    m = pkg.load()
+    par = parfiles.make(tmp_par_dir, case + "_host", CASES[case]())
+    o = oracle.Oracle(par)
+    s = m.Solver.from_par(par, fp_mode=m.FP_STRICT)
+    U, V, _ = s.download()
+    for step in range(3):
+        dt = o.cfl()
+        assert s.cfl_computedt() == dt
+        o.advance(dt)
+        if step == 1:
+            s.advance_host(dt, U)  # U alone: V rebuilt on the device, V not returned
+            _, V, _ = s.download()
+        else:
+            s.advance_host(dt, U, V)
+        np.testing.assert_array_equal(U, o.U())
+        np.testing.assert_array_equal(V, o.V())
+    s.close()
