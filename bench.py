@@ -415,6 +415,8 @@ def bench_ours(args, rank, world, local):
         line["tuning"] = tune
     if other:
         line["fast_fp"] = other
+    if world == 1 and not args.no_config0 and args.workload != "ot128_r1":
+        line["config0"] = bench_config0(m, fp, torch)
     if world == 1 and not args.no_batched:
         line["batched"] = bench_batched(m, fp, torch, limit=args.batched_limit, eager=args.eager)
     served_kept = {}
@@ -434,6 +436,32 @@ def bench_ours(args, rank, world, local):
     print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
+
+
+def bench_config0(m, fp, torch):
+    """The reference's own runnable case: Orszag-Tang 128^2, GP radius 1,
+    ell/dx = 6, to t_end = 0.5 as one graph launch (plain single solve, dt on
+    the device), after an untimed run that captures the graphs."""
+    with tempfile.TemporaryDirectory() as d:
+        par = par_for("ot128_r1", d)
+        s = m.Solver.from_par(par, fp_mode=fp)
+        U0, V0, _ = s.download()
+        tune = s.autotune(trials=5, force=True)
+        s.run()
+        s.upload(U0, V0)
+        s.set_time(0.0, s.run_info.tmax, 0, s.run_info.nstepmax)
+        stream = torch.cuda.ExternalStream(s.stream())
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        t, n = s.step(0)
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        passes = s.stats()["mood_passes"]
+        s.close()
+    return {"workload": "Orszag-Tang 128x128, GP-MOOD R=1 (3rd->1st), ell/dx=6, to t_end=0.5", "steps": n,
+            "t_end": t, "value": 128 * 128 * n / (ms / 1e3), "unit": "zone-updates/s", "ms_per_step": ms / n,
+            "mood_passes_per_step": passes / n, "tuning": tune["best"]}
 
 
 def load_problems():
@@ -633,6 +661,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="keep the default launch choices (no autotuning)")
     ap.add_argument("--no-batched", action="store_true", help="skip the 64-instance batched-vs-plain measurement")
+    ap.add_argument("--no-config0", action="store_true", help="skip the Orszag-Tang 128^2 R=1 to t_end leg")
     ap.add_argument("--eager", action="store_true",
                     help="launch kernels one by one instead of as CUDA graphs (the plain and batched legs; for "
                          "profilers, which do not see inside conditional graph nodes)")
