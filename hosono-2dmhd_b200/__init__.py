@@ -99,15 +99,16 @@ class LaunchInfo(ctypes.Structure):
 
 class Tuning(ctypes.Structure):
     _fields_ = [("pass1_staging", ctypes.c_int), ("pass1_schedule", ctypes.c_int),
-                ("pass1_blocks_per_sm", ctypes.c_int), ("pad", ctypes.c_int * 5)]
+                ("pass1_blocks_per_sm", ctypes.c_int), ("later_passes", ctypes.c_int), ("pad", ctypes.c_int * 4)]
 
     def as_dict(self):
         return {"pass1_staging": self.pass1_staging, "pass1_schedule": self.pass1_schedule,
-                "pass1_blocks_per_sm": self.pass1_blocks_per_sm}
+                "pass1_blocks_per_sm": self.pass1_blocks_per_sm, "later_passes": self.later_passes}
 
 
 STAGE_CP_ASYNC, STAGE_TMA = 0, 1
 SCHED_STATIC, SCHED_DYNAMIC = 0, 1
+LATER_KERNELS, LATER_PERSISTENT = 0, 1
 TUNE_MAX = 8
 
 

@@ -166,7 +166,7 @@ Engine::~Engine() {
     for (cudaEvent_t ev : profEv_)
         if (ev) cudaEventDestroy(ev);
     for (void* p : {(void*)d_instTiles_, (void*)d_actRange_, (void*)d_actInfo_, (void*)d_casRange_,
-                    (void*)d_casInfo_, (void*)d_hold_})
+                    (void*)d_casInfo_, (void*)d_hold_, (void*)d_gbar_})
         if (p) cudaFree(p);
     for (void* p : {(void*)d_dev_, (void*)d_st_, (void*)d_tiles_, (void*)d_ntiles_, (void*)d_flags_, (void*)staging_,
                     (void*)schemeInt_, (void*)lists_.rec, (void*)lists_.face, (void*)lists_.recF, (void*)lists_.low,
@@ -194,6 +194,8 @@ int Engine::init(int max_inst, int max_tiles, int fp_mode) {
     CUE(cudaMalloc(&d_casInfo_, sizeof(int) * 2));
     CUE(cudaMalloc(&d_hold_, sizeof(int) * maxInst_));
     CUE(cudaMemsetAsync(d_hold_, 0, sizeof(int) * maxInst_, s_));
+    CUE(cudaMalloc(&d_gbar_, sizeof(unsigned) * 2));
+    CUE(cudaMemsetAsync(d_gbar_, 0, sizeof(unsigned) * 2, s_));
     CUE(cudaMemsetAsync(d_casInfo_, 0, sizeof(int) * 2, s_));
     CUE(cudaMemsetAsync(d_instTiles_, 0, sizeof(int2) * maxInst_, s_));
     CUE(cudaMemsetAsync(d_actInfo_, 0, sizeof(int) * 2, s_));
@@ -284,6 +286,8 @@ int Engine::set_tuning(const hosono_tuning& t) {
         return fail(HOSONO_EINVAL, "pass1_blocks_per_sm %d (0 or 2..4)", t.pass1_blocks_per_sm);
     if (t.pass1_blocks_per_sm > 2 && t.pass1_staging == HOSONO_STAGE_TMA)
         return fail(HOSONO_EINVAL, "TMA staging runs at two pass-1 blocks per SM");
+    if (t.later_passes != HOSONO_LATER_KERNELS && t.later_passes != HOSONO_LATER_PERSISTENT)
+        return fail(HOSONO_EINVAL, "later_passes %d", t.later_passes);
     tune_ = t;
     drop_graphs();  // the graphs hold the launch choices in their kernel parameters
     return HOSONO_OK;
@@ -332,7 +336,7 @@ int Engine::autotune(int trials, bool force, hosono_tune_report* rep) {
                              {4, HOSONO_STAGE_CP_ASYNC}};
     for (const auto& f : forms)
         for (int sched : {HOSONO_SCHED_STATIC, HOSONO_SCHED_DYNAMIC}) {
-            hosono_tuning t{};
+            hosono_tuning t = tune_;  // the caller's later-pass choice stays
             t.pass1_blocks_per_sm = f[0];
             t.pass1_staging = f[1];
             t.pass1_schedule = sched;
@@ -404,6 +408,7 @@ Batch Engine::batch() const {
     B.casRange = d_casRange_;
     B.casInfo = d_casInfo_;
     B.hold = d_hold_;
+    B.gbar = d_gbar_;
     return B;
 }
 
@@ -798,6 +803,12 @@ int Engine::record_stage(Rec& r, int uin, int uout, cudaEvent_t ev0, cudaEvent_t
     TRYE(r.k([&](cudaStream_t s) { K->mood_flags(B, MOOD_FLAGS_DENSE, s); }));
     if (trace) TRYE(r.host([&] { return trace_snapshot(); }));
     TRYE(r.k([&](cudaStream_t s) { K->clear_low(B, s); }));
+    if (tune_.later_passes == HOSONO_LATER_PERSISTENT && !trace) {
+        // the later passes as one persistent launch (it reads anyActive itself)
+        TRYE(r.k([&](cudaStream_t s) { K->pass_end(B, 0, 1, s); }));
+        TRYE(r.k([&](cudaStream_t s) { K->mood_rest(B, uin, uout, s); }));
+        return HOSONO_OK;
+    }
     TRYE(r.cond(&hm, 0));
     TRYE(r.k([&](cudaStream_t s) { K->pass_end(B, hm, 1, s); }));
     if (trace) TRYE(r.host([&] { return trace_after_pass(); }));

@@ -143,6 +143,7 @@ struct Batch {
     int maxInst;         // capacity (slots)
     const int2* instTiles;  // per slot: first tile in the tile list, tile count (0: not live)
     const int* hold;        // per slot: nonzero = sits out the run launches (state untouched)
+    unsigned* gbar;         // grid barrier of the persistent later-pass launch: {count, generation}
     // instances still in their MOOD loop after the last pass_end, in slot
     // order: (slot, first virtual tile); actInfo = {instances, tiles}.  The
     // dense kernels of the later passes walk only these tiles.
@@ -224,6 +225,8 @@ struct KernelSet {
     // autotuner: mark the live, unfinished, not held instances as stepping
     // (on) or at rest (off) so that pass 1 can be timed outside a step
     void (*tune_mark)(const Batch&, int on, cudaStream_t);
+    // every later MOOD pass of a stage in one persistent (cooperative) launch
+    void (*mood_rest)(const Batch&, int uin, int uout, cudaStream_t);
     // grids the launchers use: the pass-1 kernel of radius R, and the
     // largest grid of the other per-tile kernels (each capped at maxTiles)
     void (*launch_info)(int R, int maxTiles, int* pass1_grid, int* tile_grid_max);

@@ -167,6 +167,7 @@ class Engine {
     int2* d_casRange_ = nullptr;
     int* d_casInfo_ = nullptr;
     int* d_hold_ = nullptr;
+    unsigned* d_gbar_ = nullptr;
     std::vector<int2> instTiles_;
     int* d_ntiles_ = nullptr;
     BatchFlags* d_flags_ = nullptr;

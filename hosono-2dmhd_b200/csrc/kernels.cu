@@ -549,13 +549,12 @@ constexpr int PASS_END_THREADS = 128;
 
 // (slot, first virtual tile) of every instance with pick(slot) true, in slot
 // order, and info = {instances, tiles}: per-thread chunks of slots, a block
-// scan of the counts, then each thread writes its chunk.  One block of
-// PASS_END_THREADS threads.
-template <class Pick>
-__device__ __forceinline__ void build_ranges(const Batch& B, Pick pick, int2* range, int* info) {
-    __shared__ int sCnt[PASS_END_THREADS / 32], sTil[PASS_END_THREADS / 32];
-    const int tid = threadIdx.x;
-    const int per = (B.maxInst + PASS_END_THREADS - 1) / PASS_END_THREADS;
+// scan of the counts, then each thread writes its chunk.  One block of NT
+// threads (thread index tid).
+template <int NT, class Pick>
+__device__ __forceinline__ void build_ranges(const Batch& B, int tid, Pick pick, int2* range, int* info) {
+    __shared__ int sCnt[NT / 32], sTil[NT / 32];
+    const int per = (B.maxInst + NT - 1) / NT;
     const int k0 = min(B.maxInst, tid * per), k1 = min(B.maxInst, k0 + per);
     int cnt = 0, til = 0;
     for (int k = k0; k < k1; k++)
@@ -588,7 +587,7 @@ __device__ __forceinline__ void build_ranges(const Batch& B, Pick pick, int2* ra
             range[c0++] = make_int2(k, t0);
             t0 += B.instTiles[k].y;
         }
-    if (tid == PASS_END_THREADS - 1) {
+    if (tid == NT - 1) {
         info[0] = ic;
         info[1] = it;
     }
@@ -599,12 +598,13 @@ __device__ __forceinline__ void build_ranges(const Batch& B, Pick pick, int2* ra
 // Face cascade (reconstruct.f90:143-171).
 // cascade_cond: per instance, whether it entered (or stays in) the cascade;
 // sets the batch condition.  Single block, one thread per slot.
-__global__ void __launch_bounds__(PASS_END_THREADS) k_cascade_cond(Batch B, cudaGraphConditionalHandle h,
-                                                                      int set_handle) {
+template <int NT>
+__device__ __forceinline__ void d_cascade_cond(const Batch& B, int tid, cudaGraphConditionalHandle h,
+                                               int set_handle) {
     __shared__ int any;
-    if (threadIdx.x == 0) any = 0;
+    if (tid == 0) any = 0;
     __syncthreads();
-    for (int k = threadIdx.x; k < B.maxInst; k += blockDim.x) {
+    for (int k = tid; k < B.maxInst; k += NT) {
         InstState& S = B.st[k];
         const int in = (S.stepping && S.stageActive && S.anyFail) ? 1 : 0;
         S.anyFail = 0;
@@ -616,12 +616,16 @@ __global__ void __launch_bounds__(PASS_END_THREADS) k_cascade_cond(Batch B, cuda
         }
     }
     __syncthreads();
-    build_ranges(B, [&](int k) { return B.st[k].nextIter != 0; }, B.casRange, B.casInfo);
-    if (threadIdx.x == 0) {
+    build_ranges<NT>(B, tid, [&](int k) { return B.st[k].nextIter != 0; }, B.casRange, B.casInfo);
+    if (tid == 0) {
         B.flags->anyFail = any;
         B.L.counts[LIST_NEXT] = 0;  // the next cascade iteration compacts its cells afresh
         if (set_handle) cudaGraphSetConditional(h, any ? 1u : 0u);
     }
+}
+__global__ void __launch_bounds__(PASS_END_THREADS) k_cascade_cond(Batch B, cudaGraphConditionalHandle h,
+                                                                      int set_handle) {
+    d_cascade_cond<PASS_END_THREADS>(B, threadIdx.x, h, set_handle);
 }
 
 // the serial lowering loop of reconstruct.f90:146-169 (order independent: a
@@ -704,11 +708,15 @@ __global__ void __launch_bounds__(NTHREADS) k_cascade_lower(Batch B) {
 // quadrature points, or quadrature points), so one item costs the latency of
 // one face value instead of a dozen in a row.  The loop runs in whole-warp
 // steps so warp collectives see every lane.
-#define FOR_GROUPS(n, GL, e, sub, act)                                                                        \
-    for (int wbase_ = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * (32 / (GL)), sub = threadIdx.x % (GL), \
-             e = wbase_ + (int)((threadIdx.x & 31) / (GL));                                                   \
-         wbase_ < (n); wbase_ += ((gridDim.x * blockDim.x) >> 5) * (32 / (GL)), e = wbase_ + (int)((threadIdx.x & 31) / (GL))) \
+// gt, gs: the calling thread's global index and the threads of the launch
+// (linear: in a 2D block of 32-wide rows, gt & 31 is still the lane).
+#define FOR_GROUPS_G(n, GL, e, sub, act, gt, gs)                                                          \
+    for (int wbase_ = ((gt) >> 5) * (32 / (GL)), sub = ((gt) & 31) % (GL), e = wbase_ + ((gt) & 31) / (GL); \
+         wbase_ < (n); wbase_ += ((gs) >> 5) * (32 / (GL)), e = wbase_ + ((gt) & 31) / (GL))                 \
         for (bool act = e < (n), once_ = true; once_; once_ = false)
+// a 1D launch's global thread index and thread count
+#define GT1 ((int)(blockIdx.x * blockDim.x + threadIdx.x))
+#define GS1 ((int)(gridDim.x * blockDim.x))
 
 // One cell of an inner pass of reconstruct_faceValsWithGP on 16 lanes: lane
 // sub = 4*f + q takes face f at quadrature point q, at rr = min(scheme(c),
@@ -771,16 +779,19 @@ __global__ void __launch_bounds__(NTHREADS) k_compact_next(Batch B) {
 }
 // ... and re-reconstruct them (list `which`: LIST_NEXT in the cascade,
 // LIST_REC at the start of a later MOOD pass)
-__global__ void __launch_bounds__(256) k_recon_group(Batch B, int uin, int which) {
+__device__ __forceinline__ void d_recon_group(const Batch& B, int uin, int which, int gt, int gs) {
     const int2* list = which == LIST_NEXT ? B.L.next : rec_list(B, false);
     const int n = min(B.L.counts[which == LIST_NEXT ? (int)LIST_NEXT : rec_count(B, false)], (int)B.L.cap);
-    FOR_GROUPS(n, RECON_GL, e, sub, act) {
+    FOR_GROUPS_G(n, RECON_GL, e, sub, act, gt, gs) {
         int2 it = make_int2(0, 0);
         if (act) it = list[e];
         InstState& S = B.st[it.x];
         const bool bad = recon_cell_group(B.dev[it.x], S, uin, it.y, sub, act);
         if (act && sub == 0 && bad) atomicOr(&S.anyFail, 1);
     }
+}
+__global__ void __launch_bounds__(256) k_recon_group(Batch B, int uin, int which) {
+    d_recon_group(B, uin, which, GT1, GS1);
 }
 
 
@@ -837,9 +848,8 @@ __global__ void __launch_bounds__(NTHREADS) k_compact_dirty(Batch B) {
 
 // List kernels walk their list grid-stride in whole-warp steps, so warp
 // collectives see every lane.
-#define FOR_LIST(n, e, act)                                                                               \
-    for (int base_ = (blockIdx.x * blockDim.x + threadIdx.x) & ~31, e = base_ + (threadIdx.x & 31);      \
-         base_ < (n); base_ += gridDim.x * blockDim.x, e = base_ + (threadIdx.x & 31))                   \
+#define FOR_LIST_G(n, e, act, gt, gs)                                                       \
+    for (int base_ = (gt) & ~31, e = base_ + ((gt) & 31); base_ < (n); base_ += (gs), e = base_ + ((gt) & 31)) \
         for (bool act = e < (n), once_ = true; once_; once_ = false)
 
 // ======================================================================
@@ -851,9 +861,9 @@ __global__ void __launch_bounds__(NTHREADS) k_compact_dirty(Batch B) {
 // group's first lane sums w_q * F_q in quadrature order, as
 // riemannSolver_getFaceFlux does.
 constexpr int FLUX_GL = 4;
-__global__ void __launch_bounds__(256) k_flux_list(Batch B, int uin) {
+__device__ __forceinline__ void d_flux_list(const Batch& B, int uin, int gt, int gs) {
     const int n = min(B.L.counts[LIST_FACE], (int)(2 * B.L.cap));
-    FOR_GROUPS(n, FLUX_GL, e, sub, act) {
+    FOR_GROUPS_G(n, FLUX_GL, e, sub, act, gt, gs) {
         int2 it = make_int2(0, 0);
         if (act) it = B.L.face[e];
         const InstDev& d = B.dev[it.x];
@@ -908,6 +918,7 @@ __global__ void __launch_bounds__(256) k_flux_list(Batch B, int uin) {
         }
     }
 }
+__global__ void __launch_bounds__(256) k_flux_list(Batch B, int uin) { d_flux_list(B, uin, GT1, GS1); }
 
 // ======================================================================
 // FLICDdivB_fluxCorrections (FLICDdivB.f90:13-70) from fluxRaw.
@@ -1128,9 +1139,9 @@ __global__ void __launch_bounds__(NTHREADS, 6) k_ct_update_detect(Batch B, int u
 }
 
 // the same on the recomputeFLICD list of a later MOOD pass
-__global__ void __launch_bounds__(256) k_ct_list(Batch B, int uin, int uout) {
+__device__ __forceinline__ void d_ct_list(const Batch& B, int uin, int uout, int gt, int gs) {
     const int n = min(B.L.counts[LIST_RECF], (int)B.L.cap);
-    FOR_LIST(n, e, act) {
+    FOR_LIST_G(n, e, act, gt, gs) {
         bool low = false;
         int2 it = make_int2(0, 0);
         if (act) {
@@ -1145,15 +1156,17 @@ __global__ void __launch_bounds__(256) k_ct_list(Batch B, int uin, int uout) {
         warp_append(B.L, LIST_LOW, B.L.low, B.L.cap, low, it);
     }
 }
+__global__ void __launch_bounds__(256) k_ct_list(Batch B, int uin, int uout) { d_ct_list(B, uin, uout, GT1, GS1); }
 
 // `lowered` back to zero on the cells this pass lowered
-__global__ void __launch_bounds__(256) k_clear_low(Batch B) {
+__device__ __forceinline__ void d_clear_low(const Batch& B, int gt, int gs) {
     const int n = min(B.L.counts[LIST_LOW], (int)B.L.cap);
-    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+    for (int e = gt; e < n; e += gs) {
         const int2 it = B.L.low[e];
         B.dev[it.x].lowered[it.y] = 0;
     }
 }
+__global__ void __launch_bounds__(256) k_clear_low(Batch B) { d_clear_low(B, GT1, GS1); }
 
 // ======================================================================
 // After detect: recompute = cross of lowered cells, recomputeFLICD = radius-2
@@ -1252,13 +1265,13 @@ __device__ __forceinline__ void sync_cell(const Batch& B, int e, int nLow, int2*
     *from_low = e < nLow;
     *it_out = *from_low ? B.L.low[e] : B.L.casc[e - nLow];
 }
-__global__ void __launch_bounds__(256) k_flags_clear(Batch B) {
+__device__ __forceinline__ void d_flags_clear(const Batch& B, int gt, int gs) {
     const int nF = min(B.L.counts[LIST_FACE], (int)(2 * B.L.cap));
     const int nR = min(B.L.counts[LIST_RECF], (int)B.L.cap);
     const int nP = min(B.L.counts[rec_count(B, false)], (int)B.L.cap);
     const int2* recCur = rec_list(B, false);
     const int nC = min(B.L.counts[LIST_CASC], (int)B.L.cap);
-    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nF + nR + nP + nC; e += gridDim.x * blockDim.x) {
+    for (int e = gt; e < nF + nR + nP + nC; e += gs) {
         if (e < nF) {  // both cells of a re-fluxed face
             const int2 it = B.L.face[e];
             const InstDev& d = B.dev[it.x];
@@ -1283,10 +1296,11 @@ __global__ void __launch_bounds__(256) k_flags_clear(Batch B) {
         }
     }
 }
-__global__ void __launch_bounds__(256) k_flags_scatter(Batch B) {
+__global__ void __launch_bounds__(256) k_flags_clear(Batch B) { d_flags_clear(B, GT1, GS1); }
+__device__ __forceinline__ void d_flags_scatter(const Batch& B, int gt, int gs) {
     const int nL = min(B.L.counts[LIST_LOW], (int)B.L.cap);
     const int nC = min(B.L.counts[LIST_CASC], (int)B.L.cap);
-    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nL + nC; e += gridDim.x * blockDim.x) {
+    for (int e = gt; e < nL + nC; e += gs) {
         int2 it;
         bool fromLow;
         sync_cell(B, e, nL, &it, &fromLow);
@@ -1325,10 +1339,11 @@ __global__ void __launch_bounds__(256) k_flags_scatter(Batch B) {
         B.L.sync[e] = (int8_t)s;
     }
 }
-__global__ void __launch_bounds__(256) k_scheme_sync(Batch B, int clear_low) {
+__global__ void __launch_bounds__(256) k_flags_scatter(Batch B) { d_flags_scatter(B, GT1, GS1); }
+__device__ __forceinline__ void d_scheme_sync(const Batch& B, int clear_low, int gt, int gs) {
     const int nL = min(B.L.counts[LIST_LOW], (int)B.L.cap);
     const int nC = min(B.L.counts[LIST_CASC], (int)B.L.cap);
-    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nL + nC; e += gridDim.x * blockDim.x) {
+    for (int e = gt; e < nL + nC; e += gs) {
         int2 it;
         bool fromLow;
         sync_cell(B, e, nL, &it, &fromLow);
@@ -1352,14 +1367,19 @@ __global__ void __launch_bounds__(256) k_scheme_sync(Batch B, int clear_low) {
         if (fromLow && clear_low) d.lowered[c0] = 0;  // k_flags_scatter has read it
     }
 }
+__global__ void __launch_bounds__(256) k_scheme_sync(Batch B, int clear_low) {
+    d_scheme_sync(B, clear_low, GT1, GS1);
+}
 
 // End of a MOOD pass (timeStep.f90:86-128 loop test): an instance whose detect
 // lowered nothing leaves the loop.  Single block, one thread per slot.
-__global__ void __launch_bounds__(PASS_END_THREADS) k_pass_end(Batch B, cudaGraphConditionalHandle h, int set_handle, int flip) {
+template <int NT>
+__device__ __forceinline__ void d_pass_end(const Batch& B, int tid, cudaGraphConditionalHandle h, int set_handle,
+                                           int flip) {
     __shared__ int any;
-    if (threadIdx.x == 0) any = 0;
+    if (tid == 0) any = 0;
     __syncthreads();
-    for (int k = threadIdx.x; k < B.maxInst; k += blockDim.x) {
+    for (int k = tid; k < B.maxInst; k += NT) {
         InstState& S = B.st[k];
         if (!(S.stepping && S.stageActive)) continue;
         if (flip) S.schemeSel = 1 - S.schemeSel;  // k_mood_flags wrote the other buffer
@@ -1388,8 +1408,8 @@ __global__ void __launch_bounds__(PASS_END_THREADS) k_pass_end(Batch B, cudaGrap
     __syncthreads();
     // the instances still in their MOOD loop and their tiles, for the dense
     // kernels of the next pass
-    build_ranges(B, [&](int k) { return B.st[k].stepping && B.st[k].stageActive; }, B.actRange, B.actInfo);
-    if (threadIdx.x == 0) {
+    build_ranges<NT>(B, tid, [&](int k) { return B.st[k].stepping && B.st[k].stageActive; }, B.actRange, B.actInfo);
+    if (tid == 0) {
         B.flags->anyActive = any;
         if (B.L.counts[LIST_OVERFLOW]) B.flags->error = HOSONO_EINVAL;
         // the next pass reads the recompute list the flag rebuild just filled
@@ -1400,6 +1420,10 @@ __global__ void __launch_bounds__(PASS_END_THREADS) k_pass_end(Batch B, cudaGrap
             if (w != (cur ? LIST_REC2 : LIST_REC)) B.L.counts[w] = 0;
         if (set_handle) cudaGraphSetConditional(h, any ? 1u : 0u);
     }
+}
+__global__ void __launch_bounds__(PASS_END_THREADS) k_pass_end(Batch B, cudaGraphConditionalHandle h, int set_handle,
+                                                                int flip) {
+    d_pass_end<PASS_END_THREADS>(B, threadIdx.x, h, set_handle, flip);
 }
 
 // timeStep_forwardEuler's reset (timeStep.f90:79-81) on every cell:
@@ -1434,6 +1458,7 @@ __global__ void __launch_bounds__(NTHREADS) k_stage_init(Batch B) {
         B.L.counts[LIST_REC] = 0;
         B.L.counts[LIST_REC2] = 0;
         for (int r = 0; r < 4; r++) B.flags->p1Next[r] = 0;  // pass 1's dynamic schedule starts over
+        B.gbar[0] = 0;  // the persistent later-pass launch's barrier count (after an aborted launch too)
     }
     FOR_TILES(B, t) t_stage_init(B, tile_at(B, t));
 }
@@ -1647,6 +1672,107 @@ __global__ void k_step_end(Batch B, cudaGraphConditionalHandle h, int set_handle
     }
 }
 
+// ======================================================================
+// The later MOOD passes of a forward-Euler stage as one persistent launch
+// (timeStep.f90:86-128 after the first pass): every phase of a pass -- the
+// re-reconstruction of the recompute list, the face cascade, the face and
+// FLICD lists, re-flux, FLICD + update + detect, the flag rebuild and the
+// pass end -- runs in turn over the whole grid, separated by grid-wide
+// barriers instead of kernel boundaries.  The blocks are all resident (a
+// cooperative launch sized by occupancy: one 256-thread block per SM, whose
+// 255-register budget holds the Riemann solver of the re-flux phase without
+// spills).  The single-block steps (cascade_cond, pass_end) run on block 0
+// while the others wait.
+
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];\n" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ int ld_acquire_s32(const int* p) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];\n" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Grid-wide barrier: each block's thread 0 publishes its block's writes
+// (fence), counts itself in, and waits for the generation counter to move;
+// the last block to arrive resets the count and moves the generation.  The
+// wait is bounded: after kWaitCycles, or as soon as some block reported an
+// error, the block reports HOSONO_ETIMEOUT (the first error stays) and the
+// function returns false so that the caller leaves.
+__device__ __forceinline__ bool grid_barrier(const Batch& B) {
+    __shared__ int sOk;
+    __syncthreads();
+    if (threadIdx.x == 0 && threadIdx.y == 0) {
+        unsigned* cnt = B.gbar;
+        unsigned* gen = B.gbar + 1;
+        const unsigned g = ld_acquire_u32(gen);
+        __threadfence();
+        int ok = 1;
+        if (atomicAdd(cnt, 1u) + 1u == gridDim.x) {
+            atomicExch(cnt, 0u);
+            __threadfence();
+            atomicAdd(gen, 1u);
+        } else {
+            const long long t0 = clock64();
+            while (ld_acquire_u32(gen) == g) {
+                if (ld_acquire_s32(&B.flags->error) || clock64() - t0 > kWaitCycles) {
+                    ok = 0;
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+        if (!ok) atomicCAS(&B.flags->error, 0, HOSONO_ETIMEOUT);
+        sOk = ok;
+    }
+    __syncthreads();
+    return sOk != 0;
+}
+
+__global__ void __launch_bounds__(NTHREADS, 1) k_mood_rest(Batch B, int uin, int uout) {
+    const int tid = threadIdx.y * TILE_X + threadIdx.x;
+    const int gt = blockIdx.x * NTHREADS + tid, gs = gridDim.x * NTHREADS;
+#define GSYNC_OR_LEAVE \
+    if (!grid_barrier(B)) return
+    for (;;) {
+        if (!ld_acquire_s32(&B.flags->anyActive)) return;  // the same value in every block (read after a barrier)
+        d_recon_group(B, uin, LIST_REC, gt, gs);
+        GSYNC_OR_LEAVE;
+        if (blockIdx.x == 0) d_cascade_cond<NTHREADS>(B, tid, 0, 0);
+        GSYNC_OR_LEAVE;
+        while (ld_acquire_s32(&B.flags->anyFail)) {
+            FOR_CASCADE_TILES(B, t) t_clear_nextpass(B, tile_at(B, t));
+            GSYNC_OR_LEAVE;
+            FOR_CASCADE_TILES(B, t) t_cascade_lower(B, tile_at(B, t));
+            GSYNC_OR_LEAVE;
+            FOR_CASCADE_TILES(B, t) t_compact_next(B, tile_at(B, t));
+            GSYNC_OR_LEAVE;
+            d_recon_group(B, uin, LIST_NEXT, gt, gs);
+            GSYNC_OR_LEAVE;
+            if (blockIdx.x == 0) d_cascade_cond<NTHREADS>(B, tid, 0, 0);
+            GSYNC_OR_LEAVE;
+        }
+        FOR_ACTIVE_TILES(B, t) t_compact_post(B, tile_at(B, t));
+        GSYNC_OR_LEAVE;
+        d_flux_list(B, uin, gt, gs);
+        GSYNC_OR_LEAVE;
+        d_ct_list(B, uin, uout, gt, gs);
+        GSYNC_OR_LEAVE;
+        d_flags_clear(B, gt, gs);
+        GSYNC_OR_LEAVE;
+        d_flags_scatter(B, gt, gs);
+        GSYNC_OR_LEAVE;
+        d_scheme_sync(B, 1, gt, gs);
+        GSYNC_OR_LEAVE;
+        if (blockIdx.x == 0) d_pass_end<NTHREADS>(B, tid, 0, 0, 0);
+        GSYNC_OR_LEAVE;
+    }
+#undef GSYNC_OR_LEAVE
+}
+
 // The autotuner times pass 1 between steps: the instances that would step
 // are marked stepping, and put back at rest afterwards (the face-cascade
 // flag pass 1 raised is cleared too; every stage starts from stage_init).
@@ -1784,6 +1910,22 @@ void l_rk_combine2(const Batch& B, cudaStream_t s) { TILE_LAUNCH(k_rk_combine2, 
 void l_rk_final(const Batch& B, cudaStream_t s) { TILE_LAUNCH(k_rk_final, B, s); }
 void l_cons2prim_all(const Batch& B, cudaStream_t s) { TILE_LAUNCH(k_cons2prim_all, B, s); }
 void l_tune_mark(const Batch& B, int on, cudaStream_t s) { k_tune_mark<<<1, 128, 0, s>>>(B, on); }
+// every block resident at once: a cooperative launch of as many blocks as
+// fit on the GPU (never more, or a barrier could not complete)
+void l_mood_rest(const Batch& B, int uin, int uout, cudaStream_t s) {
+    const int grid = resident_blocks((const void*)k_mood_rest);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = kTile;
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, k_mood_rest, B, uin, uout);
+}
 void l_launch_info(int R, int maxTiles, int* pass1, int* tile_grid_max) {
     *pass1 = R == 1 ? pass1_grid<1, false, false, 2>(maxTiles)
                     : R == 2 ? pass1_grid<2, false, false, 2>(maxTiles) : pass1_grid<3, false, false, 2>(maxTiles);
@@ -1811,7 +1953,7 @@ const KernelSet kset = {
     l_cfl_reduce, l_step_prepare, l_step_begin, l_step_end, l_stage_init, l_face_pass1, l_cascade_cond, l_cascade_lower,
     l_recon_check, l_ct_update_detect, l_mood_flags, l_pass_end, l_recon_list,
     l_compact_post, l_compact_dirty, l_flux_list, l_ct_list, l_clear_low, l_bc_fill, l_rk_combine2, l_rk_final,
-    l_cons2prim_all, l_tune_mark, l_launch_info, &mops};
+    l_cons2prim_all, l_tune_mark, l_mood_rest, l_launch_info, &mops};
 
 }  // namespace KNS
 

@@ -288,13 +288,16 @@ int hosono_gpu_stream(hosono_handle* h, void** stream);
 #define HOSONO_STAGE_TMA 1       /* ... by one TMA tensor copy (cp.async.bulk.tensor) per box */
 #define HOSONO_SCHED_STATIC 0    /* pass-1 blocks walk the tile list grid-stride */
 #define HOSONO_SCHED_DYNAMIC 1   /* ... take their next tile from a launch-wide counter */
+#define HOSONO_LATER_KERNELS 0     /* later MOOD passes: a chain of kernels per pass (graph nodes) */
+#define HOSONO_LATER_PERSISTENT 1  /* ... all of a stage's later passes in one persistent launch */
 typedef struct hosono_tuning {
     int pass1_staging;        /* HOSONO_STAGE_* */
     int pass1_schedule;       /* HOSONO_SCHED_* */
     int pass1_blocks_per_sm;  /* resident pass-1 blocks per SM the register budget aims at: 2 (0 = 2;
                                  128 registers, two stencil boxes per block), 3 or 4 (80 / 64 registers,
                                  one box; cp.async staging only) */
-    int pad[5];               /* zero */
+    int later_passes;         /* HOSONO_LATER_*; the autotuner keeps the caller's choice */
+    int pad[4];               /* zero */
 } hosono_tuning;
 int hosono_gpu_set_tuning(hosono_handle* h, const hosono_tuning* t);
 int hosono_gpu_get_tuning(hosono_handle* h, hosono_tuning* t);
