@@ -168,6 +168,7 @@ SIGNATURES = {
     "hosono_gpu_bc_mood": [_vp],
     "hosono_gpu_mood_pass_stats": [_vp, _ip, ctypes.POINTER(ctypes.c_longlong)],
     "hosono_gpu_riemann": [_vp, _i, _vp, _vp, _i, _vp],
+    "hosono_gpu_eigenvecs": [_vp, _i, _vp, _i, _i, _vp, _vp],
     "hosono_gpu_state_layout": [_vp, ctypes.POINTER(_vp), _ip, ctypes.POINTER(ctypes.c_longlong)],
     "hosono_gpu_build_info": [_ip, _ip],
     "hosono_gpu_set_device": [_i],
@@ -593,6 +594,12 @@ class Solver:
         self._check(self.lib.hosono_gpu_autotune(self.h, int(trials), 1 if force else 0, ctypes.byref(r)),
                     "autotune")
         return r.as_dict()
+
+    def eigenvecs(self, n, V_dev, direction, cons, L_dev, R_dev):
+        """eigen_vecsFromPrim on n primitive states of a device array (10, n)."""
+        self._check(self.lib.hosono_gpu_eigenvecs(self.h, int(n), ctypes.c_void_p(V_dev), int(direction),
+                                                  1 if cons else 0, ctypes.c_void_p(L_dev), ctypes.c_void_p(R_dev)),
+                    "eigenvecs")
 
     def launch_info(self):
         """Launch geometry: tiles, SMs, pass-1 grid, largest other tile-kernel grid."""

@@ -547,6 +547,7 @@ int Engine::add(const hosono_params& p, const double* pv, const double* qw, int*
     sl.dev.phys.gamma = p.gamma;
     sl.dev.phys.small_pressure = p.small_pressure;
     sl.dev.phys.small_density = p.small_density;
+    sl.dev.phys.small_b = p.small_b;
     sl.dev.phys.force_hydro = p.force_hydro ? 1 : 0;
     sl.dev.cfl = p.cfl;
     const size_t plane = (size_t)G.plane;
@@ -1233,6 +1234,17 @@ int Engine::mod_bc_mood(int slot) {
     CUE(cudaMemcpyAsync(d.scheme[st.schemeSel], M.tSch, plane, cudaMemcpyDeviceToDevice, s_));
     CUE(cudaMemcpyAsync(d.rec, M.tRec, plane, cudaMemcpyDeviceToDevice, s_));
     CUE(cudaMemcpyAsync(d.recF, M.tRecF, plane, cudaMemcpyDeviceToDevice, s_));
+    CUE(cudaStreamSynchronize(s_));
+    return HOSONO_OK;
+}
+
+int Engine::eigenvecs(int slot, int n, const double* V, int dir, int cons, double* L, double* R) {
+    if (slot < 0 || slot >= maxInst_ || !slots_[slot].live) return fail(HOSONO_EINVAL, "bad slot %d", slot);
+    if (n < 0 || (dir != XDIR && dir != YDIR) || (n > 0 && (!V || !L || !R)))
+        return fail(HOSONO_EINVAL, "eigenvecs: bad arguments");
+    K_->mod->eigen(slots_[slot].dev.phys, n, V, dir, cons, L, R, s_);
+    launches++;
+    CUE(cudaGetLastError());
     CUE(cudaStreamSynchronize(s_));
     return HOSONO_OK;
 }

@@ -186,6 +186,7 @@ struct ModuleOps {
     void (*bc_mood)(const Batch&, int slot, const Geo&, const ModBuf&, cudaStream_t);
     void (*bc)(const Batch&, int slot, const Geo&, double* A, int nv, cudaStream_t);
     void (*riemann)(const Phys&, int n, const double* uL, const double* uR, int dir, double* F, cudaStream_t);
+    void (*eigen)(const Phys&, int n, const double* V, int dir, int cons, double* L, double* R, cudaStream_t);
 };
 
 // Launchers of one arithmetic build (kernels.cu compiled strict or fast).

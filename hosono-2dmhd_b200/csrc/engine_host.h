@@ -78,6 +78,7 @@ class Engine {
     int mod_bc(int slot, int which);
     int mod_bc_mood(int slot);
     int riemann(int slot, int n, const double* uL, const double* uR, int dir, double* F);
+    int eigenvecs(int slot, int n, const double* V, int dir, int cons, double* L, double* R);
 
     // launch geometry of the kernels for radius R over this engine's tile capacity
     void launch_info(int R, int* pass1_grid, int* tile_grid_max) const { K_->launch_info(R, maxTiles_, pass1_grid, tile_grid_max); }

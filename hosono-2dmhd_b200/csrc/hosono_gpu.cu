@@ -227,6 +227,11 @@ int hosono_gpu_riemann(hosono_handle* h, int n, const double* uL_dev, const doub
     return h ? h->eng.riemann(h->slot, n, uL_dev, uR_dev, dir, flux_dev) : HOSONO_EINVAL;
 }
 
+int hosono_gpu_eigenvecs(hosono_handle* h, int n, const double* V_dev, int dir, int cons, double* L_dev,
+                         double* R_dev) {
+    return h ? h->eng.eigenvecs(h->slot, n, V_dev, dir, cons, L_dev, R_dev) : HOSONO_EINVAL;
+}
+
 int hosono_gpu_state_layout(hosono_handle* h, double** U_dev, int* pitch, long long* plane) {
     if (!h) return HOSONO_EINVAL;
     InstState st;

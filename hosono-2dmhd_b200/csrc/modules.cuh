@@ -356,6 +356,21 @@ __global__ void __launch_bounds__(256) k_mod_riemann(Phys P, int n, const double
     }
 }
 
+// eigen_vecsFromPrim (eigen.f90:20-255) on n primitive states: V is (10, n),
+// L and R are (8, 8, n), each 8x8 column-major with one wave per column
+__global__ void __launch_bounds__(128) k_mod_eigen(Phys P, int n, const double* __restrict__ V, int dir, int cons,
+                                                   double* __restrict__ L, double* __restrict__ R) {
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+        double v[NPRIM], l[NCONS * NCONS], r[NCONS * NCONS];
+        for (int k = 0; k < NPRIM; k++) v[k] = V[NPRIM * e + k];
+        eigen_vecs(P, v, dir, cons != 0, l, r);
+        for (int k = 0; k < NCONS * NCONS; k++) {
+            L[NCONS * NCONS * e + k] = l[k];
+            R[NCONS * NCONS * e + k] = r[k];
+        }
+    }
+}
+
 dim3 mod_grid(const Geo& G) { return dim3((unsigned)((G.nxt + TILE_X - 1) / TILE_X), (unsigned)((G.nyt + TILE_Y - 1) / TILE_Y)); }
 void m_recon(const Batch& B, int slot, const Geo& G, const ModBuf& M, cudaStream_t s) {
     k_mod_recon<<<mod_grid(G), kTile, 0, s>>>(B, slot, M);
@@ -390,5 +405,11 @@ void m_riemann(const Phys& P, int n, const double* uL, const double* uR, int dir
     k_mod_riemann<<<blocks, 256, 0, s>>>(P, n, uL, uR, dir, F);
 }
 
-const ModuleOps mops = {m_recon,  m_recon_lower, m_getfluxes, m_flicd,   m_update,
-                        m_detect, m_detect_lower, m_bc_mood,  m_bc,      m_riemann};
+void m_eigen(const Phys& P, int n, const double* V, int dir, int cons, double* L, double* R, cudaStream_t s) {
+    if (n <= 0) return;
+    const int blocks = (n + 127) / 128 < 4096 ? (n + 127) / 128 : 4096;
+    k_mod_eigen<<<blocks, 128, 0, s>>>(P, n, V, dir, cons, L, R);
+}
+
+const ModuleOps mops = {m_recon,  m_recon_lower,  m_getfluxes, m_flicd, m_update, m_detect,
+                        m_detect_lower, m_bc_mood, m_bc, m_riemann, m_eigen};

@@ -22,6 +22,7 @@ struct Phys {
     double gamma;
     double small_pressure;
     double small_density;
+    double small_b;  // sim_smallB (eigen_beta_T only)
     int force_hydro;
 };
 
@@ -337,6 +338,200 @@ __device__ __forceinline__ void hllc(const Phys& s, const double* uL, const doub
     SharedRecipDiv dv;
     hllc_t<FH>(s, uL, uR, dir, flux, dv);
     if (!dv.ok) hllc_ieee<FH>(s, uL, uR, dir, flux);
+}
+
+
+// ----------------------------------------------------------------------
+// eigen_vecsFromPrim (src/eigen.f90:20-255) with eigen_alpha_fs (:323-349)
+// and eigen_beta_T (:351-371): the left and right eigenvectors of the 7 MHD
+// waves, in primitive or (cons) conserved variables.  Not on the time-step
+// path (no .par option of the reference uses it); exposed by
+// hosono_gpu_eigenvecs.  Statement order of the reference; MATMUL as sums
+// over k ascending from zero.
+// alpha_f for pm = +1, alpha_s for pm = -1
+__device__ __forceinline__ double eigen_alpha_fs(double c_f, double c_s, double a, double BB, double B_N, double pm) {
+    double BB_T = BB - B_N * B_N;
+    (void)BB_T;  // computed by the reference, unused
+    double cf2_minus_cs2 = c_f * c_f - c_s * c_s;
+    double alpha;
+    if (cf2_minus_cs2 > 1.0e-14) {
+        alpha = 0.5 * (cf2_minus_cs2) + pm * (a * a - 0.5 * (c_f * c_f + c_s * c_s));
+        alpha = alpha / (cf2_minus_cs2);
+    } else if (pm > 0) {
+        alpha = 1.0;
+    } else {
+        alpha = 0.0;
+    }
+    alpha = fmin(1.0, fmax(0.0, alpha));
+    return sqrt(alpha);
+}
+// src/eigen.f90:351-371
+__device__ __forceinline__ double eigen_beta_T(double B_T1, double B_T2, double smallB) {
+    double BB_T = B_T1 * B_T1 + B_T2 * B_T2;
+    if (BB_T < smallB * smallB) return copysign(1.0, B_T1) / sqrt(2.0);
+    return B_T1 / sqrt(fmax(BB_T, 1.0e-30));
+}
+// src/eigen.f90:20-255: right eigenvectors (columns of R) and left
+// eigenvectors (columns of L) of the 7 MHD waves in direction dir, 8x8
+// column-major with the variable index as the row; cons: converted to
+// conserved variables by dU/dV and dV/dU (MATMUL as k-ascending sums from 0)
+__device__ inline void eigen_vecs(const Phys& s, const double* V, int dir, bool cons, double* Lm, double* Rm) {
+    const int vN = dir == XDIR ? VELX : VELY, vT1 = dir == XDIR ? VELY : VELX, vT2 = VELZ;
+    const int bN = dir == XDIR ? MAGX : MAGY, bT1 = dir == XDIR ? MAGY : MAGX, bT2 = MAGZ;
+#define R(r, c) Rm[(r) + NCONS * ((c) - 1)]
+#define L(r, c) Lm[(r) + NCONS * ((c) - 1)]
+    const double rho = fmax(V[DENS], s.small_density);
+    const double velN = V[vN], velT1 = V[vT1], velT2 = V[vT2];
+    const double B_N = V[bN], B_T1 = V[bT1], B_T2 = V[bT2];
+    const double p = fmax(V[PRES], s.small_pressure);
+    const double gam = V[GAMM];
+    const double BB = B_N * B_N + B_T1 * B_T1 + B_T2 * B_T2;
+    const double c_f = c_fs(gam, rho, p, BB, B_N, +1.0);
+    const double c_s = c_fs(gam, rho, p, BB, B_N, -1.0);
+    const double a = sqrt(gam * p / rho);
+    const double alpha_f = eigen_alpha_fs(c_f, c_s, a, BB, B_N, +1.0);
+    const double alpha_s = eigen_alpha_fs(c_f, c_s, a, BB, B_N, -1.0);
+    const double beta_T1 = eigen_beta_T(B_T1, B_T2, s.small_b);
+    const double beta_T2 = eigen_beta_T(B_T2, B_T1, s.small_b);
+    const double sgnBn = copysign(1.0, B_N);
+    const double sr = sqrt(rho);
+    for (int k = 0; k < NCONS * NCONS; k++) Rm[k] = Lm[k] = 0.0;
+    R(DENS, 1) = alpha_f * rho;
+    R(vN, 1) = -alpha_f * c_f;
+    R(vT1, 1) = alpha_s * c_s * beta_T1 * sgnBn;
+    R(vT2, 1) = alpha_s * c_s * beta_T2 * sgnBn;
+    R(bT1, 1) = alpha_s * sr * a * beta_T1;
+    R(bT2, 1) = alpha_s * sr * a * beta_T2;
+    R(PRES, 1) = alpha_f * rho * (a * a);
+    R(vT1, 2) = -beta_T2;
+    R(vT2, 2) = beta_T1;
+    R(bT1, 2) = -sr * beta_T2 * sgnBn;
+    R(bT2, 2) = sr * beta_T1 * sgnBn;
+    R(DENS, 3) = alpha_s * rho;
+    R(vN, 3) = -alpha_s * c_s;
+    R(vT1, 3) = -alpha_f * c_f * beta_T1 * sgnBn;
+    R(vT2, 3) = -alpha_f * c_f * beta_T2 * sgnBn;
+    R(bT1, 3) = -alpha_f * sr * a * beta_T1;
+    R(bT2, 3) = -alpha_f * sr * a * beta_T2;
+    R(PRES, 3) = alpha_s * rho * (a * a);
+    R(DENS, 4) = 1.0;
+    R(DENS, 5) = alpha_s * rho;
+    R(vN, 5) = alpha_s * c_s;
+    R(vT1, 5) = alpha_f * c_f * beta_T1 * sgnBn;
+    R(vT2, 5) = alpha_f * c_f * beta_T2 * sgnBn;
+    R(bT1, 5) = -alpha_f * sr * a * beta_T1;
+    R(bT2, 5) = -alpha_f * sr * a * beta_T2;
+    R(PRES, 5) = alpha_s * rho * (a * a);
+    R(vT1, 6) = beta_T2;
+    R(vT2, 6) = -beta_T1;
+    R(bT1, 6) = -sr * beta_T2 * sgnBn;
+    R(bT2, 6) = sr * beta_T1 * sgnBn;
+    R(DENS, 7) = alpha_f * rho;
+    R(vN, 7) = alpha_f * c_f;
+    R(vT1, 7) = -alpha_s * c_s * beta_T1 * sgnBn;
+    R(vT2, 7) = -alpha_s * c_s * beta_T2 * sgnBn;
+    R(bT1, 7) = alpha_s * sr * a * beta_T1;
+    R(bT2, 7) = alpha_s * sr * a * beta_T2;
+    R(PRES, 7) = alpha_f * rho * (a * a);
+    const double h = 1 / (2 * (a * a));
+    L(vN, 1) = h * (-alpha_f * c_f);
+    L(vT1, 1) = h * (alpha_s * c_s * beta_T1 * sgnBn);
+    L(vT2, 1) = h * (alpha_s * c_s * beta_T2 * sgnBn);
+    L(bT1, 1) = h * (alpha_s * a * beta_T1 / sr);
+    L(bT2, 1) = h * (alpha_s * a * beta_T2 / sr);
+    L(PRES, 1) = h * (alpha_f / rho);
+    L(vT1, 2) = 0.5 * (-beta_T2);
+    L(vT2, 2) = 0.5 * (beta_T1);
+    L(bT1, 2) = 0.5 * (-beta_T2 * sgnBn / sr);
+    L(bT2, 2) = 0.5 * (beta_T1 * sgnBn / sr);
+    L(vN, 3) = h * (-alpha_s * c_s);
+    L(vT1, 3) = h * (-alpha_f * c_f * beta_T1 * sgnBn);
+    L(vT2, 3) = h * (-alpha_f * c_f * beta_T2 * sgnBn);
+    L(bT1, 3) = h * (-alpha_f * a * beta_T1 / sr);
+    L(bT2, 3) = h * (-alpha_f * a * beta_T2 / sr);
+    L(PRES, 3) = h * (alpha_s / rho);
+    L(DENS, 4) = 1.0;
+    L(PRES, 4) = -1 / (a * a);
+    L(vN, 5) = h * (alpha_s * c_s);
+    L(vT1, 5) = h * (alpha_f * c_f * beta_T1 * sgnBn);
+    L(vT2, 5) = h * (alpha_f * c_f * beta_T2 * sgnBn);
+    L(bT1, 5) = h * (-alpha_f * a * beta_T1 / sr);
+    L(bT2, 5) = h * (-alpha_f * a * beta_T2 / sr);
+    L(PRES, 5) = h * (alpha_s / rho);
+    L(vT1, 6) = 0.5 * (beta_T2);
+    L(vT2, 6) = 0.5 * (-beta_T1);
+    L(bT1, 6) = 0.5 * (-beta_T2 * sgnBn / sr);
+    L(bT2, 6) = 0.5 * (beta_T1 * sgnBn / sr);
+    L(vN, 7) = h * (alpha_f * c_f);
+    L(vT1, 7) = h * (-alpha_s * c_s * beta_T1 * sgnBn);
+    L(vT2, 7) = h * (-alpha_s * c_s * beta_T2 * sgnBn);
+    L(bT1, 7) = h * (alpha_s * a * beta_T1 / sr);
+    L(bT2, 7) = h * (alpha_s * a * beta_T2 / sr);
+    L(PRES, 7) = h * (alpha_f / rho);
+    if (!cons) {
+#undef R
+#undef L
+        return;
+    }
+#undef R
+#undef L
+    const double k = 1.0 - gam;
+    double dUdV[NCONS * NCONS] = {}, dVdU[NCONS * NCONS] = {};
+#define A(r, c) dUdV[(r) + NCONS * (c)]
+#define Bm(r, c) dVdU[(r) + NCONS * (c)]
+    A(DENS, DENS) = 1.0;
+    A(VELX, DENS) = V[VELX];
+    A(VELY, DENS) = V[VELY];
+    A(VELZ, DENS) = V[VELZ];
+    A(PRES, DENS) = 0.5 * (velN * velN + velT1 * velT1 + velT2 * velT2);
+    A(VELX, VELX) = rho;
+    A(PRES, VELX) = rho * V[VELX];
+    A(VELY, VELY) = rho;
+    A(PRES, VELY) = rho * V[VELY];
+    A(VELZ, VELZ) = rho;
+    A(PRES, VELZ) = rho * V[VELZ];
+    A(MAGX, MAGX) = 1.0;
+    A(PRES, MAGX) = V[MAGX];
+    A(MAGY, MAGY) = 1.0;
+    A(PRES, MAGY) = V[MAGY];
+    A(MAGZ, MAGZ) = 1.0;
+    A(PRES, MAGZ) = V[MAGZ];
+    A(PRES, PRES) = -1 / k;
+    Bm(DENS, DENS) = 1.0;
+    Bm(VELX, DENS) = -V[VELX] / rho;
+    Bm(VELY, DENS) = -V[VELY] / rho;
+    Bm(VELZ, DENS) = -V[VELZ] / rho;
+    Bm(PRES, DENS) = -k * A(PRES, DENS);
+    Bm(VELX, VELX) = 1 / rho;
+    Bm(PRES, VELX) = k * V[VELX];
+    Bm(VELY, VELY) = 1 / rho;
+    Bm(PRES, VELY) = k * V[VELY];
+    Bm(VELZ, VELZ) = 1 / rho;
+    Bm(PRES, VELZ) = k * V[VELZ];
+    Bm(MAGX, MAGX) = 1.0;
+    Bm(PRES, MAGX) = k * V[MAGX];
+    Bm(MAGY, MAGY) = 1.0;
+    Bm(PRES, MAGY) = k * V[MAGY];
+    Bm(MAGZ, MAGZ) = 1.0;
+    Bm(PRES, MAGZ) = k * V[MAGZ];
+    Bm(PRES, PRES) = -k;
+    double Rc[NCONS * NCONS], Lc[NCONS * NCONS];
+    for (int j = 0; j < NCONS; j++)
+        for (int i = 0; i < NCONS; i++) {
+            double r = 0.0, l = 0.0;
+            for (int q = 0; q < NCONS; q++) {
+                r = r + A(i, q) * Rm[q + NCONS * j];
+                l = l + Bm(q, i) * Lm[q + NCONS * j];
+            }
+            Rc[i + NCONS * j] = r;
+            Lc[i + NCONS * j] = l;
+        }
+#undef A
+#undef Bm
+    for (int q = 0; q < NCONS * NCONS; q++) {
+        Rm[q] = Rc[q];
+        Lm[q] = Lc[q];
+    }
 }
 
 // src/detect.f90:250-265 (CAD) and :238-248 (PAD): both finite (not NaN,

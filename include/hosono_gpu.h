@@ -264,6 +264,15 @@ int hosono_gpu_mood_pass_stats(hosono_handle* h, int* npasses, long long* ntroub
  * variables of a face together), direction 0 (x) or 1 (y), with the
  * handle's gamma, floors and sim_forceHydro; returns when flux is written */
 int hosono_gpu_riemann(hosono_handle* h, int n, const double* uL_dev, const double* uR_dev, int dir, double* flux_dev);
+/* eigen_vecsFromPrim (src/eigen.f90:20-255) on n primitive states of a
+ * caller-owned device array V (10, n), direction 0 (x) or 1 (y): the left
+ * and right eigenvectors of the 7 MHD waves into L and R, each (8, 8, n),
+ * column w (1..7) = wave w, column 8 zero, in primitive variables
+ * (cons = 0, 'prim') or conserved ones (cons = 1, 'cons'); the handle's
+ * gamma floors and sim_smallB.  No .par option of the reference reaches this
+ * routine (it is not on the time-step path). */
+int hosono_gpu_eigenvecs(hosono_handle* h, int n, const double* V_dev, int dir, int cons, double* L_dev,
+                         double* R_dev);
 
 /* Device-resident access for callers that manage their own buffers
  * (benchmarks, batching): device pointer of the first U plane; planes are

@@ -100,6 +100,8 @@ FC_MIXED(!=)
 namespace std {
 inline fc::CD sqrt(fc::CD x) { fc::g_counts.sqrt++; return fc::CD(::sqrt(x.v)); }
 inline fc::CD fabs(fc::CD x) { fc::g_counts.other++; return fc::CD(::fabs(x.v)); }
+inline fc::CD copysign(fc::CD a, fc::CD b) { fc::g_counts.other++; return fc::CD(::copysign(a.v, b.v)); }
+inline fc::CD copysign(double a, fc::CD b) { return std::copysign(fc::CD(a), b); }
 inline fc::CD abs(fc::CD x) { fc::g_counts.other++; return fc::CD(::fabs(x.v)); }
 inline fc::CD sin(fc::CD x) { fc::g_counts.other++; return fc::CD(::sin(x.v)); }
 inline fc::CD fmax(fc::CD a, fc::CD b) { fc::g_counts.cmp++; return fc::CD(::fmax(a.v, b.v)); }

@@ -94,6 +94,11 @@ double orc_cons2pres(const orc_handle* h, const double* U);
 void orc_cons2flux(const orc_handle* h, const double* U, int dir, double* F);
 void orc_hllc(const orc_handle* h, const double* uL, const double* uR, int dir, double* F);
 double orc_c_fs(double gam, double rho, double p, double BB, double BN, double pm);
+/* eigen_vecsFromPrim (eigen.f90:20-255): left (L) and right (R) eigenvectors
+ * of the 7 MHD waves of the primitive state V(10) in direction dir (0 x, 1 y),
+ * each 8x8 column-major (column = wave 1..7, column 8 zero); cons != 0: in
+ * conserved variables ('cons'), else primitive ('prim'). */
+void orc_eigenvecs(const orc_handle* h, const double* V, int dir, int cons, double* L, double* R);
 
 /* Standalone GP set-up (GP.f90:37-200) for given par strings.
  * Real values are passed as decimal strings and parsed in quad precision,

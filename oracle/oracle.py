@@ -59,6 +59,7 @@ def _lib(fast=False, count=False):
     lib.orc_cons2pres.argtypes = [p, dp]
     lib.orc_cons2flux.argtypes = [p, dp, i, dp]
     lib.orc_hllc.argtypes = [p, dp, dp, i, dp]
+    lib.orc_eigenvecs.argtypes = [p, dp, i, i, dp, dp]
     lib.orc_c_fs.restype = d
     lib.orc_c_fs.argtypes = [d, d, d, d, d, d]
     lib.orc_gp_build.argtypes = [i, ctypes.c_char_p, ctypes.c_char_p, i, ctypes.c_char_p, ctypes.c_char_p, i,
@@ -303,6 +304,14 @@ class Oracle:
         f = np.zeros(8)
         self.lib.orc_cons2flux(self.h, _dp(u), int(direction), _dp(f))
         return f
+
+    def eigenvecs(self, V, direction, cons=False):
+        """eigen_vecsFromPrim: (L, R) as 8x8 arrays [row=variable, col=wave]."""
+        V = np.ascontiguousarray(V, dtype=np.float64)
+        L = np.zeros(64)
+        R = np.zeros(64)
+        self.lib.orc_eigenvecs(self.h, _dp(V), int(direction), 1 if cons else 0, _dp(L), _dp(R))
+        return L.reshape(8, 8).T, R.reshape(8, 8).T
 
     def hllc(self, uL, uR, direction):
         uL = np.ascontiguousarray(uL, dtype=np.float64)

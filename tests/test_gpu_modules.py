@@ -197,3 +197,31 @@ def test_mood_pass_stats(tmp_par_dir):
     assert ntroubled == sum(t["n_inner"] + t["n_detect"] for t in tr)
     s.close()
     o.close()
+
+
+@pytest.mark.gpu
+def test_eigenvectors_match_oracle(tmp_par_dir):
+    """eigen_vecsFromPrim through hosono_gpu_eigenvecs on random primitive
+    states (some with no tangential field), x and y, primitive and
+    conserved forms: the oracle's bits."""
+    import torch
+    from test_oracle_invariants import _random_prims
+
+    m, o, s = _fresh(tmp_par_dir, "eig", parfiles.orszag_tang(8, 1))
+    rng = np.random.default_rng(7)
+    n = 2048
+    V = _random_prims(rng, n)
+    dV = torch.from_numpy(V).cuda()
+    for direction in (0, 1):
+        for cons in (False, True):
+            L = torch.zeros((n, 8, 8), dtype=torch.float64, device="cuda")
+            R = torch.zeros_like(L)
+            torch.cuda.synchronize()
+            s.eigenvecs(n, dV.data_ptr(), direction, cons, L.data_ptr(), R.data_ptr())
+            Lg, Rg = L.cpu().numpy(), R.cpu().numpy()
+            for k in range(0, n, 7):
+                Lo, Ro = o.eigenvecs(V[k], direction, cons=cons)
+                np.testing.assert_array_equal(Lg[k].T, Lo)
+                np.testing.assert_array_equal(Rg[k].T, Ro)
+    s.close()
+    o.close()

@@ -130,3 +130,29 @@ def test_flicd_keeps_central_div_b(case, tmp_par_dir):
     if case == "blast":
         g = o.ngc
         assert o.scheme()[g:-g, g:-g].min() == 0  # MOOD lowered cells to first order
+
+
+def _random_prims(rng, n):
+    V = np.zeros((n, 10))
+    V[:, 0] = rng.uniform(0.1, 3.0, n)
+    V[:, 1:4] = rng.normal(size=(n, 3))
+    V[:, 4] = rng.uniform(0.05, 3.0, n)
+    V[:, 5:8] = rng.normal(size=(n, 3)) * rng.choice([0.0, 1e-3, 1.0, 5.0], size=(n, 1))
+    V[::7, 6:8] = 0.0  # no tangential field: the beta_T guard (eigen.f90:364-368)
+    V[:, 9] = 5.0 / 3.0
+    return V
+
+
+def test_eigenvectors_are_biorthonormal(tmp_par_dir):
+    """eigen_vecsFromPrim (eigen.f90:20-255): the left eigenvectors (columns
+    of L) and the right ones (columns of R) of the 7 waves satisfy
+    L^T R = I, in primitive and in conserved variables (dV/dU dU/dV = I),
+    also where the field or its tangential part vanishes."""
+    o = oracle.Oracle(parfiles.make(tmp_par_dir, "eig", parfiles.orszag_tang(8, 1)))
+    rng = np.random.default_rng(1)
+    for V in _random_prims(rng, 400):
+        for d in (0, 1):
+            for cons in (False, True):
+                L, R = o.eigenvecs(V, d, cons=cons)
+                np.testing.assert_allclose(L[:, :7].T @ R[:, :7], np.eye(7), rtol=0, atol=1e-12)
+                assert not L[:, 7].any() and not R[:, 7].any()
