@@ -279,7 +279,13 @@ def bench_ours(args, rank, world, local):
         sol.set_graphs(False)
     sol.upload(U0, V0)
     sol.set_time(0.0, run.tmax, 0, run.nstepmax)
-    tune = sol.autotune(trials=5, force=True) if not args.no_tune else None
+    tune = None
+    if args.tuning:  # a fixed launch choice (staging,schedule,blocks per SM), e.g. for a profiler
+        st_, sc_, bl_ = (int(x) for x in args.tuning.split(","))
+        sol.set_tuning(pass1_staging=st_, pass1_schedule=sc_, pass1_blocks_per_sm=bl_)
+        tune = {"fixed": sol.tuning()}
+    elif not args.no_tune:
+        tune = sol.autotune(trials=5, force=True)
     stream = torch.cuda.ExternalStream(sol.stream())
     zones = w["n"] * w["n"]
 
@@ -535,7 +541,7 @@ def bench_batched(m, fp, torch, manifest="blast64_seed0.json", limit=None, eager
 
 
 def bench_served(m, fp, requests, check, calibrate=0, sample=0, hashes_path=None, mean_work=None,
-                 records_path=None):
+                 records_path=None, policies=None):
     """The served request stream (workloads/served2000_seed1.json, first
     `requests` requests) under both scheduling policies.  Capacity: the
     stream's first `calibrate` requests (all of them when 0) run closed loop
@@ -555,6 +561,8 @@ def bench_served(m, fp, requests, check, calibrate=0, sample=0, hashes_path=None
     import numpy as np
     load_pkg()
     srv = importlib.import_module("hosono_2dmhd_b200.serve")
+    if policies is None:
+        policies = [("fifo", srv.SERVE_FIFO, {}), ("shortest", srv.SERVE_SHORTEST, SHORTEST_DEFAULTS)]
     path = os.path.join(ROOT, "hosono-2dmhd_b200", "workloads", "served2000_seed1.json")
     with open(path) as f:
         entries = json.load(f)["requests"][:requests]
@@ -592,20 +600,21 @@ def bench_served(m, fp, requests, check, calibrate=0, sample=0, hashes_path=None
            "unit": "zone-updates/s", "mean_work_used": mean_work}
     keys = ("zone_updates", "zone_updates_per_s", "makespan_s", "latency_p50_s", "latency_p99_s", "latency_max_s",
             "queue_wait_p50_s", "queue_wait_p99_s", "submit_lag_max_s", "peak_resident", "peak_bytes",
-            "budget_bytes", "gpu_busy_frac", "completed", "failed")
+            "budget_bytes", "gpu_busy_frac", "completed", "failed", "failed_status")
     kept_by = {}
-    for name, pol in (("fifo", srv.SERVE_FIFO), ("shortest", srv.SERVE_SHORTEST)):
-        with srv.Server(fp_mode=fp, policy=pol) as s:
+    for name, pol, kw in policies:
+        with srv.Server(fp_mode=fp, policy=pol, **kw) as s:
             rep, kept, infos = srv.run_stream(entries, rate, s, keep=keep + sampled, fp_mode=fp)
         out[name] = {k_: rep[k_] for k_ in keys}
+        out[name]["server"] = dict(policy=name, **kw)
         out[name]["mean_work_measured"] = rep["zone_updates"] / max(rep["completed"], 1)
         kept_by[name] = kept
         if name == "fifo":
             for k_ in keys:  # the default policy's figures at the top level
                 out[k_] = rep[k_]
             fifo_infos = infos
-    out["policies_identical"] = all(np.array_equal(kept_by["fifo"][i], kept_by["shortest"][i])
-                                    for i in keep + sampled)
+    out["policies_identical"] = all(np.array_equal(kept_by["fifo"][i], kept_by[n][i])
+                                    for n, _, _ in policies for i in keep + sampled)
     if records_path:
         with open(records_path, "w") as f:
             json.dump([{k_: i[k_] for k_ in ("entry", "status", "nstep", "zone_updates", "submit_s", "admit_s",
@@ -622,6 +631,10 @@ def bench_served(m, fp, requests, check, calibrate=0, sample=0, hashes_path=None
                        "requests": recs}, f, indent=1)
         out["sampled_hashes"] = {"file": os.path.basename(hashes_path), "requests": sampled}
     return out, {e["id"]: (e, kept_by["fifo"][e["id"]]) for e in entries if e["id"] in keep}
+
+
+# the shortest-first server's settings the bench runs
+SHORTEST_DEFAULTS = {}
 
 
 def cpu_baseline_served_check(kept):
@@ -660,6 +673,8 @@ def main():
     ap.add_argument("--fp", default="strict", choices=["strict", "fast"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="keep the default launch choices (no autotuning)")
+    ap.add_argument("--tuning", default=None,
+                    help="fixed pass-1 launch choice 'staging,schedule,blocks_per_sm' instead of autotuning")
     ap.add_argument("--no-batched", action="store_true", help="skip the 64-instance batched-vs-plain measurement")
     ap.add_argument("--no-config0", action="store_true", help="skip the Orszag-Tang 128^2 R=1 to t_end leg")
     ap.add_argument("--eager", action="store_true",

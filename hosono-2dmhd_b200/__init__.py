@@ -229,9 +229,9 @@ RESTYPES = {"hosono_batch_instance_bytes": ctypes.c_longlong, "hosono_serve_cloc
 NOALLOC_MAX_ROWS = 16384  # HOSONO_NOALLOC_MAX_ROWS
 
 
-def mood_cap_default(radius):
-    """HOSONO_MOOD_CAP_DEFAULT(R): MOOD passes per stage before EMOODCAP."""
-    return 16 * (radius + 1)
+def mood_cap_default(radius, nx, ny):
+    """HOSONO_MOOD_CAP_DEFAULT(R, nx, ny): MOOD passes per stage before EMOODCAP."""
+    return (radius + 1) * (nx + ny)
 
 
 def set_device(device):

@@ -601,7 +601,7 @@ int Engine::add(const hosono_params& p, const double* pv, const double* qw, int*
     st.live = 1;
     st.tmax = HUGE_VAL;
     st.nstepmax = INT_MAX;
-    st.passCap = HOSONO_MOOD_CAP_DEFAULT(R);
+    st.passCap = HOSONO_MOOD_CAP_DEFAULT(R, p.nx, p.ny);
     CUE(cudaMemcpyAsync(d_st_ + k, &st, sizeof(InstState), cudaMemcpyHostToDevice, s_));
     CUE(cudaMemsetAsync(d_hold_ + k, 0, sizeof(int), s_));
     sl.live = true;

@@ -181,9 +181,13 @@ int hosono_gpu_set_time(hosono_handle* h, double t, double tmax, int nstep, int 
  * converged would spin for hours.  A stage that reaches `cap` passes without
  * converging stops its instance with HOSONO_EMOODCAP instead (the state
  * stays at the start of that step; other instances of a batch go on).
- * Default HOSONO_MOOD_CAP_DEFAULT(R) passes per stage; cap <= 0 restores the
- * proven bound R*nx*ny + 1.  No counterpart in the reference. */
-#define HOSONO_MOOD_CAP_DEFAULT(R) (16 * ((R) + 1))
+ * Default HOSONO_MOOD_CAP_DEFAULT(R, nx, ny) passes per stage: linear in the
+ * grid's extent (a troubled region spreads by a few cells a pass), where the
+ * proven bound is quadratic; a small multiple of R+1 is not enough (Orszag-
+ * Tang 512^2, R=2, needs more than 48 passes in some stages once its shocks
+ * form).  cap <= 0 restores the proven bound R*nx*ny + 1.  No counterpart in
+ * the reference. */
+#define HOSONO_MOOD_CAP_DEFAULT(R, nx, ny) (((R) + 1) * ((nx) + (ny)))
 int hosono_gpu_set_mood_cap(hosono_handle* h, int cap);
 
 /* Continue the driver's time loop from the current t/nstep: up to max_steps
