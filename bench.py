@@ -470,6 +470,45 @@ def bench_config0(m, fp, torch):
             "mood_passes_per_step": passes / n, "tuning": tune["best"]}
 
 
+def sweep_tuning(args):
+    """--sweep-tuning: every pass-1 launch choice on the workload, whole time
+    steps (CUDA events around --steps steps after --warmup) and the pass-1
+    launches alone, in strict and fast arithmetic; one JSON line per choice."""
+    import torch
+    m = load_pkg()
+    w = WORKLOADS[args.workload]
+    choices = [(st, sc, 2) for st in (0, 1) for sc in (0, 1)] + [(0, 0, 3), (0, 1, 3), (0, 0, 4), (0, 1, 4)]
+    for fp in (m.FP_STRICT, m.FP_FAST):
+        for st, sc, bl in choices:
+            with tempfile.TemporaryDirectory() as d:
+                par = par_for(args.workload, d)
+                params, run = m.par_load(par)
+                params.fp_mode = fp
+                pv, qw, stc = m.par_gp(par, params.max_radius)
+                U0, V0 = m.ic_set(par, params)
+            sol = m.Solver(params, pv, qw, stc)
+            sol.upload(U0, V0)
+            sol.set_time(0.0, run.tmax, 0, run.nstepmax)
+            sol.set_tuning(pass1_staging=st, pass1_schedule=sc, pass1_blocks_per_sm=bl)
+            sol.step(max(args.warmup, 1))
+            stream = torch.cuda.ExternalStream(sol.stream())
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            sol.step(args.steps)
+            e1.record(stream)
+            e1.synchronize()
+            ms = e0.elapsed_time(e1) / args.steps
+            sol.profile(True)
+            sol.profile_read(reset=True)
+            sol.step(3)
+            p1, n1, _ = sol.profile_read(reset=True)
+            sol.close()
+            print(json.dumps({"workload": args.workload, "fp": "fast" if fp else "strict", "pass1_staging": st,
+                              "pass1_schedule": sc, "pass1_blocks_per_sm": bl, "ms_per_step": ms,
+                              "pass1_ms": p1 / max(n1, 1), "zone_updates_per_s": w["n"] ** 2 / (ms / 1e3)}),
+                  flush=True)
+
+
 def load_problems():
     import importlib
     load_pkg()
@@ -673,6 +712,8 @@ def main():
     ap.add_argument("--fp", default="strict", choices=["strict", "fast"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="keep the default launch choices (no autotuning)")
+    ap.add_argument("--sweep-tuning", action="store_true",
+                    help="time every pass-1 launch choice on the workload (whole steps and pass 1) and exit")
     ap.add_argument("--tuning", default=None,
                     help="fixed pass-1 launch choice 'staging,schedule,blocks_per_sm' instead of autotuning")
     ap.add_argument("--no-batched", action="store_true", help="skip the 64-instance batched-vs-plain measurement")
@@ -700,7 +741,9 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    if args.impl == "reference":
+    if args.sweep_tuning:
+        sweep_tuning(args)
+    elif args.impl == "reference":
         bench_reference(args, rank)
     else:
         bench_ours(args, rank, world, local)

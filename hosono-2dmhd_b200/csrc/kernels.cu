@@ -1067,21 +1067,15 @@ __device__ __forceinline__ void detect_prep_tile(const Batch& B, const InstState
 // writes the same value) and read from memory otherwise (nobody writes it).
 // A lowered cell sets `lowered` (cleared again after the flags are rebuilt)
 // and is appended to the lowered list.
-__device__ __forceinline__ bool ct_cell(const InstDev& d, const InstState& S, int uin, int uout, int i, int j,
-                                        long long cc) {
+// the unsplit update of timeStep.f90:107-118 and detect_ALL for one interior
+// cell, given its corrected fluxes and those of its east / north faces
+__device__ __forceinline__ bool update_detect_cell(const InstDev& d, const InstState& S, int uin, int uout,
+                                                   long long cc, double ctx, double cty, double ctx_e,
+                                                   double cty_n) {
     const Geo& G = d.geo;
-    const int g = G.g;
-    if (!d.recF[cc]) return false;
-    const double ctx = flicd_x(d, cc);
-    const double cty = flicd_y(d, cc);
-    d.CTX[cc] = ctx;
-    d.CTY[cc] = cty;
-    if (i >= g + G.nx || j >= g + G.ny) return false;  // FLICD-only row and column
     const double* U = role_ptr(d, S.parity, uin);
     double* Uo = role_ptr(d, S.parity, uout);
     const long long ce = cc + 1, cn = cc + G.pitch;
-    const double ctx_e = d.recF[ce] ? flicd_x(d, ce) : d.CTX[ce];
-    const double cty_n = d.recF[cn] ? flicd_y(d, cn) : d.CTY[cn];
     const double dt = S.dt;
     const double dtdx = dt / G.dx, dtdy = dt / G.dy;
     double un[NCONS];
@@ -1113,18 +1107,72 @@ __device__ __forceinline__ bool ct_cell(const InstDev& d, const InstState& S, in
     return low;
 }
 
-__device__ __forceinline__ void t_ct_update_detect(const Batch& B, int uin, int uout, const Cell c, double* sV) {
+// FLICD on [g, g+n]^2 where recomputeFLICD; then, on the interior, the
+// unsplit update of timeStep.f90:107-118 and detect_ALL.  A corrected flux a
+// neighbour needs is recomputed locally when the neighbour is flagged (it
+// writes the same value) and read from memory otherwise (nobody writes it).
+// A lowered cell sets `lowered` (cleared again after the flags are rebuilt)
+// and is appended to the lowered list.
+__device__ __forceinline__ bool ct_cell(const InstDev& d, const InstState& S, int uin, int uout, int i, int j,
+                                        long long cc) {
+    const Geo& G = d.geo;
+    const int g = G.g;
+    if (!d.recF[cc]) return false;
+    const double ctx = flicd_x(d, cc);
+    const double cty = flicd_y(d, cc);
+    d.CTX[cc] = ctx;
+    d.CTY[cc] = cty;
+    if (i >= g + G.nx || j >= g + G.ny) return false;  // FLICD-only row and column
+    const long long ce = cc + 1, cn = cc + G.pitch;
+    const double ctx_e = d.recF[ce] ? flicd_x(d, ce) : d.CTX[ce];
+    const double cty_n = d.recF[cn] ? flicd_y(d, cn) : d.CTY[cn];
+    return update_detect_cell(d, S, uin, uout, cc, ctx, cty, ctx_e, cty_n);
+}
+
+// The dense pass-1 form: the corrected fluxes of the tile's cells and of its
+// east column and north row are computed once into shared memory (sCT),
+// so a cell reads its east / north neighbours' values from there instead of
+// evaluating FLICD again (where a neighbour is not flagged, its stored value
+// is read, as ct_cell does).
+constexpr int CT_SX = TILE_X + 1, CT_SY = TILE_Y + 1;
+__device__ __forceinline__ void t_ct_update_detect(const Batch& B, int uin, int uout, const Cell c, double* sV,
+                                                   double* sCT) {
     InstState& S = B.st[c.k];
     if (!(S.stepping && S.stageActive)) return;  // uniform over the block
-    detect_prep_tile(B, S, uin, c, sV);
+    detect_prep_tile(B, S, uin, c, sV);  // starts with a barrier: the last tile's reads of sCT are done
     const InstDev& d = B.dev[c.k];
     const Geo& G = d.geo;
     const int g = G.g;
+    const int x0 = c.i - (int)threadIdx.x, y0 = c.j - (int)threadIdx.y;
+    const int tid = threadIdx.y * TILE_X + threadIdx.x;
+    for (int e = tid; e < CT_SX * CT_SY; e += NTHREADS) {
+        const int ly = e / CT_SX, lx = e - ly * CT_SX;
+        const int i = x0 + lx, j = y0 + ly;
+        if (i >= g && j >= g && i <= g + G.nx && j <= g + G.ny) {
+            const long long q = (long long)j * G.pitch + i;
+            if (d.recF[q]) {
+                sCT[e] = flicd_x(d, q);
+                sCT[CT_SX * CT_SY + e] = flicd_y(d, q);
+            }
+        }
+    }
+    __syncthreads();
     bool low = false;
     long long cc = 0;
     if (c.i >= g && c.j >= g && c.i <= g + G.nx && c.j <= g + G.ny) {
         cc = (long long)c.j * G.pitch + c.i;
-        low = ct_cell(d, S, uin, uout, c.i, c.j, cc);
+        if (d.recF[cc]) {
+            const int e = threadIdx.y * CT_SX + threadIdx.x;
+            const double ctx = sCT[e], cty = sCT[CT_SX * CT_SY + e];
+            d.CTX[cc] = ctx;
+            d.CTY[cc] = cty;
+            if (c.i < g + G.nx && c.j < g + G.ny) {
+                const long long ce = cc + 1, cn = cc + G.pitch;
+                const double ctx_e = d.recF[ce] ? sCT[e + 1] : d.CTX[ce];
+                const double cty_n = d.recF[cn] ? sCT[CT_SX * CT_SY + e + CT_SX] : d.CTY[cn];
+                low = update_detect_cell(d, S, uin, uout, cc, ctx, cty, ctx_e, cty_n);
+            }
+        }
     }
     warp_count(&S.nDetect, low);
     warp_append(B.L, LIST_LOW, B.L.low, B.L.cap, low, entry(c.k, cc));
@@ -1135,7 +1183,8 @@ __device__ __forceinline__ void t_ct_update_detect(const Batch& B, int uin, int 
 // 4 blocks 11.23 ms, 5 blocks 11.14 ms, 6 blocks 11.08 ms.
 __global__ void __launch_bounds__(NTHREADS, 6) k_ct_update_detect(Batch B, int uin, int uout) {
     __shared__ double sV[4 * DP_SX * DP_SY];
-    FOR_TILES(B, t) t_ct_update_detect(B, uin, uout, tile_at(B, t), sV);
+    __shared__ double sCT[2 * CT_SX * CT_SY];
+    FOR_TILES(B, t) t_ct_update_detect(B, uin, uout, tile_at(B, t), sV, sCT);
 }
 
 // the same on the recomputeFLICD list of a later MOOD pass
