@@ -790,7 +790,7 @@ __device__ __forceinline__ void d_recon_group(const Batch& B, int uin, int which
         if (act && sub == 0 && bad) atomicOr(&S.anyFail, 1);
     }
 }
-__global__ void __launch_bounds__(256) k_recon_group(Batch B, int uin, int which) {
+__global__ void __launch_bounds__(256, 2) k_recon_group(Batch B, int uin, int which) {
     d_recon_group(B, uin, which, GT1, GS1);
 }
 
@@ -918,7 +918,7 @@ __device__ __forceinline__ void d_flux_list(const Batch& B, int uin, int gt, int
         }
     }
 }
-__global__ void __launch_bounds__(256) k_flux_list(Batch B, int uin) { d_flux_list(B, uin, GT1, GS1); }
+__global__ void __launch_bounds__(256, 2) k_flux_list(Batch B, int uin) { d_flux_list(B, uin, GT1, GS1); }
 
 // ======================================================================
 // FLICDdivB_fluxCorrections (FLICDdivB.f90:13-70) from fluxRaw.

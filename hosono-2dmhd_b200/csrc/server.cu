@@ -508,7 +508,7 @@ int hosono_serve_create(const hosono_serve_config* cfg, hosono_server** out) {
     if (c.max_chunk_steps <= 0) c.max_chunk_steps = 64;
     if (c.fp_mode != HOSONO_FP_STRICT && c.fp_mode != HOSONO_FP_FAST) return HOSONO_EINVAL;
     if (c.policy != HOSONO_SERVE_FIFO && c.policy != HOSONO_SERVE_SHORTEST) return HOSONO_EINVAL;
-    if (!(c.aging_s > 0)) c.aging_s = 20.0;
+    if (!(c.aging_s > 0)) c.aging_s = 5.0;
     if (c.fill_tiles <= 0) {
         int dev = 0, sms = 148;
         if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) !=
@@ -516,7 +516,7 @@ int hosono_serve_create(const hosono_serve_config* cfg, hosono_server** out) {
             cudaGetLastError();
             sms = 148;
         }
-        c.fill_tiles = 8 * sms;
+        c.fill_tiles = 40 * sms;
     }
     hosono_server* S = new (std::nothrow) hosono_server();
     if (!S) return HOSONO_ENOMEM;

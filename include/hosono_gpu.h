@@ -461,8 +461,8 @@ typedef struct hosono_serve_config {
     double chunk_ms;         /* target GPU time of one batched launch; <= 0: 25 ms          */
     int max_chunk_steps;     /* time steps per batched launch at most; <= 0: 64             */
     int policy;              /* HOSONO_SERVE_*                                              */
-    double aging_s;          /* SHORTEST: wait after which a solve goes first; <= 0: 20 s    */
-    int fill_tiles;          /* SHORTEST: tiles a launch steps at least; <= 0: 8 per SM     */
+    double aging_s;          /* SHORTEST: wait after which a solve goes first; <= 0: 5 s     */
+    int fill_tiles;          /* SHORTEST: tiles a launch steps at least; <= 0: 40 per SM    */
     int pad;
 } hosono_serve_config;
 
