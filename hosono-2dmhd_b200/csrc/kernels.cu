@@ -1129,50 +1129,18 @@ __device__ __forceinline__ bool ct_cell(const InstDev& d, const InstState& S, in
     return update_detect_cell(d, S, uin, uout, cc, ctx, cty, ctx_e, cty_n);
 }
 
-// The dense pass-1 form: the corrected fluxes of the tile's cells and of its
-// east column and north row are computed once into shared memory (sCT),
-// so a cell reads its east / north neighbours' values from there instead of
-// evaluating FLICD again (where a neighbour is not flagged, its stored value
-// is read, as ct_cell does).
-constexpr int CT_SX = TILE_X + 1, CT_SY = TILE_Y + 1;
-__device__ __forceinline__ void t_ct_update_detect(const Batch& B, int uin, int uout, const Cell c, double* sV,
-                                                   double* sCT) {
+__device__ __forceinline__ void t_ct_update_detect(const Batch& B, int uin, int uout, const Cell c, double* sV) {
     InstState& S = B.st[c.k];
     if (!(S.stepping && S.stageActive)) return;  // uniform over the block
-    detect_prep_tile(B, S, uin, c, sV);  // starts with a barrier: the last tile's reads of sCT are done
+    detect_prep_tile(B, S, uin, c, sV);
     const InstDev& d = B.dev[c.k];
     const Geo& G = d.geo;
     const int g = G.g;
-    const int x0 = c.i - (int)threadIdx.x, y0 = c.j - (int)threadIdx.y;
-    const int tid = threadIdx.y * TILE_X + threadIdx.x;
-    for (int e = tid; e < CT_SX * CT_SY; e += NTHREADS) {
-        const int ly = e / CT_SX, lx = e - ly * CT_SX;
-        const int i = x0 + lx, j = y0 + ly;
-        if (i >= g && j >= g && i <= g + G.nx && j <= g + G.ny) {
-            const long long q = (long long)j * G.pitch + i;
-            if (d.recF[q]) {
-                sCT[e] = flicd_x(d, q);
-                sCT[CT_SX * CT_SY + e] = flicd_y(d, q);
-            }
-        }
-    }
-    __syncthreads();
     bool low = false;
     long long cc = 0;
     if (c.i >= g && c.j >= g && c.i <= g + G.nx && c.j <= g + G.ny) {
         cc = (long long)c.j * G.pitch + c.i;
-        if (d.recF[cc]) {
-            const int e = threadIdx.y * CT_SX + threadIdx.x;
-            const double ctx = sCT[e], cty = sCT[CT_SX * CT_SY + e];
-            d.CTX[cc] = ctx;
-            d.CTY[cc] = cty;
-            if (c.i < g + G.nx && c.j < g + G.ny) {
-                const long long ce = cc + 1, cn = cc + G.pitch;
-                const double ctx_e = d.recF[ce] ? sCT[e + 1] : d.CTX[ce];
-                const double cty_n = d.recF[cn] ? sCT[CT_SX * CT_SY + e + CT_SX] : d.CTY[cn];
-                low = update_detect_cell(d, S, uin, uout, cc, ctx, cty, ctx_e, cty_n);
-            }
-        }
+        low = ct_cell(d, S, uin, uout, c.i, c.j, cc);
     }
     warp_count(&S.nDetect, low);
     warp_append(B.L, LIST_LOW, B.L.low, B.L.cap, low, entry(c.k, cc));
@@ -1180,11 +1148,13 @@ __device__ __forceinline__ void t_ct_update_detect(const Batch& B, int uin, int 
 // six resident blocks (a 40-register budget, a few hundred bytes of spills):
 // the tile's loads wait at two barriers, so more warps in flight keep HBM
 // busier.  Per step on Orszag-Tang 2048^2: 3 blocks (80 registers) 11.66 ms,
-// 4 blocks 11.23 ms, 5 blocks 11.14 ms, 6 blocks 11.08 ms.
+// 4 blocks 11.23 ms, 5 blocks 11.14 ms, 6 blocks 11.08 ms.  Computing each
+// cell's corrected fluxes once into shared memory (instead of a cell also
+// evaluating its east and north neighbours' FLICD) made a launch about 5 %
+// slower: the extra barrier costs more than the loads it saves, which hit L1.
 __global__ void __launch_bounds__(NTHREADS, 6) k_ct_update_detect(Batch B, int uin, int uout) {
     __shared__ double sV[4 * DP_SX * DP_SY];
-    __shared__ double sCT[2 * CT_SX * CT_SY];
-    FOR_TILES(B, t) t_ct_update_detect(B, uin, uout, tile_at(B, t), sV, sCT);
+    FOR_TILES(B, t) t_ct_update_detect(B, uin, uout, tile_at(B, t), sV);
 }
 
 // the same on the recomputeFLICD list of a later MOOD pass
