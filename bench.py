@@ -509,6 +509,58 @@ def sweep_tuning(args):
                   flush=True)
 
 
+def sweep_later_passes(args):
+    """--sweep-later-passes: the later MOOD passes as a kernel chain and as one
+    persistent launch per stage, on the reference's runnable case to t_end,
+    Sedov 1024^2 (10 steps) and the blast64 batch; one JSON line each."""
+    import torch
+    m = load_pkg()
+    problems = load_problems()
+
+    def timed(stream, fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        r = fn()
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1), r
+    for later in (0, 1):
+        name = "persistent" if later else "kernels"
+        with tempfile.TemporaryDirectory() as d:
+            s = m.Solver.from_par(par_for("ot128_r1", d))
+            s.set_tuning(later_passes=later)
+            U0, V0, _ = s.download()
+            s.run()
+            s.upload(U0, V0)
+            s.set_time(0.0, 0.5, 0, 1 << 30)
+            ms, (t, n) = timed(torch.cuda.ExternalStream(s.stream()), lambda: s.step(0))
+            s.close()
+            print(json.dumps({"later_passes": name, "workload": "ot128_r1 to t_end", "steps": n,
+                              "ms_per_step": ms / n}), flush=True)
+            import parfiles
+            s = m.Solver.from_par(parfiles.make(d, "sedov1024", parfiles.sedov(1024, 2)))
+            s.set_tuning(later_passes=later)
+            s.set_time(0.0, 1e30, 0, 1 << 30)
+            s.step(3)
+            ms, _ = timed(torch.cuda.ExternalStream(s.stream()), lambda: s.step(10))
+            passes = s.stats()["mood_passes"]
+            s.close()
+            print(json.dumps({"later_passes": name, "workload": "sedov1024_r2, 10 steps", "ms_per_step": ms / 10,
+                              "mood_passes": passes}), flush=True)
+            with open(os.path.join(ROOT, "hosono-2dmhd_b200", "workloads", "blast64_seed0.json")) as f:
+                entries = json.load(f)["instances"]
+            pars = [problems.make(d, f"i{e['id']}", problems.from_entry(e)) for e in entries]
+            b = m.Batch(len(pars), sum(m.Batch.tiles_for(m.par_load(p)[0]) for p in pars))
+            b.set_tuning(later_passes=later)
+            slots = [b.add_par(p) for p in pars]
+            b.run(max_steps=1)
+            ms, _ = timed(torch.cuda.ExternalStream(b.stream()), lambda: b.run())
+            zu = sum(e["n"] ** 2 * (b.status(k)["nstep"] - 1) for k, e in zip(slots, entries))
+            b.close()
+            print(json.dumps({"later_passes": name, "workload": "blast64 batch to t_end", "s": ms / 1e3,
+                              "zone_updates_per_s": zu / (ms / 1e3)}), flush=True)
+
+
 def load_problems():
     import importlib
     load_pkg()
@@ -712,6 +764,8 @@ def main():
     ap.add_argument("--fp", default="strict", choices=["strict", "fast"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="keep the default launch choices (no autotuning)")
+    ap.add_argument("--sweep-later-passes", action="store_true",
+                    help="time the later MOOD passes as a kernel chain and as one persistent launch, and exit")
     ap.add_argument("--sweep-tuning", action="store_true",
                     help="time every pass-1 launch choice on the workload (whole steps and pass 1) and exit")
     ap.add_argument("--tuning", default=None,
@@ -743,6 +797,8 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.sweep_tuning:
         sweep_tuning(args)
+    elif args.sweep_later_passes:
+        sweep_later_passes(args)
     elif args.impl == "reference":
         bench_reference(args, rank)
     else:
