@@ -792,7 +792,7 @@ int Engine::record_stage(Rec& r, int uin, int uout, cudaEvent_t ev0, cudaEvent_t
         return [&, hc, later](Rec& c) -> int {
             TRYE(c.k([&](cudaStream_t s) { K->cascade_lower(B, later, s); }));
             TRYE(c.k([&](cudaStream_t s) { K->recon_check(B, uin, later, s); }));
-            if (!c.graph()) launches += 2;  // both launch two kernels
+            if (!c.graph()) launches += 1;  // recon_check launches two kernels
             TRYE(c.k([&](cudaStream_t s) { K->cascade_cond(B, hc, s); }));
             return HOSONO_OK;
         };

@@ -45,9 +45,9 @@ hosono_stats stats_delta(const InstState& a, const InstState& b) {
 // kernels one graph execution launched, from the work counters: per step 4
 // time-loop kernels (cfl path) or 1 (host dt), 3 RK kernels; per stage 11
 // (MOOD pass 1, three of them the per-radius face kernels); per cascade
-// iteration 5; per further MOOD pass 9.
+// iteration 4; per further MOOD pass 9.
 long long graph_launches(const hosono_stats& s, int steps, bool host_dt) {
-    return (long long)steps * ((host_dt ? 1 : 4) + 3) + 11LL * s.stages + 5LL * s.cascade_iters +
+    return (long long)steps * ((host_dt ? 1 : 4) + 3) + 11LL * s.stages + 4LL * s.cascade_iters +
            9LL * (s.mood_passes - s.stages);
 }
 

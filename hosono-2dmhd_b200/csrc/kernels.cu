@@ -631,16 +631,9 @@ __global__ void __launch_bounds__(PASS_END_THREADS) k_cascade_cond(Batch B, cuda
 // the serial lowering loop of reconstruct.f90:146-169 (order independent: a
 // cell lowers only its own scheme; every flag write sets): for each failing
 // cell in [g-2, g+n+1]^2, gridBlock_lowerOrder (gridBlock.f90:194-235) and
-// mark the cross for the next inner pass.  nextPass is cleared first.
-__device__ __forceinline__ void t_clear_nextpass(const Batch& B, const Cell c) {
-    const InstState& S = B.st[c.k];
-    if (!S.nextIter) return;
-    const InstDev& d = B.dev[c.k];
-    if (c.i < d.geo.nxt && c.j < d.geo.nyt) d.nextPass[(long long)c.j * d.geo.pitch + c.i] = 0;
-}
-__global__ void __launch_bounds__(NTHREADS) k_clear_nextpass(Batch B) {
-    FOR_CASCADE_TILES(B, t) t_clear_nextpass(B, tile_at(B, t));
-}
+// mark the cross for the next inner pass.  The marks in the reconstruct
+// range start the iteration clear: compact_next, their only reader, clears
+// each mark of the range as it reads it, in the same iteration.
 
 // gridBlock_lowerOrder (gridBlock.f90:194-235) of cell (i,j) plus the mark of
 // its cross for the next inner pass
@@ -771,6 +764,7 @@ __device__ __forceinline__ void t_compact_next(const Batch& B, const Cell c) {
     if (c.i >= g - 2 && c.j >= g - 2 && c.i <= g + G.nx + 1 && c.j <= g + G.ny + 1) {
         cc = (long long)c.j * G.pitch + c.i;
         p = d.nextPass[cc] != 0;
+        if (p) d.nextPass[cc] = 0;  // read and cleared: the next iteration's lowering marks afresh
     }
     warp_append(B.L, LIST_NEXT, B.L.next, B.L.cap, p, entry(c.k, cc));
 }
@@ -1763,8 +1757,6 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_mood_rest(Batch B, int uin, int
         if (blockIdx.x == 0) d_cascade_cond<NTHREADS>(B, tid, 0, 0);
         GSYNC_OR_LEAVE;
         while (ld_acquire_s32(&B.flags->anyFail)) {
-            FOR_CASCADE_TILES(B, t) t_clear_nextpass(B, tile_at(B, t));
-            GSYNC_OR_LEAVE;
             FOR_CASCADE_TILES(B, t) t_cascade_lower(B, tile_at(B, t));
             GSYNC_OR_LEAVE;
             FOR_CASCADE_TILES(B, t) t_compact_next(B, tile_at(B, t));
@@ -1895,10 +1887,7 @@ void l_face_pass1(const Batch& B, int uin, cudaStream_t s) {
 void l_cascade_cond(const Batch& B, cudaGraphConditionalHandle h, cudaStream_t s) {
     k_cascade_cond<<<1, PASS_END_THREADS, 0, s>>>(B, h, h != 0);
 }
-void l_cascade_lower(const Batch& B, int /*later*/, cudaStream_t s) {
-    TILE_LAUNCH(k_clear_nextpass, B, s);
-    TILE_LAUNCH(k_cascade_lower, B, s);
-}
+void l_cascade_lower(const Batch& B, int /*later*/, cudaStream_t s) { TILE_LAUNCH(k_cascade_lower, B, s); }
 void l_recon_check(const Batch& B, int uin, int /*later*/, cudaStream_t s) {
     TILE_LAUNCH(k_compact_next, B, s);
     LIST_LAUNCH(k_recon_group, B, s, uin, (int)LIST_NEXT);
@@ -1948,7 +1937,7 @@ void l_mood_rest(const Batch& B, int uin, int uout, cudaStream_t s) {
 void l_launch_info(int R, int maxTiles, int* pass1, int* tile_grid_max) {
     *pass1 = R == 1 ? pass1_grid<1, false, false, 2>(maxTiles)
                     : R == 2 ? pass1_grid<2, false, false, 2>(maxTiles) : pass1_grid<3, false, false, 2>(maxTiles);
-    const void* tile_kernels[] = {(const void*)k_cfl_reduce,     (const void*)k_stage_init,   (const void*)k_clear_nextpass,
+    const void* tile_kernels[] = {(const void*)k_cfl_reduce,     (const void*)k_stage_init,
                                   (const void*)k_cascade_lower,  (const void*)k_compact_next, (const void*)k_compact_post,
                                   (const void*)k_compact_dirty,  (const void*)k_ct_update_detect, (const void*)k_mood_flags,
                                   (const void*)k_bc_fill,        (const void*)k_rk_combine2,  (const void*)k_rk_final,
