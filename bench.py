@@ -280,9 +280,10 @@ def bench_ours(args, rank, world, local):
     sol.upload(U0, V0)
     sol.set_time(0.0, run.tmax, 0, run.nstepmax)
     tune = None
-    if args.tuning:  # a fixed launch choice (staging,schedule,blocks per SM), e.g. for a profiler
-        st_, sc_, bl_ = (int(x) for x in args.tuning.split(","))
-        sol.set_tuning(pass1_staging=st_, pass1_schedule=sc_, pass1_blocks_per_sm=bl_)
+    if args.tuning:  # a fixed launch choice (staging,schedule,blocks per SM[,boxes]), e.g. for a profiler
+        f = [int(x) for x in args.tuning.split(",")]
+        sol.set_tuning(pass1_staging=f[0], pass1_schedule=f[1], pass1_blocks_per_sm=f[2],
+                       pass1_boxes=f[3] if len(f) > 3 else 0)
         tune = {"fixed": sol.tuning()}
     elif not args.no_tune:
         tune = sol.autotune(trials=5, force=True)
@@ -477,9 +478,10 @@ def sweep_tuning(args):
     import torch
     m = load_pkg()
     w = WORKLOADS[args.workload]
-    choices = [(st, sc, 2) for st in (0, 1) for sc in (0, 1)] + [(0, 0, 3), (0, 1, 3), (0, 0, 4), (0, 1, 4)]
+    choices = ([(st, sc, 2, bx) for bx in (1, 2) for st in (0, 1) for sc in (0, 1)] +
+               [(0, 0, 3, 1), (0, 1, 3, 1), (0, 0, 4, 1), (0, 1, 4, 1)])
     for fp in (m.FP_STRICT, m.FP_FAST):
-        for st, sc, bl in choices:
+        for st, sc, bl, bx in choices:
             with tempfile.TemporaryDirectory() as d:
                 par = par_for(args.workload, d)
                 params, run = m.par_load(par)
@@ -489,7 +491,7 @@ def sweep_tuning(args):
             sol = m.Solver(params, pv, qw, stc)
             sol.upload(U0, V0)
             sol.set_time(0.0, run.tmax, 0, run.nstepmax)
-            sol.set_tuning(pass1_staging=st, pass1_schedule=sc, pass1_blocks_per_sm=bl)
+            sol.set_tuning(pass1_staging=st, pass1_schedule=sc, pass1_blocks_per_sm=bl, pass1_boxes=bx)
             sol.step(max(args.warmup, 1))
             stream = torch.cuda.ExternalStream(sol.stream())
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -504,7 +506,7 @@ def sweep_tuning(args):
             p1, n1, _ = sol.profile_read(reset=True)
             sol.close()
             print(json.dumps({"workload": args.workload, "fp": "fast" if fp else "strict", "pass1_staging": st,
-                              "pass1_schedule": sc, "pass1_blocks_per_sm": bl, "ms_per_step": ms,
+                              "pass1_schedule": sc, "pass1_blocks_per_sm": bl, "pass1_boxes": bx, "ms_per_step": ms,
                               "pass1_ms": p1 / max(n1, 1), "zone_updates_per_s": w["n"] ** 2 / (ms / 1e3)}),
                   flush=True)
 
@@ -769,7 +771,7 @@ def main():
     ap.add_argument("--sweep-tuning", action="store_true",
                     help="time every pass-1 launch choice on the workload (whole steps and pass 1) and exit")
     ap.add_argument("--tuning", default=None,
-                    help="fixed pass-1 launch choice 'staging,schedule,blocks_per_sm' instead of autotuning")
+                    help="fixed pass-1 launch choice 'staging,schedule,blocks_per_sm[,boxes]' instead of autotuning")
     ap.add_argument("--no-batched", action="store_true", help="skip the 64-instance batched-vs-plain measurement")
     ap.add_argument("--no-config0", action="store_true", help="skip the Orszag-Tang 128^2 R=1 to t_end leg")
     ap.add_argument("--eager", action="store_true",

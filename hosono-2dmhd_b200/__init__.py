@@ -99,17 +99,24 @@ class LaunchInfo(ctypes.Structure):
 
 class Tuning(ctypes.Structure):
     _fields_ = [("pass1_staging", ctypes.c_int), ("pass1_schedule", ctypes.c_int),
-                ("pass1_blocks_per_sm", ctypes.c_int), ("later_passes", ctypes.c_int), ("pad", ctypes.c_int * 4)]
+                ("pass1_blocks_per_sm", ctypes.c_int), ("later_passes", ctypes.c_int),
+                ("pass1_boxes", ctypes.c_int), ("pad", ctypes.c_int * 3)]
+    KEYS = ("pass1_staging", "pass1_schedule", "pass1_blocks_per_sm", "later_passes", "pass1_boxes")
 
     def as_dict(self):
-        return {"pass1_staging": self.pass1_staging, "pass1_schedule": self.pass1_schedule,
-                "pass1_blocks_per_sm": self.pass1_blocks_per_sm, "later_passes": self.later_passes}
+        return {k: getattr(self, k) for k in self.KEYS}
+
+    def update(self, kw):
+        for k, v in kw.items():
+            if k not in self.KEYS:
+                raise TypeError(f"unknown tuning field {k!r} (one of {', '.join(self.KEYS)})")
+            setattr(self, k, int(v))
 
 
 STAGE_CP_ASYNC, STAGE_TMA = 0, 1
 SCHED_STATIC, SCHED_DYNAMIC = 0, 1
 LATER_KERNELS, LATER_PERSISTENT = 0, 1
-TUNE_MAX = 8
+TUNE_MAX = 12
 
 
 class TuneReport(ctypes.Structure):
@@ -579,8 +586,7 @@ class Solver:
         """Launch choices (results are the same bits for every choice)."""
         t = Tuning()
         self._check(self.lib.hosono_gpu_get_tuning(self.h, ctypes.byref(t)), "get_tuning")
-        for k, v in kw.items():
-            setattr(t, k, int(v))
+        t.update(kw)
         self._check(self.lib.hosono_gpu_set_tuning(self.h, ctypes.byref(t)), "set_tuning")
 
     def tuning(self):
@@ -746,8 +752,7 @@ class Batch:
     def set_tuning(self, **kw):
         t = Tuning()
         self._check(self.lib.hosono_batch_get_tuning(self.h, ctypes.byref(t)), "get_tuning")
-        for k, v in kw.items():
-            setattr(t, k, int(v))
+        t.update(kw)
         self._check(self.lib.hosono_batch_set_tuning(self.h, ctypes.byref(t)), "set_tuning")
 
     def autotune(self, trials=5, force=False):

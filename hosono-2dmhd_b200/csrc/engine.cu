@@ -288,6 +288,10 @@ int Engine::set_tuning(const hosono_tuning& t) {
         return fail(HOSONO_EINVAL, "TMA staging runs at two pass-1 blocks per SM");
     if (t.later_passes != HOSONO_LATER_KERNELS && t.later_passes != HOSONO_LATER_PERSISTENT)
         return fail(HOSONO_EINVAL, "later_passes %d", t.later_passes);
+    if (t.pass1_boxes < 0 || t.pass1_boxes > 2)
+        return fail(HOSONO_EINVAL, "pass1_boxes %d (0, 1 or 2)", t.pass1_boxes);
+    if (t.pass1_boxes == 2 && t.pass1_blocks_per_sm > 2)
+        return fail(HOSONO_EINVAL, "two stencil boxes run at two pass-1 blocks per SM");
     tune_ = t;
     drop_graphs();  // the graphs hold the launch choices in their kernel parameters
     return HOSONO_OK;
@@ -328,17 +332,18 @@ int Engine::autotune(int trials, bool force, hosono_tune_report* rep) {
     }
     CUE(cudaStreamSynchronize(s_));
     const hosono_tuning saved = tune_;
-    // candidates: two blocks per SM with cp.async or TMA staging, three and
-    // four blocks per SM with cp.async; each with the static and the dynamic
-    // tile schedule
+    // candidates: two blocks per SM with cp.async or TMA staging and one or
+    // two stencil boxes, three and four blocks per SM with cp.async and one
+    // box; each with the static and the dynamic tile schedule
     std::vector<hosono_tuning> cands;
-    const int forms[4][2] = {{2, HOSONO_STAGE_CP_ASYNC}, {2, HOSONO_STAGE_TMA}, {3, HOSONO_STAGE_CP_ASYNC},
-                             {4, HOSONO_STAGE_CP_ASYNC}};
+    const int forms[6][3] = {{2, HOSONO_STAGE_CP_ASYNC, 1}, {2, HOSONO_STAGE_TMA, 1}, {2, HOSONO_STAGE_CP_ASYNC, 2},
+                             {2, HOSONO_STAGE_TMA, 2},      {3, HOSONO_STAGE_CP_ASYNC, 1}, {4, HOSONO_STAGE_CP_ASYNC, 1}};
     for (const auto& f : forms)
         for (int sched : {HOSONO_SCHED_STATIC, HOSONO_SCHED_DYNAMIC}) {
             hosono_tuning t = tune_;  // the caller's later-pass choice stays
             t.pass1_blocks_per_sm = f[0];
             t.pass1_staging = f[1];
+            t.pass1_boxes = f[2];
             t.pass1_schedule = sched;
             cands.push_back(t);
         }
@@ -394,6 +399,8 @@ Batch Engine::batch() const {
     B.p1Tma = tune_.pass1_staging == HOSONO_STAGE_TMA ? 1 : 0;
     B.p1Dyn = tune_.pass1_schedule == HOSONO_SCHED_DYNAMIC ? 1 : 0;
     B.p1Blocks = tune_.pass1_blocks_per_sm == 0 ? 2 : tune_.pass1_blocks_per_sm;
+    B.p1Boxes = tune_.pass1_boxes == 2 ? 2 : 1;
+    B.p1Radii = radii_;
     B.dev = d_dev_;
     B.st = d_st_;
     B.tiles = d_tiles_;
@@ -464,6 +471,9 @@ int Engine::upload_tables() {
     CUE(cudaMemcpyAsync(&d_flags_->radii, &radii_, sizeof(int), cudaMemcpyHostToDevice, s_));
     CUE(cudaMemcpyAsync(d_instTiles_, instTiles_.data(), sizeof(int2) * maxInst_, cudaMemcpyHostToDevice, s_));
     CUE(cudaStreamSynchronize(s_));
+    // the graphs launch pass 1 for the radii held when they were recorded:
+    // a new radius needs new graphs
+    if (radii_ & ~graphRadii_) drop_graphs();
     return HOSONO_OK;
 }
 
@@ -784,6 +794,7 @@ int Engine::record_stage(Rec& r, int uin, int uout, cudaEvent_t ev0, cudaEvent_t
     TRYE(r.k([&](cudaStream_t s) { K->stage_init(B, s); }));
     if (ev0) TRYE(r.event(ev0));
     TRYE(r.k([&](cudaStream_t s) { K->face_pass1(B, uin, s); }));
+    if (!r.graph()) launches += radii_held() - 1;  // one pass-1 kernel per radius held
     if (ev1) TRYE(r.event(ev1));
     cudaGraphConditionalHandle hc1, hm;
     TRYE(r.cond(&hc1, 0));
@@ -867,6 +878,7 @@ int Engine::record_step(Rec& r, bool host_dt, cudaGraphConditionalHandle run_con
 
 int Engine::build_graphs() {
     if (gAdvance_) return HOSONO_OK;
+    graphRadii_ = radii_;
     for (int which = 0; which < 3; which++) {
         cudaGraph_t g;
         CUE(cudaGraphCreate(&g, 0));

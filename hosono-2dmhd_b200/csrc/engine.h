@@ -139,6 +139,8 @@ struct Batch {
     int p1Tma;           // pass 1 stages its stencil box with TMA (1) or cp.async (0)
     int p1Dyn;           // pass-1 blocks take tiles from a shared counter (1) or grid-stride (0)
     int p1Blocks;        // resident pass-1 blocks per SM the variant aims at (2, 3 or 4)
+    int p1Boxes;         // stencil boxes per pass-1 block at two blocks per SM (1 or 2)
+    int p1Radii;         // bit R: the host launches the radius-R pass-1 kernel (radii held)
     int maxTiles;        // capacity of the tile list
     int maxInst;         // capacity (slots)
     const int2* instTiles;  // per slot: first tile in the tile list, tile count (0: not live)

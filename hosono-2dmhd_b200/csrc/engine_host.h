@@ -106,6 +106,8 @@ class Engine {
     // time the candidate tunings on the live instances, apply the fastest
     int autotune(int trials, bool force, hosono_tune_report* rep);
     const hosono_tuning& tuning() const { return tune_; }
+    // GP radii among the held instances (one pass-1 launch each per stage)
+    int radii_held() const { return __builtin_popcount((unsigned)radii_); }
     bool use_graphs = true;
     bool trace = false;
     std::vector<TraceRec> traces;
@@ -129,7 +131,9 @@ class Engine {
     int mod_ensure(int slot);
     int encode_tmaps(InstDev& dev);
     void drop_graphs();
-    hosono_tuning tune_{};
+    // a new engine's launch choices: the fastest on the benchmarked workloads
+    // (TMA staging, dynamic tile schedule, two blocks per SM with one box each)
+    hosono_tuning tune_{HOSONO_STAGE_TMA, HOSONO_SCHED_DYNAMIC, 2, HOSONO_LATER_KERNELS, 1, {0, 0, 0}};
     class Rec;
     friend class Rec;
 
@@ -158,7 +162,8 @@ class Engine {
     const KernelSet* K_ = nullptr;
     cudaStream_t s_ = nullptr;
     int maxInst_ = 0, maxTiles_ = 0;
-    int radii_ = 0;  // BatchFlags::radii of the committed tile list
+    int radii_ = 0;       // BatchFlags::radii of the committed tile list
+    int graphRadii_ = 0;  // radii_ when the step graphs were recorded (their pass-1 launches)
     InstDev* d_dev_ = nullptr;
     InstState* d_st_ = nullptr;
     int4* d_tiles_ = nullptr;

@@ -43,11 +43,11 @@ hosono_stats stats_delta(const InstState& a, const InstState& b) {
 }
 
 // kernels one graph execution launched, from the work counters: per step 4
-// time-loop kernels (cfl path) or 1 (host dt), 3 RK kernels; per stage 11
-// (MOOD pass 1, three of them the per-radius face kernels); per cascade
-// iteration 4; per further MOOD pass 9.
-long long graph_launches(const hosono_stats& s, int steps, bool host_dt) {
-    return (long long)steps * ((host_dt ? 1 : 4) + 3) + 11LL * s.stages + 4LL * s.cascade_iters +
+// time-loop kernels (cfl path) or 1 (host dt), 3 RK kernels; per stage 8
+// plus one pass-1 face kernel per GP radius held; per cascade iteration 4;
+// per further MOOD pass 9.
+long long graph_launches(const hosono_stats& s, int steps, bool host_dt, int radii) {
+    return (long long)steps * ((host_dt ? 1 : 4) + 3) + (8LL + radii) * s.stages + 4LL * s.cascade_iters +
            9LL * (s.mood_passes - s.stages);
 }
 
@@ -100,7 +100,7 @@ int hosono_gpu_advance(hosono_handle* h, double dt) {
     if (!rc) rc = h->eng.state(h->slot, &b);
     if (!rc) {
         h->stats = stats_delta(a, b);
-        if (h->eng.use_graphs && !h->eng.trace) h->eng.launches += graph_launches(h->stats, 1, true);
+        if (h->eng.use_graphs && !h->eng.trace) h->eng.launches += graph_launches(h->stats, 1, true, h->eng.radii_held());
     }
     return rc;
 }
@@ -138,7 +138,7 @@ int hosono_gpu_step(hosono_handle* h, int max_steps, double* t_out, int* nstep_o
     rc = h->eng.state(h->slot, &b);
     if (rc) return rc;
     h->stats = stats_delta(a, b);
-    if (h->eng.use_graphs && !h->eng.trace) h->eng.launches += graph_launches(h->stats, b.nstep - a.nstep, false);
+    if (h->eng.use_graphs && !h->eng.trace) h->eng.launches += graph_launches(h->stats, b.nstep - a.nstep, false, h->eng.radii_held());
     if (t_out) *t_out = b.t;
     if (nstep_out) *nstep_out = b.nstep;
     return HOSONO_OK;

@@ -433,16 +433,19 @@ __device__ __forceinline__ void pass1_stage_tma(const Batch& B, int uin, int t, 
 }
 
 // One launch per radius: blocks skip tiles of instances with another GP
-// radius.  Shared memory: two stencil boxes with their prediction vectors
-// (the next tile's are copied in asynchronously while the current one is
-// computed), the per-thread flux accumulators and, with TMA staging, the two
-// boxes' mbarriers.  TMA = false stages with per-thread cp.async copies.
+// radius.  Shared memory: NBUF stencil boxes with their prediction vectors,
+// the per-thread flux accumulators and, with TMA staging, the boxes'
+// mbarriers.  TMA = false stages with per-thread cp.async copies.
 //
 // MINB is the number of resident blocks per SM the register budget aims at
-// (launch bounds: 128 registers at 2, 80 at 3, 64 at 4).  Two blocks keep
-// two boxes (the next one loads while the current one is computed); three
-// or four keep one box each, which fits their shared memory, and rely on the
-// other resident blocks to hide the load.
+// (launch bounds: 128 registers at 2, 80 at 3, 64 at 4).  With two boxes the
+// next tile's box loads while the current one is computed; with one box a
+// block loads, computes, then loads the next, and relies on the other
+// resident blocks to hide the load.  One box takes 36 KB less shared memory
+// per block, which the SM gives to L1, where the kernel's register spills
+// live: at two blocks per SM that wins over double-buffering on the 2048^2
+// workloads.  Three or four blocks per SM keep one box (their shared memory
+// would not fit two).
 template <int R>
 struct P1Smem {  // dynamic shared memory layout (doubles): boxes, accumulators, prediction vectors, mbarriers
     static constexpr int box(int nbuf) { return nbuf * P1Box<R>::DOUBLES; }
@@ -450,10 +453,9 @@ struct P1Smem {  // dynamic shared memory layout (doubles): boxes, accumulators,
         return (nbuf * P1Box<R>::DOUBLES + NCONS * NTHREADS + nbuf * P1Box<R>::PVN) * (int)sizeof(double) + 2 * 8;
     }
 };
-template <int R, bool TMA, bool DYN, int MINB>
+template <int R, bool TMA, bool DYN, int MINB, int NBUF>
 __global__ void __launch_bounds__(NTHREADS, MINB) k_face_pass1(Batch B, int uin) {
-    constexpr int NBUF = MINB <= 2 ? 2 : 1;
-    static_assert(NBUF == 2 || !TMA, "TMA staging is double-buffered");
+    static_assert(NBUF == 1 || NBUF == 2, "one or two stencil boxes");
     extern __shared__ __align__(128) double smem[];
     __shared__ int sTile;  // the dynamic schedule's tile, as thread 0 took it
     using Box = P1Box<R>;
@@ -485,8 +487,18 @@ __global__ void __launch_bounds__(NTHREADS, MINB) k_face_pass1(Batch B, int uin)
     int buf = 0;
     if constexpr (NBUF == 1) {  // one box: load, compute, next
         while (t < n) {
-            pass1_stage<R>(B, uin, t, smem, pvBuf, tid);
-            cp_async_wait<0>();
+            if (!TMA) {
+                pass1_stage<R>(B, uin, t, smem, pvBuf, tid);
+                cp_async_wait<0>();
+            } else {
+                if (tid == 0) pass1_stage_tma<R>(B, uin, t, smem, pvBuf, bars);
+                const bool ok = mbar_wait(bars, phase & 1u);
+                phase ^= 1u;
+                if (!__syncthreads_and(ok)) {  // a copy that never lands: report it, leave without reading
+                    if (tid == 0) atomicExch(&B.flags->error, HOSONO_ETIMEOUT);
+                    return;
+                }
+            }
             __syncthreads();  // tile t's box is in place for every thread
             const Cell c = tile_at(B, t);
             InstState& S = B.st[c.k];
@@ -1227,9 +1239,13 @@ __device__ __forceinline__ bool mood_flags_cell(const InstDev& d, const InstStat
     d.detMask[cc] &= (uint8_t)~DM_CASC;
     return rec;
 }
+// An instance whose pass lowered no cell (neither the face cascade nor
+// detect) keeps its scheme, and its MOOD loop ends here: the rebuild is
+// skipped, and pass_end leaves its scheme buffer where it is.
+__device__ __forceinline__ bool pass_lowered(const InstState& S) { return S.nInner != 0 || S.nDetect != 0; }
 __device__ __forceinline__ void t_mood_flags(const Batch& B, const Cell c) {
     const InstState& S = B.st[c.k];
-    if (!(S.stepping && S.stageActive)) return;
+    if (!(S.stepping && S.stageActive) || !pass_lowered(S)) return;
     const InstDev& d = B.dev[c.k];
     const Geo& G = d.geo;
     const int i = c.i, j = c.j;
@@ -1395,7 +1411,7 @@ __device__ __forceinline__ void d_pass_end(const Batch& B, int tid, cudaGraphCon
     for (int k = tid; k < B.maxInst; k += NT) {
         InstState& S = B.st[k];
         if (!(S.stepping && S.stageActive)) continue;
-        if (flip) S.schemeSel = 1 - S.schemeSel;  // k_mood_flags wrote the other buffer
+        if (flip && pass_lowered(S)) S.schemeSel = 1 - S.schemeSel;  // k_mood_flags wrote the other buffer
         S.passes++;
         S.passesTotal++;
         S.innerTotal += S.nInner;
@@ -1836,53 +1852,64 @@ void l_step_end(const Batch& B, cudaGraphConditionalHandle h, cudaStream_t s) {
 }
 void l_stage_init(const Batch& B, cudaStream_t s) { TILE_LAUNCH(k_stage_init, B, s); }
 // dynamic shared memory of a pass-1 kernel variant
-template <int R, int MINB>
+template <int R, int NBUF>
 constexpr int pass1_smem() {
-    return P1Smem<R>::bytes(MINB <= 2 ? 2 : 1);
+    return P1Smem<R>::bytes(NBUF);
 }
-template <int R, bool TMA, bool DYN, int MINB>
+template <int R, bool TMA, bool DYN, int MINB, int NBUF>
 int pass1_grid(int maxTiles) {
     static const bool attr =  // once per process (thread-safe static initialisation)
-        cudaFuncSetAttribute((const void*)k_face_pass1<R, TMA, DYN, MINB>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize, pass1_smem<R, MINB>()) == cudaSuccess;
+        cudaFuncSetAttribute((const void*)k_face_pass1<R, TMA, DYN, MINB, NBUF>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, pass1_smem<R, NBUF>()) == cudaSuccess;
     (void)attr;
-    const int r = resident_blocks((const void*)k_face_pass1<R, TMA, DYN, MINB>, pass1_smem<R, MINB>());
+    const int r = resident_blocks((const void*)k_face_pass1<R, TMA, DYN, MINB, NBUF>, pass1_smem<R, NBUF>());
     return r < maxTiles ? r : maxTiles;
 }
-template <int R, bool TMA, bool DYN, int MINB>
+template <int R, bool TMA, bool DYN, int MINB, int NBUF>
 void launch_pass1_v(const Batch& B, int uin, cudaStream_t s) {
-    k_face_pass1<R, TMA, DYN, MINB>
-        <<<dim3((unsigned)pass1_grid<R, TMA, DYN, MINB>(B.maxTiles)), kTile, pass1_smem<R, MINB>(), s>>>(B, uin);
+    k_face_pass1<R, TMA, DYN, MINB, NBUF><<<dim3((unsigned)pass1_grid<R, TMA, DYN, MINB, NBUF>(B.maxTiles)), kTile,
+                                            pass1_smem<R, NBUF>(), s>>>(B, uin);
 }
-// the variant the tuning asks for: TMA staging only with two blocks per SM
+template <int R, int MINB, int NBUF>
+void launch_pass1_s(const Batch& B, int uin, cudaStream_t s) {  // staging and schedule
+    if (B.p1Tma) {
+        if (B.p1Dyn)
+            launch_pass1_v<R, true, true, MINB, NBUF>(B, uin, s);
+        else
+            launch_pass1_v<R, true, false, MINB, NBUF>(B, uin, s);
+    } else {
+        if (B.p1Dyn)
+            launch_pass1_v<R, false, true, MINB, NBUF>(B, uin, s);
+        else
+            launch_pass1_v<R, false, false, MINB, NBUF>(B, uin, s);
+    }
+}
+// the variant the tuning asks for: TMA staging and two boxes only with two
+// blocks per SM
 template <int R>
 void launch_pass1(const Batch& B, int uin, cudaStream_t s) {
     if (B.p1Blocks == 3) {
         if (B.p1Dyn)
-            launch_pass1_v<R, false, true, 3>(B, uin, s);
+            launch_pass1_v<R, false, true, 3, 1>(B, uin, s);
         else
-            launch_pass1_v<R, false, false, 3>(B, uin, s);
+            launch_pass1_v<R, false, false, 3, 1>(B, uin, s);
     } else if (B.p1Blocks == 4) {
         if (B.p1Dyn)
-            launch_pass1_v<R, false, true, 4>(B, uin, s);
+            launch_pass1_v<R, false, true, 4, 1>(B, uin, s);
         else
-            launch_pass1_v<R, false, false, 4>(B, uin, s);
-    } else if (B.p1Tma) {
-        if (B.p1Dyn)
-            launch_pass1_v<R, true, true, 2>(B, uin, s);
-        else
-            launch_pass1_v<R, true, false, 2>(B, uin, s);
+            launch_pass1_v<R, false, false, 4, 1>(B, uin, s);
+    } else if (B.p1Boxes == 1) {
+        launch_pass1_s<R, 2, 1>(B, uin, s);
     } else {
-        if (B.p1Dyn)
-            launch_pass1_v<R, false, true, 2>(B, uin, s);
-        else
-            launch_pass1_v<R, false, false, 2>(B, uin, s);
+        launch_pass1_s<R, 2, 2>(B, uin, s);
     }
 }
+// one launch per radius held (the kernels also skip radii the device's
+// tile list does not hold)
 void l_face_pass1(const Batch& B, int uin, cudaStream_t s) {
-    launch_pass1<2>(B, uin, s);
-    launch_pass1<1>(B, uin, s);
-    launch_pass1<3>(B, uin, s);
+    if (B.p1Radii & (1 << 2)) launch_pass1<2>(B, uin, s);
+    if (B.p1Radii & (1 << 1)) launch_pass1<1>(B, uin, s);
+    if (B.p1Radii & (1 << 3)) launch_pass1<3>(B, uin, s);
 }
 void l_cascade_cond(const Batch& B, cudaGraphConditionalHandle h, cudaStream_t s) {
     k_cascade_cond<<<1, PASS_END_THREADS, 0, s>>>(B, h, h != 0);
@@ -1935,8 +1962,9 @@ void l_mood_rest(const Batch& B, int uin, int uout, cudaStream_t s) {
     cudaLaunchKernelEx(&cfg, k_mood_rest, B, uin, uout);
 }
 void l_launch_info(int R, int maxTiles, int* pass1, int* tile_grid_max) {
-    *pass1 = R == 1 ? pass1_grid<1, false, false, 2>(maxTiles)
-                    : R == 2 ? pass1_grid<2, false, false, 2>(maxTiles) : pass1_grid<3, false, false, 2>(maxTiles);
+    *pass1 = R == 1   ? pass1_grid<1, false, false, 2, 2>(maxTiles)
+             : R == 2 ? pass1_grid<2, false, false, 2, 2>(maxTiles)
+                      : pass1_grid<3, false, false, 2, 2>(maxTiles);
     const void* tile_kernels[] = {(const void*)k_cfl_reduce,     (const void*)k_stage_init,
                                   (const void*)k_cascade_lower,  (const void*)k_compact_next, (const void*)k_compact_post,
                                   (const void*)k_compact_dirty,  (const void*)k_ct_update_detect, (const void*)k_mood_flags,

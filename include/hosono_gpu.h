@@ -296,7 +296,9 @@ int hosono_gpu_stream(hosono_handle* h, void** stream);
 /* Launch choices of the time-step kernels (no counterpart in the reference,
  * whose loops are OpenMP regions).  Results do not depend on them: every
  * choice gives the same bits.  Setting them rebuilds the handle's step
- * graphs on the next step. */
+ * graphs on the next step.  A new handle or batch starts with TMA staging,
+ * the dynamic schedule, two blocks per SM and one box per block (the fastest
+ * choice on the 2048^2 Orszag-Tang and Sedov workloads). */
 #define HOSONO_STAGE_CP_ASYNC 0  /* pass-1 stencil box staged by per-thread cp.async copies */
 #define HOSONO_STAGE_TMA 1       /* ... by one TMA tensor copy (cp.async.bulk.tensor) per box */
 #define HOSONO_SCHED_STATIC 0    /* pass-1 blocks walk the tile list grid-stride */
@@ -307,10 +309,13 @@ typedef struct hosono_tuning {
     int pass1_staging;        /* HOSONO_STAGE_* */
     int pass1_schedule;       /* HOSONO_SCHED_* */
     int pass1_blocks_per_sm;  /* resident pass-1 blocks per SM the register budget aims at: 2 (0 = 2;
-                                 128 registers, two stencil boxes per block), 3 or 4 (80 / 64 registers,
-                                 one box; cp.async staging only) */
+                                 128 registers), 3 or 4 (80 / 64 registers, one stencil box per
+                                 block, cp.async staging only) */
     int later_passes;         /* HOSONO_LATER_*; the autotuner keeps the caller's choice */
-    int pad[4];               /* zero */
+    int pass1_boxes;          /* stencil boxes per pass-1 block at two blocks per SM: 1 (0 = 1; load,
+                                 compute, load the next; the shared memory saved goes to L1) or 2 (the
+                                 next tile's box loads while the current one is computed) */
+    int pad[3];               /* zero */
 } hosono_tuning;
 int hosono_gpu_set_tuning(hosono_handle* h, const hosono_tuning* t);
 int hosono_gpu_get_tuning(hosono_handle* h, hosono_tuning* t);
@@ -323,7 +328,7 @@ int hosono_gpu_get_tuning(hosono_handle* h, hosono_tuning* t);
  * by (arithmetic mode, GP radii present, size class = floor(log2(interior
  * cells)), floor(log2(instances))); a later call with the same key applies
  * the cached choice without timing unless `force` is set. */
-#define HOSONO_TUNE_MAX 8
+#define HOSONO_TUNE_MAX 12
 typedef struct hosono_tune_report {
     int candidates;                    /* entries of tried/ms filled                  */
     int cached;                        /* 1: taken from the cache, nothing was timed  */

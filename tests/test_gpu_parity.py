@@ -122,17 +122,21 @@ def test_orszag_tang_128_r1_to_t_end(tmp_par_dir):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("staging", ["tma", "cp_async_static"])
 @pytest.mark.parametrize("case", ["ot32_r1", "ot24_r3_refic", "sedov33x40_r1", "blast40_r2"])
-def test_tma_staging_bitwise(case, tmp_par_dir):
+def test_pass1_staging_bitwise(case, staging, tmp_par_dir):
     """Pass 1 with its stencil box staged by TMA (one cp.async.bulk.tensor per
-    box, zero fill beyond the array) gives the oracle's bits, as the
-    per-thread cp.async staging does."""
+    box, zero fill beyond the array; the default) or by per-thread cp.async
+    copies on the round-robin tile schedule gives the oracle's bits."""
     m = pkg.load()
-    par = parfiles.make(tmp_par_dir, case + "_tma", CASES[case]())
+    par = parfiles.make(tmp_par_dir, f"{case}_{staging}", CASES[case]())
     o = oracle.Oracle(par)
     s = m.Solver.from_par(par, fp_mode=m.FP_STRICT)
-    s.set_tuning(pass1_staging=m.STAGE_TMA)
-    assert s.tuning()["pass1_staging"] == m.STAGE_TMA
+    if staging == "tma":
+        assert s.tuning()["pass1_staging"] == m.STAGE_TMA  # the default
+    else:
+        s.set_tuning(pass1_staging=m.STAGE_CP_ASYNC, pass1_schedule=m.SCHED_STATIC)
+        assert s.tuning()["pass1_staging"] == m.STAGE_CP_ASYNC
     s.set_time(0.0, o.tmax, 0, 1 << 30)
     for chunk in (1, 3):
         for _ in range(chunk):

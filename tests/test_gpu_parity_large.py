@@ -8,8 +8,9 @@ detect.f90:18-236), at the sizes the bench measures:
 * Sedov 2048^2, R=2 (MOOD-heavy, outflow, hydro);
 * Orszag-Tang 1024^2, R=2, ell/Delta=12;
 * Orszag-Tang 640^2, R=2, ell/Delta=12: more tiles than any per-tile kernel
-  keeps resident blocks, so every grid-stride tile loop takes several trips
-  and the pass-1 kernel's double-buffered prefetch of the next tile runs;
+  keeps resident blocks, so every grid-stride tile loop takes several trips,
+  the pass-1 kernel's double-buffered prefetch of the next tile runs, and
+  its one-box form reloads its box per tile;
 * Orszag-Tang 512^2, R=2, ell/Delta=12 to t_end = 0.5: the accuracy gate at
   t_end (relative L1 <= 1e-8 per conserved variable, div(B) within 2x of the
   oracle's, output.f90:261-274), on top of bitwise equality.
@@ -39,12 +40,12 @@ def oracle_threads():
     oracle.set_threads(os.cpu_count() or 1)
 
 
-def _traced_steps(m, par, nsteps, staging=None):
+def _traced_steps(m, par, nsteps, **tuning):
     """nsteps host-launched, traced steps on both sides, compared after each."""
     o = oracle.Oracle(par)
     s = m.Solver.from_par(par, fp_mode=m.FP_STRICT)
-    if staging is not None:
-        s.set_tuning(pass1_staging=staging)
+    if tuning:
+        s.set_tuning(**tuning)
     o.trace(True)
     s.trace(True)
     for step in range(nsteps):
@@ -87,14 +88,17 @@ def test_benchmarked_config_bitwise(case, tmp_par_dir):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("boxes", [1, 2])
 @pytest.mark.parametrize("staging", ["cp_async", "tma"])
-def test_multi_tile_path_bitwise(staging, tmp_par_dir):
+def test_multi_tile_path_bitwise(staging, boxes, tmp_par_dir):
     """A grid with more tiles than any tile kernel's grid: blocks take
-    several tiles each, and pass 1 stages the next tile while computing one
-    (per-thread cp.async copies, or one TMA copy per box)."""
+    several tiles each, and pass 1 either stages the next tile while
+    computing one (two boxes) or reloads its one box per tile, with
+    per-thread cp.async copies or one TMA copy per box."""
     m = pkg.load()
     par = parfiles.make(tmp_par_dir, "ot640", parfiles.orszag_tang(640, 2, ell=12.0))
-    o, s = _traced_steps(m, par, 3, staging=m.STAGE_TMA if staging == "tma" else m.STAGE_CP_ASYNC)
+    o, s = _traced_steps(m, par, 3, pass1_staging=m.STAGE_TMA if staging == "tma" else m.STAGE_CP_ASYNC,
+                         pass1_boxes=boxes)
     info = s.launch_info()
     assert info["tiles"] > 2 * info["pass1_grid"], info
     assert info["tiles"] > info["tile_grid_max"], info

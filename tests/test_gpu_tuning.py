@@ -12,18 +12,21 @@ import pkg
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("boxes", [1, 2])
 @pytest.mark.parametrize("staging", [0, 1])
 @pytest.mark.parametrize("case", ["ot96_r2", "blast40_r1", "sedov36_r3"])
-def test_every_tuning_is_bitwise(case, staging, tmp_par_dir):
+def test_every_tuning_is_bitwise(case, staging, boxes, tmp_par_dir):
     """The dynamic tile schedule of pass 1 (blocks take tiles from a shared
-    counter) with either staging, through the step graph, equals the oracle."""
+    counter) with either staging and one or two stencil boxes per block,
+    through the step graph, equals the oracle."""
     m = pkg.load()
     kv = {"ot96_r2": lambda: parfiles.orszag_tang(96, 2), "blast40_r1": lambda: parfiles.blast(40, 1, p_ratio=500.0),
           "sedov36_r3": lambda: parfiles.sedov(36, 3)}[case]()
-    par = parfiles.make(tmp_par_dir, f"{case}_{staging}", kv)
+    par = parfiles.make(tmp_par_dir, f"{case}_{staging}_{boxes}", kv)
     o = oracle.Oracle(par)
     s = m.Solver.from_par(par, fp_mode=m.FP_STRICT)
-    s.set_tuning(pass1_staging=staging, pass1_schedule=m.SCHED_DYNAMIC)
+    s.set_tuning(pass1_staging=staging, pass1_schedule=m.SCHED_DYNAMIC, pass1_boxes=boxes)
+    assert s.tuning()["pass1_boxes"] == boxes
     s.set_time(0.0, o.tmax, 0, 1 << 30)
     for _ in range(3):
         o.advance(o.cfl())
@@ -45,7 +48,7 @@ def test_autotune_plain_solve(tmp_par_dir):
     o.advance(o.cfl())
     s.step(1)
     rep = s.autotune(trials=3, force=True)
-    assert not rep["cached"] and len(rep["table"]) == 8
+    assert not rep["cached"] and len(rep["table"]) == m.TUNE_MAX
     assert all(row["pass1_ms"] > 0 for row in rep["table"])
     best = min(rep["table"], key=lambda r: r["pass1_ms"])
     assert rep["best"] == {k: best[k] for k in rep["best"]}
@@ -77,7 +80,7 @@ def test_autotune_batch_mix(tmp_par_dir):
     for k in slots:
         b.set_time(k, 0.0, 1e30)
     rep = b.autotune(trials=2, force=True)
-    assert rep["instances"] == len(pars) and len(rep["table"]) == 8
+    assert rep["instances"] == len(pars) and len(rep["table"]) == m.TUNE_MAX
     b.run(max_steps=2)
     for k, p in zip(slots, pars):
         o = oracle.Oracle(p)
