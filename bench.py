@@ -425,7 +425,8 @@ def bench_ours(args, rank, world, local):
     if world == 1 and not args.no_config0 and args.workload != "ot128_r1":
         line["config0"] = bench_config0(m, fp, torch)
     if world == 1 and not args.no_batched:
-        line["batched"] = bench_batched(m, fp, torch, limit=args.batched_limit, eager=args.eager)
+        line["batched"] = bench_batched(m, fp, torch, limit=args.batched_limit, eager=args.eager,
+                                        tune=not args.no_tune)
     served_kept = {}
     if world == 1 and args.serve_requests > 0:
         line["served"], served_kept = bench_served(m, fp, args.serve_requests, args.serve_check,
@@ -569,7 +570,7 @@ def load_problems():
     return importlib.import_module("hosono_2dmhd_b200.problems")
 
 
-def bench_batched(m, fp, torch, manifest="blast64_seed0.json", limit=None, eager=False):
+def bench_batched(m, fp, torch, manifest="blast64_seed0.json", limit=None, eager=False, tune=True):
     """The 64-instance MHD-blast workload (uneven N in {128..512}) advanced to
     t_end=0.02 as one batch (one graph launch for the whole run) and, for
     comparison, as 64 plain single solves one after the other.  Set-up (host
@@ -587,7 +588,7 @@ def bench_batched(m, fp, torch, manifest="blast64_seed0.json", limit=None, eager
         if eager:
             b.set_graphs(False)
         slots = [b.add_par(p) for p in pars]
-        tune_b = b.autotune(trials=3, force=True)
+        tune_b = b.autotune(trials=3, force=True) if tune else {"fixed": b.tuning()}
         b.run(max_steps=1)
         n0 = {k: b.status(k)["nstep"] for k in slots}
         stream = torch.cuda.ExternalStream(b.stream())
@@ -612,7 +613,8 @@ def bench_batched(m, fp, torch, manifest="blast64_seed0.json", limit=None, eager
         zu_p = 0
         for p, e in zip(pars, entries):
             s = m.Solver.from_par(p, fp_mode=fp)
-            s.autotune(trials=3)  # per size class: timed once, then taken from the cache
+            if tune:
+                s.autotune(trials=3)  # per size class: timed once, then taken from the cache
             s.set_time(0.0, e["tmax"], 0, 1 << 30)
             s.step(1)
             st_ = torch.cuda.ExternalStream(s.stream())

@@ -755,6 +755,11 @@ class Batch:
         t.update(kw)
         self._check(self.lib.hosono_batch_set_tuning(self.h, ctypes.byref(t)), "set_tuning")
 
+    def tuning(self):
+        t = Tuning()
+        self._check(self.lib.hosono_batch_get_tuning(self.h, ctypes.byref(t)), "get_tuning")
+        return t.as_dict()
+
     def autotune(self, trials=5, force=False):
         """Time the candidate launch choices on the batch's instances; apply the fastest."""
         r = TuneReport()
