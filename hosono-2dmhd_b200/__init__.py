@@ -100,8 +100,8 @@ class LaunchInfo(ctypes.Structure):
 class Tuning(ctypes.Structure):
     _fields_ = [("pass1_staging", ctypes.c_int), ("pass1_schedule", ctypes.c_int),
                 ("pass1_blocks_per_sm", ctypes.c_int), ("later_passes", ctypes.c_int),
-                ("pass1_boxes", ctypes.c_int), ("pad", ctypes.c_int * 3)]
-    KEYS = ("pass1_staging", "pass1_schedule", "pass1_blocks_per_sm", "later_passes", "pass1_boxes")
+                ("pass1_boxes", ctypes.c_int), ("upload_bands", ctypes.c_int), ("pad", ctypes.c_int * 2)]
+    KEYS = ("pass1_staging", "pass1_schedule", "pass1_blocks_per_sm", "later_passes", "pass1_boxes", "upload_bands")
 
     def as_dict(self):
         return {k: getattr(self, k) for k in self.KEYS}
@@ -117,6 +117,7 @@ STAGE_CP_ASYNC, STAGE_TMA = 0, 1
 SCHED_STATIC, SCHED_DYNAMIC = 0, 1
 LATER_KERNELS, LATER_PERSISTENT = 0, 1
 TUNE_MAX = 12
+UPLOAD_BANDS_MAX = 16
 
 
 class TuneReport(ctypes.Structure):
@@ -445,7 +446,7 @@ class Solver:
         self._check(self.lib.hosono_gpu_advance(self.h, float(dt)), "advance")
 
     def advance_host(self, dt, U, V=None):
-        """Drop-in on host arrays: U (and V) in, advanced U (and V) out, in place."""
+        """Drop-in on host arrays: U in, advanced U (and V) out, in place."""
         assert U.flags.c_contiguous and U.dtype == np.float64
         self._check(self.lib.hosono_gpu_advance_host(self.h, float(dt), _p(U), _p(V) if V is not None else None),
                     "advance_host")

@@ -161,10 +161,14 @@ Engine::~Engine() {
         for (void* p : sl.allocs) dfree(p);
         if (sl.modAlloc) cudaFree(sl.modAlloc);
     }
-    for (cudaGraphExec_t g : {gAdvance_, gRun_, gProf_})
+    if (sCopy_) cudaStreamSynchronize(sCopy_);
+    for (cudaGraphExec_t g : {gAdvance_, gRun_, gProf_, gAdvRest_})
         if (g) cudaGraphExecDestroy(g);
     for (cudaEvent_t ev : profEv_)
         if (ev) cudaEventDestroy(ev);
+    for (cudaEvent_t ev : bandEv_)
+        if (ev) cudaEventDestroy(ev);
+    if (sCopy_) cudaStreamDestroy(sCopy_);
     for (void* p : {(void*)d_instTiles_, (void*)d_actRange_, (void*)d_actInfo_, (void*)d_casRange_,
                     (void*)d_casInfo_, (void*)d_hold_, (void*)d_gbar_})
         if (p) cudaFree(p);
@@ -270,7 +274,7 @@ int Engine::encode_tmaps(InstDev& dev) {
 
 void Engine::drop_graphs() {
     if (s_) cudaStreamSynchronize(s_);
-    for (cudaGraphExec_t* g : {&gAdvance_, &gRun_, &gProf_})
+    for (cudaGraphExec_t* g : {&gAdvance_, &gRun_, &gProf_, &gAdvRest_})
         if (*g) {
             cudaGraphExecDestroy(*g);
             *g = nullptr;
@@ -292,6 +296,8 @@ int Engine::set_tuning(const hosono_tuning& t) {
         return fail(HOSONO_EINVAL, "pass1_boxes %d (0, 1 or 2)", t.pass1_boxes);
     if (t.pass1_boxes == 2 && t.pass1_blocks_per_sm > 2)
         return fail(HOSONO_EINVAL, "two stencil boxes run at two pass-1 blocks per SM");
+    if (t.upload_bands < 0 || t.upload_bands > HOSONO_UPLOAD_BANDS_MAX)
+        return fail(HOSONO_EINVAL, "upload_bands %d (0..%d)", t.upload_bands, HOSONO_UPLOAD_BANDS_MAX);
     tune_ = t;
     drop_graphs();  // the graphs hold the launch choices in their kernel parameters
     return HOSONO_OK;
@@ -326,6 +332,8 @@ int Engine::autotune(int trials, bool force, hosono_tune_report* rep) {
         if (it != g_tune_cache.end()) {
             r.cached = 1;
             r.best = it->second;
+            r.best.later_passes = tune_.later_passes;  // the caller's choices stay
+            r.best.upload_bands = tune_.upload_bands;
             if (rep) *rep = r;
             return set_tuning(r.best);
         }
@@ -401,6 +409,8 @@ Batch Engine::batch() const {
     B.p1Blocks = tune_.pass1_blocks_per_sm == 0 ? 2 : tune_.pass1_blocks_per_sm;
     B.p1Boxes = tune_.pass1_boxes == 2 ? 2 : 1;
     B.p1Radii = radii_;
+    B.p1First = 0;
+    B.p1End = INT_MAX;
     B.dev = d_dev_;
     B.st = d_st_;
     B.tiles = d_tiles_;
@@ -665,6 +675,94 @@ int Engine::upload(int slot, const double* U, const double* V) {
     return HOSONO_OK;
 }
 
+int Engine::upload_u(int slot, const double* U) {
+    if (slot < 0 || slot >= maxInst_ || !slots_[slot].live || !U) return fail(HOSONO_EINVAL, "bad upload");
+    InstState st;
+    TRYE(state(slot, &st));
+    const Slot& sl = slots_[slot];
+    const Geo& G = sl.dev.geo;
+    CUE(cudaMemcpyAsync(staging_, U, (size_t)G.nxt * G.nyt * NCONS * sizeof(double), cudaMemcpyHostToDevice, s_));
+    launch_aos_to_soa(G, staging_, sl.dev.U[st.parity], NCONS, s_);
+    launches++;
+    CUE(cudaGetLastError());
+    return HOSONO_OK;
+}
+
+// timeStep_advanceSolution on host arrays (mhd_driver.f90:117-144 with
+// grid_state on the host).  Banded form: every band's rows go up on sCopy_
+// back to back (one DMA stream); the main stream sets up the first stage
+// (scheme = R, flags: timeStep.f90:77-81), then per band waits for its rows,
+// converts them and runs pass 1 on the band's tile rows -- whose stencil
+// boxes reach R + 1 rows past the band, so a band's copy ends that far
+// beyond its last tile row -- and finally the step graph without the first
+// stage's set-up and pass 1.  Tiles are independent in pass 1, so the
+// result bits do not depend on the banding.
+int Engine::advance_host(int slot, double dt, double* U, double* V) {
+    if (slot < 0 || slot >= maxInst_ || !slots_[slot].live || !U) return fail(HOSONO_EINVAL, "bad advance_host");
+    if (!(dt >= 0.0) || !std::isfinite(dt)) return fail(HOSONO_ENANDT, "dt = %g is not a valid time step", dt);
+    const Slot& sl = slots_[slot];
+    const Geo& G = sl.dev.geo;
+    int nb = tune_.upload_bands ? tune_.upload_bands : (G.nyt >= 1024 ? 8 : 1);
+    const int tileRows = (G.nyt + TILE_Y - 1) / TILE_Y, tilesPerRow = (G.nxt + TILE_X - 1) / TILE_X;
+    if (nb > tileRows) nb = tileRows;
+    // one instance per engine, step graphs in use: otherwise upload, then step
+    int liveCount = 0;
+    for (const Slot& x : slots_) liveCount += x.live ? 1 : 0;
+    if (nb <= 1 || liveCount != 1 || !use_graphs || trace) {
+        TRYE(upload_u(slot, U));
+        TRYE(advance(slot, dt));
+        return download(slot, U, V, nullptr);
+    }
+    if (!sCopy_) {
+        CUE(cudaStreamCreateWithFlags(&sCopy_, cudaStreamNonBlocking));
+        for (cudaEvent_t& ev : bandEv_) CUE(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    }
+    InstState st;
+    TRYE(state(slot, &st));
+    st.dt = dt;
+    st.stepping = 1;
+    st.error = 0;
+    CUE(cudaMemcpyAsync(d_st_ + slot, &st, sizeof(InstState), cudaMemcpyHostToDevice, s_));
+    TRYE(build_graphs());
+    // the copies start once everything before on the main stream is done with the staging buffer
+    CUE(cudaEventRecord(bandEv_[HOSONO_UPLOAD_BANDS_MAX], s_));
+    CUE(cudaStreamWaitEvent(sCopy_, bandEv_[HOSONO_UPLOAD_BANDS_MAX], 0));
+    const size_t rowBytes = (size_t)G.nxt * NCONS * sizeof(double), rowDoubles = (size_t)G.nxt * NCONS;
+    const int R = G.R;
+    int rowEnd[HOSONO_UPLOAD_BANDS_MAX], trEnd[HOSONO_UPLOAD_BANDS_MAX];
+    for (int b = 0, r0 = 0; b < nb; b++) {
+        trEnd[b] = (int)((long long)tileRows * (b + 1) / nb);
+        const int want = b == nb - 1 ? G.nyt : trEnd[b] * TILE_Y + R + 1;  // last row a band's boxes read + 1
+        rowEnd[b] = want < G.nyt ? want : G.nyt;
+        if (rowEnd[b] < r0) rowEnd[b] = r0;
+        if (rowEnd[b] > r0)
+            CUE(cudaMemcpyAsync(staging_ + (size_t)r0 * rowDoubles, U + (size_t)r0 * rowDoubles,
+                                (size_t)(rowEnd[b] - r0) * rowBytes, cudaMemcpyHostToDevice, sCopy_));
+        CUE(cudaEventRecord(bandEv_[b], sCopy_));
+        r0 = rowEnd[b];
+    }
+    const Batch B = batch();
+    K_->stage_init(B, s_);
+    launches++;
+    const int base = instTiles_[slot].x;
+    for (int b = 0, r0 = 0, tr0 = 0; b < nb; b++) {
+        CUE(cudaStreamWaitEvent(s_, bandEv_[b], 0));
+        launch_aos_to_soa_rows(G, staging_, sl.dev.U[st.parity], NCONS, r0, rowEnd[b], s_);
+        if (b > 0) CUE(cudaMemsetAsync(d_flags_->p1Next, 0, sizeof d_flags_->p1Next, s_));
+        Batch Bb = B;
+        Bb.p1First = base + tr0 * tilesPerRow;
+        Bb.p1End = base + trEnd[b] * tilesPerRow;
+        K_->face_pass1(Bb, ROLE_STATE, s_);
+        launches += 1 + radii_held();
+        r0 = rowEnd[b];
+        tr0 = trEnd[b];
+    }
+    CUE(cudaGetLastError());
+    CUE(cudaGraphLaunch(gAdvRest_, s_));
+    TRYE(check_errors());
+    return download(slot, U, V, nullptr);
+}
+
 int Engine::ic(int slot, const hosono_ic_desc& d, const double* xtab, const double* ytab) {
     if (slot < 0 || slot >= maxInst_ || !slots_[slot].live || !xtab || !ytab) return fail(HOSONO_EINVAL, "bad ic");
     if (d.type != HOSONO_IC_EXPLOSION && d.type != HOSONO_IC_SEDOV && d.type != HOSONO_IC_ORSZAG_TANG)
@@ -787,15 +885,17 @@ int Engine::set_time(int slot, double t, double tmax, int nstep, int nstepmax) {
 
 // ----------------------------------------------------------------------
 // The forward-Euler stage (timeStep.f90:45-130).
-int Engine::record_stage(Rec& r, int uin, int uout, cudaEvent_t ev0, cudaEvent_t ev1) {
+int Engine::record_stage(Rec& r, int uin, int uout, cudaEvent_t ev0, cudaEvent_t ev1, bool head) {
     const Batch B = batch();
     const KernelSet* K = K_;
     const long long cap = (long long)INT_MAX;
-    TRYE(r.k([&](cudaStream_t s) { K->stage_init(B, s); }));
-    if (ev0) TRYE(r.event(ev0));
-    TRYE(r.k([&](cudaStream_t s) { K->face_pass1(B, uin, s); }));
-    if (!r.graph()) launches += radii_held() - 1;  // one pass-1 kernel per radius held
-    if (ev1) TRYE(r.event(ev1));
+    if (head) {
+        TRYE(r.k([&](cudaStream_t s) { K->stage_init(B, s); }));
+        if (ev0) TRYE(r.event(ev0));
+        TRYE(r.k([&](cudaStream_t s) { K->face_pass1(B, uin, s); }));
+        if (!r.graph()) launches += radii_held() - 1;  // one pass-1 kernel per radius held
+        if (ev1) TRYE(r.event(ev1));
+    }
     cudaGraphConditionalHandle hc1, hm;
     TRYE(r.cond(&hc1, 0));
     TRYE(r.k([&](cudaStream_t s) { K->cascade_cond(B, hc1, s); }));
@@ -854,7 +954,8 @@ int Engine::record_stage(Rec& r, int uin, int uout, cudaEvent_t ev0, cudaEvent_t
 // One time step (timeStep_RK3 + advanceSolution; with the driver's cfl and
 // validTimeStep unless the host supplies dt).  With profile, CUDA events
 // bracket the pass-1 kernel of each stage.
-int Engine::record_step(Rec& r, bool host_dt, cudaGraphConditionalHandle run_cond, bool profile) {
+int Engine::record_step(Rec& r, bool host_dt, cudaGraphConditionalHandle run_cond, bool profile,
+                        bool first_head) {
     const Batch B = batch();
     const KernelSet* K = K_;
     if (!host_dt) {
@@ -867,7 +968,7 @@ int Engine::record_step(Rec& r, bool host_dt, cudaGraphConditionalHandle run_con
     const int uout[3] = {ROLE_A, ROLE_B, ROLE_B};
     for (int st = 0; st < 3; st++) {
         TRYE(record_stage(r, uin[st], uout[st], profile ? profEv_[2 * st] : nullptr,
-                          profile ? profEv_[2 * st + 1] : nullptr));
+                          profile ? profEv_[2 * st + 1] : nullptr, st > 0 || first_head));
         if (st == 0) TRYE(r.k([&](cudaStream_t s) { K->bc_fill(B, ROLE_A, s); }));
         if (st == 1) TRYE(r.k([&](cudaStream_t s) { K->rk_combine2(B, s); }));
         if (st == 2) TRYE(r.k([&](cudaStream_t s) { K->rk_final(B, s); }));
@@ -879,13 +980,15 @@ int Engine::record_step(Rec& r, bool host_dt, cudaGraphConditionalHandle run_con
 int Engine::build_graphs() {
     if (gAdvance_) return HOSONO_OK;
     graphRadii_ = radii_;
-    for (int which = 0; which < 3; which++) {
+    for (int which = 0; which < 4; which++) {
         cudaGraph_t g;
         CUE(cudaGraphCreate(&g, 0));
         Rec r(this, g);
         int rc;
         if (which == 0) {
             rc = record_step(r, true, 0, false);
+        } else if (which == 3) {  // the banded upload ran the first stage's set-up and pass 1
+            rc = record_step(r, true, 0, false, false);
         } else if (which == 2) {
             // one step at the graph's top level: event records are not allowed
             // inside conditional bodies, and pass 1 sits outside the MOOD loops
@@ -906,7 +1009,7 @@ int Engine::build_graphs() {
         cudaError_t e = cudaGraphInstantiate(&ex, g, 0);
         cudaGraphDestroy(g);
         if (e != cudaSuccess) return fail(HOSONO_ECUDA, "graph instantiate: %s", cudaGetErrorString(e));
-        (which == 0 ? gAdvance_ : which == 1 ? gRun_ : gProf_) = ex;
+        (which == 0 ? gAdvance_ : which == 1 ? gRun_ : which == 2 ? gProf_ : gAdvRest_) = ex;
     }
     return HOSONO_OK;
 }

@@ -141,6 +141,7 @@ struct Batch {
     int p1Blocks;        // resident pass-1 blocks per SM the variant aims at (2, 3 or 4)
     int p1Boxes;         // stencil boxes per pass-1 block at two blocks per SM (1 or 2)
     int p1Radii;         // bit R: the host launches the radius-R pass-1 kernel (radii held)
+    int p1First, p1End;  // pass 1 covers tiles [p1First, min(p1End, ntiles)) of the tile list
     int maxTiles;        // capacity of the tile list
     int maxInst;         // capacity (slots)
     const int2* instTiles;  // per slot: first tile in the tile list, tile count (0: not live)
@@ -241,6 +242,7 @@ const KernelSet* kernelset_fast();
 
 // layout conversions for one instance (no arithmetic; one build)
 void launch_aos_to_soa(const Geo& G, const double* aos, double* soa, int nvar, cudaStream_t s);
+void launch_aos_to_soa_rows(const Geo& G, const double* aos, double* soa, int nvar, int j0, int j1, cudaStream_t s);
 void launch_soa_to_aos(const Geo& G, const double* soa, double* aos, int nvar, cudaStream_t s);
 void launch_scheme_to_int(const Geo& G, const int8_t* scheme, int* out, cudaStream_t s);
 // initialCondition_set on the device (ic.cu)

@@ -40,6 +40,12 @@ class Engine {
     int reserve_staging(size_t cells);
     void set_allocator(DeviceAllocator* a) { alloc_ = a; }
     int upload(int slot, const double* U, const double* V);
+    // U host -> device (Fortran-order AoS with guards), nothing else
+    int upload_u(int slot, const double* U);
+    // hosono_gpu_advance_host: U up, one step of dt, U (and V) down.  With
+    // upload bands, U goes up in row bands on a second stream while the first
+    // stage's pass 1 computes the tiles of the bands already landed.
+    int advance_host(int slot, double dt, double* U, double* V);
     int download(int slot, double* U, double* V, int* scheme);
     // the initial state built on the device (hosono_ic_describe's output)
     int ic(int slot, const hosono_ic_desc& d, const double* xtab, const double* ytab);
@@ -133,7 +139,7 @@ class Engine {
     void drop_graphs();
     // a new engine's launch choices: the fastest on the benchmarked workloads
     // (TMA staging, dynamic tile schedule, two blocks per SM with one box each)
-    hosono_tuning tune_{HOSONO_STAGE_TMA, HOSONO_SCHED_DYNAMIC, 2, HOSONO_LATER_KERNELS, 1, {0, 0, 0}};
+    hosono_tuning tune_{HOSONO_STAGE_TMA, HOSONO_SCHED_DYNAMIC, 2, HOSONO_LATER_KERNELS, 1, 0, {0, 0}};
     class Rec;
     friend class Rec;
 
@@ -145,8 +151,10 @@ class Engine {
         const InstState* z = nullptr;
         return write_state_field(slot, (size_t)((const char*)&(z->*field) - (const char*)z), &value, sizeof(T));
     }
-    int record_stage(Rec& r, int uin, int uout, cudaEvent_t ev0, cudaEvent_t ev1);
-    int record_step(Rec& r, bool host_dt, cudaGraphConditionalHandle run_cond, bool profile);
+    // head = false leaves out the stage's set-up and pass 1 (run before, by the banded upload)
+    int record_stage(Rec& r, int uin, int uout, cudaEvent_t ev0, cudaEvent_t ev1, bool head = true);
+    int record_step(Rec& r, bool host_dt, cudaGraphConditionalHandle run_cond, bool profile,
+                    bool first_head = true);
     int build_graphs();
     int launch(cudaGraphExec_t g);
     int sync();
@@ -186,6 +194,9 @@ class Engine {
     std::vector<Slot> slots_;
     std::vector<int4> tiles_;
     cudaGraphExec_t gAdvance_ = nullptr, gRun_ = nullptr, gProf_ = nullptr;
+    cudaGraphExec_t gAdvRest_ = nullptr;  // gAdvance_ without the first stage's set-up and pass 1
+    cudaStream_t sCopy_ = nullptr;        // the banded upload's copy stream
+    cudaEvent_t bandEv_[HOSONO_UPLOAD_BANDS_MAX + 1] = {};
     cudaEvent_t profEv_[6] = {};
     std::vector<long long> tracePassesSeen_;
     std::vector<std::vector<unsigned char>> snapInner_, snapLow_;

@@ -153,9 +153,14 @@ int hosono_gpu_run(hosono_handle* h, double tmax, int nstepmax, int max_steps, d
 
 int hosono_gpu_advance_host(hosono_handle* h, double dt, double* U, double* V) {
     if (!h || !U) return HOSONO_EINVAL;
-    int rc = h->eng.upload(h->slot, U, V);
-    if (!rc) rc = hosono_gpu_advance(h, dt);
-    if (!rc) rc = h->eng.download(h->slot, U, V, nullptr);
+    InstState a, b;
+    int rc = h->eng.state(h->slot, &a);
+    if (!rc) rc = h->eng.advance_host(h->slot, dt, U, V);
+    if (!rc) rc = h->eng.state(h->slot, &b);
+    if (!rc) {
+        h->stats = stats_delta(a, b);
+        if (h->eng.use_graphs && !h->eng.trace) h->eng.launches += graph_launches(h->stats, 1, true, h->eng.radii_held());
+    }
     return rc;
 }
 

@@ -382,11 +382,12 @@ __device__ __forceinline__ int pass1_next(const Batch& B, int t, int n) {
 }
 
 // the dynamic schedule: the next tile of this radius from the launch-wide
-// counter (one atomic per tile taken; n when none is left)
+// counter, counted from the launch's first tile (one atomic per tile taken;
+// n when none is left)
 template <int R>
 __device__ __forceinline__ int pass1_take(const Batch& B, int n) {
     for (;;) {
-        const int t = atomicAdd(&B.flags->p1Next[R], 1);
+        const int t = B.p1First + atomicAdd(&B.flags->p1Next[R], 1);
         if (t >= n) return n;
         const int k = B.tiles[t].x;
         if (B.st[k].stepping && B.dev[k].geo.R == R) return t;
@@ -473,7 +474,7 @@ __global__ void __launch_bounds__(NTHREADS, MINB) k_face_pass1(Batch B, int uin)
         __syncthreads();
     }
     unsigned phase = 0;  // bit b: parity of buffer b's next completion
-    const int n = __ldg(B.ntiles);
+    const int n = min(__ldg(B.ntiles), B.p1End);  // the launch covers tiles [p1First, n)
     // the block's next tile: grid-stride (every thread computes it), or
     // taken from the counter by thread 0 and broadcast
     auto next_tile = [&](int after) -> int {
@@ -483,7 +484,7 @@ __global__ void __launch_bounds__(NTHREADS, MINB) k_face_pass1(Batch B, int uin)
         __syncthreads();
         return sTile;
     };
-    int t = next_tile(blockIdx.x);
+    int t = next_tile(B.p1First + blockIdx.x);
     int buf = 0;
     if constexpr (NBUF == 1) {  // one box: load, compute, next
         while (t < n) {

@@ -8,9 +8,11 @@ namespace hosono {
 namespace {
 constexpr int TX = 32, TY = 8;
 
-__global__ void k_aos_to_soa(Geo G, const double* __restrict__ aos, double* __restrict__ soa, int nvar) {
-    const int i = blockIdx.x * TX + threadIdx.x, j = blockIdx.y * TY + threadIdx.y;
-    if (i >= G.nxt || j >= G.nyt) return;
+// rows [j0, j1) of the array (the whole array: 0, nyt)
+__global__ void k_aos_to_soa(Geo G, const double* __restrict__ aos, double* __restrict__ soa, int nvar, int j0,
+                             int j1) {
+    const int i = blockIdx.x * TX + threadIdx.x, j = j0 + blockIdx.y * TY + threadIdx.y;
+    if (i >= G.nxt || j >= j1) return;
     const long long f = ((long long)j * G.nxt + i) * nvar;
     const long long c = (long long)j * G.pitch + i;
     for (int v = 0; v < nvar; v++) soa[v * G.plane + c] = aos[f + v];
@@ -34,7 +36,12 @@ dim3 grid_of(const Geo& G) { return dim3((G.nxt + TX - 1) / TX, (G.nyt + TY - 1)
 }  // namespace
 
 void launch_aos_to_soa(const Geo& G, const double* aos, double* soa, int nvar, cudaStream_t s) {
-    k_aos_to_soa<<<grid_of(G), dim3(TX, TY), 0, s>>>(G, aos, soa, nvar);
+    k_aos_to_soa<<<grid_of(G), dim3(TX, TY), 0, s>>>(G, aos, soa, nvar, 0, G.nyt);
+}
+void launch_aos_to_soa_rows(const Geo& G, const double* aos, double* soa, int nvar, int j0, int j1, cudaStream_t s) {
+    if (j1 <= j0) return;
+    const dim3 grid((G.nxt + TX - 1) / TX, (j1 - j0 + TY - 1) / TY);
+    k_aos_to_soa<<<grid, dim3(TX, TY), 0, s>>>(G, aos, soa, nvar, j0, j1);
 }
 void launch_soa_to_aos(const Geo& G, const double* soa, double* aos, int nvar, cudaStream_t s) {
     k_soa_to_aos<<<grid_of(G), dim3(TX, TY), 0, s>>>(G, soa, aos, nvar);

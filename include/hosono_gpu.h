@@ -199,9 +199,14 @@ int hosono_gpu_step(hosono_handle* h, int max_steps, double* t_out, int* nstep_o
  * host-driven launches (off; always the case while tracing). */
 int hosono_gpu_set_graphs(hosono_handle* h, int on);
 
-/* Drop-in with host buffers: upload U (and V if not NULL), advance by dt,
- * download U and V.  The form a Fortran caller that keeps grid_state on
- * the host binds (timeStep_advanceSolution with state%U/state%V). */
+/* Drop-in with host buffers: upload U, advance by dt, download U (and V if
+ * not NULL).  The form a Fortran caller that keeps grid_state on the host
+ * binds (timeStep_advanceSolution with state%U/state%V).  V is output only:
+ * like timeStep_advanceSolution, the step reads U and recomputes V from the
+ * new U.  On large grids (hosono_tuning.upload_bands) U goes up in row bands
+ * on a second stream, and the first stage's MOOD pass 1 computes each band's
+ * tiles as soon as their rows and halo have landed, so the upload and that
+ * kernel overlap; results are the same bits either way. */
 int hosono_gpu_advance_host(hosono_handle* h, double dt, double* U, double* V);
 
 int hosono_gpu_stats(hosono_handle* h, hosono_stats* s);
@@ -315,8 +320,12 @@ typedef struct hosono_tuning {
     int pass1_boxes;          /* stencil boxes per pass-1 block at two blocks per SM: 1 (0 = 1; load,
                                  compute, load the next; the shared memory saved goes to L1) or 2 (the
                                  next tile's box loads while the current one is computed) */
-    int pad[3];               /* zero */
+    int upload_bands;         /* hosono_gpu_advance_host: row bands of the overlapped upload (0 = by size:
+                                 8 from 1024 array rows up, else 1; 1 = upload, then step; at most
+                                 HOSONO_UPLOAD_BANDS_MAX) */
+    int pad[2];               /* zero */
 } hosono_tuning;
+#define HOSONO_UPLOAD_BANDS_MAX 16
 int hosono_gpu_set_tuning(hosono_handle* h, const hosono_tuning* t);
 int hosono_gpu_get_tuning(hosono_handle* h, hosono_tuning* t);
 

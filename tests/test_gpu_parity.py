@@ -149,6 +149,44 @@ def test_pass1_staging_bitwise(case, staging, tmp_par_dir):
     s.close()
 
 
+BANDED = {
+    "ot96_r2_b4": (lambda: parfiles.orszag_tang(96, 2), 4),
+    "sedov100_r2_b3": (lambda: parfiles.sedov(100, 2), 3),
+    "blast72_r3_b16": (lambda: parfiles.blast(72, 3, p_ratio=300.0, theta=0.4), 16),
+    "ot64_r1_b2": (lambda: parfiles.orszag_tang(64, 1), 2),
+}
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", sorted(BANDED))
+def test_advance_host_banded_upload(case, tmp_par_dir):
+    """hosono_gpu_advance_host with the upload in row bands overlapped with the
+    first stage's pass 1 (each band's tiles computed once its rows and halo
+    have landed): three steps equal the oracle bit for bit, and the same as
+    the unbanded call."""
+    m = pkg.load()
+    make, bands = BANDED[case]
+    par = parfiles.make(tmp_par_dir, case, make())
+    o = oracle.Oracle(par)
+    s = m.Solver.from_par(par, fp_mode=m.FP_STRICT)
+    s.set_tuning(upload_bands=bands)
+    assert s.tuning()["upload_bands"] == bands
+    U, V, _ = s.download()
+    for step in range(3):
+        dt = o.cfl()
+        assert s.cfl_computedt() == dt
+        o.advance(dt)
+        s.advance_host(dt, U, V)
+        np.testing.assert_array_equal(U, o.U())
+        np.testing.assert_array_equal(V, o.V())
+    _, _, S = s.download()
+    np.testing.assert_array_equal(S, o.scheme())
+    with pytest.raises(m.HosonoError):
+        s.set_tuning(upload_bands=m.UPLOAD_BANDS_MAX + 1)
+    s.close()
+    o.close()
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("case", ["ot32_r2", "sedov32_r2", "blast40_r2"])
 def test_advance_host_drop_in(case, tmp_par_dir):

@@ -116,6 +116,31 @@ def test_multi_tile_path_bitwise(staging, boxes, tmp_par_dir):
 
 
 @pytest.mark.gpu
+def test_advance_host_banded_ot1024(tmp_par_dir):
+    """The drop-in with host buffers on Orszag-Tang 1024^2, R=2, ell/Delta=12:
+    its 1032 array rows take the banded upload by default (8 bands, the
+    first stage's pass 1 overlapped with the copies); two steps of
+    cfl_computedt + advance_host equal the oracle bit for bit."""
+    m = pkg.load()
+    par = parfiles.make(tmp_par_dir, "ot1024_host", parfiles.orszag_tang(1024, 2, ell=12.0))
+    o = oracle.Oracle(par)
+    s = m.Solver.from_par(par, fp_mode=m.FP_STRICT)
+    assert s.tuning()["upload_bands"] == 0  # by size: banded from 1024 array rows
+    U, _, _ = s.download()
+    for _ in range(2):
+        dt = o.cfl()
+        assert s.cfl_computedt() == dt
+        o.advance(dt)
+        s.advance_host(dt, U)
+        np.testing.assert_array_equal(U, o.U())
+    _, V, S = s.download()
+    np.testing.assert_array_equal(V, o.V())
+    np.testing.assert_array_equal(S, o.scheme())
+    s.close()
+    o.close()
+
+
+@pytest.mark.gpu
 def test_t_end_gate_ot512_r2(tmp_par_dir):
     """Orszag-Tang 512^2, R=2, ell/Delta=12 to t_end = 0.5 from the CUDA
     graph: the accuracy gate (<= 1e-8 relative L1 on every conserved
