@@ -429,9 +429,14 @@ def bench_ours(args, rank, world, local):
                                         tune=not args.no_tune)
     served_kept = {}
     if world == 1 and args.serve_requests > 0:
+        import importlib
+        srv_mod = importlib.import_module("hosono_2dmhd_b200.serve")
+        pols = {"fifo": ("fifo", srv_mod.SERVE_FIFO, {}),
+                "shortest": ("shortest", srv_mod.SERVE_SHORTEST, SHORTEST_DEFAULTS)}
+        chosen = list(pols.values()) if args.serve_policy == "both" else [pols[args.serve_policy]]
         line["served"], served_kept = bench_served(m, fp, args.serve_requests, args.serve_check,
                                                    args.serve_calibrate, args.serve_sample, args.serve_hashes,
-                                                   args.serve_mean_work, args.serve_records)
+                                                   args.serve_mean_work, args.serve_records, policies=chosen)
     if not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         rate, el, nst = run_cpu_baseline(args.workload, 1, threads, to_end=args.to_end)
@@ -704,28 +709,28 @@ def bench_served(m, fp, requests, check, calibrate=0, sample=0, hashes_path=None
         out[name]["server"] = dict(policy=name, **kw)
         out[name]["mean_work_measured"] = rep["zone_updates"] / max(rep["completed"], 1)
         kept_by[name] = kept
-        if name == "fifo":
-            for k_ in keys:  # the default policy's figures at the top level
+        if name == policies[0][0]:
+            for k_ in keys:  # the first policy's figures at the top level
                 out[k_] = rep[k_]
-            fifo_infos = infos
-    out["policies_identical"] = all(np.array_equal(kept_by["fifo"][i], kept_by[n][i])
+            first_infos = infos
+    out["policies_identical"] = all(np.array_equal(kept_by[policies[0][0]][i], kept_by[n][i])
                                     for n, _, _ in policies for i in keep + sampled)
     if records_path:
         with open(records_path, "w") as f:
             json.dump([{k_: i[k_] for k_ in ("entry", "status", "nstep", "zone_updates", "submit_s", "admit_s",
-                                              "finish_s")} for i in fifo_infos], f)
+                                              "finish_s")} for i in first_infos], f)
     if sampled and hashes_path:
         recs = {}
-        for i in fifo_infos:
+        for i in first_infos:
             if i["entry"] in sampled:
-                U = kept_by["fifo"][i["entry"]]
+                U = kept_by[policies[0][0]][i["entry"]]
                 recs[str(i["entry"])] = {"sha256": hashlib.sha256(np.ascontiguousarray(U).tobytes()).hexdigest(),
                                          "nstep": i["nstep"], "t": i["t"], "zone_updates": i["zone_updates"]}
         with open(hashes_path, "w") as f:
             json.dump({"manifest": "served2000_seed1.json", "sample_seed": 2, "fp": "strict" if fp == 0 else "fast",
                        "requests": recs}, f, indent=1)
         out["sampled_hashes"] = {"file": os.path.basename(hashes_path), "requests": sampled}
-    return out, {e["id"]: (e, kept_by["fifo"][e["id"]]) for e in entries if e["id"] in keep}
+    return out, {e["id"]: (e, kept_by[policies[0][0]][e["id"]]) for e in entries if e["id"] in keep}
 
 
 # the shortest-first server's settings the bench runs
@@ -795,6 +800,8 @@ def main():
                     help="mean zone-updates per request of the stream when known from an earlier run (the "
                          "results, and so the work, are deterministic); else predicted from the calibration")
     ap.add_argument("--serve-records", default=None, help="output JSON of per-request work and timestamps")
+    ap.add_argument("--serve-policy", choices=("both", "fifo", "shortest"), default="both",
+                    help="scheduling policies the served stream runs under")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

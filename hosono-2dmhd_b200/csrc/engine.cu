@@ -708,9 +708,22 @@ int Engine::advance_host(int slot, double dt, double* U, double* V) {
     // one instance per engine, step graphs in use: otherwise upload, then step
     int liveCount = 0;
     for (const Slot& x : slots_) liveCount += x.live ? 1 : 0;
+    // a step that stops with an error leaves U as uploaded: V is rebuilt from
+    // it, so the device state stays consistent for the caller's next cfl
+    auto restore_v = [&](int rc) -> int {
+        const std::string m = msg;
+        if (write_field(slot, &InstState::stepping, 1) == HOSONO_OK) {
+            K_->cons2prim_all(batch(), s_);
+            launches++;
+            write_field(slot, &InstState::stepping, 0);
+        }
+        err = rc;
+        msg = m;
+        return rc;
+    };
     if (nb <= 1 || liveCount != 1 || !use_graphs || trace) {
         TRYE(upload_u(slot, U));
-        TRYE(advance(slot, dt));
+        if (int rc = advance(slot, dt)) return restore_v(rc);
         return download(slot, U, V, nullptr);
     }
     if (!sCopy_) {
@@ -759,7 +772,7 @@ int Engine::advance_host(int slot, double dt, double* U, double* V) {
     }
     CUE(cudaGetLastError());
     CUE(cudaGraphLaunch(gAdvRest_, s_));
-    TRYE(check_errors());
+    if (int rc = check_errors()) return restore_v(rc);
     return download(slot, U, V, nullptr);
 }
 

@@ -188,6 +188,34 @@ def test_advance_host_banded_upload(case, tmp_par_dir):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("bands", [1, 3])
+def test_advance_host_failed_step_keeps_state(bands, tmp_par_dir):
+    """A host-buffer step that stops with HOSONO_EMOODCAP (MOOD pass cap 1 on
+    a blast that needs several passes) leaves the caller's U untouched and
+    the device holding the uploaded U with its V: the next cfl_computedt is
+    the oracle's on that state."""
+    m = pkg.load()
+    par = parfiles.make(tmp_par_dir, f"capfail_{bands}", parfiles.blast(40, 2, p_ratio=1000.0, theta=0.3))
+    o = oracle.Oracle(par)
+    s = m.Solver.from_par(par, fp_mode=m.FP_STRICT)
+    s.set_tuning(upload_bands=bands)
+    o.advance(o.cfl())  # a state the device has not seen: one oracle step ahead
+    U1 = o.U().copy()
+    s.set_mood_cap(1)
+    U_in = U1.copy()
+    with pytest.raises(m.HosonoError) as e:
+        s.advance_host(o.cfl(), U_in)
+    assert e.value.code == m.EMOODCAP
+    np.testing.assert_array_equal(U_in, U1)
+    assert s.cfl_computedt() == o.cfl()
+    U_dev, V_dev, _ = s.download()
+    np.testing.assert_array_equal(U_dev, U1)
+    np.testing.assert_array_equal(V_dev, o.V())
+    s.close()
+    o.close()
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("case", ["ot32_r2", "sedov32_r2", "blast40_r2"])
 def test_advance_host_drop_in(case, tmp_par_dir):
     """hosono_gpu_advance_host, the form a driver that keeps grid_state on
