@@ -689,13 +689,13 @@ int Engine::upload_u(int slot, const double* U) {
 }
 
 // timeStep_advanceSolution on host arrays (mhd_driver.f90:117-144 with
-// grid_state on the host).  Banded form: every band's rows go up on sCopy_
-// back to back (one DMA stream); the main stream sets up the first stage
-// (scheme = R, flags: timeStep.f90:77-81), then per band waits for its rows,
-// converts them and runs pass 1 on the band's tile rows -- whose stencil
-// boxes reach R + 1 rows past the band, so a band's copy ends that far
-// beyond its last tile row -- and finally the step graph without the first
-// stage's set-up and pass 1.  Tiles are independent in pass 1, so the
+// grid_state on the host).  Banded form: the band copies go up on sCopy_
+// one after another (one DMA stream); the main stream sets up the first
+// stage (scheme = R, flags: timeStep.f90:77-81), then per band waits for its
+// rows, converts them and runs pass 1 on the band's tile rows -- whose
+// stencil boxes reach R + 1 rows past the band, so a band's copy ends that
+// far beyond its last tile row -- and finally the step graph without the
+// first stage's set-up and pass 1.  Tiles are independent in pass 1, so the
 // result bits do not depend on the banding.
 int Engine::advance_host(int slot, double dt, double* U, double* V) {
     if (slot < 0 || slot >= maxInst_ || !slots_[slot].live || !U) return fail(HOSONO_EINVAL, "bad advance_host");
@@ -741,34 +741,32 @@ int Engine::advance_host(int slot, double dt, double* U, double* V) {
     CUE(cudaEventRecord(bandEv_[HOSONO_UPLOAD_BANDS_MAX], s_));
     CUE(cudaStreamWaitEvent(sCopy_, bandEv_[HOSONO_UPLOAD_BANDS_MAX], 0));
     const size_t rowBytes = (size_t)G.nxt * NCONS * sizeof(double), rowDoubles = (size_t)G.nxt * NCONS;
-    const int R = G.R;
-    int rowEnd[HOSONO_UPLOAD_BANDS_MAX], trEnd[HOSONO_UPLOAD_BANDS_MAX];
-    for (int b = 0, r0 = 0; b < nb; b++) {
-        trEnd[b] = (int)((long long)tileRows * (b + 1) / nb);
-        const int want = b == nb - 1 ? G.nyt : trEnd[b] * TILE_Y + R + 1;  // last row a band's boxes read + 1
-        rowEnd[b] = want < G.nyt ? want : G.nyt;
-        if (rowEnd[b] < r0) rowEnd[b] = r0;
-        if (rowEnd[b] > r0)
-            CUE(cudaMemcpyAsync(staging_ + (size_t)r0 * rowDoubles, U + (size_t)r0 * rowDoubles,
-                                (size_t)(rowEnd[b] - r0) * rowBytes, cudaMemcpyHostToDevice, sCopy_));
-        CUE(cudaEventRecord(bandEv_[b], sCopy_));
-        r0 = rowEnd[b];
-    }
     const Batch B = batch();
     K_->stage_init(B, s_);
     launches++;
     const int base = instTiles_[slot].x;
+    // band by band: the copy on sCopy_, then on the main stream the wait,
+    // the conversion and pass 1 on the band's tile rows.  Interleaved, so
+    // that with a pageable host U (whose copies return only once the data
+    // has left it) a band's pass 1 is queued before the next band's copy.
     for (int b = 0, r0 = 0, tr0 = 0; b < nb; b++) {
+        const int tr1 = (int)((long long)tileRows * (b + 1) / nb);
+        const int want = b == nb - 1 ? G.nyt : tr1 * TILE_Y + G.R + 1;  // last row the band's boxes read + 1
+        const int r1 = want < G.nyt ? (want > r0 ? want : r0) : G.nyt;
+        if (r1 > r0)
+            CUE(cudaMemcpyAsync(staging_ + (size_t)r0 * rowDoubles, U + (size_t)r0 * rowDoubles,
+                                (size_t)(r1 - r0) * rowBytes, cudaMemcpyHostToDevice, sCopy_));
+        CUE(cudaEventRecord(bandEv_[b], sCopy_));
         CUE(cudaStreamWaitEvent(s_, bandEv_[b], 0));
-        launch_aos_to_soa_rows(G, staging_, sl.dev.U[st.parity], NCONS, r0, rowEnd[b], s_);
+        launch_aos_to_soa_rows(G, staging_, sl.dev.U[st.parity], NCONS, r0, r1, s_);
         if (b > 0) CUE(cudaMemsetAsync(d_flags_->p1Next, 0, sizeof d_flags_->p1Next, s_));
         Batch Bb = B;
         Bb.p1First = base + tr0 * tilesPerRow;
-        Bb.p1End = base + trEnd[b] * tilesPerRow;
+        Bb.p1End = base + tr1 * tilesPerRow;
         K_->face_pass1(Bb, ROLE_STATE, s_);
         launches += 1 + radii_held();
-        r0 = rowEnd[b];
-        tr0 = trEnd[b];
+        r0 = r1;
+        tr0 = tr1;
     }
     CUE(cudaGetLastError());
     CUE(cudaGraphLaunch(gAdvRest_, s_));
