@@ -518,9 +518,11 @@ def sweep_tuning(args):
 
 
 def sweep_later_passes(args):
-    """--sweep-later-passes: the later MOOD passes as a kernel chain and as one
-    persistent launch per stage, on the reference's runnable case to t_end,
-    Sedov 1024^2 (10 steps) and the blast64 batch; one JSON line each."""
+    """--sweep-launch: the step's launch forms -- the later MOOD passes as a
+    kernel chain (with and without programmatic dependent launches) and as
+    one persistent launch per stage -- on the reference's runnable case to
+    t_end, Sedov 1024^2 (10 steps), Orszag-Tang 2048^2 (5 steps) and the
+    blast64 batch; one JSON line each."""
     import torch
     m = load_pkg()
     problems = load_problems()
@@ -532,11 +534,12 @@ def sweep_later_passes(args):
         e1.record(stream)
         e1.synchronize()
         return e0.elapsed_time(e1), r
-    for later in (0, 1):
-        name = "persistent" if later else "kernels"
+    forms = [("kernels", dict(later_passes=0, pdl=0)), ("kernels+pdl", dict(later_passes=0, pdl=1)),
+             ("persistent", dict(later_passes=1, pdl=0))]
+    for name, tune in forms:
         with tempfile.TemporaryDirectory() as d:
             s = m.Solver.from_par(par_for("ot128_r1", d))
-            s.set_tuning(later_passes=later)
+            s.set_tuning(**tune)
             U0, V0, _ = s.download()
             s.run()
             s.upload(U0, V0)
@@ -547,7 +550,7 @@ def sweep_later_passes(args):
                               "ms_per_step": ms / n}), flush=True)
             import parfiles
             s = m.Solver.from_par(parfiles.make(d, "sedov1024", parfiles.sedov(1024, 2)))
-            s.set_tuning(later_passes=later)
+            s.set_tuning(**tune)
             s.set_time(0.0, 1e30, 0, 1 << 30)
             s.step(3)
             ms, _ = timed(torch.cuda.ExternalStream(s.stream()), lambda: s.step(10))
@@ -555,11 +558,19 @@ def sweep_later_passes(args):
             s.close()
             print(json.dumps({"later_passes": name, "workload": "sedov1024_r2, 10 steps", "ms_per_step": ms / 10,
                               "mood_passes": passes}), flush=True)
+            s = m.Solver.from_par(par_for("ot2048_r2", d))
+            s.set_tuning(**tune)
+            s.set_time(0.0, 1e30, 0, 1 << 30)
+            s.step(3)
+            ms, _ = timed(torch.cuda.ExternalStream(s.stream()), lambda: s.step(5))
+            s.close()
+            print(json.dumps({"later_passes": name, "workload": "ot2048_r2, 5 steps", "ms_per_step": ms / 5}),
+                  flush=True)
             with open(os.path.join(ROOT, "hosono-2dmhd_b200", "workloads", "blast64_seed0.json")) as f:
                 entries = json.load(f)["instances"]
             pars = [problems.make(d, f"i{e['id']}", problems.from_entry(e)) for e in entries]
             b = m.Batch(len(pars), sum(m.Batch.tiles_for(m.par_load(p)[0]) for p in pars))
-            b.set_tuning(later_passes=later)
+            b.set_tuning(**tune)
             slots = [b.add_par(p) for p in pars]
             b.run(max_steps=1)
             ms, _ = timed(torch.cuda.ExternalStream(b.stream()), lambda: b.run())
@@ -773,8 +784,9 @@ def main():
     ap.add_argument("--fp", default="strict", choices=["strict", "fast"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="keep the default launch choices (no autotuning)")
-    ap.add_argument("--sweep-later-passes", action="store_true",
-                    help="time the later MOOD passes as a kernel chain and as one persistent launch, and exit")
+    ap.add_argument("--sweep-launch", "--sweep-later-passes", dest="sweep_later_passes", action="store_true",
+                    help="time the step's launch forms (kernel chain, with programmatic dependent launches, one "
+                         "persistent later-pass launch) and exit")
     ap.add_argument("--sweep-tuning", action="store_true",
                     help="time every pass-1 launch choice on the workload (whole steps and pass 1) and exit")
     ap.add_argument("--tuning", default=None,

@@ -44,6 +44,19 @@ namespace hosono {
         if (rc_) return rc_; \
     } while (0)
 
+namespace {
+thread_local bool tl_pdl_next = false, tl_pdl_chain = false;
+}  // namespace
+void pdl_arm(bool first, bool chain) {
+    tl_pdl_next = first;
+    tl_pdl_chain = chain;
+}
+bool pdl_take() {
+    const bool r = tl_pdl_next;
+    tl_pdl_next = tl_pdl_chain;
+    return r;
+}
+
 int Engine::fail(int code, const char* fmt, ...) {
     char buf[512];
     va_list ap;
@@ -68,6 +81,7 @@ class Engine::Rec {
                                                           deps_.size(), cudaStreamCaptureModeThreadLocal);
             if (r != cudaSuccess) return e_->fail(HOSONO_ECUDA, "begin capture: %s", cudaGetErrorString(r));
             open_ = true;
+            afterKernel_ = false;  // the segment's first launch depends on nodes of an earlier segment
         }
         return HOSONO_OK;
     }
@@ -87,10 +101,16 @@ class Engine::Rec {
         }
         return HOSONO_OK;
     }
+    // a kernel launch (or a few in a row): programmatic when the tuning asks
+    // for it and the previous operation recorded was a kernel launch too
     template <class F>
     int k(F&& f) {
         TRYE(begin());
+        const bool pdl = e_->tune_.pdl != 0;
+        pdl_arm(pdl && afterKernel_, pdl);
         f(e_->s_);
+        pdl_arm(false, false);
+        afterKernel_ = true;
         if (!g_) e_->launches++;
         cudaError_t r = cudaGetLastError();
         if (r != cudaSuccess) return e_->fail(HOSONO_ECUDA, "kernel launch: %s", cudaGetErrorString(r));
@@ -98,6 +118,7 @@ class Engine::Rec {
     }
     int event(cudaEvent_t ev) {
         TRYE(begin());
+        afterKernel_ = false;
         // External: under capture this becomes an event-record node of the graph
         cudaError_t r = g_ ? cudaEventRecordWithFlags(ev, e_->s_, cudaEventRecordExternal) : cudaEventRecord(ev, e_->s_);
         if (r != cudaSuccess) return e_->fail(HOSONO_ECUDA, "event record: %s", cudaGetErrorString(r));
@@ -117,6 +138,7 @@ class Engine::Rec {
     int loop(cudaGraphConditionalHandle h, int BatchFlags::*field, long long cap, Body&& body) {
         if (!g_) {
             TRYE(e_->sync());
+            afterKernel_ = false;
             long long it = 0;
             while (e_->h_flags_->*field) {
                 if (++it > cap) return e_->fail(HOSONO_EMOODCAP, "loop exceeded %lld iterations", cap);
@@ -138,12 +160,14 @@ class Engine::Rec {
         TRYE(body(sub));
         TRYE(sub.end());
         deps_.assign(1, node);
+        afterKernel_ = false;
         return HOSONO_OK;
     }
     template <class H>
     int host(H&& h) {
         if (g_) return HOSONO_OK;
         TRYE(e_->sync());
+        afterKernel_ = false;  // h may queue copies
         return h();
     }
 
@@ -152,6 +176,7 @@ class Engine::Rec {
     cudaGraph_t g_;
     std::vector<cudaGraphNode_t> deps_;
     bool open_ = false;
+    bool afterKernel_ = false;  // the last operation recorded was a kernel launch
 };
 
 // ----------------------------------------------------------------------
@@ -296,6 +321,7 @@ int Engine::set_tuning(const hosono_tuning& t) {
         return fail(HOSONO_EINVAL, "pass1_boxes %d (0, 1 or 2)", t.pass1_boxes);
     if (t.pass1_boxes == 2 && t.pass1_blocks_per_sm > 2)
         return fail(HOSONO_EINVAL, "two stencil boxes run at two pass-1 blocks per SM");
+    if (t.pdl != 0 && t.pdl != 1) return fail(HOSONO_EINVAL, "pdl %d (0 or 1)", t.pdl);
     if (t.upload_bands < 0 || t.upload_bands > HOSONO_UPLOAD_BANDS_MAX)
         return fail(HOSONO_EINVAL, "upload_bands %d (0..%d)", t.upload_bands, HOSONO_UPLOAD_BANDS_MAX);
     tune_ = t;
@@ -334,6 +360,7 @@ int Engine::autotune(int trials, bool force, hosono_tune_report* rep) {
             r.best = it->second;
             r.best.later_passes = tune_.later_passes;  // the caller's choices stay
             r.best.upload_bands = tune_.upload_bands;
+            r.best.pdl = tune_.pdl;
             if (rep) *rep = r;
             return set_tuning(r.best);
         }

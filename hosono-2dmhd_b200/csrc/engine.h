@@ -241,6 +241,13 @@ const KernelSet* kernelset_strict();
 const KernelSet* kernelset_fast();
 
 // layout conversions for one instance (no arithmetic; one build)
+// Programmatic dependent launch of the next kernel launch on this host
+// thread: pdl_arm(first, chain) before a step's launches (first: the next
+// launch may overlap its predecessor; chain: the launches after it too),
+// pdl_take() in each launch helper.  Off outside the step recorder.
+void pdl_arm(bool first, bool chain);
+bool pdl_take();
+
 void launch_aos_to_soa(const Geo& G, const double* aos, double* soa, int nvar, cudaStream_t s);
 void launch_aos_to_soa_rows(const Geo& G, const double* aos, double* soa, int nvar, int j0, int j1, cudaStream_t s);
 void launch_soa_to_aos(const Geo& G, const double* soa, double* aos, int nvar, cudaStream_t s);

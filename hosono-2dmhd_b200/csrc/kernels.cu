@@ -179,6 +179,19 @@ __device__ __forceinline__ int rec_sel(const Batch& B, bool next) { return B.fla
 __device__ __forceinline__ int2* rec_list(const Batch& B, bool next) { return rec_sel(B, next) ? B.L.rec2 : B.L.rec; }
 __device__ __forceinline__ int rec_count(const Batch& B, bool next) { return rec_sel(B, next) ? LIST_REC2 : LIST_REC; }
 
+// Programmatic dependent launch.  A kernel launched with
+// cudaLaunchAttributeProgrammaticStreamSerialization may be scheduled while
+// its predecessor on the stream still runs: every block first waits here,
+// before it touches memory, until the predecessor grid has completed and its
+// writes are visible, then lets its own successor be scheduled (whose blocks
+// wait here in turn, so at most two grids are resident and the earlier one
+// has all its blocks running).  Without the attribute both are no-ops.
+#define PDL_ENTRY()                                                     \
+    do {                                                                \
+        asm volatile("griddepcontrol.wait;\n" ::: "memory");             \
+        asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory"); \
+    } while (0)
+
 // ======================================================================
 // MOOD pass 1 (every scheme == R): reconstruct_faceValsWithGP + face CAD/PAD
 // + getFluxes_ fused.  A thread owns the x-face between (i-1,j) and (i,j) and
@@ -455,7 +468,7 @@ struct P1Smem {  // dynamic shared memory layout (doubles): boxes, accumulators,
     }
 };
 template <int R, bool TMA, bool DYN, int MINB, int NBUF>
-__global__ void __launch_bounds__(NTHREADS, MINB) k_face_pass1(Batch B, int uin) {
+__global__ void __launch_bounds__(NTHREADS, MINB) k_face_pass1(Batch B, int uin) { PDL_ENTRY();
     static_assert(NBUF == 1 || NBUF == 2, "one or two stencil boxes");
     extern __shared__ __align__(128) double smem[];
     __shared__ int sTile;  // the dynamic schedule's tile, as thread 0 took it
@@ -637,7 +650,7 @@ __device__ __forceinline__ void d_cascade_cond(const Batch& B, int tid, cudaGrap
     }
 }
 __global__ void __launch_bounds__(PASS_END_THREADS) k_cascade_cond(Batch B, cudaGraphConditionalHandle h,
-                                                                      int set_handle) {
+                                                                      int set_handle) { PDL_ENTRY();
     d_cascade_cond<PASS_END_THREADS>(B, threadIdx.x, h, set_handle);
 }
 
@@ -704,7 +717,7 @@ __device__ __forceinline__ void t_cascade_lower(const Batch& B, const Cell c) {
     if (first) d.detMask[cc] |= DM_CASC;
     warp_append(B.L, LIST_CASC, B.L.casc, B.L.cap, first, entry(c.k, cc));
 }
-__global__ void __launch_bounds__(NTHREADS) k_cascade_lower(Batch B) {
+__global__ void __launch_bounds__(NTHREADS) k_cascade_lower(Batch B) { PDL_ENTRY();
     FOR_CASCADE_TILES(B, t) t_cascade_lower(B, tile_at(B, t));
 }
 
@@ -781,7 +794,7 @@ __device__ __forceinline__ void t_compact_next(const Batch& B, const Cell c) {
     }
     warp_append(B.L, LIST_NEXT, B.L.next, B.L.cap, p, entry(c.k, cc));
 }
-__global__ void __launch_bounds__(NTHREADS) k_compact_next(Batch B) {
+__global__ void __launch_bounds__(NTHREADS) k_compact_next(Batch B) { PDL_ENTRY();
     FOR_CASCADE_TILES(B, t) t_compact_next(B, tile_at(B, t));
 }
 // ... and re-reconstruct them (list `which`: LIST_NEXT in the cascade,
@@ -797,7 +810,7 @@ __device__ __forceinline__ void d_recon_group(const Batch& B, int uin, int which
         if (act && sub == 0 && bad) atomicOr(&S.anyFail, 1);
     }
 }
-__global__ void __launch_bounds__(256, 2) k_recon_group(Batch B, int uin, int which) {
+__global__ void __launch_bounds__(256, 2) k_recon_group(Batch B, int uin, int which) { PDL_ENTRY();
     d_recon_group(B, uin, which, GT1, GS1);
 }
 
@@ -826,7 +839,7 @@ __device__ __forceinline__ void t_compact_post(const Batch& B, const Cell c) {
     warp_append(B.L, LIST_FACE, B.L.face, 2 * B.L.cap, py, make_int2(c.k, (int)(2 * cc + YDIR)));
     warp_append(B.L, LIST_RECF, B.L.recF, B.L.cap, pf, entry(c.k, cc));
 }
-__global__ void __launch_bounds__(NTHREADS) k_compact_post(Batch B) {
+__global__ void __launch_bounds__(NTHREADS) k_compact_post(Batch B) { PDL_ENTRY();
     FOR_ACTIVE_TILES(B, t) t_compact_post(B, tile_at(B, t));
 }
 
@@ -849,7 +862,7 @@ __device__ __forceinline__ void t_compact_dirty(const Batch& B, const Cell c) {
     warp_append(B.L, LIST_FACE, B.L.face, 2 * B.L.cap, px, make_int2(c.k, (int)(2 * cc + XDIR)));
     warp_append(B.L, LIST_FACE, B.L.face, 2 * B.L.cap, py, make_int2(c.k, (int)(2 * cc + YDIR)));
 }
-__global__ void __launch_bounds__(NTHREADS) k_compact_dirty(Batch B) {
+__global__ void __launch_bounds__(NTHREADS) k_compact_dirty(Batch B) { PDL_ENTRY();
     FOR_TILES(B, t) t_compact_dirty(B, tile_at(B, t));
 }
 
@@ -925,7 +938,7 @@ __device__ __forceinline__ void d_flux_list(const Batch& B, int uin, int gt, int
         }
     }
 }
-__global__ void __launch_bounds__(256, 2) k_flux_list(Batch B, int uin) { d_flux_list(B, uin, GT1, GS1); }
+__global__ void __launch_bounds__(256, 2) k_flux_list(Batch B, int uin) { PDL_ENTRY(); d_flux_list(B, uin, GT1, GS1); }
 
 // ======================================================================
 // FLICDdivB_fluxCorrections (FLICDdivB.f90:13-70) from fluxRaw.
@@ -1159,7 +1172,7 @@ __device__ __forceinline__ void t_ct_update_detect(const Batch& B, int uin, int 
 // cell's corrected fluxes once into shared memory (instead of a cell also
 // evaluating its east and north neighbours' FLICD) made a launch about 5 %
 // slower: the extra barrier costs more than the loads it saves, which hit L1.
-__global__ void __launch_bounds__(NTHREADS, 6) k_ct_update_detect(Batch B, int uin, int uout) {
+__global__ void __launch_bounds__(NTHREADS, 6) k_ct_update_detect(Batch B, int uin, int uout) { PDL_ENTRY();
     __shared__ double sV[4 * DP_SX * DP_SY];
     FOR_TILES(B, t) t_ct_update_detect(B, uin, uout, tile_at(B, t), sV);
 }
@@ -1182,7 +1195,7 @@ __device__ __forceinline__ void d_ct_list(const Batch& B, int uin, int uout, int
         warp_append(B.L, LIST_LOW, B.L.low, B.L.cap, low, it);
     }
 }
-__global__ void __launch_bounds__(256) k_ct_list(Batch B, int uin, int uout) { d_ct_list(B, uin, uout, GT1, GS1); }
+__global__ void __launch_bounds__(256) k_ct_list(Batch B, int uin, int uout) { PDL_ENTRY(); d_ct_list(B, uin, uout, GT1, GS1); }
 
 // `lowered` back to zero on the cells this pass lowered
 __device__ __forceinline__ void d_clear_low(const Batch& B, int gt, int gs) {
@@ -1192,7 +1205,7 @@ __device__ __forceinline__ void d_clear_low(const Batch& B, int gt, int gs) {
         B.dev[it.x].lowered[it.y] = 0;
     }
 }
-__global__ void __launch_bounds__(256) k_clear_low(Batch B) { d_clear_low(B, GT1, GS1); }
+__global__ void __launch_bounds__(256) k_clear_low(Batch B) { PDL_ENTRY(); d_clear_low(B, GT1, GS1); }
 
 // ======================================================================
 // After detect: recompute = cross of lowered cells, recomputeFLICD = radius-2
@@ -1260,7 +1273,7 @@ __device__ __forceinline__ void t_mood_flags(const Batch& B, const Cell c) {
 }
 // eight resident blocks (32 registers): a latency-bound byte-gather over the
 // lowered flags, faster with more warps in flight
-__global__ void __launch_bounds__(NTHREADS, 8) k_mood_flags(Batch B) {
+__global__ void __launch_bounds__(NTHREADS, 8) k_mood_flags(Batch B) { PDL_ENTRY();
     FOR_TILES(B, t) t_mood_flags(B, tile_at(B, t));
 }
 
@@ -1326,7 +1339,7 @@ __device__ __forceinline__ void d_flags_clear(const Batch& B, int gt, int gs) {
         }
     }
 }
-__global__ void __launch_bounds__(256) k_flags_clear(Batch B) { d_flags_clear(B, GT1, GS1); }
+__global__ void __launch_bounds__(256) k_flags_clear(Batch B) { PDL_ENTRY(); d_flags_clear(B, GT1, GS1); }
 __device__ __forceinline__ void d_flags_scatter(const Batch& B, int gt, int gs) {
     const int nL = min(B.L.counts[LIST_LOW], (int)B.L.cap);
     const int nC = min(B.L.counts[LIST_CASC], (int)B.L.cap);
@@ -1369,7 +1382,7 @@ __device__ __forceinline__ void d_flags_scatter(const Batch& B, int gt, int gs) 
         B.L.sync[e] = (int8_t)s;
     }
 }
-__global__ void __launch_bounds__(256) k_flags_scatter(Batch B) { d_flags_scatter(B, GT1, GS1); }
+__global__ void __launch_bounds__(256) k_flags_scatter(Batch B) { PDL_ENTRY(); d_flags_scatter(B, GT1, GS1); }
 __device__ __forceinline__ void d_scheme_sync(const Batch& B, int clear_low, int gt, int gs) {
     const int nL = min(B.L.counts[LIST_LOW], (int)B.L.cap);
     const int nC = min(B.L.counts[LIST_CASC], (int)B.L.cap);
@@ -1397,7 +1410,7 @@ __device__ __forceinline__ void d_scheme_sync(const Batch& B, int clear_low, int
         if (fromLow && clear_low) d.lowered[c0] = 0;  // k_flags_scatter has read it
     }
 }
-__global__ void __launch_bounds__(256) k_scheme_sync(Batch B, int clear_low) {
+__global__ void __launch_bounds__(256) k_scheme_sync(Batch B, int clear_low) { PDL_ENTRY();
     d_scheme_sync(B, clear_low, GT1, GS1);
 }
 
@@ -1452,7 +1465,7 @@ __device__ __forceinline__ void d_pass_end(const Batch& B, int tid, cudaGraphCon
     }
 }
 __global__ void __launch_bounds__(PASS_END_THREADS) k_pass_end(Batch B, cudaGraphConditionalHandle h, int set_handle,
-                                                                int flip) {
+                                                                int flip) { PDL_ENTRY();
     d_pass_end<PASS_END_THREADS>(B, threadIdx.x, h, set_handle, flip);
 }
 
@@ -1483,7 +1496,7 @@ __device__ __forceinline__ void t_stage_init(const Batch& B, const Cell c) {
     d.dirty[cc] = 0;
     d.innerCount[cc] = 0;
 }
-__global__ void __launch_bounds__(NTHREADS) k_stage_init(Batch B) {
+__global__ void __launch_bounds__(NTHREADS) k_stage_init(Batch B) { PDL_ENTRY();
     if (blockIdx.x == 0 && threadIdx.x == 0 && threadIdx.y == 0) {  // the recompute lists start empty
         B.L.counts[LIST_REC] = 0;
         B.L.counts[LIST_REC2] = 0;
@@ -1514,7 +1527,7 @@ __device__ __forceinline__ void t_bc_fill(const Batch& B, int role, const Cell c
 #pragma unroll
     for (int v = 0; v < NCONS; v++) A[v * G.plane + cc] = A[v * G.plane + s];
 }
-__global__ void __launch_bounds__(NTHREADS) k_bc_fill(Batch B, int role) {
+__global__ void __launch_bounds__(NTHREADS) k_bc_fill(Batch B, int role) { PDL_ENTRY();
     FOR_TILES(B, t) t_bc_fill(B, role, tile_at(B, t));
 }
 
@@ -1533,7 +1546,7 @@ __device__ __forceinline__ void t_rk_combine2(const Batch& B, const Cell c) {
 #pragma unroll
     for (int v = 0; v < NCONS; v++) out[v * G.plane + cc] = (3 * Un[v * G.plane + s] + Bb[v * G.plane + s]) / 4.0;
 }
-__global__ void __launch_bounds__(NTHREADS) k_rk_combine2(Batch B) {
+__global__ void __launch_bounds__(NTHREADS) k_rk_combine2(Batch B) { PDL_ENTRY();
     FOR_TILES(B, t) t_rk_combine2(B, tile_at(B, t));
 }
 
@@ -1561,7 +1574,7 @@ __device__ __forceinline__ void t_rk_final(const Batch& B, const Cell c) {
     for (int v = 0; v < NPRIM; v++) d.V[v * G.plane + cc] = V[v];
 }
 // six resident blocks (40 registers) for more loads in flight
-__global__ void __launch_bounds__(NTHREADS, 6) k_rk_final(Batch B) {
+__global__ void __launch_bounds__(NTHREADS, 6) k_rk_final(Batch B) { PDL_ENTRY();
     FOR_TILES(B, t) t_rk_final(B, tile_at(B, t));
 }
 
@@ -1581,7 +1594,7 @@ __device__ __forceinline__ void t_cons2prim_all(const Batch& B, const Cell c) {
 #pragma unroll
     for (int v = 0; v < NPRIM; v++) d.V[v * G.plane + cc] = w[v];
 }
-__global__ void __launch_bounds__(NTHREADS) k_cons2prim_all(Batch B) {
+__global__ void __launch_bounds__(NTHREADS) k_cons2prim_all(Batch B) { PDL_ENTRY();
     FOR_TILES(B, t) t_cons2prim_all(B, tile_at(B, t));
 }
 
@@ -1636,14 +1649,14 @@ __device__ __forceinline__ void t_cfl_reduce(const Batch& B, const Cell c) {
     }
     __syncthreads();  // sx/sy are reused by the block's next tile
 }
-__global__ void __launch_bounds__(NTHREADS) k_cfl_reduce(Batch B) {
+__global__ void __launch_bounds__(NTHREADS) k_cfl_reduce(Batch B) { PDL_ENTRY();
     FOR_TILES(B, t) t_cfl_reduce(B, tile_at(B, t));
 }
 
 // Step begin: dt = cfl * min(dx/xmax, dy/ymax) (cfl.f90:50) and validTimeStep
 // (mhd_driver.f90:117-144: clamp to tmax first, then reject negative, NaN or
 // infinite dt).  With use_host_dt the host already stored dt.
-__global__ void k_step_begin(Batch B, int use_host_dt) {
+__global__ void k_step_begin(Batch B, int use_host_dt) { PDL_ENTRY();
     for (int k = threadIdx.x; k < B.maxInst; k += blockDim.x) {
         InstState& S = B.st[k];
         if (!S.stepping) continue;
@@ -1665,7 +1678,7 @@ __global__ void k_step_begin(Batch B, int use_host_dt) {
 
 // Step start: which instances take part, fresh CFL accumulators.  (The step
 // budget flags->stepsLeft is set by the host before each run launch.)
-__global__ void k_step_prepare(Batch B, int /*unused*/) {
+__global__ void k_step_prepare(Batch B, int /*unused*/) { PDL_ENTRY();
     for (int k = threadIdx.x; k < B.maxInst; k += blockDim.x) {
         InstState& S = B.st[k];
         S.stepping = (S.live && !S.done && !B.hold[k]) ? 1 : 0;
@@ -1677,7 +1690,7 @@ __global__ void k_step_prepare(Batch B, int /*unused*/) {
 // Step end: the new state is buffer A (parity flips), t += dt, nstep += 1,
 // and the time-loop test of mhd_driver.f90:76; next step's participants and
 // the batch condition.
-__global__ void k_step_end(Batch B, cudaGraphConditionalHandle h, int set_handle) {
+__global__ void k_step_end(Batch B, cudaGraphConditionalHandle h, int set_handle) { PDL_ENTRY();
     __shared__ int any;
     if (threadIdx.x == 0) any = 0;
     __syncthreads();
@@ -1804,7 +1817,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_mood_rest(Batch B, int uin, int
 // The autotuner times pass 1 between steps: the instances that would step
 // are marked stepping, and put back at rest afterwards (the face-cascade
 // flag pass 1 raised is cleared too; every stage starts from stage_init).
-__global__ void k_tune_mark(Batch B, int on) {
+__global__ void k_tune_mark(Batch B, int on) { PDL_ENTRY();
     for (int k = threadIdx.x; k < B.maxInst; k += blockDim.x) {
         InstState& S = B.st[k];
         S.stepping = (on && S.live && !S.done && !B.hold[k]) ? 1 : 0;
@@ -1842,14 +1855,33 @@ dim3 grid_for(K kernel, const Batch& B) {
     const int r = resident_blocks((const void*)kernel);
     return dim3((unsigned)(r < B.maxTiles ? r : B.maxTiles));
 }
-#define TILE_LAUNCH(kern, B, s, ...) kern<<<grid_for(kern, B), kTile, 0, s>>>(B, ##__VA_ARGS__)
-#define LIST_LAUNCH(kern, B, s, ...) kern<<<dim3((unsigned)resident_blocks((const void*)kern)), dim3(256), 0, s>>>(B, ##__VA_ARGS__)
+// launch kern on s; programmatic (PDL_ENTRY) when the engine asked for it
+// for this launch (pdl_take: the recorder's choice for the kernels of a step)
+template <typename... KArgs, typename... Args>
+void lk(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    if (pdl_take()) {
+        attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attr[0].val.programmaticStreamSerializationAllowed = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+    }
+    cudaLaunchKernelEx(&cfg, kern, args...);
+}
+#define TILE_LAUNCH(kern, B, s, ...) lk(kern, grid_for(kern, B), kTile, 0, s, B, ##__VA_ARGS__)
+#define LIST_LAUNCH(kern, B, s, ...) \
+    lk(kern, dim3((unsigned)resident_blocks((const void*)kern)), dim3(256), 0, s, B, ##__VA_ARGS__)
 
 void l_cfl_reduce(const Batch& B, cudaStream_t s) { TILE_LAUNCH(k_cfl_reduce, B, s); }
-void l_step_prepare(const Batch& B, int steps, cudaStream_t s) { k_step_prepare<<<1, 128, 0, s>>>(B, steps); }
-void l_step_begin(const Batch& B, int use_host_dt, cudaStream_t s) { k_step_begin<<<1, 128, 0, s>>>(B, use_host_dt); }
+void l_step_prepare(const Batch& B, int steps, cudaStream_t s) { lk(k_step_prepare, dim3(1), dim3(128), 0, s, B, steps); }
+void l_step_begin(const Batch& B, int use_host_dt, cudaStream_t s) { lk(k_step_begin, dim3(1), dim3(128), 0, s, B, use_host_dt); }
 void l_step_end(const Batch& B, cudaGraphConditionalHandle h, cudaStream_t s) {
-    k_step_end<<<1, 128, 0, s>>>(B, h, h != 0);
+    lk(k_step_end, dim3(1), dim3(128), 0, s, B, h, (int)(h != 0));
 }
 void l_stage_init(const Batch& B, cudaStream_t s) { TILE_LAUNCH(k_stage_init, B, s); }
 // dynamic shared memory of a pass-1 kernel variant
@@ -1868,8 +1900,8 @@ int pass1_grid(int maxTiles) {
 }
 template <int R, bool TMA, bool DYN, int MINB, int NBUF>
 void launch_pass1_v(const Batch& B, int uin, cudaStream_t s) {
-    k_face_pass1<R, TMA, DYN, MINB, NBUF><<<dim3((unsigned)pass1_grid<R, TMA, DYN, MINB, NBUF>(B.maxTiles)), kTile,
-                                            pass1_smem<R, NBUF>(), s>>>(B, uin);
+    lk(k_face_pass1<R, TMA, DYN, MINB, NBUF>, dim3((unsigned)pass1_grid<R, TMA, DYN, MINB, NBUF>(B.maxTiles)), kTile,
+       (size_t)pass1_smem<R, NBUF>(), s, B, uin);
 }
 template <int R, int MINB, int NBUF>
 void launch_pass1_s(const Batch& B, int uin, cudaStream_t s) {  // staging and schedule
@@ -1913,7 +1945,7 @@ void l_face_pass1(const Batch& B, int uin, cudaStream_t s) {
     if (B.p1Radii & (1 << 3)) launch_pass1<3>(B, uin, s);
 }
 void l_cascade_cond(const Batch& B, cudaGraphConditionalHandle h, cudaStream_t s) {
-    k_cascade_cond<<<1, PASS_END_THREADS, 0, s>>>(B, h, h != 0);
+    lk(k_cascade_cond, dim3(1), dim3(PASS_END_THREADS), 0, s, B, h, (int)(h != 0));
 }
 void l_cascade_lower(const Batch& B, int /*later*/, cudaStream_t s) { TILE_LAUNCH(k_cascade_lower, B, s); }
 void l_recon_check(const Batch& B, int uin, int /*later*/, cudaStream_t s) {
@@ -1933,7 +1965,7 @@ void l_mood_flags(const Batch& B, int mode, cudaStream_t s) {
     }
 }
 void l_pass_end(const Batch& B, cudaGraphConditionalHandle h, int flip, cudaStream_t s) {
-    k_pass_end<<<1, PASS_END_THREADS, 0, s>>>(B, h, h != 0, flip);
+    lk(k_pass_end, dim3(1), dim3(PASS_END_THREADS), 0, s, B, h, (int)(h != 0), flip);
 }
 void l_compact_post(const Batch& B, cudaStream_t s) { TILE_LAUNCH(k_compact_post, B, s); }
 void l_compact_dirty(const Batch& B, cudaStream_t s) { TILE_LAUNCH(k_compact_dirty, B, s); }
@@ -1945,7 +1977,7 @@ void l_bc_fill(const Batch& B, int role, cudaStream_t s) { TILE_LAUNCH(k_bc_fill
 void l_rk_combine2(const Batch& B, cudaStream_t s) { TILE_LAUNCH(k_rk_combine2, B, s); }
 void l_rk_final(const Batch& B, cudaStream_t s) { TILE_LAUNCH(k_rk_final, B, s); }
 void l_cons2prim_all(const Batch& B, cudaStream_t s) { TILE_LAUNCH(k_cons2prim_all, B, s); }
-void l_tune_mark(const Batch& B, int on, cudaStream_t s) { k_tune_mark<<<1, 128, 0, s>>>(B, on); }
+void l_tune_mark(const Batch& B, int on, cudaStream_t s) { lk(k_tune_mark, dim3(1), dim3(128), 0, s, B, on); }
 // every block resident at once: a cooperative launch of as many blocks as
 // fit on the GPU (never more, or a barrier could not complete)
 void l_mood_rest(const Batch& B, int uin, int uout, cudaStream_t s) {

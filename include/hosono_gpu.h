@@ -323,7 +323,10 @@ typedef struct hosono_tuning {
     int upload_bands;         /* hosono_gpu_advance_host: row bands of the overlapped upload (0 = by size:
                                  8 from 1024 array rows up, else 1; 1 = upload, then step; at most
                                  HOSONO_UPLOAD_BANDS_MAX) */
-    int pad[2];               /* zero */
+    int pdl;                  /* 1: the step's kernels are launched as programmatic dependent launches
+                                 (each may be scheduled while its predecessor drains and waits on
+                                 the GPU for its completion); 0: plain stream order */
+    int pad[1];               /* zero */
 } hosono_tuning;
 #define HOSONO_UPLOAD_BANDS_MAX 16
 int hosono_gpu_set_tuning(hosono_handle* h, const hosono_tuning* t);

@@ -149,3 +149,54 @@ def test_persistent_later_passes_batch(tmp_par_dir):
         np.testing.assert_array_equal(U, o.U())
         np.testing.assert_array_equal(S, o.scheme())
     b.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("graphs", [True, False])
+@pytest.mark.parametrize("case", sorted(PERSISTENT_CASES))
+def test_programmatic_launch_bitwise(case, graphs, tmp_par_dir):
+    """The step's kernels as programmatic dependent launches (each waits on
+    the GPU for its predecessor before touching memory) give the oracle's
+    bits, from the step graph and from host launches."""
+    m = pkg.load()
+    par = parfiles.make(tmp_par_dir, f"pdl_{case}_{int(graphs)}", PERSISTENT_CASES[case]())
+    o = oracle.Oracle(par)
+    s = m.Solver.from_par(par, fp_mode=m.FP_STRICT)
+    s.set_tuning(pdl=1)
+    assert s.tuning()["pdl"] == 1
+    s.set_graphs(graphs)
+    s.set_time(0.0, o.tmax, 0, 1 << 30)
+    for chunk in (1, 4):
+        for _ in range(chunk):
+            o.advance(o.cfl())
+        s.step(chunk)
+        U, V, S = s.download()
+        np.testing.assert_array_equal(U, o.U())
+        np.testing.assert_array_equal(V, o.V())
+        np.testing.assert_array_equal(S, o.scheme())
+    s.close()
+
+
+@pytest.mark.gpu
+def test_programmatic_launch_batch(tmp_par_dir):
+    """Programmatic dependent launches over a batch of uneven MOOD-active
+    instances: each equals its own oracle run."""
+    m = pkg.load()
+    kvs = [parfiles.blast(64, 2, p_ratio=300.0, theta=0.2), parfiles.orszag_tang(48, 1),
+           parfiles.blast(96, 2, p_ratio=30.0, theta=1.1), parfiles.sedov(40, 2)]
+    pars = [parfiles.make(tmp_par_dir, f"pdlb{i}", kv) for i, kv in enumerate(kvs)]
+    tiles = sum(m.Batch.tiles_for(m.par_load(p)[0]) for p in pars)
+    b = m.Batch(len(pars), tiles, fp_mode=m.FP_STRICT)
+    b.set_tuning(pdl=1)
+    slots = [b.add_par(p) for p in pars]
+    for k in slots:
+        b.set_time(k, 0.0, 1e30)
+    b.run(max_steps=3)
+    for k, p in zip(slots, pars):
+        o = oracle.Oracle(p)
+        for _ in range(3):
+            o.advance(o.cfl())
+        U, V, S = b.download(k)
+        np.testing.assert_array_equal(U, o.U())
+        np.testing.assert_array_equal(S, o.scheme())
+    b.close()
