@@ -101,9 +101,9 @@ class Tuning(ctypes.Structure):
     _fields_ = [("pass1_staging", ctypes.c_int), ("pass1_schedule", ctypes.c_int),
                 ("pass1_blocks_per_sm", ctypes.c_int), ("later_passes", ctypes.c_int),
                 ("pass1_boxes", ctypes.c_int), ("upload_bands", ctypes.c_int), ("pdl", ctypes.c_int),
-                ("pad", ctypes.c_int * 1)]
+                ("update_staging", ctypes.c_int)]
     KEYS = ("pass1_staging", "pass1_schedule", "pass1_blocks_per_sm", "later_passes", "pass1_boxes", "upload_bands",
-            "pdl")
+            "pdl", "update_staging")
 
     def as_dict(self):
         return {k: getattr(self, k) for k in self.KEYS}

@@ -288,12 +288,20 @@ int Engine::encode_tmaps(InstDev& dev) {
     const cuuint64_t strides[2] = {(cuuint64_t)G.pitch * sizeof(double), (cuuint64_t)G.plane * sizeof(double)};
     const cuuint32_t box[3] = {(cuuint32_t)P1_SX, (cuuint32_t)p1_sy(G.R), (cuuint32_t)NCONS};
     const cuuint32_t es[3] = {1, 1, 1};
+    const cuuint32_t boxU[3] = {(cuuint32_t)CT_SX, (cuuint32_t)CT_UY, (cuuint32_t)NCONS};
+    const cuuint32_t boxF[3] = {(cuuint32_t)CT_SX, (cuuint32_t)CT_FY, (cuuint32_t)NCONS};
+    auto one = [&](CUtensorMap* m, double* base, const cuuint32_t* b) {
+        return enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, base, dims, strides, b, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                   CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    };
     for (int r = 0; r < 3; r++) {
-        const CUresult e = enc(&dev.tmU[r], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, dev.U[r], dims, strides, box, es,
-                               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                               CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        CUresult e = one(&dev.tmU[r], dev.U[r], box);
+        if (e == CUDA_SUCCESS) e = one(&dev.tmCU[r], dev.U[r], boxU);
         if (e != CUDA_SUCCESS) return fail(HOSONO_ECUDA, "cuTensorMapEncodeTiled failed (%d)", (int)e);
     }
+    CUresult e = one(&dev.tmFX, dev.FX, boxF);
+    if (e == CUDA_SUCCESS) e = one(&dev.tmFY, dev.FY, boxF);
+    if (e != CUDA_SUCCESS) return fail(HOSONO_ECUDA, "cuTensorMapEncodeTiled failed (%d)", (int)e);
     return HOSONO_OK;
 }
 
@@ -322,6 +330,8 @@ int Engine::set_tuning(const hosono_tuning& t) {
     if (t.pass1_boxes == 2 && t.pass1_blocks_per_sm > 2)
         return fail(HOSONO_EINVAL, "two stencil boxes run at two pass-1 blocks per SM");
     if (t.pdl != 0 && t.pdl != 1) return fail(HOSONO_EINVAL, "pdl %d (0 or 1)", t.pdl);
+    if (t.update_staging != HOSONO_STAGE_CP_ASYNC && t.update_staging != HOSONO_STAGE_TMA)
+        return fail(HOSONO_EINVAL, "update_staging %d", t.update_staging);
     if (t.upload_bands < 0 || t.upload_bands > HOSONO_UPLOAD_BANDS_MAX)
         return fail(HOSONO_EINVAL, "upload_bands %d (0..%d)", t.upload_bands, HOSONO_UPLOAD_BANDS_MAX);
     tune_ = t;
@@ -361,6 +371,7 @@ int Engine::autotune(int trials, bool force, hosono_tune_report* rep) {
             r.best.later_passes = tune_.later_passes;  // the caller's choices stay
             r.best.upload_bands = tune_.upload_bands;
             r.best.pdl = tune_.pdl;
+            r.best.update_staging = tune_.update_staging;
             if (rep) *rep = r;
             return set_tuning(r.best);
         }
@@ -438,6 +449,7 @@ Batch Engine::batch() const {
     B.p1Radii = radii_;
     B.p1First = 0;
     B.p1End = INT_MAX;
+    B.ctStaged = tune_.update_staging == HOSONO_STAGE_TMA ? 1 : 0;
     B.dev = d_dev_;
     B.st = d_st_;
     B.tiles = d_tiles_;

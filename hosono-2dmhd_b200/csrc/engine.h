@@ -65,7 +65,14 @@ struct InstDev {
     // TMA descriptors of U[0..2] as (x: pitch, y: nyt, var: 8) boxes of the
     // pass-1 stencil box shape (zero fill outside the array)
     CUtensorMap tmU[3];
+    // the same tensors in the boxes the staged pass-1 update reads: U[0..2]
+    // as CT_SX x CT_UY x 8 boxes, fluxRaw FX and FY as CT_SX x CT_FY x 8
+    CUtensorMap tmCU[3];
+    CUtensorMap tmFX, tmFY;
 };
+// the staged pass-1 update's boxes around tile (x0, y0): U over
+// [x0-4, x0+36) x [y0-2, y0+10), FX and FY over [x0-4, x0+36) x [y0-1, y0+10)
+constexpr int CT_SX = TILE_X + 8, CT_UY = TILE_Y + 4, CT_FY = TILE_Y + 3;
 
 // Per-instance mutable scalars (device memory).
 struct InstState {
@@ -142,6 +149,7 @@ struct Batch {
     int p1Boxes;         // stencil boxes per pass-1 block at two blocks per SM (1 or 2)
     int p1Radii;         // bit R: the host launches the radius-R pass-1 kernel (radii held)
     int p1First, p1End;  // pass 1 covers tiles [p1First, min(p1End, ntiles)) of the tile list
+    int ctStaged;        // the pass-1 update reads TMA-staged boxes (1) or the planes (0)
     int maxTiles;        // capacity of the tile list
     int maxInst;         // capacity (slots)
     const int2* instTiles;  // per slot: first tile in the tile list, tile count (0: not live)

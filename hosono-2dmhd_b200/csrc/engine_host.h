@@ -139,7 +139,7 @@ class Engine {
     void drop_graphs();
     // a new engine's launch choices: the fastest on the benchmarked workloads
     // (TMA staging, dynamic tile schedule, two blocks per SM with one box each)
-    hosono_tuning tune_{HOSONO_STAGE_TMA, HOSONO_SCHED_DYNAMIC, 2, HOSONO_LATER_KERNELS, 1, 0, 0, {0}};
+    hosono_tuning tune_{HOSONO_STAGE_TMA, HOSONO_SCHED_DYNAMIC, 2, HOSONO_LATER_KERNELS, 1, 0, 0, HOSONO_STAGE_CP_ASYNC};
     class Rec;
     friend class Rec;
 

@@ -941,20 +941,22 @@ __device__ __forceinline__ void d_flux_list(const Batch& B, int uin, int gt, int
 __global__ void __launch_bounds__(256, 2) k_flux_list(Batch B, int uin) { PDL_ENTRY(); d_flux_list(B, uin, GT1, GS1); }
 
 // ======================================================================
-// FLICDdivB_fluxCorrections (FLICDdivB.f90:13-70) from fluxRaw.
+// FLICDdivB_fluxCorrections (FLICDdivB.f90:13-70) from fluxRaw: fxy =
+// FX(magy), fyx = FY(magx), rows p doubles apart (the instance's planes, or
+// a box of them staged in shared memory)
+__device__ __forceinline__ double flicd_x_at(const double* fxy, const double* fyx, long long c, long long p) {
+    return (2 * fxy[c] + fxy[c + 1] + fxy[c - 1] - fyx[c + p] - fyx[c] - fyx[c - 1] - fyx[c - 1 + p]) / 8.0;
+}
+__device__ __forceinline__ double flicd_y_at(const double* fxy, const double* fyx, long long c, long long p) {
+    return (2 * fyx[c] + fyx[c + p] + fyx[c - p] - fxy[c + 1] - fxy[c] - fxy[c - p] - fxy[c + 1 - p]) / 8.0;
+}
 __device__ __forceinline__ double flicd_x(const InstDev& d, long long c) {
     const Geo& G = d.geo;
-    const double* fxy = d.FX + MAGY * G.plane;
-    const double* fyx = d.FY + MAGX * G.plane;
-    const long long p = G.pitch;
-    return (2 * fxy[c] + fxy[c + 1] + fxy[c - 1] - fyx[c + p] - fyx[c] - fyx[c - 1] - fyx[c - 1 + p]) / 8.0;
+    return flicd_x_at(d.FX + MAGY * G.plane, d.FY + MAGX * G.plane, c, G.pitch);
 }
 __device__ __forceinline__ double flicd_y(const InstDev& d, long long c) {
     const Geo& G = d.geo;
-    const double* fxy = d.FX + MAGY * G.plane;
-    const double* fyx = d.FY + MAGX * G.plane;
-    const long long p = G.pitch;
-    return (2 * fyx[c] + fyx[c + p] + fyx[c - p] - fxy[c + 1] - fxy[c] - fxy[c - p] - fxy[c + 1 - p]) / 8.0;
+    return flicd_y_at(d.FX + MAGY * G.plane, d.FY + MAGX * G.plane, c, G.pitch);
 }
 
 // detect_ALL (detect.f90:84-213).  Everything but CAD, PAD and the DMP reads
@@ -965,16 +967,15 @@ __device__ __forceinline__ double flicd_y(const InstDev& d, long long c) {
 // and the per-pass test keeps the reference's order of decisions.
 
 
-__device__ __forceinline__ bool detect_cell(const InstDev& d, const double* __restrict__ U, long long c,
-                                            const double un[NCONS]) {
-    const Geo& G = d.geo;
-    const double presNew = cons2pres(d.phys, un);
+// the per-pass test on the new state un of a cell: its detect terms in
+// *mask, the stage input's density at rho[c] (rows p doubles apart)
+__device__ __forceinline__ bool detect_cell_at(const Phys& P, const uint8_t* mask, const double* __restrict__ rho,
+                                               long long c, long long p, const double un[NCONS]) {
+    const double presNew = cons2pres(P, un);
     if (!admissible(un[DENS], presNew)) return true;  // CAD, PAD
-    const int m = d.detMask[c];
+    const int m = *mask;
     if (!(m & DM_SHOCK)) return false;
     if (m & DM_PLATEAU) return false;
-    const double* rho = U + DENS * G.plane;
-    const long long p = G.pitch;
     const double d1 = rho[c], d2 = rho[c + 1], d3 = rho[c - 1], d4 = rho[c + p], d5 = rho[c - p];
     const double mn = fmin(fmin(fmin(fmin(d1, d2), d3), d4), d5);
     const double mx = fmax(fmax(fmax(fmax(d1, d2), d3), d4), d5);
@@ -987,13 +988,15 @@ __device__ __forceinline__ bool detect_cell(const InstDev& d, const double* __re
 // the pass-1 update kernel (it reads only the stage input U).  The primitive
 // variables of the tile and a one-cell halo are computed once into shared
 // memory.  Called by every thread of the block (it synchronises).
+// load(v, gx, gy) gives U(v) of array cell (gx, gy); rho[rc] is the cell's
+// stage-input density, rows rp doubles apart (the instance's plane, or a
+// staged box).
 constexpr int DP_SX = TILE_X + 2, DP_SY = TILE_Y + 2;
-__device__ __forceinline__ void detect_prep_tile(const Batch& B, const InstState& S, int uin, const Cell c,
-                                                 double* sV) {
-    const InstDev& d = B.dev[c.k];
+template <class LoadU>
+__device__ __forceinline__ void detect_prep_tile_t(const InstDev& d, const Cell c, double* sV, LoadU load,
+                                                   const double* __restrict__ rho, long long rc, long long rp) {
     const Geo& G = d.geo;
     const Phys& P = d.phys;
-    const double* U = role_ptr(d, S.parity, uin);
     const int x0 = c.i - (int)threadIdx.x - 1, y0 = c.j - (int)threadIdx.y - 1;
     const int tid = threadIdx.y * TILE_X + threadIdx.x;
     __syncthreads();  // the previous tile's reads of sV are done
@@ -1003,9 +1006,8 @@ __device__ __forceinline__ void detect_prep_tile(const Batch& B, const InstState
         double vx = 0.0, vy = 0.0, pr = 1.0, rho = 1.0;
         if (gx >= 0 && gx < G.nxt && gy >= 0 && gy < G.nyt) {
             double u[NCONS], V[NPRIM];
-            const long long g = (long long)gy * G.pitch + gx;
 #pragma unroll
-            for (int v = 0; v < NCONS; v++) u[v] = U[v * G.plane + g];
+            for (int v = 0; v < NCONS; v++) u[v] = load(v, gx, gy);
             cons2prim(P, u, V);
             vx = V[VELX];
             vy = V[VELY];
@@ -1040,9 +1042,8 @@ __device__ __forceinline__ void detect_prep_tile(const Batch& B, const InstState
     int m = 0;
     if (shock1 && shock2 && shock3) {
         m |= DM_SHOCK;
-        const double* rho = U + DENS * G.plane;
-        const long long p = G.pitch;
-        const double d1 = rho[cc], d2 = rho[cc + 1], d3 = rho[cc - 1], d4 = rho[cc + p], d5 = rho[cc - p];
+        const long long p = rp;
+        const double d1 = rho[rc], d2 = rho[rc + 1], d3 = rho[rc - 1], d4 = rho[rc + p], d5 = rho[rc - p];
         const double mn = fmin(fmin(fmin(fmin(d1, d2), d3), d4), d5);
         const double mx = fmax(fmax(fmax(fmax(d1, d2), d3), d4), d5);
         if (mx - mn < G.mindxdy * G.mindxdy * G.mindxdy) m |= DM_PLATEAU;
@@ -1053,7 +1054,7 @@ __device__ __forceinline__ void detect_prep_tile(const Batch& B, const InstState
 #pragma unroll
             for (int jj = -1; jj <= 1; jj++) {
                 if (iabs_c(ii) + iabs_c(jj) <= 1) {
-                    const long long q = cc + ii + jj * p;
+                    const long long q = rc + ii + jj * p;
                     const double ddx = (rho[q + 1] - 2 * rho[q] + rho[q - 1]) / (dx * dx);
                     const double ddy = (rho[q + p] - 2 * rho[q] + rho[q - p]) / (dy * dy);
                     if (k == 0) {
@@ -1080,22 +1081,41 @@ __device__ __forceinline__ void detect_prep_tile(const Batch& B, const InstState
     }
     d.detMask[cc] = (uint8_t)(m | (d.detMask[cc] & DM_CASC));
 }
-
-// FLICD on [g, g+n]^2 where recomputeFLICD; then, on the interior, the
-// unsplit update of timeStep.f90:107-118 and detect_ALL.  A corrected flux a
-// neighbour needs is recomputed locally when the neighbour is flagged (it
-// writes the same value) and read from memory otherwise (nobody writes it).
-// A lowered cell sets `lowered` (cleared again after the flags are rebuilt)
-// and is appended to the lowered list.
-// the unsplit update of timeStep.f90:107-118 and detect_ALL for one interior
-// cell, given its corrected fluxes and those of its east / north faces
-__device__ __forceinline__ bool update_detect_cell(const InstDev& d, const InstState& S, int uin, int uout,
-                                                   long long cc, double ctx, double cty, double ctx_e,
-                                                   double cty_n) {
+// from the instance's planes
+__device__ __forceinline__ void detect_prep_tile(const Batch& B, const InstState& S, int uin, const Cell c,
+                                                 double* sV) {
+    const InstDev& d = B.dev[c.k];
     const Geo& G = d.geo;
     const double* U = role_ptr(d, S.parity, uin);
+    detect_prep_tile_t(
+        d, c, sV, [&](int v, int gx, int gy) { return U[v * G.plane + (long long)gy * G.pitch + gx]; },
+        U + DENS * G.plane, (long long)c.j * G.pitch + c.i, (long long)G.pitch);
+}
+
+// Where a cell's inputs are read: the stage input U around the cell (index
+// uc, planes uplane and rows up doubles apart) and fluxRaw FX / FY (index
+// fc, planes fplane, rows fp apart) -- the instance's planes, or boxes of
+// them staged in shared memory.  Either way the same values in the same
+// expressions.
+struct CellSrc {
+    const double* U;
+    long long uc, uplane, up;
+    const double* FX;
+    const double* FY;
+    long long fc, fplane, fp;
+};
+__device__ __forceinline__ CellSrc global_src(const InstDev& d, const InstState& S, int uin, long long cc) {
+    const Geo& G = d.geo;
+    return CellSrc{role_ptr(d, S.parity, uin), cc, G.plane, G.pitch, d.FX, d.FY, cc, G.plane, G.pitch};
+}
+
+// the unsplit update of timeStep.f90:107-118 and detect_ALL for one interior
+// cell cc, given its corrected fluxes and those of its east / north faces
+__device__ __forceinline__ bool update_detect_at(const InstDev& d, const InstState& S, int uout, long long cc,
+                                                 const CellSrc& src, double ctx, double cty, double ctx_e,
+                                                 double cty_n) {
+    const Geo& G = d.geo;
     double* Uo = role_ptr(d, S.parity, uout);
-    const long long ce = cc + 1, cn = cc + G.pitch;
     const double dt = S.dt;
     const double dtdx = dt / G.dx, dtdy = dt / G.dy;
     double un[NCONS];
@@ -1113,16 +1133,17 @@ __device__ __forceinline__ bool update_detect_cell(const InstDev& d, const InstS
             g0 = 0.0;
             g1 = 0.0;
         } else {
-            f0 = d.FX[v * G.plane + cc];
-            f1 = d.FX[v * G.plane + ce];
-            g0 = d.FY[v * G.plane + cc];
-            g1 = d.FY[v * G.plane + cn];
+            f0 = src.FX[v * src.fplane + src.fc];
+            f1 = src.FX[v * src.fplane + src.fc + 1];
+            g0 = src.FY[v * src.fplane + src.fc];
+            g1 = src.FY[v * src.fplane + src.fc + src.fp];
         }
-        un[v] = U[v * G.plane + cc] - dtdx * (f1 - f0) - dtdy * (g1 - g0);
+        un[v] = src.U[v * src.uplane + src.uc] - dtdx * (f1 - f0) - dtdy * (g1 - g0);
         Uo[v * G.plane + cc] = un[v];
     }
     bool low = false;
-    if (d.scheme[S.schemeSel][cc] > 0) low = detect_cell(d, U, cc, un);
+    if (d.scheme[S.schemeSel][cc] > 0)
+        low = detect_cell_at(d.phys, d.detMask + cc, src.U + DENS * src.uplane, src.uc, src.up, un);
     if (low) d.lowered[cc] = 1;
     return low;
 }
@@ -1133,20 +1154,26 @@ __device__ __forceinline__ bool update_detect_cell(const InstDev& d, const InstS
 // writes the same value) and read from memory otherwise (nobody writes it).
 // A lowered cell sets `lowered` (cleared again after the flags are rebuilt)
 // and is appended to the lowered list.
-__device__ __forceinline__ bool ct_cell(const InstDev& d, const InstState& S, int uin, int uout, int i, int j,
-                                        long long cc) {
+__device__ __forceinline__ bool ct_cell_at(const InstDev& d, const InstState& S, int uout, int i, int j, long long cc,
+                                           const CellSrc& src) {
     const Geo& G = d.geo;
     const int g = G.g;
     if (!d.recF[cc]) return false;
-    const double ctx = flicd_x(d, cc);
-    const double cty = flicd_y(d, cc);
+    const double* fxy = src.FX + MAGY * src.fplane;
+    const double* fyx = src.FY + MAGX * src.fplane;
+    const double ctx = flicd_x_at(fxy, fyx, src.fc, src.fp);
+    const double cty = flicd_y_at(fxy, fyx, src.fc, src.fp);
     d.CTX[cc] = ctx;
     d.CTY[cc] = cty;
     if (i >= g + G.nx || j >= g + G.ny) return false;  // FLICD-only row and column
     const long long ce = cc + 1, cn = cc + G.pitch;
-    const double ctx_e = d.recF[ce] ? flicd_x(d, ce) : d.CTX[ce];
-    const double cty_n = d.recF[cn] ? flicd_y(d, cn) : d.CTY[cn];
-    return update_detect_cell(d, S, uin, uout, cc, ctx, cty, ctx_e, cty_n);
+    const double ctx_e = d.recF[ce] ? flicd_x_at(fxy, fyx, src.fc + 1, src.fp) : d.CTX[ce];
+    const double cty_n = d.recF[cn] ? flicd_y_at(fxy, fyx, src.fc + src.fp, src.fp) : d.CTY[cn];
+    return update_detect_at(d, S, uout, cc, src, ctx, cty, ctx_e, cty_n);
+}
+__device__ __forceinline__ bool ct_cell(const InstDev& d, const InstState& S, int uin, int uout, int i, int j,
+                                        long long cc) {
+    return ct_cell_at(d, S, uout, i, j, cc, global_src(d, S, uin, cc));
 }
 
 __device__ __forceinline__ void t_ct_update_detect(const Batch& B, int uin, int uout, const Cell c, double* sV) {
@@ -1175,6 +1202,71 @@ __device__ __forceinline__ void t_ct_update_detect(const Batch& B, int uin, int 
 __global__ void __launch_bounds__(NTHREADS, 6) k_ct_update_detect(Batch B, int uin, int uout) { PDL_ENTRY();
     __shared__ double sV[4 * DP_SX * DP_SY];
     FOR_TILES(B, t) t_ct_update_detect(B, uin, uout, tile_at(B, t), sV);
+}
+
+// The same with the tile's inputs staged by TMA: one copy each of the
+// stage input U over [x0-4, x0+36) x [y0-2, y0+10) and of fluxRaw FX and FY
+// over [x0-4, x0+36) x [y0-1, y0+10), all 8 planes, completing on one
+// mbarrier (zero fill outside the array; the x origin x0 - 4 is a multiple of
+// 4 doubles), then the per-stage detect terms, FLICD, the update and detect
+// read shared memory.  The boxes replace the dependent load chains of the
+// cached version by three bulk copies per tile; two blocks per SM, so one
+// block's copies overlap the other's arithmetic.  This GPU's own memory
+// only, no multicast.  Waits are bounded as in pass 1 (HOSONO_ETIMEOUT).
+constexpr int CT_UPL = CT_SX * CT_UY, CT_FPL = CT_SX * CT_FY;
+constexpr int CT_SMEM_BYTES = (NCONS * CT_UPL + 2 * NCONS * CT_FPL + 4 * DP_SX * DP_SY) * (int)sizeof(double) + 16;
+__global__ void __launch_bounds__(NTHREADS, 2) k_ct_update_detect_tma(Batch B, int uin, int uout) { PDL_ENTRY();
+    extern __shared__ __align__(128) double smem[];
+    double* sU = smem;
+    double* sFX = sU + NCONS * CT_UPL;
+    double* sFY = sFX + NCONS * CT_FPL;
+    double* sV = sFY + NCONS * CT_FPL;
+    uint64_t* bar = reinterpret_cast<uint64_t*>(sV + 4 * DP_SX * DP_SY);
+    const int tid = threadIdx.y * TILE_X + threadIdx.x;
+    if (tid == 0) {
+        mbar_init(bar);
+        mbar_fence_init();
+    }
+    __syncthreads();
+    unsigned phase = 0;
+    FOR_TILES(B, t) {
+        const Cell c = tile_at(B, t);
+        InstState& S = B.st[c.k];
+        if (!(S.stepping && S.stageActive)) continue;  // uniform over the block
+        const InstDev& d = B.dev[c.k];
+        const Geo& G = d.geo;
+        const int x0 = c.i - (int)threadIdx.x, y0 = c.j - (int)threadIdx.y;  // the tile's origin
+        const int ux0 = x0 - 4, uy0 = y0 - 2, fy0 = y0 - 1;              // the boxes' origins
+        __syncthreads();  // every read of the previous tile's boxes is done
+        if (tid == 0) {
+            const int par = S.parity;
+            const int u = uin == ROLE_STATE ? par : uin == ROLE_A ? 1 - par : 2;  // role_ptr's buffer index
+            mbar_expect_tx(bar, (unsigned)((NCONS * CT_UPL + 2 * NCONS * CT_FPL) * sizeof(double)));
+            tma_box3(sU, &d.tmCU[u], ux0, uy0, 0, bar);
+            tma_box3(sFX, &d.tmFX, ux0, fy0, 0, bar);
+            tma_box3(sFY, &d.tmFY, ux0, fy0, 0, bar);
+        }
+        const bool ok = mbar_wait(bar, phase & 1u);
+        phase ^= 1u;
+        if (!__syncthreads_and(ok)) {  // a copy that never lands: report it, leave without reading
+            if (tid == 0) atomicExch(&B.flags->error, HOSONO_ETIMEOUT);
+            return;
+        }
+        detect_prep_tile_t(
+            d, c, sV, [&](int v, int gx, int gy) { return sU[v * CT_UPL + (gy - uy0) * CT_SX + (gx - ux0)]; },
+            sU + DENS * CT_UPL, (long long)(c.j - uy0) * CT_SX + (c.i - ux0), (long long)CT_SX);
+        const int g = G.g;
+        bool low = false;
+        long long cc = 0;
+        if (c.i >= g && c.j >= g && c.i <= g + G.nx && c.j <= g + G.ny) {
+            cc = (long long)c.j * G.pitch + c.i;
+            const CellSrc src{sU,  (long long)(c.j - uy0) * CT_SX + (c.i - ux0), CT_UPL, CT_SX,
+                              sFX, sFY, (long long)(c.j - fy0) * CT_SX + (c.i - ux0), CT_FPL, CT_SX};
+            low = ct_cell_at(d, S, uout, c.i, c.j, cc, src);
+        }
+        warp_count(&S.nDetect, low);
+        warp_append(B.L, LIST_LOW, B.L.low, B.L.cap, low, entry(c.k, cc));
+    }
 }
 
 // the same on the recomputeFLICD list of a later MOOD pass
@@ -1953,7 +2045,17 @@ void l_recon_check(const Batch& B, int uin, int /*later*/, cudaStream_t s) {
     LIST_LAUNCH(k_recon_group, B, s, uin, (int)LIST_NEXT);
 }
 void l_ct_update_detect(const Batch& B, int uin, int uout, cudaStream_t s) {
-    TILE_LAUNCH(k_ct_update_detect, B, s, uin, uout);
+    if (!B.ctStaged) {
+        TILE_LAUNCH(k_ct_update_detect, B, s, uin, uout);
+        return;
+    }
+    static const bool attr =  // once per process (thread-safe static initialisation)
+        cudaFuncSetAttribute((const void*)k_ct_update_detect_tma, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             CT_SMEM_BYTES) == cudaSuccess;
+    (void)attr;
+    const int r = resident_blocks((const void*)k_ct_update_detect_tma, CT_SMEM_BYTES);
+    lk(k_ct_update_detect_tma, dim3((unsigned)(r < B.maxTiles ? r : B.maxTiles)), kTile, (size_t)CT_SMEM_BYTES, s, B,
+       uin, uout);
 }
 void l_mood_flags(const Batch& B, int mode, cudaStream_t s) {
     if (mode == MOOD_FLAGS_DENSE) {

@@ -326,7 +326,9 @@ typedef struct hosono_tuning {
     int pdl;                  /* 1: the step's kernels are launched as programmatic dependent launches
                                  (each may be scheduled while its predecessor drains and waits on
                                  the GPU for its completion); 0: plain stream order */
-    int pad[1];               /* zero */
+    int update_staging;       /* the pass-1 update (FLICD, update, detect): HOSONO_STAGE_CP_ASYNC (0) reads
+                                 the planes through the caches, HOSONO_STAGE_TMA (1) stages the tile's
+                                 boxes of U, FX and FY in shared memory with TMA copies first */
 } hosono_tuning;
 #define HOSONO_UPLOAD_BANDS_MAX 16
 int hosono_gpu_set_tuning(hosono_handle* h, const hosono_tuning* t);

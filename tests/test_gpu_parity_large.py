@@ -116,6 +116,20 @@ def test_multi_tile_path_bitwise(staging, boxes, tmp_par_dir):
 
 
 @pytest.mark.gpu
+def test_multi_tile_staged_update_bitwise(tmp_par_dir):
+    """The pass-1 update from TMA-staged boxes on a grid with more tiles than
+    its grid of blocks (each block stages and computes several tiles in
+    turn): three traced steps equal the oracle."""
+    m = pkg.load()
+    par = parfiles.make(tmp_par_dir, "ot640_stu", parfiles.orszag_tang(640, 2, ell=12.0))
+    o, s = _traced_steps(m, par, 3, update_staging=m.STAGE_TMA)
+    info = s.launch_info()
+    assert info["tiles"] > 2 * info["pass1_grid"], info
+    s.close()
+    o.close()
+
+
+@pytest.mark.gpu
 def test_advance_host_banded_ot1024(tmp_par_dir):
     """The drop-in with host buffers on Orszag-Tang 1024^2, R=2, ell/Delta=12:
     its 1032 array rows take the banded upload by default (8 bands, the

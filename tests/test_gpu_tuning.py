@@ -200,3 +200,55 @@ def test_programmatic_launch_batch(tmp_par_dir):
         np.testing.assert_array_equal(U, o.U())
         np.testing.assert_array_equal(S, o.scheme())
     b.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("graphs", [True, False])
+@pytest.mark.parametrize("case", sorted(PERSISTENT_CASES) + ["ot96_r2"])
+def test_staged_update_bitwise(case, graphs, tmp_par_dir):
+    """The pass-1 update (per-stage detect terms, FLICD, update, detect) from
+    TMA-staged boxes of U, FX and FY gives the oracle's bits, as the cached
+    version does."""
+    m = pkg.load()
+    kv = parfiles.orszag_tang(96, 2) if case == "ot96_r2" else PERSISTENT_CASES[case]()
+    par = parfiles.make(tmp_par_dir, f"stu_{case}_{int(graphs)}", kv)
+    o = oracle.Oracle(par)
+    s = m.Solver.from_par(par, fp_mode=m.FP_STRICT)
+    s.set_tuning(update_staging=m.STAGE_TMA)
+    assert s.tuning()["update_staging"] == m.STAGE_TMA
+    s.set_graphs(graphs)
+    s.set_time(0.0, o.tmax, 0, 1 << 30)
+    for chunk in (1, 4):
+        for _ in range(chunk):
+            o.advance(o.cfl())
+        s.step(chunk)
+        U, V, S = s.download()
+        np.testing.assert_array_equal(U, o.U())
+        np.testing.assert_array_equal(V, o.V())
+        np.testing.assert_array_equal(S, o.scheme())
+    s.close()
+
+
+@pytest.mark.gpu
+def test_staged_update_batch(tmp_par_dir):
+    """The staged pass-1 update over a batch of uneven instances (outflow and
+    periodic, R = 1 and 2): each equals its own oracle run."""
+    m = pkg.load()
+    kvs = [parfiles.blast(64, 2, p_ratio=300.0, theta=0.2), parfiles.orszag_tang(48, 1),
+           parfiles.blast(96, 2, p_ratio=30.0, theta=1.1), parfiles.sedov(40, 2)]
+    pars = [parfiles.make(tmp_par_dir, f"stub{i}", kv) for i, kv in enumerate(kvs)]
+    tiles = sum(m.Batch.tiles_for(m.par_load(p)[0]) for p in pars)
+    b = m.Batch(len(pars), tiles, fp_mode=m.FP_STRICT)
+    b.set_tuning(update_staging=m.STAGE_TMA)
+    slots = [b.add_par(p) for p in pars]
+    for k in slots:
+        b.set_time(k, 0.0, 1e30)
+    b.run(max_steps=3)
+    for k, p in zip(slots, pars):
+        o = oracle.Oracle(p)
+        for _ in range(3):
+            o.advance(o.cfl())
+        U, V, S = b.download(k)
+        np.testing.assert_array_equal(U, o.U())
+        np.testing.assert_array_equal(S, o.scheme())
+    b.close()
