@@ -719,6 +719,9 @@ def bench_served(m, fp, requests, check, calibrate=0, sample=0, hashes_path=None
         out[name] = {k_: rep[k_] for k_ in keys}
         out[name]["server"] = dict(policy=name, **kw)
         out[name]["mean_work_measured"] = rep["zone_updates"] / max(rep["completed"], 1)
+        # the load the stream actually offered: its arrival rate times the
+        # measured work per request, over the closed-loop throughput
+        out[name]["offered_load"] = rate * out[name]["mean_work_measured"] / closed["zone_updates_per_s"]
         kept_by[name] = kept
         if name == policies[0][0]:
             for k_ in keys:  # the first policy's figures at the top level
@@ -799,12 +802,13 @@ def main():
     ap.add_argument("--batched-limit", type=int, default=64, help="instances of the batched workload to run")
     ap.add_argument("--to-end", action="store_true",
                     help="time the whole run from the initial state to t_end instead of --steps steps")
-    ap.add_argument("--serve-requests", type=int, default=100,
+    ap.add_argument("--serve-requests", type=int, default=50,
                     help="requests of the served stream to run (0: skip the served measurement)")
     ap.add_argument("--serve-check", type=int, default=20,
                     help="served requests (least predicted work first) checked against the CPU oracle")
-    ap.add_argument("--serve-calibrate", type=int, default=30,
-                    help="first requests run closed loop to measure capacity (0: all of them)")
+    ap.add_argument("--serve-calibrate", type=int, default=0,
+                    help="first requests run closed loop to measure capacity (0: all of them, which measures the "
+                         "stream's mean work exactly; fewer predict it, and a poor prediction skews the load)")
     ap.add_argument("--serve-sample", type=int, default=0,
                     help="seeded-random served requests whose final-state SHA-256 is written to --serve-hashes")
     ap.add_argument("--serve-hashes", default=None, help="output JSON of the sampled hashes")
