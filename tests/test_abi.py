@@ -128,3 +128,43 @@ def test_serve_create_without_gpu_fails_cleanly():
         return
     s.close()
     pytest.skip("a GPU is present")
+
+
+STRUCTS = {"hosono_params": "Params", "hosono_run_info": "RunInfo", "hosono_stats": "Stats",
+           "hosono_serve_config": "ServeConfig", "hosono_request_info": "RequestInfo",
+           "hosono_serve_totals": "ServeTotals", "hosono_launch_info": "LaunchInfo", "hosono_tuning": "Tuning",
+           "hosono_tune_report": "TuneReport", "hosono_ic_desc": "ICDesc"}
+
+
+def test_binding_structs_match_the_header(tmp_path):
+    """Every struct the Python binding mirrors has the header's size and the
+    header's field offsets (a C program compiled against include/hosono_gpu.h
+    prints them)."""
+    import subprocess
+    m = pkg.load()
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "hosono_gpu.h"', "int main(void) {"]
+    for c, py in STRUCTS.items():
+        lines.append(f'printf("{c} size %zu\\n", sizeof({c}));')
+        for name, _ in getattr(m, py)._fields_:
+            lines.append(f'printf("{c} {name} %zu\\n", offsetof({c}, {name}));')
+    lines.append("return 0; }")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c11", "-I", os.path.dirname(HEADER), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
+    got = {tuple(l.split()[:2]): int(l.split()[2]) for l in out if l}
+    for c, py in STRUCTS.items():
+        cls = getattr(m, py)
+        assert got[(c, "size")] == ctypes.sizeof(cls), c
+        for name, _ in cls._fields_:
+            assert got[(c, name)] == getattr(cls, name).offset, (c, name)
+
+
+def test_tuning_rejects_unknown_fields():
+    m = pkg.load()
+    t = m.Tuning()
+    t.update({"pass1_boxes": 2, "pdl": 1})
+    assert t.as_dict()["pass1_boxes"] == 2 and t.as_dict()["pdl"] == 1
+    with pytest.raises(TypeError):
+        t.update({"pass1_box": 1})
