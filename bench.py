@@ -332,8 +332,8 @@ def bench_ours(args, rank, world, local):
     # Fortran driver that keeps grid_state%U on the host makes them each step:
     # dt = cfl_computedt (hosono_gpu_cfl, dt to the host), then
     # timeStep_advanceSolution on the host array (hosono_gpu_advance_host:
-    # U from pinned memory to the device -- V = cons2prim(U) is rebuilt there,
-    # bit-identical to the host's -- the step, U back to the host)
+    # U from pinned memory to the device, in row bands that overlap the first
+    # stage's pass 1; the step, which rebuilds V; U back to the host)
     Uh = torch.from_numpy(np.ascontiguousarray(U0)).pin_memory().numpy()
     sol.upload(Uh, None)
     e2e_steps = max(1, min(args.steps, 5))

@@ -321,8 +321,8 @@ typedef struct hosono_tuning {
                                  compute, load the next; the shared memory saved goes to L1) or 2 (the
                                  next tile's box loads while the current one is computed) */
     int upload_bands;         /* hosono_gpu_advance_host: row bands of the overlapped upload (0 = by size:
-                                 8 from 1024 array rows up, else 1; 1 = upload, then step; at most
-                                 HOSONO_UPLOAD_BANDS_MAX) */
+                                 16 from 2048 array rows, 8 from 1024, else 1; 1 = upload, then step;
+                                 at most HOSONO_UPLOAD_BANDS_MAX) */
     int pdl;                  /* 1: the step's kernels are launched as programmatic dependent launches
                                  (each may be scheduled while its predecessor drains and waits on
                                  the GPU for its completion); 0: plain stream order */
