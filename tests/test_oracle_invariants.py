@@ -4,8 +4,7 @@ the known-answer tests the oracle is held to properties the scheme has by
 construction: a uniform state stays uniform, a state that varies along x
 only keeps identical rows through MOOD lowerings, the MHD HLLC solver
 reduces to the Euler HLLC solver when B = 0, and the flux-interpolated CT
-correction
-(FLICDdivB_fluxCorrections, src/FLICDdivB.f90:13-70) keeps the
+correction (FLICDdivB_fluxCorrections, src/FLICDdivB.f90:13-70) keeps the
 central-difference div(B) of src/output.f90:261-274 at round-off."""
 import math
 
